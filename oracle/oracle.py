@@ -1,0 +1,266 @@
+"""ctypes binding of the CPU restatement (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by the test suite, the smoke check and the
+CPU-baseline leg of the benchmark, never by the product package.
+
+Arrays are numpy arrays in the reference's Fortran layout (order='F'), halos
+included, exactly as the Fortran routines declare them (see
+thirring_oracle.h for the shapes).
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def _load():
+    if not os.path.exists(_LIB):
+        build()
+    return C.CDLL(_LIB)
+
+
+lib = _load()
+
+
+class Lat(C.Structure):
+    _fields_ = [("lx", C.c_int), ("ly", C.c_int), ("lt", C.c_int), ("ls", C.c_int),
+                ("kernel", C.c_int), ("ndiag", C.c_int), ("am3", C.c_float),
+                ("beta", C.c_float), ("ibound", C.c_int), ("nf", C.c_int),
+                ("strict_sums", C.c_int)]
+
+
+class Rational(C.Structure):
+    _fields_ = [("ndiag", C.c_int), ("ndiagg", C.c_int)] + [
+        (n, C.POINTER(C.c_double)) for n in (
+            "anum2", "aden2", "bnum2", "bden2", "anum4", "aden4", "bnum4", "bden4",
+            "anum2g", "aden2g", "bnum2g", "bden2g", "anum4g", "aden4g", "bnum4g", "bden4g")]
+
+
+class TrajResult(C.Structure):
+    _fields_ = [("h0", C.c_double), ("h1", C.c_double), ("dh", C.c_double), ("ds", C.c_double),
+                ("s0", C.c_double), ("s1", C.c_double), ("accepted", C.c_int), ("steps", C.c_int),
+                ("y", C.c_float)]
+
+
+class Counts(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("ancg", "ancgpv", "ancgf", "ancgfpv", "ancgh",
+                                          "ancghpv", "ancgpf", "ancgpfpv")]
+
+
+def P(a):
+    """numpy array -> void pointer (must be contiguous in Fortran order)."""
+    if a is None:
+        return None
+    assert a.flags.f_contiguous or a.flags.c_contiguous
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def lat(lx, ly, lt, ls, kernel=0, ndiag=25, am3=1.0, beta=0.4, ibound=-1, nf=1, strict_sums=0):
+    return Lat(lx, ly, lt, ls, kernel, ndiag, am3, beta, ibound, nf, strict_sums)
+
+
+def spinor(L, dtype=np.complex128):
+    return np.zeros((L.ls + 2, L.lx + 2, L.ly + 2, L.lt + 2, 4), dtype=dtype, order="F")
+
+
+def links(L):
+    return np.zeros((L.lx + 2, L.ly + 2, L.lt + 2, 3), dtype=np.complex128, order="F")
+
+
+def field3(L, dtype=np.float64):
+    return np.zeros((L.lx, L.ly, L.lt, 3), dtype=dtype, order="F")
+
+
+def ps_field(L):
+    return np.zeros((L.lx + 2, L.ly + 2, L.lt + 2, 2), dtype=np.float32, order="F")
+
+
+def shift_out(L, ndiag=None):
+    return np.zeros((L.ls, L.lx, L.ly, L.lt, 4, ndiag or L.ndiag), dtype=np.complex128, order="F")
+
+
+def interior(a):
+    """Interior of a halo'd spinor (drops the first four halos)."""
+    return a[1:-1, 1:-1, 1:-1, 1:-1, :]
+
+
+_v = C.c_void_p
+_L = C.POINTER(Lat)
+for name, res, args in [
+    ("orc_update_halo_5", None, [_L, _v]),
+    ("orc_update_halo_4", None, [_L, C.c_int, _v]),
+    ("orc_update_halo_4_real", None, [_L, C.c_int, _v]),
+    ("orc_coef", None, [_L, _v, _v]),
+    ("orc_dslash", None, [_L, _v, _v, _v, C.c_float, C.c_int]),
+    ("orc_dslashd", None, [_L, _v, _v, _v, C.c_float, C.c_int]),
+    ("orc_dslash_sp", None, [_L, _v, _v, _v, C.c_float, C.c_int]),
+    ("orc_dslashd_sp", None, [_L, _v, _v, _v, C.c_float, C.c_int]),
+    ("orc_dirac_operator", None, [_L, _v, _v, _v, C.c_float, C.c_int]),
+    ("orc_congrad", C.c_int, [_L, _v, _v, _v, C.c_float, C.c_float, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    ("orc_multishift_solver", None, [_L, _v, C.c_float, C.c_int, C.c_int, _v, _v, _v, _v, C.c_float, C.c_int,
+                                     C.POINTER(C.c_int), _v]),
+    ("orc_multishift_solver_sp", None, [_L, _v, C.c_float, C.c_int, C.c_int, _v, _v, _v, _v, C.c_float, C.c_int,
+                                        C.POINTER(C.c_int), _v]),
+    ("orc_derivs", None, [_L, _v, _v, C.c_double, C.c_int, C.c_float, C.c_int, _v]),
+    ("orc_qmrherm", C.c_int, [_L, _v, _v, _v, C.c_float, C.POINTER(C.c_int), C.c_float, C.c_int, _v, _v, C.c_int,
+                              C.c_int, C.c_int, C.c_int, _v, _v, _v, _v]),
+    ("orc_rng_create", _v, [_L, C.c_int]),
+    ("orc_rng_destroy", None, [_v]),
+    ("orc_init_random", C.c_int, [_v, C.c_double]),
+    ("orc_rano", C.c_float, [_v, C.c_int, C.c_int, C.c_int]),
+    ("orc_dranf", C.c_double, [_v, C.c_int, C.c_int, C.c_int]),
+    ("orc_gauss0", None, [_L, _v, _v]),
+    ("orc_gaussp", None, [_L, _v, _v]),
+    ("orc_read_remez_file", C.c_int, [C.c_char_p, C.c_int, _v, _v, _v, _v]),
+    ("orc_starting_state", None, [_L, _v, _v, _v, _v, _v, _v]),
+    ("orc_initialise_phi", C.c_int, [_L, _v, _v, C.POINTER(Rational), _v, C.c_float, C.c_int, C.c_float, C.c_int,
+                                     C.POINTER(Counts)]),
+    ("orc_initialise_pp", None, [_L, _v, _v]),
+    ("orc_force", C.c_int, [_L, _v, _v, C.POINTER(Rational), _v, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int,
+                            _v, C.POINTER(Counts)]),
+    ("orc_hamilton", C.c_int, [_L, _v, _v, _v, C.POINTER(Rational), _v, C.c_float, C.c_float, C.c_int, C.c_int,
+                               C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                               C.POINTER(C.c_double), C.POINTER(Counts)]),
+    ("orc_evolve_theta_pp", C.c_int, [_L, _v, _v, _v, _v, C.POINTER(Rational), _v, C.c_int, C.c_float, C.c_float,
+                                      C.c_float, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), _v,
+                                      C.POINTER(Counts)]),
+    ("orc_trajectory", C.c_int, [_L, _v, _v, C.POINTER(Rational), C.c_int, C.c_float, C.c_float, C.c_int, C.c_float,
+                                 C.c_float, C.c_int, C.c_int, C.c_int, C.POINTER(TrajResult), C.POINTER(Counts)]),
+    ("orc_num_threads", C.c_int, []),
+    ("orc_set_num_threads", None, [C.c_int]),
+]:
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = args
+
+
+# ---------------------------------------------------------------- wrappers
+def starting_state(L, Phi=True, u=True, R=False, X=False, dSdpi=False, Phi0=False):
+    """tests/test_utils.F90:35-151 analytic state; returns dict of arrays."""
+    out = {}
+    out["Phi"] = spinor(L) if Phi else None
+    out["u"] = links(L) if u else None
+    out["R"] = spinor(L) if R else None
+    out["X"] = spinor(L) if X else None
+    out["dSdpi"] = field3(L) if dSdpi else None
+    out["Phi0"] = (np.zeros((L.ls + 2, L.lx + 2, L.ly + 2, L.lt + 2, 4, 25), np.complex128, order="F")
+                   if Phi0 else None)
+    lib.orc_starting_state(C.byref(L), P(out["Phi"]), P(out["u"]), P(out["R"]), P(out["X"]),
+                           P(out["dSdpi"]), P(out["Phi0"]))
+    return out
+
+
+def dslash(L, R, u, am, imass):
+    Phi = spinor(L)
+    lib.orc_dslash(C.byref(L), P(Phi), P(R), P(u), am, imass)
+    return Phi
+
+
+def dslashd(L, R, u, am, imass):
+    Phi = spinor(L)
+    lib.orc_dslashd(C.byref(L), P(Phi), P(R), P(u), am, imass)
+    return Phi
+
+
+def update_halo_5(L, a):
+    lib.orc_update_halo_5(C.byref(L), P(a))
+    return a
+
+
+def update_halo_4(L, a, n=3):
+    lib.orc_update_halo_4(C.byref(L), n, P(a))
+    return a
+
+
+def coef(L, theta):
+    u = links(L)
+    lib.orc_coef(C.byref(L), P(u), P(np.asfortranarray(theta, np.float32)))
+    return u
+
+
+def congrad(L, Phi, X, u, res, am, imass, niterc=None):
+    it = C.c_int(0)
+    niterc = niterc if niterc is not None else L.ls * L.lx * L.ly * L.lt
+    itercg = lib.orc_congrad(C.byref(L), P(Phi), P(X), P(u), res, am, imass, niterc, C.byref(it))
+    return itercg, it.value
+
+
+def multishift(L, u, am, imass, anum, aden, inp, res, maxcg, sp=False):
+    nq = len(aden)
+    out = shift_out(L)
+    ret = C.c_int(0)
+    cgr = np.zeros(nq, np.int32)
+    fn = lib.orc_multishift_solver_sp if sp else lib.orc_multishift_solver
+    fn(C.byref(L), P(u), am, imass, nq, P(np.ascontiguousarray(aden, np.float64)),
+       P(np.ascontiguousarray(anum, np.float64)), P(out), P(inp), res, maxcg, C.byref(ret), P(cgr))
+    return out, ret.value, cgr
+
+
+def qmrherm(L, u, Phi, res, am, imass, anum, aden, iflag, use_sp=False, max_iters=50000,
+            dSdpi=None, Phi0=None):
+    """anum has ndiagq+1 entries; returns (x, itercg, cg_returns, rc)."""
+    nq = len(aden)
+    x = spinor(L)
+    it = C.c_int(0)
+    cgr = np.zeros(nq, np.int32)
+    if dSdpi is None:
+        dSdpi = field3(L)
+    if Phi0 is None:
+        Phi0 = np.zeros((L.ls + 2, L.lx + 2, L.ly + 2, L.lt + 2, 4, L.ndiag), np.complex128, order="F")
+    rc = lib.orc_qmrherm(C.byref(L), P(u), P(Phi), P(x), res, C.byref(it), am, imass,
+                         P(np.ascontiguousarray(anum, np.float64)), P(np.ascontiguousarray(aden, np.float64)),
+                         nq, iflag, int(use_sp), max_iters, P(cgr), P(dSdpi), P(Phi0), None)
+    return x, it.value, cgr, rc
+
+
+def derivs(L, R, X2, anum, iflag, am, imass, dSdpi):
+    lib.orc_derivs(C.byref(L), P(R), P(X2), anum, iflag, am, imass, P(dSdpi))
+    return dSdpi
+
+
+class RNG:
+    def __init__(self, L, site=True):
+        self.L = L
+        self.h = lib.orc_rng_create(C.byref(L), int(site))
+
+    def init(self, seed):
+        rc = lib.orc_init_random(self.h, seed)
+        assert rc == 0
+        return self
+
+    def rano(self, ix=1, iy=1, it=1):
+        return lib.orc_rano(self.h, ix, iy, it)
+
+    def gauss0(self):
+        ps = ps_field(self.L)
+        lib.orc_gauss0(C.byref(self.L), self.h, P(ps))
+        return ps
+
+    def gaussp(self):
+        ps = ps_field(self.L)
+        lib.orc_gaussp(C.byref(self.L), self.h, P(ps))
+        return ps
+
+    def __del__(self):
+        try:
+            lib.orc_rng_destroy(self.h)
+        except Exception:
+            pass
+
+
+def read_remez(path, n):
+    a = np.zeros(n + 1)
+    b = np.zeros(n + 1)
+    ad = np.zeros(n)
+    bd = np.zeros(n)
+    rc = lib.orc_read_remez_file(path.encode(), n, P(a), P(b), P(ad), P(bd))
+    assert rc == 0, path
+    return a, ad, b, bd
