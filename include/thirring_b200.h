@@ -1,0 +1,121 @@
+/*
+ * thirring_b200.h -- C ABI of the B200 fermion hot path for thirring-rhmc.
+ *
+ * A drop-in for the Fortran routines of the reference (j-ostmeyer/
+ * thirring-rhmc) on the RHMC fermion path.  Every entry point keeps the
+ * argument list of the Fortran routine it replaces (cited per function);
+ * the module globals that routine reads or writes (trial::u, vector::X,
+ * gforce::dSdpi, qmrherm_module::Phi0, random's state) become explicit
+ * arguments or live in the context.  A Fortran caller binds these with
+ * ISO_C_BINDING (see the shim module described alongside this header).
+ *
+ * Host arrays use the reference's Fortran layout and element types, halos
+ * included:
+ *   spinor   complex(dp) (0:Ls+1, 0:Lx+1, 0:Ly+1, 0:Lt+1, 4)        double[2*...]
+ *   links    complex(dp) (0:Lx+1, 0:Ly+1, 0:Lt+1, 3)
+ *   shifts   complex(dp) (Ls, Lx, Ly, Lt, 4, ndiag)   (no halo)
+ *   theta,pp real        (Lx, Ly, Lt, 3)
+ *   dSdpi    real(dp)    (Lx, Ly, Lt, 3)
+ *   ps       real        (0:Lx+1, 0:Ly+1, 0:Lt+1, 2)
+ * Input halos are ignored (neighbours are periodic, as the reference's halo
+ * exchange on a 1x1x1x1 process grid makes them); output halos receive the
+ * periodic images.  Scalars keep the reference's kinds: `real` -> float,
+ * `real(dp)` -> double, `integer` -> int.
+ *
+ * Every function returns a thr_status (0 = success).  Calls on one context
+ * are serialised on that context's CUDA stream and return when their
+ * results are in the caller's host arrays.
+ */
+#ifndef THIRRING_B200_H
+#define THIRRING_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference aborts the run (MPI_Abort / exit(1)) where
+ * these are returned: qmrherm_module.F90:66-81, dwf3d_lib.F90:860-881. */
+enum thr_status {
+  THR_OK = 0,
+  THR_ERR_BADARG = 1,      /* NULL pointer, bad imass, bad seed ...          */
+  THR_ERR_BADSHAPE = 2,    /* Ls not a multiple of 4, ndiagq > ndiag ...     */
+  THR_ERR_MAXITER = 3,     /* solver hit its iteration cap                   */
+  THR_ERR_NAN = 4,         /* non-finite residual                            */
+  THR_ERR_CUDA = 5,        /* CUDA runtime error                             */
+  THR_ERR_NOMEM = 6,       /* device allocation failed                       */
+  THR_ERR_UNSUPPORTED = 7  /* e.g. imass = 5 with the Wilson kernel          */
+};
+
+enum thr_kernel { THR_SHAMIR = 0, THR_WILSON = 1 };
+enum thr_layout { THR_NATURAL = 0, THR_EVEN_ODD = 1 };
+enum thr_precision {
+  THR_FP64 = 0,        /* everything in FP64 (the reference's DP path)                        */
+  THR_FP32_REF = 1,    /* multishift_solver_sp semantics: FP32 vectors, FP64 scalars          */
+  THR_MIXED_FP32 = 2,  /* FP32 inner solve, FP64 reliable residual and defect correction     */
+  THR_MIXED_BF16 = 3   /* BF16 spinor storage, FP32 arithmetic, FP64 defect correction       */
+};
+
+/* Runtime replacement of params.F90:12-17 (compile-time sizes) and the
+ * runtime parameters read from midout (dwf3d_lib.F90:143). */
+typedef struct thr_params {
+  int lx, ly, lt, ls; /* ksizex_l, ksizey_l, ksizet_l, kthird_l                         */
+  int kernel;         /* thr_kernel: GENERATE_WITH_SHAMIR / _WILSON                      */
+  int layout;         /* thr_layout of the device fields (results do not depend on it)   */
+  int ndiag;          /* shift extent of x1/Phi0 arrays (params.F90: ndiag = 25)         */
+  float am3;          /* domain-wall height                                              */
+  float beta;         /* gauge coupling                                                  */
+  int ibound;         /* -1: antiperiodic fermions in t                                  */
+  int device;         /* CUDA device ordinal                                             */
+} thr_params;
+
+typedef struct thr_ctx thr_ctx;
+
+/* ---- context ------------------------------------------------------------ */
+int thr_create(const thr_params *p, thr_ctx **ctx);
+int thr_destroy(thr_ctx *ctx);
+const char *thr_status_string(int status);
+/* Runtime parameter updates (params.F90:69-72 are module variables). */
+int thr_set_am3(thr_ctx *ctx, float am3);
+int thr_set_beta(thr_ctx *ctx, float beta);
+/* Page-lock a caller array so its transfers run at full PCIe/C2C speed. */
+int thr_host_register(void *ptr, unsigned long long bytes);
+int thr_host_unregister(void *ptr);
+
+/* ---- gauge.F90 ------------------------------------------------------------ */
+/* coef(u, theta), gauge.F90:12-43: u = 1 + i*theta (FP32, widened), antiperiodic
+ * flip of the t-links on the last time slice when ibound = -1, halo images.
+ * The context keeps the result as its current links. */
+int thr_coef(thr_ctx *ctx, double *u, const float *theta);
+/* Make `u` (links layout) the context's current links (trial::u). */
+int thr_set_links(thr_ctx *ctx, const double *u);
+
+/* ---- dirac.F90 ------------------------------------------------------------ */
+/* dslash(Phi, R, u, am, imass), dirac.F90:11-27: Phi = M R.
+ * u may be NULL to use the context's current links. */
+int thr_dslash(thr_ctx *ctx, double *Phi, const double *R, const double *u, float am, int imass);
+/* dslashd(Phi, R, u, am, imass[, reqs_R]), dirac.F90:410-431: Phi = M^dagger R.
+ * (reqs_R has no counterpart: there is no halo exchange to complete.) */
+int thr_dslashd(thr_ctx *ctx, double *Phi, const double *R, const double *u, float am, int imass);
+
+/* ---- device-resident fields ------------------------------------------- */
+/* Spinor fields kept in HBM in the device layout (no halos), so that solver
+ * and MD loops never cross PCIe.  `precision` is a thr_precision storage
+ * choice: THR_FP64 (complex double), THR_FP32_REF (complex float) or
+ * THR_MIXED_BF16 (bf16 pairs).  Operations on device fields are enqueued on
+ * the context's CUDA stream and return without synchronising; thr_sync()
+ * waits for them.  No counterpart in the reference (its fields are module
+ * arrays in host memory). */
+int thr_field_create(thr_ctx *ctx, int precision, void **field);
+int thr_field_destroy(thr_ctx *ctx, void *field);
+int thr_field_upload(thr_ctx *ctx, void *field, int precision, const double *host_spinor);
+int thr_field_download(thr_ctx *ctx, double *host_spinor, const void *field, int precision);
+/* out = M in (dag = 0) or M^dagger in (dag = 1) with the current links */
+int thr_dslash_dev(thr_ctx *ctx, void *out, const void *in, int precision, float am, int imass, int dag);
+int thr_sync(thr_ctx *ctx);
+/* the context's cudaStream_t, for event timing by the caller */
+int thr_get_stream(thr_ctx *ctx, void **stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,84 @@
+"""dslash / dslashd on the GPU against the oracle (dirac.F90).
+
+FP64 tolerance: max|GPU - oracle| <= 1e-13 * max|oracle|.
+Also: the even-odd storage order gives bit-identical results to the natural
+one, and M^dagger is the adjoint of M.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import thirring
+from helpers import interior, rand_links, rand_spinor, rel_err
+
+TOL = 1e-13
+
+CASES = [(k, im, lay) for k in (0, 1) for im in ((1, 3, 5) if k == 0 else (1, 3)) for lay in (0, 1)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel,imass,layout", CASES)
+@pytest.mark.parametrize("dims", [(4, 6, 8, 8), (6, 4, 4, 12)])
+def test_dslash_random(kernel, imass, layout, dims):
+    rng = np.random.default_rng(hash((kernel, imass, layout) + dims) % 2**32)
+    lx, ly, lt, ls = dims
+    L = O.lat(lx, ly, lt, ls, kernel=kernel, am3=1.0)
+    u = rand_links(L, rng)
+    R = rand_spinor(L, rng)
+    with thirring.Lattice(lx, ly, lt, ls, kernel=kernel, layout=layout) as G:
+        for dag in (False, True):
+            ref = (O.dslashd if dag else O.dslash)(L, R, u, 0.01, imass)
+            got = (G.dslashd if dag else G.dslash)(R, u, 0.01, imass)
+            e = rel_err(interior(got), interior(ref))
+            assert e <= TOL, (dag, e)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel,imass", [(0, 1), (0, 3), (0, 5), (1, 1), (1, 3)])
+def test_dslash_reference_fixture(kernel, imass):
+    # tests/test_dslash_shamir.F90: 12^3 x 24 analytic state, am = 0.05
+    L = O.lat(12, 12, 12, 24, kernel=kernel)
+    st = O.starting_state(L, R=True)
+    with thirring.Lattice(12, 12, 12, 24, kernel=kernel) as G:
+        for dag in (False, True):
+            ref = (O.dslashd if dag else O.dslash)(L, st["R"], st["u"], 0.05, imass)
+            got = (G.dslashd if dag else G.dslash)(st["R"], st["u"], 0.05, imass)
+            assert rel_err(interior(got), interior(ref)) <= TOL
+
+
+@pytest.mark.gpu
+def test_output_halos_are_periodic_images():
+    rng = np.random.default_rng(1)
+    L = O.lat(4, 4, 4, 8)
+    u, R = rand_links(L, rng), rand_spinor(L, rng)
+    with thirring.Lattice(4, 4, 4, 8) as G:
+        got = G.dslash(R, u, 0.1, 1)
+    ref = O.update_halo_5(L, got.copy())
+    # faces equal their periodic images
+    assert np.array_equal(got[0, 1:-1, 1:-1, 1:-1], ref[0, 1:-1, 1:-1, 1:-1])
+    assert np.array_equal(got[1:-1, 0, 1:-1, 1:-1], ref[1:-1, 0, 1:-1, 1:-1])
+    assert np.array_equal(got[1:-1, 1:-1, 1:-1, -1], ref[1:-1, 1:-1, 1:-1, -1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_even_odd_bit_identical(kernel):
+    rng = np.random.default_rng(7)
+    L = O.lat(6, 4, 8, 8, kernel=kernel)
+    u, R = rand_links(L, rng), rand_spinor(L, rng)
+    outs = []
+    for layout in (0, 1):
+        with thirring.Lattice(6, 4, 8, 8, kernel=kernel, layout=layout) as G:
+            outs.append((G.dslash(R, u, 0.02, 3), G.dslashd(R, u, 0.02, 3)))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+@pytest.mark.gpu
+def test_wilson_imass5_rejected():
+    rng = np.random.default_rng(2)
+    L = O.lat(4, 4, 4, 4, kernel=1)
+    u, R = rand_links(L, rng), rand_spinor(L, rng)
+    with thirring.Lattice(4, 4, 4, 4, kernel=1) as G:
+        with pytest.raises(thirring.ThirringError) as ei:
+            G.dslash(R, u, 0.1, 5)
+        assert ei.value.status == 7

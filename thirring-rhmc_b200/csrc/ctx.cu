@@ -1,0 +1,299 @@
+// ctx.cu -- context lifetime, host<->device transfers, links, and the
+// dirac.F90 / gauge.F90 entry points of the C ABI.
+#include <cstdlib>
+#include <cstring>
+
+#include "ctx.h"
+
+using namespace thr;
+
+int thr_ctx::ensure_w64(int count) {
+  while ((int)w64.size() < count) {
+    double2* p = nullptr;
+    if (cudaMalloc(&p, n4() * sizeof(double2)) != cudaSuccess) return THR_ERR_NOMEM;
+    cudaMemsetAsync(p, 0, n4() * sizeof(double2), st);
+    w64.push_back(p);
+  }
+  return THR_OK;
+}
+
+int thr_ctx::upload_spinor(double2* dst, const double* host) {
+  THR_CUDA(cudaMemcpyAsync(stage, host, nf5() * sizeof(double2), cudaMemcpyHostToDevice, st));
+  from_fortran_spinor<double2>(g, dst, stage, st);
+  return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+
+int thr_ctx::download_spinor(double* host, const double2* src) {
+  to_fortran_spinor(g, stage, src, st);
+  THR_CUDA(cudaMemcpyAsync(host, stage, nf5() * sizeof(double2), cudaMemcpyDeviceToHost, st));
+  return THR_OK;
+}
+
+namespace {
+__global__ void k_links_f32(float2* d, const double2* s, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    d[i] = make_float2((float)s[i].x, (float)s[i].y);  // u = cmplx(udp): multishift_module.F90:351
+}
+// coef: gauge.F90:27-32
+__global__ void k_coef(double2* u, const float* theta, Geom g, int ibound) {
+  int n = g.v3 * 3;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int site = i % g.v3, mu = i / g.v3;
+    int x, y, t;
+    site_coords(g, site, x, y, t);
+    float re = 1.0f + 0.0f, im = theta[i];
+    double2 v = make_double2((double)re, (double)im);
+    if (ibound == -1 && mu == 2 && t == g.lt - 1) v = make_double2(-v.x, -v.y);
+    u[i] = v;
+  }
+}
+}  // namespace
+
+int thr_ctx::use_links(const double* u_host) {
+  if (u_host) {
+    THR_CUDA(cudaMemcpyAsync(stage, u_host, nfl() * sizeof(double2), cudaMemcpyHostToDevice, st));
+    from_fortran_links(g, u64, stage, st);
+    links_ok = true;
+  }
+  if (!links_ok) return THR_ERR_BADARG;
+  k_links_f32<<<(g.v3 * 3 + 255) / 256, 256, 0, st>>>(u32, u64, g.v3 * 3);
+  return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+
+int thr_ctx::sync() {
+  THR_CUDA(cudaStreamSynchronize(st));
+  return THR_OK;
+}
+
+// ---------------------------------------------------------------- C ABI
+extern "C" {
+
+const char* thr_status_string(int s) {
+  switch (s) {
+    case THR_OK: return "ok";
+    case THR_ERR_BADARG: return "bad argument";
+    case THR_ERR_BADSHAPE: return "bad shape";
+    case THR_ERR_MAXITER: return "iteration cap reached";
+    case THR_ERR_NAN: return "non-finite value";
+    case THR_ERR_CUDA: return "CUDA error";
+    case THR_ERR_NOMEM: return "out of device memory";
+    case THR_ERR_UNSUPPORTED: return "unsupported option";
+    default: return "unknown status";
+  }
+}
+
+int thr_create(const thr_params* p, thr_ctx** out) {
+  if (!p || !out) return THR_ERR_BADARG;
+  *out = nullptr;
+  if (p->lx < 2 || p->ly < 2 || p->lt < 2 || p->ls < 1 || p->ls > 1024) return THR_ERR_BADSHAPE;
+  if (p->kernel != 0 && p->kernel != 1) return THR_ERR_BADARG;
+  if (p->layout == 1 && (p->lx % 2 != 0)) return THR_ERR_BADSHAPE;
+  thr_ctx* c = new thr_ctx();
+  c->p = *p;
+  if (c->p.ndiag <= 0) c->p.ndiag = 25;
+  c->g.lx = p->lx; c->g.ly = p->ly; c->g.lt = p->lt; c->g.ls = p->ls;
+  c->g.v3 = p->lx * p->ly * p->lt;
+  c->g.v5 = (long long)c->g.v3 * p->ls;
+  c->g.layout = p->layout;
+  c->g.hv3 = c->g.v3 / 2;
+  c->dev = p->device;
+  int rc = THR_OK;
+  if (cudaSetDevice(c->dev) != cudaSuccess) rc = THR_ERR_CUDA;
+  if (!rc && cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) rc = THR_ERR_CUDA;
+  if (!rc && (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)) rc = THR_ERR_CUDA;
+  if (!rc && cudaMalloc(&c->u64, (size_t)c->g.v3 * 3 * sizeof(double2)) != cudaSuccess) rc = THR_ERR_NOMEM;
+  if (!rc && cudaMalloc(&c->u32, (size_t)c->g.v3 * 3 * sizeof(float2)) != cudaSuccess) rc = THR_ERR_NOMEM;
+  c->stage_elems = c->nf5();
+  if (!rc && cudaMalloc(&c->stage, c->stage_elems * sizeof(double2)) != cudaSuccess) rc = THR_ERR_NOMEM;
+  if (!rc && cudaMalloc(&c->partials, kMaxPartials * 8 * sizeof(double)) != cudaSuccess) rc = THR_ERR_NOMEM;
+  if (!rc && cudaMalloc(&c->dscal, 4096 * sizeof(double)) != cudaSuccess) rc = THR_ERR_NOMEM;
+  if (!rc && cudaMalloc(&c->iscal, 1024 * sizeof(int)) != cudaSuccess) rc = THR_ERR_NOMEM;
+  if (!rc && cudaMallocHost(&c->hscal, 4096 * sizeof(double)) != cudaSuccess) rc = THR_ERR_NOMEM;
+  if (!rc && cudaMallocHost(&c->hiscal, 1024 * sizeof(int)) != cudaSuccess) rc = THR_ERR_NOMEM;
+  if (rc) {
+    thr_destroy(c);
+    return rc;
+  }
+  cudaMemsetAsync(c->dscal, 0, 4096 * sizeof(double), c->st);
+  cudaMemsetAsync(c->iscal, 0, 1024 * sizeof(int), c->st);
+  *out = c;
+  return THR_OK;
+}
+
+int thr_destroy(thr_ctx* c) {
+  if (!c) return THR_OK;
+  cudaSetDevice(c->dev);
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (auto p : c->w64) cudaFree(p);
+  cudaFree(c->u64);
+  cudaFree(c->u32);
+  cudaFree(c->stage);
+  cudaFree(c->stage2);
+  cudaFree(c->partials);
+  cudaFree(c->dscal);
+  cudaFree(c->iscal);
+  if (c->hscal) cudaFreeHost(c->hscal);
+  if (c->hiscal) cudaFreeHost(c->hiscal);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return THR_OK;
+}
+
+int thr_set_am3(thr_ctx* c, float am3) {
+  if (!c) return THR_ERR_BADARG;
+  c->p.am3 = am3;
+  return THR_OK;
+}
+int thr_set_beta(thr_ctx* c, float beta) {
+  if (!c) return THR_ERR_BADARG;
+  c->p.beta = beta;
+  return THR_OK;
+}
+
+int thr_host_register(void* ptr, unsigned long long bytes) {
+  if (!ptr) return THR_ERR_BADARG;
+  return cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault) == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+int thr_host_unregister(void* ptr) {
+  if (!ptr) return THR_ERR_BADARG;
+  return cudaHostUnregister(ptr) == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+
+int thr_set_links(thr_ctx* c, const double* u) {
+  if (!c || !u) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  THR_TRY(c->use_links(u));
+  return c->sync();
+}
+
+int thr_coef(thr_ctx* c, double* u, const float* theta) {
+  if (!c || !theta) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  float* th = reinterpret_cast<float*>(c->stage2 ? c->stage2 : c->stage);
+  // theta (Lx,Ly,Lt,3) -> staging (raw) -> device order in the second half of stage
+  size_t n3 = (size_t)c->g.v3 * 3;
+  float* thd = th + n3;
+  THR_CUDA(cudaMemcpyAsync(th, theta, n3 * sizeof(float), cudaMemcpyHostToDevice, c->st));
+  from_fortran_f3(c->g, thd, th, c->st);
+  k_coef<<<(unsigned)((n3 + 255) / 256), 256, 0, c->st>>>(c->u64, thd, c->g, c->p.ibound);
+  c->links_ok = true;
+  THR_TRY(c->use_links(nullptr));
+  if (u) {
+    to_fortran_links(c->g, c->stage, c->u64, c->st);
+    THR_CUDA(cudaMemcpyAsync(u, c->stage, c->nfl() * sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+  }
+  return c->sync();
+}
+
+static int dslash_common(thr_ctx* c, double* Phi, const double* R, const double* u, float am, int imass, bool dag) {
+  if (!c || !Phi || !R) return THR_ERR_BADARG;
+  if (imass != 1 && imass != 3 && imass != 5) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  THR_TRY(c->ensure_w64(2));
+  THR_TRY(c->use_links(u));
+  THR_TRY(c->upload_spinor(c->w64[0], R));
+  THR_TRY(launch_dslash<double2>(c->g, c->p.kernel, dag, c->w64[1], c->w64[0], c->u64, am, imass, c->p.am3, c->st));
+  THR_TRY(c->download_spinor(Phi, c->w64[1]));
+  return c->sync();
+}
+
+int thr_dslash(thr_ctx* c, double* Phi, const double* R, const double* u, float am, int imass) {
+  return dslash_common(c, Phi, R, u, am, imass, false);
+}
+int thr_dslashd(thr_ctx* c, double* Phi, const double* R, const double* u, float am, int imass) {
+  return dslash_common(c, Phi, R, u, am, imass, true);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- device fields
+static size_t prec_bytes(int precision) {
+  switch (precision) {
+    case THR_FP64: return sizeof(double2);
+    case THR_FP32_REF:
+    case THR_MIXED_FP32: return sizeof(float2);
+    case THR_MIXED_BF16: return sizeof(__nv_bfloat162);
+    default: return 0;
+  }
+}
+
+extern "C" {
+
+int thr_field_create(thr_ctx* c, int precision, void** f) {
+  if (!c || !f || !prec_bytes(precision)) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  void* p = nullptr;
+  if (cudaMalloc(&p, c->n4() * prec_bytes(precision)) != cudaSuccess) return THR_ERR_NOMEM;
+  THR_CUDA(cudaMemsetAsync(p, 0, c->n4() * prec_bytes(precision), c->st));
+  *f = p;
+  return THR_OK;
+}
+
+int thr_field_destroy(thr_ctx* c, void* f) {
+  if (!c) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  cudaStreamSynchronize(c->st);
+  return cudaFree(f) == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+
+int thr_field_upload(thr_ctx* c, void* f, int precision, const double* host) {
+  if (!c || !f || !host || !prec_bytes(precision)) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  THR_CUDA(cudaMemcpyAsync(c->stage, host, c->nf5() * sizeof(double2), cudaMemcpyHostToDevice, c->st));
+  if (precision == THR_FP64) from_fortran_spinor<double2>(c->g, (double2*)f, c->stage, c->st);
+  else if (precision == THR_MIXED_BF16) {
+    THR_TRY(c->ensure_w64(1));
+    from_fortran_spinor<double2>(c->g, c->w64[0], c->stage, c->st);
+    convert<__nv_bfloat162, double2>((__nv_bfloat162*)f, c->w64[0], c->n4(), c->st);
+  } else from_fortran_spinor<float2>(c->g, (float2*)f, c->stage, c->st);
+  return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+
+int thr_field_download(thr_ctx* c, double* host, const void* f, int precision) {
+  if (!c || !f || !host || !prec_bytes(precision)) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  const double2* src = (const double2*)f;
+  if (precision != THR_FP64) {
+    THR_TRY(c->ensure_w64(1));
+    if (precision == THR_MIXED_BF16) convert<double2, __nv_bfloat162>(c->w64[0], (const __nv_bfloat162*)f, c->n4(), c->st);
+    else convert<double2, float2>(c->w64[0], (const float2*)f, c->n4(), c->st);
+    src = c->w64[0];
+  }
+  THR_TRY(c->download_spinor(host, src));
+  return c->sync();
+}
+
+int thr_dslash_dev(thr_ctx* c, void* out, const void* in, int precision, float am, int imass, int dag) {
+  if (!c || !out || !in) return THR_ERR_BADARG;
+  if (imass != 1 && imass != 3 && imass != 5) return THR_ERR_BADARG;
+  if (!c->links_ok) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  switch (precision) {
+    case THR_FP64:
+      return launch_dslash<double2>(c->g, c->p.kernel, dag != 0, (double2*)out, (const double2*)in, c->u64, am, imass,
+                                    c->p.am3, c->st);
+    case THR_FP32_REF:
+    case THR_MIXED_FP32:
+      return launch_dslash<float2>(c->g, c->p.kernel, dag != 0, (float2*)out, (const float2*)in, c->u32, am, imass,
+                                   c->p.am3, c->st);
+    case THR_MIXED_BF16:
+      return launch_dslash<__nv_bfloat162>(c->g, c->p.kernel, dag != 0, (__nv_bfloat162*)out,
+                                           (const __nv_bfloat162*)in, c->u32, am, imass, c->p.am3, c->st);
+    default: return THR_ERR_BADARG;
+  }
+}
+
+int thr_sync(thr_ctx* c) {
+  if (!c) return THR_ERR_BADARG;
+  return c->sync();
+}
+
+int thr_get_stream(thr_ctx* c, void** s) {
+  if (!c || !s) return THR_ERR_BADARG;
+  *s = (void*)c->st;
+  return THR_OK;
+}
+
+}  // extern "C"

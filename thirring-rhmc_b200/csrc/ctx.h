@@ -1,0 +1,57 @@
+// ctx.h -- the device context behind a thr_ctx handle.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/thirring_b200.h"
+#include "thr_common.cuh"
+#include "thr_kernels.h"
+
+#define THR_CUDA(call)                                 \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return THR_ERR_CUDA;   \
+  } while (0)
+#define THR_TRY(call)                 \
+  do {                                \
+    int rc_ = (call);                 \
+    if (rc_ != THR_OK) return rc_; \
+  } while (0)
+
+struct thr_ctx {
+  thr_params p;
+  thr::Geom g;
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  // current links (trial::u) in FP64 and FP32
+  double2* u64 = nullptr;
+  float2* u32 = nullptr;
+  bool links_ok = false;
+
+  // staging for Fortran-layout host arrays (sized for one halo'd spinor)
+  double2* stage = nullptr;
+  size_t stage_elems = 0;
+  double2* stage2 = nullptr;
+
+  // FP64 work fields, one spinor each (4*V5 complex)
+  std::vector<double2*> w64;
+  // reduction scratch and device scalars
+  double* partials = nullptr;
+  double* dscal = nullptr;   // general device scalar block
+  int* iscal = nullptr;
+  double* hscal = nullptr;   // pinned host mirror
+  int* hiscal = nullptr;
+
+  size_t n4() const { return (size_t)g.v5 * 4; }  // complex elements of one spinor
+  size_t nf5() const { return (size_t)(g.ls + 2) * (g.lx + 2) * (g.ly + 2) * (g.lt + 2) * 4; }
+  size_t nfl() const { return (size_t)(g.lx + 2) * (g.ly + 2) * (g.lt + 2) * 3; }
+
+  int ensure_w64(int count);
+  int upload_spinor(double2* dst, const double* host);     // Fortran halo'd -> device
+  int download_spinor(double* host, const double2* src);   // device -> Fortran halo'd
+  int use_links(const double* u_host);                    // NULL keeps current links
+  int sync();
+};

@@ -1,0 +1,265 @@
+// dslash.cu -- domain-wall Dirac operator M and M^dagger on one B200.
+//
+// One thread owns one 5D site (s, x, y, t) and all four spin components.
+// A block is (Ls lanes) x (sites per block); consecutive threads read
+// consecutive s of one spin plane, so every load is a coalesced 512-byte
+// warp transaction (FP64).  The six spatial neighbours are periodic index
+// arithmetic: the halo exchange of comms5.F90 is folded into the indexing,
+// and the antiperiodic time boundary lives in the links (gauge.F90:30-32).
+//
+// Shamir kernel: dirac.F90:29-179 (M) and :303-494 (M^dagger), one pass.
+// Wilson kernel: dirac.F90:226-301 (M) and :539-626 (M^dagger).  The
+// reference applies the 3D Wilson operator D_W to 2*Ls+2 projected slices;
+// by linearity of D_W each output slice is
+//   M:      Phi(s) = D_W Q(s) + 2 R(s) - Q(s),
+//           Q(s) = R(s) + P+ R(s-1) + P- R(s+1)   (walls: c1 P+ R(Ls), c2 P- R(1))
+//   M^dag:  Phi(s)[P-] = D_W^dag Qm(s) + 2 R(s) - Qm(s),  Qm = R(s) + R(s-1) (wall z R(Ls))
+//           Phi(s)[P+] = D_W^dag Qp(s) + 2 R(s) - Qp(s),  Qp = R(s) + R(s+1) (wall z' R(1))
+// so the whole operator is again one pass over memory.
+#include "thr_common.cuh"
+#include "thr_kernels.h"
+
+namespace thr {
+
+template <class S>
+struct SpinorView {
+  const S* p;
+  Geom g;
+  __device__ __forceinline__ typename Sto<S>::C operator()(int s, int site, int d) const {
+    return Sto<S>::ld(p, sidx(g, s, site, d));
+  }
+};
+
+// ---------------------------------------------------------------- Shamir
+template <class S, bool DAG>
+__global__ void __launch_bounds__(256) k_dslash_shamir(S* __restrict__ out, const S* __restrict__ in,
+                                                       const typename Sto<S>::C* __restrict__ u, Geom g,
+                                                       float am, int imass, float am3) {
+  using St = Sto<S>;
+  using R = typename St::R;
+  using C = typename St::C;
+  const int s = threadIdx.x;
+  const int site = blockIdx.x * blockDim.y + threadIdx.y;
+  if (site >= g.v3) return;
+  int x, y, t;
+  site_coords(g, site, x, y, t);
+  const Nbr nb = neighbours(g, x, y, t);
+  SpinorView<S> Rv{in, g};
+  const int Ls = g.ls;
+
+  C acc[4];
+  const R diag = (R)((3.0f - am3) + 1.0f);  // dirac.F90:45, default real
+#pragma unroll
+  for (int d = 0; d < 4; d++) acc[d] = diag * Rv(s, site, d);
+
+  auto hop = [&]() {
+#pragma unroll
+    for (int mu = 0; mu < 3; mu++) {
+      const C U = __ldg(u + (size_t)mu * g.v3 + site);
+      const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
+      C A[4], B[4];
+#pragma unroll
+      for (int d = 0; d < 4; d++) {
+        A[d] = cmul(U, Rv(s, nb.f[mu], d));
+        B[d] = cmul(Ub, Rv(s, nb.b[mu], d));
+      }
+#pragma unroll
+      for (int d = 0; d < 4; d++) {
+        const GammaEntry ge = gamma_entry(mu, d);
+        const C w = R(0.5) * (A[d] + B[d]);
+        const C dd = gmul<C, R>(ge, A[ge.gin] - B[ge.gin]);
+        acc[d] = DAG ? ((acc[d] - w) - dd) : ((acc[d] - w) + dd);
+      }
+    }
+  };
+  // s-like term (np_third == 1): dirac.F90:80-87 (M), :317-324 (M^dagger)
+  auto shop = [&]() {
+    if (!DAG) {
+      if (s < Ls - 1) { acc[2] = acc[2] - Rv(s + 1, site, 2); acc[3] = acc[3] - Rv(s + 1, site, 3); }
+      if (s > 0) { acc[0] = acc[0] - Rv(s - 1, site, 0); acc[1] = acc[1] - Rv(s - 1, site, 1); }
+    } else {
+      if (s < Ls - 1) { acc[0] = acc[0] - Rv(s + 1, site, 0); acc[1] = acc[1] - Rv(s + 1, site, 1); }
+      if (s > 0) { acc[2] = acc[2] - Rv(s - 1, site, 2); acc[3] = acc[3] - Rv(s - 1, site, 3); }
+    }
+  };
+  // wall mass term: dirac.F90:119-176 (M), :356-402 (M^dagger)
+  auto mass = [&]() {
+    const R a = (R)am;
+    if (!DAG) {
+      if (imass == 1) {
+        const C zk = mk(a, R(0));
+        if (s == Ls - 1) { acc[2] = acc[2] + cmul(zk, Rv(0, site, 2)); acc[3] = acc[3] + cmul(zk, Rv(0, site, 3)); }
+        if (s == 0) { acc[0] = acc[0] + cmul(zk, Rv(Ls - 1, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(Ls - 1, site, 1)); }
+      } else if (imass == 3) {
+        const C zk = mk(R(0), -a);
+        if (s == Ls - 1) { acc[2] = acc[2] - cmul(zk, Rv(0, site, 2)); acc[3] = acc[3] - cmul(zk, Rv(0, site, 3)); }
+        if (s == 0) { acc[0] = acc[0] + cmul(zk, Rv(Ls - 1, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(Ls - 1, site, 1)); }
+      } else if (imass == 5) {
+        const C zk = mk(R(0), -a);
+        if (s == Ls - 1) { acc[2] = acc[2] - cmul(zk, Rv(Ls - 1, site, 0)); acc[3] = acc[3] - cmul(zk, Rv(Ls - 1, site, 1)); }
+        if (s == 0) { acc[0] = acc[0] - cmul(zk, Rv(0, site, 2)); acc[1] = acc[1] - cmul(zk, Rv(0, site, 3)); }
+      }
+    } else {
+      if (imass == 1) {
+        const C zk = mk(a, R(0));
+        if (s == Ls - 1) { acc[0] = acc[0] + cmul(zk, Rv(0, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(0, site, 1)); }
+        if (s == 0) { acc[2] = acc[2] + cmul(zk, Rv(Ls - 1, site, 2)); acc[3] = acc[3] + cmul(zk, Rv(Ls - 1, site, 3)); }
+      } else if (imass == 3) {
+        const C zk = mk(R(0), a);
+        if (s == Ls - 1) { acc[0] = acc[0] + cmul(zk, Rv(0, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(0, site, 1)); }
+        if (s == 0) { acc[2] = acc[2] - cmul(zk, Rv(Ls - 1, site, 2)); acc[3] = acc[3] - cmul(zk, Rv(Ls - 1, site, 3)); }
+      } else if (imass == 5) {
+        const C zk = mk(R(0), a);
+        if (s == Ls - 1) { acc[0] = acc[0] - cmul(zk, Rv(Ls - 1, site, 2)); acc[1] = acc[1] - cmul(zk, Rv(Ls - 1, site, 3)); }
+        if (s == 0) { acc[2] = acc[2] - cmul(zk, Rv(0, site, 0)); acc[3] = acc[3] - cmul(zk, Rv(0, site, 1)); }
+      }
+    }
+  };
+  if (!DAG) { hop(); shop(); mass(); }
+  else { shop(); mass(); hop(); }
+#pragma unroll
+  for (int d = 0; d < 4; d++) St::st(out, sidx(g, s, site, d), acc[d]);
+}
+
+// ---------------------------------------------------------------- Wilson
+// Q(s) components for the forward operator at (s, site)
+template <class S>
+__device__ __forceinline__ void wilson_q(const SpinorView<S>& Rv, int s, int site, int Ls,
+                                         typename Sto<S>::C c1, typename Sto<S>::C c2,
+                                         typename Sto<S>::C* q) {
+  using C = typename Sto<S>::C;
+  C r[4];
+#pragma unroll
+  for (int d = 0; d < 4; d++) r[d] = Rv(s, site, d);
+  // P+ (spins 0,1) from s-1, wall: c1 * R(Ls)
+#pragma unroll
+  for (int d = 0; d < 2; d++) q[d] = (s > 0) ? r[d] + Rv(s - 1, site, d) : r[d] + cmul(c1, Rv(Ls - 1, site, d));
+  // P- (spins 2,3) from s+1, wall: c2 * R(1)
+#pragma unroll
+  for (int d = 2; d < 4; d++) q[d] = (s < Ls - 1) ? r[d] + Rv(s + 1, site, d) : r[d] + cmul(c2, Rv(0, site, d));
+}
+
+// Q for the adjoint: all four spins of R(s) + (inner ? R(s+ds) : z * R(wall))
+template <class S>
+__device__ __forceinline__ void wilson_qd(const SpinorView<S>& Rv, int s, int site, int sn, bool inner, int swall,
+                                          typename Sto<S>::C z, typename Sto<S>::C* q) {
+#pragma unroll
+  for (int d = 0; d < 4; d++) q[d] = inner ? Rv(s, site, d) + Rv(sn, site, d) : Rv(s, site, d) + cmul(z, Rv(swall, site, d));
+}
+
+template <class S, bool DAG>
+__global__ void __launch_bounds__(256) k_dslash_wilson(S* __restrict__ out, const S* __restrict__ in,
+                                                       const typename Sto<S>::C* __restrict__ u, Geom g,
+                                                       float am, int imass, float am3) {
+  using St = Sto<S>;
+  using R = typename St::R;
+  using C = typename St::C;
+  const int s = threadIdx.x;
+  const int site = blockIdx.x * blockDim.y + threadIdx.y;
+  if (site >= g.v3) return;
+  int x, y, t;
+  site_coords(g, site, x, y, t);
+  const Nbr nb = neighbours(g, x, y, t);
+  SpinorView<S> Rv{in, g};
+  const int Ls = g.ls;
+  const R a = (R)am;
+  const R dgw = (R)(3.0f + (-am3));  // DWilson(…, -am3) diagonal: dirac.F90:191, :505
+  C res[4];
+
+  if (!DAG) {
+    // c1 = -am | -i am  (dirac.F90:274-278),  c2 = -am | +i am  (dirac.F90:287-291)
+    const C c1 = imass == 1 ? mk(-a, R(0)) : mk(R(0), -a);
+    const C c2 = imass == 1 ? mk(-a, R(0)) : mk(R(0), a);
+    C q[4];
+    wilson_q<S>(Rv, s, site, Ls, c1, c2, q);
+#pragma unroll
+    for (int d = 0; d < 4; d++) res[d] = (dgw - R(1)) * q[d] + R(2) * Rv(s, site, d);
+#pragma unroll
+    for (int mu = 0; mu < 3; mu++) {
+      const C U = __ldg(u + (size_t)mu * g.v3 + site);
+      const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
+      C qf[4], qb[4], A[4], B[4];
+      wilson_q<S>(Rv, s, nb.f[mu], Ls, c1, c2, qf);
+      wilson_q<S>(Rv, s, nb.b[mu], Ls, c1, c2, qb);
+#pragma unroll
+      for (int d = 0; d < 4; d++) { A[d] = cmul(U, qf[d]); B[d] = cmul(Ub, qb[d]); }
+#pragma unroll
+      for (int d = 0; d < 4; d++) {
+        const GammaEntry ge = gamma_entry(mu, d);
+        res[d] = (res[d] - R(0.5) * (A[d] + B[d])) + gmul<C, R>(ge, A[ge.gin] - B[ge.gin]);
+      }
+    }
+  } else {
+    // z = -am | -i am (upper right, dirac.F90:602-606); z' = -am | +i am (lower left, :615-619)
+    const C z = imass == 1 ? mk(-a, R(0)) : mk(R(0), -a);
+    const C zp = imass == 1 ? mk(-a, R(0)) : mk(R(0), a);
+    // half 0: output spins 0,1 use Qp = R(s) + R(s+1) | z' R(1); half 1: spins 2,3 use Qm = R(s) + R(s-1) | z R(Ls)
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      const bool inner = half == 0 ? (s < Ls - 1) : (s > 0);
+      const int sn = half == 0 ? s + 1 : s - 1;
+      const int sw = half == 0 ? 0 : Ls - 1;
+      const C zz = half == 0 ? zp : z;
+      C q[4];
+      wilson_qd<S>(Rv, s, site, sn, inner, sw, zz, q);
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        const int d = 2 * half + k;
+        res[d] = (dgw - R(1)) * q[d] + R(2) * Rv(s, site, d);
+      }
+#pragma unroll
+      for (int mu = 0; mu < 3; mu++) {
+        const C U = __ldg(u + (size_t)mu * g.v3 + site);
+        const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
+        C qf[4], qb[4];
+        wilson_qd<S>(Rv, s, nb.f[mu], sn, inner, sw, zz, qf);
+        wilson_qd<S>(Rv, s, nb.b[mu], sn, inner, sw, zz, qb);
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          const int d = 2 * half + k;
+          const GammaEntry ge = gamma_entry(mu, d);
+          const C w = R(0.5) * (cmul(U, qf[d]) + cmul(Ub, qb[d]));
+          const C dd = gmul<C, R>(ge, cmul(U, qf[ge.gin]) - cmul(Ub, qb[ge.gin]));
+          res[d] = (res[d] - w) - dd;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 4; d++) St::st(out, sidx(g, s, site, d), res[d]);
+}
+
+// ---------------------------------------------------------------- launch
+dim3 stencil_block(const Geom& g) {
+  int spb = 256 / g.ls;
+  if (spb < 1) spb = 1;
+  return dim3(g.ls, spb, 1);
+}
+
+template <class S>
+int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
+                  int imass, float am3, cudaStream_t st) {
+  if (g.ls > 1024) return THR_ERR_BADSHAPE;
+  dim3 blk = stencil_block(g);
+  dim3 grd((g.v3 + blk.y - 1) / blk.y);
+  if (kernel == 1) {
+    if (imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
+    if (dag) k_dslash_wilson<S, true><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3);
+    else k_dslash_wilson<S, false><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3);
+  } else {
+    if (dag) k_dslash_shamir<S, true><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3);
+    else k_dslash_shamir<S, false><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3);
+  }
+  return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+
+template int launch_dslash<double2>(const Geom&, int, bool, double2*, const double2*, const double2*, float, int, float,
+                                    cudaStream_t);
+template int launch_dslash<float2>(const Geom&, int, bool, float2*, const float2*, const float2*, float, int, float,
+                                   cudaStream_t);
+template int launch_dslash<__nv_bfloat162>(const Geom&, int, bool, __nv_bfloat162*, const __nv_bfloat162*,
+                                           const float2*, float, int, float, cudaStream_t);
+template int launch_dslash<__half2>(const Geom&, int, bool, __half2*, const __half2*, const float2*, float, int, float,
+                                    cudaStream_t);
+
+}  // namespace thr

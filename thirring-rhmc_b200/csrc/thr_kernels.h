@@ -1,0 +1,52 @@
+// thr_kernels.h -- launchers shared between the translation units of the
+// CUDA library.  Host-callable, stream-ordered, no allocation.
+#pragma once
+#include "thr_common.cuh"
+
+namespace thr {
+
+// number of per-block partial sums a reduction may write (>= any grid used)
+constexpr int kMaxPartials = 4096;
+
+dim3 stencil_block(const Geom& g);
+
+// dslash.cu
+template <class S>
+int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
+                  int imass, float am3, cudaStream_t st);
+
+// layout.cu: Fortran halo'd host layout <-> device fields
+// spinor (0:Ls+1,0:Lx+1,0:Ly+1,0:Lt+1,4) complex(dp)  <-> S[4][V3][Ls]
+template <class S>
+void from_fortran_spinor(const Geom& g, S* out, const double2* fin, cudaStream_t st);
+void to_fortran_spinor(const Geom& g, double2* fout, const double2* in, cudaStream_t st);
+// shift outputs (Ls,Lx,Ly,Lt,4) per shift, no halo
+void to_fortran_noh(const Geom& g, double2* fout, const double2* in, cudaStream_t st);
+void from_fortran_noh(const Geom& g, double2* out, const double2* fin, cudaStream_t st);
+// links (0:Lx+1,0:Ly+1,0:Lt+1,3) complex(dp) <-> double2[3][V3]
+void from_fortran_links(const Geom& g, double2* out, const double2* fin, cudaStream_t st);
+void to_fortran_links(const Geom& g, double2* fout, const double2* in, cudaStream_t st);
+// (Lx,Ly,Lt,3) real or real(dp) <-> [3][V3]
+void from_fortran_f3(const Geom& g, float* out, const float* fin, cudaStream_t st);
+void to_fortran_f3(const Geom& g, float* fout, const float* in, cudaStream_t st);
+void from_fortran_d3(const Geom& g, double* out, const double* fin, cudaStream_t st);
+void to_fortran_d3(const Geom& g, double* fout, const double* in, cudaStream_t st);
+// ps (0:Lx+1,0:Ly+1,0:Lt+1,2) real from device [2][V3] (halo = periodic images)
+void to_fortran_ps(const Geom& g, float* fout, const float* in, cudaStream_t st);
+
+// blas.cu
+template <class Sd, class Ss>
+void convert(Sd* dst, const Ss* src, size_t n, cudaStream_t st);
+void links_to_float(float2* dst, const double2* src, size_t n, cudaStream_t st);
+// per-block partial sums of sum |a|^2 (FP64 accumulation); returns #blocks written
+template <class S>
+int norm2_partials(const S* a, size_t n, double* partials, cudaStream_t st);
+template <class S>
+int redot_partials(const S* a, const S* b, size_t n, double* partials, cudaStream_t st);
+// out = sum of partials (single block, fixed order)
+void finish_sum(const double* partials, int nparts, double* out, cudaStream_t st);
+// y = a*x + y / y = x + a*y etc. with device or host scalars
+void axpy_d(double2* y, const double2* x, double a, size_t n, cudaStream_t st);
+void scale_copy_d(double2* y, const double2* x, double a, size_t n, cudaStream_t st);  // y = a*x
+
+}  // namespace thr

@@ -1,0 +1,11 @@
+"""thirring -- host-side mirror of the thirring-rhmc fermion-path routines on B200.
+
+The functions of `Lattice` carry the names and argument meanings of the
+reference's Fortran routines (dirac.F90 dslash/dslashd, gauge.F90 coef,
+measure_module.F90 congrad, qmrherm_module.F90 qmrherm, derivs_module.F90
+derivs, gaussian.F90 gauss0/gaussp, ...) and operate on numpy arrays in the
+reference's Fortran layout.  All compute runs in libthirring_b200.so on the
+GPU; errors are raised as ThirringError with the library's status code.
+"""
+from ._lib import LibraryMissing, header_functions, lib  # noqa: F401
+from .api import Lattice, ThirringError, spinor, links, field3, ps_field, shift_out  # noqa: F401

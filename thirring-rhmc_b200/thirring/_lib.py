@@ -1,0 +1,83 @@
+"""ctypes loader for libthirring_b200.so and the declarations of its C ABI.
+
+The library is the product: there is no fallback.  If the shared library is
+missing or cannot be loaded this module raises, so nothing downstream can
+silently run on the CPU.
+"""
+import ctypes as C
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "libthirring_b200.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "thirring_b200.h")
+
+
+class Params(C.Structure):
+    _fields_ = [("lx", C.c_int), ("ly", C.c_int), ("lt", C.c_int), ("ls", C.c_int),
+                ("kernel", C.c_int), ("layout", C.c_int), ("ndiag", C.c_int),
+                ("am3", C.c_float), ("beta", C.c_float), ("ibound", C.c_int), ("device", C.c_int)]
+
+
+_v = C.c_void_p
+_i = C.c_int
+_f = C.c_float
+_d = C.c_double
+_pi = C.POINTER(C.c_int)
+_pd = C.POINTER(C.c_double)
+
+# name -> (restype, argtypes); every function declared in include/thirring_b200.h
+SIGNATURES = {
+    "thr_create": (_i, [C.POINTER(Params), C.POINTER(_v)]),
+    "thr_destroy": (_i, [_v]),
+    "thr_status_string": (C.c_char_p, [_i]),
+    "thr_set_am3": (_i, [_v, _f]),
+    "thr_set_beta": (_i, [_v, _f]),
+    "thr_host_register": (_i, [_v, C.c_ulonglong]),
+    "thr_host_unregister": (_i, [_v]),
+    "thr_coef": (_i, [_v, _v, _v]),
+    "thr_set_links": (_i, [_v, _v]),
+    "thr_dslash": (_i, [_v, _v, _v, _v, _f, _i]),
+    "thr_dslashd": (_i, [_v, _v, _v, _v, _f, _i]),
+    "thr_field_create": (_i, [_v, _i, C.POINTER(_v)]),
+    "thr_field_destroy": (_i, [_v, _v]),
+    "thr_field_upload": (_i, [_v, _v, _i, _v]),
+    "thr_field_download": (_i, [_v, _v, _v, _i]),
+    "thr_dslash_dev": (_i, [_v, _v, _v, _i, _f, _i, _i]),
+    "thr_sync": (_i, [_v]),
+    "thr_get_stream": (_i, [_v, C.POINTER(_v)]),
+}
+
+
+def header_functions(path=HEADER):
+    """Names of all functions declared in the C header."""
+    txt = open(path).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:int|const char \*|void)\s*\**\s*(thr_\w+)\s*\(", txt, flags=re.M)))
+
+
+class LibraryMissing(RuntimeError):
+    pass
+
+
+def load(path=LIB_PATH):
+    if not os.path.exists(path):
+        raise LibraryMissing(
+            f"{path} is not built; run `python thirring-rhmc_b200/build.py` (the CUDA library is required)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        _LIB = load()
+    return _LIB

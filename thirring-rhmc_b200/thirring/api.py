@@ -1,0 +1,146 @@
+"""Reference-shaped API over the C ABI.
+
+Array shapes (numpy, order='F'), as declared in the reference:
+  spinor  complex128 (Ls+2, Lx+2, Ly+2, Lt+2, 4)      dirac.F90:13-15
+  links   complex128 (Lx+2, Ly+2, Lt+2, 3)            trial.F90:6
+  theta   float32    (Lx, Ly, Lt, 3)                  trial.F90:7
+  dSdpi   float64    (Lx, Ly, Lt, 3)                  gforce.F90:6
+  ps      float32    (Lx+2, Ly+2, Lt+2, 2)            dum1.F90:6
+  shifts  complex128 (Ls, Lx, Ly, Lt, 4, ndiag)       multishift_module.F90:29
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+SHAMIR, WILSON = 0, 1
+NATURAL, EVEN_ODD = 0, 1
+FP64, FP32_REF, MIXED_FP32, MIXED_BF16 = 0, 1, 2, 3
+
+
+class ThirringError(RuntimeError):
+    def __init__(self, status, where):
+        self.status = status
+        msg = _lib.lib().thr_status_string(status).decode()
+        super().__init__(f"{where}: {msg} (status {status})")
+
+
+def _check(rc, where):
+    if rc != 0:
+        raise ThirringError(rc, where)
+
+
+def _p(a):
+    if a is None:
+        return None
+    if not (a.flags.f_contiguous or a.flags.c_contiguous):
+        raise ValueError("array must be contiguous")
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def spinor(L):
+    return np.zeros((L.ls + 2, L.lx + 2, L.ly + 2, L.lt + 2, 4), np.complex128, order="F")
+
+
+def links(L):
+    return np.zeros((L.lx + 2, L.ly + 2, L.lt + 2, 3), np.complex128, order="F")
+
+
+def field3(L, dtype=np.float64):
+    return np.zeros((L.lx, L.ly, L.lt, 3), dtype, order="F")
+
+
+def ps_field(L):
+    return np.zeros((L.lx + 2, L.ly + 2, L.lt + 2, 2), np.float32, order="F")
+
+
+def shift_out(L, ndiag=None):
+    return np.zeros((L.ls, L.lx, L.ly, L.lt, 4, ndiag or L.ndiag), np.complex128, order="F")
+
+
+def _need(a, shape, dtype, name):
+    if a.shape != shape or a.dtype != dtype or not a.flags.f_contiguous:
+        raise ValueError(f"{name}: expected Fortran-ordered {dtype} array of shape {shape}, got "
+                         f"{a.dtype} {a.shape}")
+
+
+class Lattice:
+    """One lattice (sizes, kernel, layout) bound to one GPU context."""
+
+    def __init__(self, lx, ly, lt, ls, kernel=SHAMIR, layout=NATURAL, ndiag=25, am3=1.0, beta=0.4,
+                 ibound=-1, device=0):
+        self.lx, self.ly, self.lt, self.ls = lx, ly, lt, ls
+        self.kernel, self.layout, self.ndiag = kernel, layout, ndiag
+        self.am3, self.beta, self.ibound = am3, beta, ibound
+        self._L = _lib.lib()
+        prm = _lib.Params(lx, ly, lt, ls, kernel, layout, ndiag, am3, beta, ibound, device)
+        h = C.c_void_p()
+        _check(self._L.thr_create(C.byref(prm), C.byref(h)), "thr_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.thr_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- shapes
+    @property
+    def sshape(self):
+        return (self.ls + 2, self.lx + 2, self.ly + 2, self.lt + 2, 4)
+
+    @property
+    def ushape(self):
+        return (self.lx + 2, self.ly + 2, self.lt + 2, 3)
+
+    def set_am3(self, am3):
+        self.am3 = am3
+        _check(self._L.thr_set_am3(self.h, am3), "thr_set_am3")
+
+    def set_beta(self, beta):
+        self.beta = beta
+        _check(self._L.thr_set_beta(self.h, beta), "thr_set_beta")
+
+    # ---- gauge.F90
+    def coef(self, theta):
+        """u = coef(theta): gauge.F90:12-43.  Also becomes the current links."""
+        theta = np.asfortranarray(theta, np.float32)
+        _need(theta, (self.lx, self.ly, self.lt, 3), np.float32, "theta")
+        u = links(self)
+        _check(self._L.thr_coef(self.h, _p(u), _p(theta)), "coef")
+        return u
+
+    def set_links(self, u):
+        _need(u, self.ushape, np.complex128, "u")
+        _check(self._L.thr_set_links(self.h, _p(u)), "set_links")
+
+    # ---- dirac.F90
+    def dslash(self, R, u, am, imass, out=None):
+        """Phi = M R  (dirac.F90:11-27).  u=None uses the current links."""
+        _need(R, self.sshape, np.complex128, "R")
+        if u is not None:
+            _need(u, self.ushape, np.complex128, "u")
+        Phi = out if out is not None else spinor(self)
+        _check(self._L.thr_dslash(self.h, _p(Phi), _p(R), _p(u), am, imass), "dslash")
+        return Phi
+
+    def dslashd(self, R, u, am, imass, out=None):
+        """Phi = M^dagger R  (dirac.F90:410-431)."""
+        _need(R, self.sshape, np.complex128, "R")
+        if u is not None:
+            _need(u, self.ushape, np.complex128, "u")
+        Phi = out if out is not None else spinor(self)
+        _check(self._L.thr_dslashd(self.h, _p(Phi), _p(R), _p(u), am, imass), "dslashd")
+        return Phi
