@@ -97,6 +97,72 @@ int thr_dslash(thr_ctx *ctx, double *Phi, const double *R, const double *u, floa
  * (reqs_R has no counterpart: there is no halo exchange to complete.) */
 int thr_dslashd(thr_ctx *ctx, double *Phi, const double *R, const double *u, float am, int imass);
 
+/* ---- measure_module.F90 -------------------------------------------------- */
+/* congrad(Phi, res, itercg, am, imass[, iterations]), measure_module.F90:9-140:
+ * CG on M^dagger M x = Phi with the context's current links.  X is the
+ * module variable vector::X: initial guess in, solution out.  Stops when
+ * |r|^2 < 4*Lx*Ly*Lt*Ls*res^2 or after niterc = Ls*Lx*Ly*Lt iterations
+ * (then returns THR_ERR_MAXITER with X holding the last iterate, where the
+ * reference writes a notice).  *iterations gets the Fortran loop index nx. */
+int thr_congrad(thr_ctx *ctx, const double *Phi, double *X, float res, int *itercg, float am, int imass,
+                int *iterations);
+
+/* ---- multishift_module.F90 ----------------------------------------------- */
+/* multishift_solver(u, am, imass, ndiagq, aden, anum, output, input, res,
+ * maxcg, cg_return[, cg_returns]), multishift_module.F90:13-284: solves
+ * (M^dagger M + aden(i)) output(i) = input for i = 1..ndiagq.  output is
+ * (Ls,Lx,Ly,Lt,4,ndiag) and is zeroed beyond ndiagq like the reference.
+ * u may be NULL (current links).  cg_returns may be NULL. */
+int thr_multishift_solver(thr_ctx *ctx, const double *u, float am, int imass, int ndiagq, const double *aden,
+                          const double *anum, double *output, const double *input, float res, int maxcg,
+                          int *cg_return, int *cg_returns);
+/* multishift_solver_sp, multishift_module.F90:289-534: the same with FP32
+ * vectors and links, FP64 scalars (its precision, not better). */
+int thr_multishift_solver_sp(thr_ctx *ctx, const double *u, float am, int imass, int ndiagq, const double *aden,
+                             const double *anum, double *output, const double *input, float res, int maxcg,
+                             int *cg_return, int *cg_returns);
+
+/* ---- qmrherm_module.F90 -------------------------------------------------- */
+/* qmrherm(Phi, x, res, itercg, am, imass, anum, aden, ndiagq, iflag[, use_sp]
+ * [, cg_returns]), qmrherm_module.F90:20-197, with the current links:
+ *   iflag 0: x = anum(0) Phi + sum_i anum(i) (M^dagger M + aden(i))^-1 Phi
+ *   iflag 1: as 0, and Phi0(…, i) = the i-th shifted solution
+ *   iflag 2: x = anum(0) Phi; dSdpi += sum_i derivs(x_i, M x_i, anum(i), 0)
+ *   iflag 3: x = anum(0) Phi; dSdpi += sum_i [derivs(Phi0_i, M x_i, -anum(i), 0)
+ *                                            + derivs(M Phi0_i, x_i, -anum(i), 1)]
+ * anum has ndiagq+1 entries (anum(0:ndiagq)).  use_sp != 0 selects the
+ * single-precision multishift (Shamir only, as in the reference).
+ * dSdpi (gforce::dSdpi, accumulated) and Phi0 (qmrherm_module::Phi0,
+ * (0:Ls+1,…,4,ndiag)) may be NULL to keep them in the context only; the
+ * context always keeps the last Phi0 written by iflag 1.
+ * max_qmr_iters <= 0 means the reference default 50000 (params.F90:56).
+ * Returns THR_ERR_BADSHAPE where the reference aborts (:66-81). */
+int thr_qmrherm(thr_ctx *ctx, const double *Phi, double *x, float res, int *itercg, float am, int imass,
+                const double *anum, const double *aden, int ndiagq, int iflag, int use_sp, int *cg_returns,
+                double *dSdpi, double *Phi0, int max_qmr_iters);
+
+/* ---- derivs_module.F90 --------------------------------------------------- */
+/* derivs(R, X2, anum, iflag, am, imass), derivs_module.F90:8-26: adds the
+ * force term of (R, X2) to dSdpi (gforce::dSdpi, (Lx,Ly,Lt,3), in/out; NULL
+ * accumulates into the context's copy).  Shamir or Wilson per the context. */
+int thr_derivs(thr_ctx *ctx, const double *R, const double *X2, double anum, int iflag, float am, int imass,
+               double *dSdpi);
+
+/* ---- random.f90 / site_random.f90 / gaussian.F90 ------------------------- */
+/* init_random(seed), site_random.f90:133-148 (site_streams = 1, one stream per
+ * 3D site, seeded seed + x + Lx*y + Lx*Lx*t, on the device) or
+ * random.f90:119-126 (site_streams = 0, one sequential stream, on the host).
+ * seed must be an integer value in [0, 2^48). */
+int thr_init_random(thr_ctx *ctx, double seed, int site_streams);
+/* gauss0(ps), gaussian.F90:63-104: unit Gaussian pairs (variance 1/2 per
+ * component); ps is (0:Lx+1,0:Ly+1,0:Lt+1,2) with periodic halos. */
+int thr_gauss0(thr_ctx *ctx, float *ps);
+/* gaussp(ps), gaussian.F90:14-61: variance 1 per component. */
+int thr_gaussp(thr_ctx *ctx, float *ps);
+/* rano(yran, idum, ix, iy, it): one uniform draw from the stream of 1-based
+ * site (ix,iy,it) (ignored for the global stream), random.f90:28-58. */
+int thr_rano(thr_ctx *ctx, int ix, int iy, int it, float *out);
+
 /* ---- device-resident fields ------------------------------------------- */
 /* Spinor fields kept in HBM in the device layout (no halos), so that solver
  * and MD loops never cross PCIe.  `precision` is a thr_precision storage

@@ -170,6 +170,13 @@ def dslashd(L, R, u, am, imass):
     return Phi
 
 
+def dirac_operator(L, X, u, am, imass):
+    """M^dagger M X with halos refreshed (inverter_utils.F90:20-54)."""
+    out = spinor(L)
+    lib.orc_dirac_operator(C.byref(L), P(out), P(X), P(u), am, imass)
+    return out
+
+
 def update_halo_5(L, a):
     lib.orc_update_halo_5(C.byref(L), P(a))
     return a

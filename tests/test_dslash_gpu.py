@@ -53,7 +53,7 @@ def test_output_halos_are_periodic_images():
     u, R = rand_links(L, rng), rand_spinor(L, rng)
     with thirring.Lattice(4, 4, 4, 8) as G:
         got = G.dslash(R, u, 0.1, 1)
-    ref = O.update_halo_5(L, got.copy())
+    ref = O.update_halo_5(L, got.copy(order="F"))
     # faces equal their periodic images
     assert np.array_equal(got[0, 1:-1, 1:-1, 1:-1], ref[0, 1:-1, 1:-1, 1:-1])
     assert np.array_equal(got[1:-1, 0, 1:-1, 1:-1], ref[1:-1, 0, 1:-1, 1:-1])

@@ -1,0 +1,141 @@
+"""congrad, multishift_solver(_sp), qmrherm and derivs on the GPU vs the oracle.
+
+Tolerances: the FP64 paths run the same recurrences as the oracle (and stop
+at the same iteration), so solutions agree to 1e-10 relative; the
+single-precision reference solver (multishift_solver_sp) to 1e-4.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+import thirring
+from helpers import interior, rand_links, rand_spinor, rel_err
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def remez(name, n):
+    return O.read_remez(os.path.join(GOLD, name), n)  # (anumA, adenA, anumB, adenB)
+
+
+@pytest.mark.gpu
+def test_congrad_kat_and_parity():
+    # tests/test_congrad.F90: itercg == 27 on the 12^3 x 24 analytic state
+    L = O.lat(12, 12, 12, 24)
+    st = O.starting_state(L, X=True)
+    X_ref = st["X"].copy(order="F")
+    it_ref, _ = O.congrad(L, st["Phi"], X_ref, st["u"], 0.1, 0.05, 3)
+    with thirring.Lattice(12, 12, 12, 24) as G:
+        G.set_links(st["u"])
+        X = st["X"].copy(order="F")
+        itercg, nx = G.congrad(st["Phi"], X, 0.1, 0.05, 3)
+    assert itercg == 27 == it_ref and nx == 27
+    assert rel_err(interior(X), interior(X_ref)) <= 1e-10
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel,imass,layout", [(0, 1, 0), (0, 3, 1), (0, 5, 0), (1, 1, 0), (1, 3, 1)])
+def test_congrad_tight(kernel, imass, layout):
+    rng = np.random.default_rng(11 + kernel + imass)
+    L = O.lat(4, 4, 6, 8, kernel=kernel)
+    u = rand_links(L, rng)
+    Phi = rand_spinor(L, rng)
+    X_ref = O.spinor(L)
+    it_ref, _ = O.congrad(L, Phi, X_ref, u, 1e-9, 0.05, imass)
+    with thirring.Lattice(4, 4, 6, 8, kernel=kernel, layout=layout) as G:
+        G.set_links(u)
+        X = O.spinor(L)
+        it, _ = G.congrad(Phi, X, 1e-9, 0.05, imass)
+    assert abs(it - it_ref) <= 1
+    assert rel_err(interior(X), interior(X_ref)) <= 1e-9
+    # true residual of the GPU solution (stopping rule |r|^2 < 4 V Ls res^2)
+    r = interior(Phi) - interior(O.dirac_operator(L, X, u, 0.05, imass))
+    assert np.linalg.norm(r) <= 10 * np.sqrt(4 * 4 * 4 * 6 * 8) * 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sp", [False, True])
+def test_multishift_vs_oracle(sp):
+    rng = np.random.default_rng(3)
+    L = O.lat(4, 4, 4, 8)
+    u = rand_links(L, rng)
+    inp = rand_spinor(L, rng)
+    an, ad, _, _ = remez("remez2g", 12)
+    res = 1e-6 if sp else 1e-9
+    out_ref, it_ref, cgr_ref = O.multishift(L, u, 0.05, 1, an[1:], ad, inp, res, 5000, sp=sp)
+    with thirring.Lattice(4, 4, 4, 8) as G:
+        out, it, cgr = G.multishift_solver(u, 0.05, 1, ad, an[1:], inp, res, 5000, sp=sp)
+    if sp:
+        assert abs(it - it_ref) <= 3
+        assert rel_err(out[..., :12], out_ref[..., :12]) <= 1e-4
+    else:
+        assert it == it_ref and np.array_equal(cgr, cgr_ref)
+        assert rel_err(out[..., :12], out_ref[..., :12]) <= 1e-10
+    assert np.all(out[..., 12:] == 0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_qmrherm_all_iflags(kernel):
+    rng = np.random.default_rng(17 + kernel)
+    L = O.lat(4, 4, 6, 8, kernel=kernel)
+    u = rand_links(L, rng)
+    Phi = rand_spinor(L, rng)
+    an, ad, _, _ = remez("remez4g", 12)
+    Phi0_ref = np.zeros((L.ls + 2, L.lx + 2, L.ly + 2, L.lt + 2, 4, 25), np.complex128, order="F")
+    dS_ref = O.field3(L)
+    with thirring.Lattice(4, 4, 6, 8, kernel=kernel) as G:
+        G.set_links(u)
+        Phi0 = np.zeros_like(Phi0_ref)
+        dS = O.field3(L)
+        for iflag in (0, 1, 2, 3):
+            x_ref, it_ref, _, rc = O.qmrherm(L, u, Phi, 1e-9, 0.05, 3, an, ad, iflag, dSdpi=dS_ref, Phi0=Phi0_ref)
+            assert rc == 0
+            x, it, _ = G.qmrherm(Phi, 1e-9, 0.05, 3, an, ad, iflag, dSdpi=dS, Phi0=Phi0)
+            assert it == it_ref
+            assert rel_err(interior(x), interior(x_ref)) <= 1e-10, iflag
+            if iflag == 1:
+                assert rel_err(Phi0[1:-1, 1:-1, 1:-1, 1:-1, :, :12], Phi0_ref[1:-1, 1:-1, 1:-1, 1:-1, :, :12]) <= 1e-10
+            if iflag >= 2:
+                assert rel_err(dS, dS_ref) <= 1e-9, iflag
+
+
+@pytest.mark.gpu
+def test_qmrherm_guards():
+    # qmrherm_module.F90:66-81: ndiagq > ndiag and Ls % 4 != 0 abort the reference
+    rng = np.random.default_rng(4)
+    L = O.lat(4, 4, 4, 6)
+    Phi = rand_spinor(L, rng)
+    an, ad, _, _ = remez("remez4g", 12)
+    with thirring.Lattice(4, 4, 4, 6) as G:
+        G.coef(np.zeros((4, 4, 4, 3), np.float32))
+        with pytest.raises(thirring.ThirringError) as e:
+            G.qmrherm(Phi, 1e-6, 0.05, 1, an, ad, 0)
+        assert e.value.status == 2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel,iflag,imass", [(0, 0, 1), (0, 1, 3), (1, 0, 1), (1, 1, 3), (1, 0, 3), (1, 1, 1)])
+def test_derivs_vs_oracle(kernel, iflag, imass):
+    rng = np.random.default_rng(100 + 10 * kernel + iflag)
+    L = O.lat(4, 6, 4, 8, kernel=kernel)
+    R, X2 = rand_spinor(L, rng), rand_spinor(L, rng)
+    dS0 = np.asfortranarray(rng.standard_normal((4, 6, 4, 3)))
+    ref = O.derivs(L, R, X2, 0.37, iflag, 0.05, imass, dS0.copy(order="F"))
+    with thirring.Lattice(4, 6, 4, 8, kernel=kernel) as G:
+        got = G.derivs(R, X2, 0.37, iflag, 0.05, imass, dS0.copy(order="F"))
+    assert rel_err(got, ref) <= 1e-12
+
+
+@pytest.mark.gpu
+def test_derivs_reference_fixture():
+    # tests/test_derivs_shamir.F90: anum = tau, iflag 0, imass 3, am 0.05, dSdpi = fixture
+    L = O.lat(12, 12, 12, 24)
+    st = O.starting_state(L, R=True, X=True, dSdpi=True)
+    tau = 8 * np.arctan(1.0)
+    ref = O.derivs(L, st["R"], st["X"], tau, 0, 0.05, 3, st["dSdpi"].copy(order="F"))
+    with thirring.Lattice(12, 12, 12, 24) as G:
+        got = G.derivs(st["R"], st["X"], tau, 0, 0.05, 3, st["dSdpi"].copy(order="F"))
+    assert rel_err(got, ref) <= 1e-12

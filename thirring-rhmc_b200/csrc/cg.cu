@@ -1,0 +1,175 @@
+// cg.cu -- congrad (measure_module.F90:9-140) on the device.
+//
+// Every scalar of the recurrence lives in device memory and is updated by a
+// one-thread kernel, so the host only enqueues iterations and polls a
+// `done` flag every few iterations; iterations enqueued after convergence
+// return immediately (each kernel tests `done` first).  Vector work per
+// iteration: x1 = M p | |x1|^2 | x2 = M^dagger x1 | r -= alpha x2, |r|^2 |
+// x += alpha p, p = r + beta p.
+#include "ctx.h"
+#include "solver.h"
+
+namespace thr {
+
+namespace {
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double sh[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  int nw = (blockDim.x + 31) >> 5;
+  v = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+  if (w == 0) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+
+__device__ double sum_partials(const double* p, int n) {
+  // one thread, fixed order (n <= a few thousand)
+  double a = 0.0;
+  for (int i = 0; i < n; i++) a += p[i];
+  return a;
+}
+
+__global__ void k_cg_norm2(const CgState* cs, const double2* a, size_t n, double* partials) {
+  if (cs->done) return;
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double2 v = a[i];
+    acc += v.x * v.x + v.y * v.y;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+// measure_module.F90:57, :66-75
+__global__ void k_cg_alpha(CgState* cs, const double* partials, int np) {
+  if (cs->done) return;
+  cs->nx += 1;
+  cs->itercg += 1;
+  if (cs->nx != 1) {
+    double alphad = sum_partials(partials, np);
+    cs->alpha = cs->alphan / alphad;
+  }
+}
+
+// r = r - alpha*x2 (:92) fused with betacgn = |r|^2 (:102)
+__global__ void k_cg_rupdate(CgState* cs, double2* r, const double2* x2, size_t n, double* partials) {
+  if (cs->done) return;
+  const double alpha = cs->alpha;
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double2 v = r[i] - alpha * x2[i];
+    r[i] = v;
+    acc += v.x * v.x + v.y * v.y;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+// :102-110, :120
+__global__ void k_cg_beta(CgState* cs, const double* partials, int np) {
+  if (cs->done) return;
+  double betacgn = sum_partials(partials, np);
+  double betacg = betacgn / cs->betacgd;
+  cs->betacgd = betacgn;
+  cs->alphan = betacgn;
+  if (cs->nx == 1) betacg = 0.0;
+  cs->betacg = betacg;
+  cs->betacgn = betacgn;
+  if (!(betacgn == betacgn)) { cs->status = THR_ERR_NAN; cs->pending_done = 1; }
+  if (betacgn < cs->resid) cs->pending_done = 1;
+  else if (cs->nx >= cs->niterc) { cs->pending_done = 1; cs->capped = 1; }
+}
+
+// x = x + alpha*p (:77, skipped at nx == 1); p = r + betacg*p (:119); then latch done
+__global__ void k_cg_xp(CgState* cs, double2* x, double2* p, const double2* r, size_t n) {
+  if (cs->done) return;
+  const double alpha = cs->alpha, beta = cs->betacg;
+  const bool upd = cs->nx != 1;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double2 pv = p[i];
+    if (upd) x[i] = x[i] + alpha * pv;
+    p[i] = r[i] + beta * pv;
+  }
+}
+__global__ void k_cg_latch(CgState* cs) {
+  if (cs->pending_done) cs->done = 1;
+}
+
+inline unsigned vec_grid(size_t n) {
+  size_t b = (n + kThreads - 1) / kThreads;
+  if (b > 148 * 8) b = 148 * 8;
+  return (unsigned)(b ? b : 1);
+}
+}  // namespace
+
+// Runs congrad on device fields: Phi (rhs), X (guess in, solution out).
+int congrad_dev(thr_ctx* c, const double2* Phi, double2* X, float res, float am, int imass, int niterc, int* itercg,
+                int* iterations) {
+  const size_t n = c->n4();
+  THR_TRY(c->ensure_w64(6));
+  double2 *p = c->w64[2], *r = c->w64[3], *x1 = c->w64[4], *x2 = c->w64[5];
+  CgState* cs = reinterpret_cast<CgState*>(c->dscal);
+  CgState h{};
+  // resid = 4*ksize*ksize*ksizet*kthird*res*res in default real (measure_module.F90:41)
+  int ivol = 4 * c->g.lx * c->g.ly * c->g.lt * c->g.ls;
+  float resid = ((float)ivol * res) * res;
+  h.resid = (double)resid;
+  h.alpha = 1.0;
+  h.alphan = 0.0;
+  h.betacgd = 1.0;
+  h.niterc = niterc;
+  THR_CUDA(cudaMemcpyAsync(cs, &h, sizeof(CgState), cudaMemcpyHostToDevice, c->st));
+  THR_CUDA(cudaMemcpyAsync(p, X, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
+  THR_CUDA(cudaMemcpyAsync(r, Phi, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
+  const unsigned gb = vec_grid(n);
+  const int chunk = 8;
+  for (int base = 0; base < niterc + chunk; base += chunk) {
+    for (int k = 0; k < chunk; k++) {
+      THR_TRY(launch_dslash_guarded<double2>(c, false, x1, p, c->u64, am, imass, &cs->done));
+      k_cg_norm2<<<gb, kThreads, 0, c->st>>>(cs, x1, n, c->partials);
+      k_cg_alpha<<<1, 1, 0, c->st>>>(cs, c->partials, gb);
+      THR_TRY(launch_dslash_guarded<double2>(c, true, x2, x1, c->u64, am, imass, &cs->done));
+      k_cg_rupdate<<<gb, kThreads, 0, c->st>>>(cs, r, x2, n, c->partials);
+      k_cg_beta<<<1, 1, 0, c->st>>>(cs, c->partials, gb);
+      k_cg_xp<<<gb, kThreads, 0, c->st>>>(cs, X, p, r, n);
+      k_cg_latch<<<1, 1, 0, c->st>>>(cs);
+    }
+    THR_CUDA(cudaMemcpyAsync(&h, cs, sizeof(CgState), cudaMemcpyDeviceToHost, c->st));
+    THR_CUDA(cudaStreamSynchronize(c->st));
+    if (h.done) break;
+  }
+  if (itercg) *itercg = h.itercg;
+  // Fortran DO semantics: nx ends at niterc+1 when the loop runs out (:124)
+  if (iterations) *iterations = h.capped ? h.nx + 1 : h.nx;
+  if (h.status) return h.status;
+  return h.capped ? THR_ERR_MAXITER : THR_OK;
+}
+
+}  // namespace thr
+
+using namespace thr;
+
+extern "C" int thr_congrad(thr_ctx* c, const double* Phi, double* X, float res, int* itercg, float am, int imass,
+                           int* iterations) {
+  if (!c || !Phi || !X) return THR_ERR_BADARG;
+  if (imass != 1 && imass != 3 && imass != 5) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  THR_TRY(c->ensure_w64(6));
+  THR_TRY(c->use_links(nullptr));
+  THR_TRY(c->upload_spinor(c->w64[0], Phi));
+  THR_TRY(c->upload_spinor(c->w64[1], X));
+  int niterc = c->g.ls * c->g.v3;  // params.F90:57
+  int rc = congrad_dev(c, c->w64[0], c->w64[1], res, am, imass, niterc, itercg, iterations);
+  if (rc != THR_OK && rc != THR_ERR_MAXITER) return rc;
+  THR_TRY(c->download_spinor(X, c->w64[1]));
+  int rs = c->sync();
+  return rs ? rs : rc;
+}

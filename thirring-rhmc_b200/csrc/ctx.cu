@@ -17,6 +17,22 @@ int thr_ctx::ensure_w64(int count) {
   return THR_OK;
 }
 
+int thr_ctx::buffer(int id, size_t bytes, void** out) {
+  if (id < 0 || id >= B_COUNT) return THR_ERR_BADARG;
+  if (buf_bytes[id] < bytes) {
+    cudaStreamSynchronize(st);
+    cudaFree(bufs[id]);
+    bufs[id] = nullptr;
+    buf_bytes[id] = 0;
+    if (cudaMalloc(&bufs[id], bytes) != cudaSuccess) return THR_ERR_NOMEM;
+    buf_bytes[id] = bytes;
+    cudaMemsetAsync(bufs[id], 0, bytes, st);
+    if (id == B_PHI0) phi0_valid = false;
+  }
+  *out = bufs[id];
+  return THR_OK;
+}
+
 int thr_ctx::upload_spinor(double2* dst, const double* host) {
   THR_CUDA(cudaMemcpyAsync(stage, host, nf5() * sizeof(double2), cudaMemcpyHostToDevice, st));
   from_fortran_spinor<double2>(g, dst, stage, st);
@@ -125,6 +141,8 @@ int thr_destroy(thr_ctx* c) {
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
   for (auto p : c->w64) cudaFree(p);
+  for (int i = 0; i < thr_ctx::B_COUNT; i++) cudaFree(c->bufs[i]);
+  c->rng.release();
   cudaFree(c->u64);
   cudaFree(c->u32);
   cudaFree(c->stage);

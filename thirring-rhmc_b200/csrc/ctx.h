@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "../../include/thirring_b200.h"
+#include "rng.h"
 #include "thr_common.cuh"
 #include "thr_kernels.h"
 
@@ -44,6 +45,24 @@ struct thr_ctx {
   int* iscal = nullptr;
   double* hscal = nullptr;   // pinned host mirror
   int* hiscal = nullptr;
+
+  // named device buffers that grow on demand (solver workspaces, Phi0, dSdpi)
+  enum Buf {
+    B_X1 = 0,   // multishift outputs x1 (FP64), ndiag fields
+    B_SF64,     // FP64 shift vectors
+    B_OUT32,    // FP32 multishift outputs
+    B_SF32,     // FP32 shift vectors
+    B_WORK32,   // FP32 work vectors
+    B_PHI0,     // qmrherm_module::Phi0 (FP64), ndiag fields
+    B_DSDPI,    // gforce::dSdpi, [3][V3] FP64
+    B_AUX,      // misc
+    B_COUNT = 16
+  };
+  void* bufs[B_COUNT] = {};
+  size_t buf_bytes[B_COUNT] = {};
+  bool phi0_valid = false;
+  thr::Rng rng;  // random's module state
+  int buffer(int id, size_t bytes, void** out);  // contents preserved only if not regrown
 
   size_t n4() const { return (size_t)g.v5 * 4; }  // complex elements of one spinor
   size_t nf5() const { return (size_t)(g.ls + 2) * (g.lx + 2) * (g.ly + 2) * (g.lt + 2) * 4; }

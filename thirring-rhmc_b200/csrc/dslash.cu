@@ -34,7 +34,8 @@ struct SpinorView {
 template <class S, bool DAG>
 __global__ void __launch_bounds__(256) k_dslash_shamir(S* __restrict__ out, const S* __restrict__ in,
                                                        const typename Sto<S>::C* __restrict__ u, Geom g,
-                                                       float am, int imass, float am3) {
+                                                       float am, int imass, float am3, const int* skip) {
+  if (skip && *skip) return;
   using St = Sto<S>;
   using R = typename St::R;
   using C = typename St::C;
@@ -150,7 +151,8 @@ __device__ __forceinline__ void wilson_qd(const SpinorView<S>& Rv, int s, int si
 template <class S, bool DAG>
 __global__ void __launch_bounds__(256) k_dslash_wilson(S* __restrict__ out, const S* __restrict__ in,
                                                        const typename Sto<S>::C* __restrict__ u, Geom g,
-                                                       float am, int imass, float am3) {
+                                                       float am, int imass, float am3, const int* skip) {
+  if (skip && *skip) return;
   using St = Sto<S>;
   using R = typename St::R;
   using C = typename St::C;
@@ -238,28 +240,28 @@ dim3 stencil_block(const Geom& g) {
 
 template <class S>
 int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
-                  int imass, float am3, cudaStream_t st) {
+                  int imass, float am3, cudaStream_t st, const int* skip) {
   if (g.ls > 1024) return THR_ERR_BADSHAPE;
   dim3 blk = stencil_block(g);
   dim3 grd((g.v3 + blk.y - 1) / blk.y);
   if (kernel == 1) {
     if (imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
-    if (dag) k_dslash_wilson<S, true><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3);
-    else k_dslash_wilson<S, false><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3);
+    if (dag) k_dslash_wilson<S, true><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip);
+    else k_dslash_wilson<S, false><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip);
   } else {
-    if (dag) k_dslash_shamir<S, true><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3);
-    else k_dslash_shamir<S, false><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3);
+    if (dag) k_dslash_shamir<S, true><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip);
+    else k_dslash_shamir<S, false><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip);
   }
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
 
 template int launch_dslash<double2>(const Geom&, int, bool, double2*, const double2*, const double2*, float, int, float,
-                                    cudaStream_t);
+                                    cudaStream_t, const int*);
 template int launch_dslash<float2>(const Geom&, int, bool, float2*, const float2*, const float2*, float, int, float,
-                                   cudaStream_t);
+                                   cudaStream_t, const int*);
 template int launch_dslash<__nv_bfloat162>(const Geom&, int, bool, __nv_bfloat162*, const __nv_bfloat162*,
-                                           const float2*, float, int, float, cudaStream_t);
+                                           const float2*, float, int, float, cudaStream_t, const int*);
 template int launch_dslash<__half2>(const Geom&, int, bool, __half2*, const __half2*, const float2*, float, int, float,
-                                    cudaStream_t);
+                                    cudaStream_t, const int*);
 
 }  // namespace thr

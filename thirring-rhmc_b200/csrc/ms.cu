@@ -1,0 +1,275 @@
+// ms.cu -- multishift CG (multishift_module.F90:13-284 and :289-534).
+//
+// Device-resident recurrences: the per-shift zeta/omega/gamma scalars, the
+// convergence flags and the active window [minishift, maxishift] are kept in
+// device memory and advanced by one-thread kernels; vector kernels read their
+// coefficients from there.  The shift update touches every active shift in
+// one pass over r and p (r and p are read once per iteration, not once per
+// shift).  V = double2 gives the FP64 solver, V = float2 the reference's
+// single-precision solver (FP32 vectors and FP32-rounded coefficients, FP64
+// scalars and FP64 accumulation of FP32 terms as reduce_real_dp5d does).
+#include <cmath>
+
+#include "ctx.h"
+#include "ms.h"
+#include "solver.h"
+
+namespace thr {
+
+namespace {
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double sh[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  int nw = (blockDim.x + 31) >> 5;
+  v = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+  if (w == 0) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+__device__ double sum_partials(const double* p, int n) {
+  double a = 0.0;
+  for (int i = 0; i < n; i++) a += p[i];
+  return a;
+}
+
+template <class V> struct VT;
+template <> struct VT<double2> {
+  using R = double;
+  // |z|^2 term and Re(conj(a) b) term in the working precision
+  static __device__ __forceinline__ double abs2(double2 a) { return a.x * a.x + a.y * a.y; }
+  static __device__ __forceinline__ double redot(double2 a, double2 b) { return a.x * b.x + a.y * b.y; }
+  static __device__ __forceinline__ double cast(double v) { return v; }
+};
+template <> struct VT<float2> {
+  using R = float;
+  // FP32 terms summed into FP64 (reductions.F90:6-32)
+  static __device__ __forceinline__ double abs2(float2 a) { return (double)(a.x * a.x + a.y * a.y); }
+  static __device__ __forceinline__ double redot(float2 a, float2 b) { return (double)(a.x * b.x + a.y * b.y); }
+  static __device__ __forceinline__ float cast(double v) { return (float)v; }  // real(omega) etc.
+};
+
+template <class V>
+__global__ void k_norm2(const MsState* ms, const V* a, size_t n, double* partials) {
+  if (ms && ms->done) return;
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    acc += VT<V>::abs2(a[i]);
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+template <class V>
+__global__ void k_redot(const MsState* ms, const V* a, const V* b, size_t n, double* partials) {
+  if (ms->done) return;
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    acc += VT<V>::redot(a[i], b[i]);
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+__global__ void k_ms_init(MsState* ms, const double* partials, int np) {
+  ms->delta = sum_partials(partials, np);  // :73
+}
+
+// iteration start + alpha: :104, :118-135
+__global__ void k_ms_alpha(MsState* ms, const double* partials, int np) {
+  if (ms->done) return;
+  ms->it += 1;
+  const double alpha = sum_partials(partials, np);
+  ms->alpha = alpha;
+  const double omega_save = ms->omega;
+  const double omega = -ms->delta / alpha;
+  ms->omega_save = omega_save;
+  ms->omega = omega;
+  for (int k = ms->lo; k <= ms->hi; k++) {
+    ms->zeta_iii[k] = (ms->zeta_i[k] * ms->zeta_ii[k] * omega_save) /
+                      (omega * ms->gammag * (ms->zeta_i[k] - ms->zeta_ii[k]) +
+                       ms->zeta_i[k] * omega_save * (1.0 - ms->aden[k] * omega));
+    ms->omegas[k] = omega * ms->zeta_iii[k] / ms->zeta_ii[k];
+  }
+}
+
+// r = r + omega*s (:137) fused with lambda = |r|^2 (:138)
+template <class V>
+__global__ void k_ms_rupdate(const MsState* ms, V* r, const V* s, size_t n, double* partials) {
+  if (ms->done) return;
+  using R = typename VT<V>::R;
+  const R om = VT<V>::cast(ms->omega);
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    V v = r[i] + om * s[i];
+    r[i] = v;
+    acc += VT<V>::abs2(v);
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+// :143, :148-150
+__global__ void k_ms_lambda(MsState* ms, const double* partials, int np) {
+  if (ms->done) return;
+  const double lambda = sum_partials(partials, np);
+  ms->lambda = lambda;
+  ms->gammag = lambda / ms->delta;
+  for (int k = ms->lo; k <= ms->hi; k++)
+    ms->gammas[k] = ms->gammag * ms->zeta_iii[k] * ms->omegas[k] / (ms->zeta_ii[k] * ms->omega);
+}
+
+// p = r + gammag*p (:145) and, for every shift in the window,
+// out -= omegas*sf ; sf = sf*gammas + r*zeta_iii (:155-176)
+template <class V>
+__global__ void k_ms_pshift(const MsState* ms, V* p, const V* r, V* out, V* sf, size_t n, size_t stride) {
+  if (ms->done) return;
+  using R = typename VT<V>::R;
+  const R gg = VT<V>::cast(ms->gammag);
+  const int lo = ms->lo, hi = ms->hi;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const V rv = r[i];
+    p[i] = rv + gg * p[i];
+    for (int k = lo; k <= hi; k++) {
+      const R om = VT<V>::cast(ms->omegas[k]), ga = VT<V>::cast(ms->gammas[k]), ze = VT<V>::cast(ms->zeta_iii[k]);
+      V* o = out + k * stride;
+      V* f = sf + k * stride;
+      const V fv = f[i];
+      o[i] = o[i] - om * fv;
+      f[i] = ga * fv + ze * rv;
+    }
+  }
+}
+
+// :178-180, :230-275
+__global__ void k_ms_converge(MsState* ms) {
+  if (ms->done) return;
+  for (int k = ms->lo; k <= ms->hi; k++) ms->cg_returns[k] = ms->it;
+  int maxi = -1, mini = ms->ndiagq;
+  for (int k = 0; k < ms->ndiagq; k++) {
+    if (ms->flags[k]) {
+      if (sqrt(ms->delta * ms->zeta_ii[k] * ms->zeta_ii[k]) * ms->correction[k] < (double)ms->res) {
+        ms->flags[k] = 0;
+      } else {
+        maxi = k > maxi ? k : maxi;
+        mini = k < mini ? k : mini;
+      }
+    }
+  }
+  ms->lo = mini;
+  ms->hi = maxi;
+  for (int k = mini; k <= maxi; k++) {
+    ms->zeta_i[k] = ms->zeta_ii[k];
+    ms->zeta_ii[k] = ms->zeta_iii[k];
+  }
+  ms->delta = ms->lambda;
+  if (!(ms->lambda == ms->lambda)) ms->status = THR_ERR_NAN;
+  if (maxi < mini || ms->it >= ms->maxcg || ms->status) ms->done = 1;
+}
+
+template <class V>
+__global__ void k_fill_shifts(V* sf, const V* in, size_t n, size_t stride, int nq) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    V v = in[i];
+    for (int k = 0; k < nq; k++) sf[k * stride + i] = v;
+  }
+}
+
+inline unsigned vec_grid(size_t n) {
+  size_t b = (n + kThreads - 1) / kThreads;
+  if (b > 148 * 8) b = 148 * 8;
+  return (unsigned)(b ? b : 1);
+}
+}  // namespace
+
+int ms_prepare_state(thr_ctx* c, MsState* h, int ndiagq, const double* aden, const double* anum, float res,
+                     int maxcg) {
+  if (ndiagq < 1 || ndiagq > kMaxShift) return THR_ERR_BADSHAPE;
+  memset(h, 0, sizeof(MsState));
+  // correction = |anum/aden| / geometric mean (:87-88)
+  double slog = 0.0;
+  for (int k = 0; k < ndiagq; k++) {
+    h->correction[k] = std::fabs(anum[k] / aden[k]);
+    slog += std::log(h->correction[k]);
+  }
+  const double gm = std::exp(slog / ndiagq);
+  for (int k = 0; k < ndiagq; k++) {
+    h->correction[k] = h->correction[k] / gm;
+    h->flags[k] = 1;
+    h->zeta_i[k] = 1.0;
+    h->zeta_ii[k] = 1.0;
+    h->gammas[k] = 0.0;
+    h->aden[k] = aden[k];
+  }
+  h->omega = 1.0;
+  h->gammag = 0.0;
+  h->alpha = 0.0;
+  h->ndiagq = ndiagq;
+  h->lo = 0;
+  h->hi = ndiagq - 1;
+  h->maxcg = maxcg;
+  h->res = res;
+  h->done = (maxcg <= 0);
+  (void)c;
+  return THR_OK;
+}
+
+// Multishift solve on device vectors.  in: the source (precision V);
+// out/sf: ndiagq shift fields each `stride` elements; r, p, h, s: work.
+template <class V>
+int multishift_dev(thr_ctx* c, const V* u_dummy, const V* in, V* out, V* sf, V* r, V* p, V* hv, V* s,
+                   int ndiagq, const double* aden, const double* anum, float res, float am, int imass, int maxcg,
+                   int* cg_return, int* cg_returns) {
+  (void)u_dummy;
+  const size_t n = c->n4();
+  const size_t stride = n;
+  MsState* ms = reinterpret_cast<MsState*>(c->dscal);
+  MsState* h = reinterpret_cast<MsState*>(c->hscal);
+  THR_TRY(ms_prepare_state(c, h, ndiagq, aden, anum, res, maxcg));
+  THR_CUDA(cudaMemcpyAsync(ms, h, sizeof(MsState), cudaMemcpyHostToDevice, c->st));
+  THR_CUDA(cudaMemcpyAsync(r, in, n * sizeof(V), cudaMemcpyDeviceToDevice, c->st));
+  THR_CUDA(cudaMemcpyAsync(p, in, n * sizeof(V), cudaMemcpyDeviceToDevice, c->st));
+  const unsigned gb = vec_grid(n);
+  k_norm2<V><<<gb, kThreads, 0, c->st>>>(nullptr, r, n, c->partials);
+  k_ms_init<<<1, 1, 0, c->st>>>(ms, c->partials, gb);
+  THR_CUDA(cudaMemsetAsync(out, 0, (size_t)ndiagq * stride * sizeof(V), c->st));
+  k_fill_shifts<V><<<gb, kThreads, 0, c->st>>>(sf, in, n, stride, ndiagq);
+  const bool sp = sizeof(V) == sizeof(float2);
+  const void* u = sp ? (const void*)c->u32 : (const void*)c->u64;
+  const int chunk = 8;
+  int it_host = 0;
+  for (;;) {
+    for (int k = 0; k < chunk; k++) {
+      THR_TRY(launch_dslash_guarded<V>(c, false, hv, p, (const V*)u, am, imass, &ms->done));
+      THR_TRY(launch_dslash_guarded<V>(c, true, s, hv, (const V*)u, am, imass, &ms->done));
+      k_redot<V><<<gb, kThreads, 0, c->st>>>(ms, p, s, n, c->partials);
+      k_ms_alpha<<<1, 1, 0, c->st>>>(ms, c->partials, gb);
+      k_ms_rupdate<V><<<gb, kThreads, 0, c->st>>>(ms, r, s, n, c->partials);
+      k_ms_lambda<<<1, 1, 0, c->st>>>(ms, c->partials, gb);
+      k_ms_pshift<V><<<gb, kThreads, 0, c->st>>>(ms, p, r, out, sf, n, stride);
+      k_ms_converge<<<1, 1, 0, c->st>>>(ms);
+    }
+    it_host += chunk;
+    THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
+    THR_CUDA(cudaStreamSynchronize(c->st));
+    if (h->done) break;
+    if (it_host > maxcg + 2 * chunk) return THR_ERR_CUDA;  // the device state stopped advancing
+  }
+  if (cg_return) *cg_return = h->it;
+  if (cg_returns)
+    for (int k = 0; k < ndiagq; k++) cg_returns[k] = h->cg_returns[k];
+  return h->status ? h->status : THR_OK;
+}
+
+template int multishift_dev<double2>(thr_ctx*, const double2*, const double2*, double2*, double2*, double2*, double2*,
+                                     double2*, double2*, int, const double*, const double*, float, float, int, int,
+                                     int*, int*);
+template int multishift_dev<float2>(thr_ctx*, const float2*, const float2*, float2*, float2*, float2*, float2*,
+                                    float2*, float2*, int, const double*, const double*, float, float, int, int, int*,
+                                    int*);
+
+}  // namespace thr

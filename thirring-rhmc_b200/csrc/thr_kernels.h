@@ -13,7 +13,7 @@ dim3 stencil_block(const Geom& g);
 // dslash.cu
 template <class S>
 int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
-                  int imass, float am3, cudaStream_t st);
+                  int imass, float am3, cudaStream_t st, const int* skip = nullptr);
 
 // layout.cu: Fortran halo'd host layout <-> device fields
 // spinor (0:Ls+1,0:Lx+1,0:Ly+1,0:Lt+1,4) complex(dp)  <-> S[4][V3][Ls]

@@ -40,6 +40,15 @@ SIGNATURES = {
     "thr_set_links": (_i, [_v, _v]),
     "thr_dslash": (_i, [_v, _v, _v, _v, _f, _i]),
     "thr_dslashd": (_i, [_v, _v, _v, _v, _f, _i]),
+    "thr_congrad": (_i, [_v, _v, _v, _f, _pi, _f, _i, _pi]),
+    "thr_multishift_solver": (_i, [_v, _v, _f, _i, _i, _v, _v, _v, _v, _f, _i, _pi, _v]),
+    "thr_multishift_solver_sp": (_i, [_v, _v, _f, _i, _i, _v, _v, _v, _v, _f, _i, _pi, _v]),
+    "thr_qmrherm": (_i, [_v, _v, _v, _f, _pi, _f, _i, _v, _v, _i, _i, _i, _v, _v, _v, _i]),
+    "thr_derivs": (_i, [_v, _v, _v, _d, _i, _f, _i, _v]),
+    "thr_init_random": (_i, [_v, _d, _i]),
+    "thr_gauss0": (_i, [_v, _v]),
+    "thr_gaussp": (_i, [_v, _v]),
+    "thr_rano": (_i, [_v, _i, _i, _i, C.POINTER(C.c_float)]),
     "thr_field_create": (_i, [_v, _i, C.POINTER(_v)]),
     "thr_field_destroy": (_i, [_v, _v]),
     "thr_field_upload": (_i, [_v, _v, _i, _v]),

@@ -144,3 +144,81 @@ class Lattice:
         Phi = out if out is not None else spinor(self)
         _check(self._L.thr_dslashd(self.h, _p(Phi), _p(R), _p(u), am, imass), "dslashd")
         return Phi
+
+    # ---- random.f90 / site_random.f90 / gaussian.F90
+    def init_random(self, seed, site=True):
+        """init_random(seed): site streams (site_random.f90) or one global stream (random.f90)."""
+        _check(self._L.thr_init_random(self.h, float(seed), int(site)), "init_random")
+
+    def gauss0(self):
+        ps = ps_field(self)
+        _check(self._L.thr_gauss0(self.h, _p(ps)), "gauss0")
+        return ps
+
+    def gaussp(self):
+        ps = ps_field(self)
+        _check(self._L.thr_gaussp(self.h, _p(ps)), "gaussp")
+        return ps
+
+    def rano(self, ix=1, iy=1, it=1):
+        v = C.c_float(0)
+        _check(self._L.thr_rano(self.h, ix, iy, it, C.byref(v)), "rano")
+        return v.value
+
+    # ---- measure_module.F90
+    def congrad(self, Phi, X, res, am, imass):
+        """congrad(Phi, res, itercg, am, imass, iterations): X (vector::X) in/out.
+        Returns (itercg, iterations); raises on a non-finite residual.  Hitting
+        niterc is reported by the return value status like the reference's notice."""
+        _need(Phi, self.sshape, np.complex128, "Phi")
+        _need(X, self.sshape, np.complex128, "X")
+        it = C.c_int(0)
+        nx = C.c_int(0)
+        rc = self._L.thr_congrad(self.h, _p(Phi), _p(X), res, C.byref(it), am, imass, C.byref(nx))
+        if rc not in (0, 3):
+            _check(rc, "congrad")
+        return it.value, nx.value
+
+    # ---- multishift_module.F90
+    def multishift_solver(self, u, am, imass, aden, anum, inp, res, maxcg, sp=False):
+        """Returns (output (Ls,Lx,Ly,Lt,4,ndiag), cg_return, cg_returns)."""
+        _need(inp, self.sshape, np.complex128, "input")
+        nq = len(aden)
+        out = shift_out(self)
+        ret = C.c_int(0)
+        cgr = np.zeros(nq, np.int32)
+        fn = self._L.thr_multishift_solver_sp if sp else self._L.thr_multishift_solver
+        _check(fn(self.h, _p(u), am, imass, nq, _p(np.ascontiguousarray(aden, np.float64)),
+                  _p(np.ascontiguousarray(anum, np.float64)), _p(out), _p(inp), res, maxcg, C.byref(ret), _p(cgr)),
+               "multishift_solver")
+        return out, ret.value, cgr
+
+    # ---- qmrherm_module.F90
+    def qmrherm(self, Phi, res, am, imass, anum, aden, iflag, use_sp=False, dSdpi=None, Phi0=None,
+                max_qmr_iters=0):
+        """x = qmrherm(Phi, …): returns (x, itercg, cg_returns).  dSdpi/Phi0 are
+        updated in place when given (gforce::dSdpi, qmrherm_module::Phi0)."""
+        _need(Phi, self.sshape, np.complex128, "Phi")
+        nq = len(aden)
+        assert len(anum) == nq + 1
+        x = spinor(self)
+        it = C.c_int(0)
+        cgr = np.zeros(nq, np.int32)
+        if dSdpi is not None:
+            _need(dSdpi, (self.lx, self.ly, self.lt, 3), np.float64, "dSdpi")
+        if Phi0 is not None:
+            _need(Phi0, self.sshape + (self.ndiag,), np.complex128, "Phi0")
+        _check(self._L.thr_qmrherm(self.h, _p(Phi), _p(x), res, C.byref(it), am, imass,
+                                   _p(np.ascontiguousarray(anum, np.float64)),
+                                   _p(np.ascontiguousarray(aden, np.float64)), nq, iflag, int(use_sp), _p(cgr),
+                                   _p(dSdpi), _p(Phi0), max_qmr_iters), "qmrherm")
+        return x, it.value, cgr
+
+    # ---- derivs_module.F90
+    def derivs(self, R, X2, anum, iflag, am, imass, dSdpi):
+        """dSdpi += force of (R, X2): derivs_module.F90:8-26 (in place)."""
+        _need(R, self.sshape, np.complex128, "R")
+        _need(X2, self.sshape, np.complex128, "X2")
+        _need(dSdpi, (self.lx, self.ly, self.lt, 3), np.float64, "dSdpi")
+        _check(self._L.thr_derivs(self.h, _p(R), _p(X2), float(anum), iflag, am, imass, _p(dSdpi)), "derivs")
+        return dSdpi
