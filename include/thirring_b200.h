@@ -163,6 +163,51 @@ int thr_gaussp(thr_ctx *ctx, float *ps);
  * site (ix,iy,it) (ignored for the global stream), random.f90:28-58. */
 int thr_rano(thr_ctx *ctx, int ix, int iy, int it, float *out);
 
+/* ---- RHMC: remez.F90, force_module.F90, evolution.F90, dwf3d_lib.F90 ----- */
+/* The rational approximations read by dwf3d_lib.F90:205-209 (module remez:
+ * anum2/aden2/bnum2/bden2/anum4/aden4/bnum4/bden4 with ndiag poles; module
+ * remezg: the same with ndiagg poles).  anum/bnum have n+1 entries (0:n). */
+int thr_set_remez(thr_ctx *ctx, int ndiag, const double *anum2, const double *aden2, const double *bnum2,
+                  const double *bden2, const double *anum4, const double *aden4, const double *bnum4,
+                  const double *bden4, int ndiagg, const double *anum2g, const double *aden2g,
+                  const double *bnum2g, const double *bden2g, const double *anum4g, const double *aden4g,
+                  const double *bnum4g, const double *bden4g);
+/* Inverter residuals rescga (Hamiltonian, pseudofermion), rescgg (guidance)
+ * and spmd (single-precision guidance solves), params.F90:60-64; defaults
+ * 1e-8, 1e-6, 1.  max_qmr_iters <= 0 keeps 50000. */
+int thr_set_residuals(thr_ctx *ctx, float rescga, float rescgg, int spmd, int max_qmr_iters);
+/* force(Phi, res1, am, imass), force_module.F90:9-113, with the current
+ * links; theta (trial::theta) feeds the gauge term; dSdpi is overwritten. */
+int thr_force(thr_ctx *ctx, const double *Phi, float res1, float am, int imass, const float *theta, double *dSdpi);
+/* hamilton(Phi, h, hg, hp, s, res2, am, imass), dwf3d_lib.F90:511-616, with
+ * the current links, theta and pp (trial::theta, trial::pp).  hp and hg are
+ * accumulated in FP64 (the reference sums them in single precision). */
+int thr_hamilton(thr_ctx *ctx, const double *Phi, double *h, double *hg, double *hp, double *s, float res2,
+                 float am, int imass, const float *theta, const float *pp);
+/* initialise_phi_1flavour(phi, am, imass), evolution.F90:7-75 (site streams). */
+int thr_initialise_phi(thr_ctx *ctx, double *Phi, float am, int imass);
+/* initialise_pp(pp), evolution.F90:77-111 (site streams). */
+int thr_initialise_pp(thr_ctx *ctx, float *pp);
+/* evolve_theta_pp(iterl, dt, pp, phi, res, am, imass, itot), evolution.F90:113-179.
+ * theta (trial::theta) and pp in/out; u (trial::u) and dSdpi receive the final
+ * links and force when non-NULL.  fixed_steps > 0 replaces the random length by
+ * exactly that many steps (the exit draw at site (1,1,1) is still consumed). */
+int thr_evolve_theta_pp(thr_ctx *ctx, int iterl, float dt, float *pp, const double *Phi, float res, float am,
+                        int imass, int *itot, float *theta, double *u, double *dSdpi, int fixed_steps);
+/* One trajectory of the sweep loop, dwf3d_lib.F90:265-323: coef, pseudofermion
+ * and momentum refresh, H0, leapfrog, H1, Metropolis.  theta is replaced by
+ * the new field when accepted. */
+typedef struct thr_traj_result {
+  double h0, h1, dh, ds, s0, s1;
+  int accepted, steps;
+  float y;
+} thr_traj_result;
+int thr_trajectory(thr_ctx *ctx, float *theta, int iterl, float dt, float am, int imass, int fixed_steps,
+                   thr_traj_result *out);
+/* Solver iteration sums (counters.F90): ancg, ancgpv, ancgf, ancgfpv, ancgh,
+ * ancghpv, ancgpf, ancgpfpv. */
+int thr_md_counters(thr_ctx *ctx, double *counts8, int reset);
+
 /* ---- device-resident fields ------------------------------------------- */
 /* Spinor fields kept in HBM in the device layout (no halos), so that solver
  * and MD loops never cross PCIe.  `precision` is a thr_precision storage

@@ -271,3 +271,64 @@ def read_remez(path, n):
     rc = lib.orc_read_remez_file(path.encode(), n, P(a), P(b), P(ad), P(bd))
     assert rc == 0, path
     return a, ad, b, bd
+
+
+# ---------------------------------------------------------------- RHMC
+_RKEYS = ("anum2", "aden2", "bnum2", "bden2", "anum4", "aden4", "bnum4", "bden4")
+
+
+def rational(rat, ratg):
+    """orc_rational from the remez / remezg dicts (see thirring.remez_set)."""
+    r = Rational()
+    r.ndiag = len(rat["aden2"])
+    r.ndiagg = len(ratg["aden2"])
+    keep = []
+    for suffix, d in (("", rat), ("g", ratg)):
+        for k in _RKEYS:
+            a = np.ascontiguousarray(d[k], np.float64)
+            keep.append(a)
+            setattr(r, k + suffix, a.ctypes.data_as(C.POINTER(C.c_double)))
+    r._keep = keep
+    return r
+
+
+def force(L, u, theta, rat, Phi, res1, am, imass, use_sp, max_iters=50000):
+    dS = field3(L)
+    cnt = Counts()
+    rc = lib.orc_force(C.byref(L), P(u), P(np.asfortranarray(theta, np.float32)), C.byref(rat), P(Phi), res1, am,
+                       imass, int(use_sp), max_iters, P(dS), C.byref(cnt))
+    assert rc == 0
+    return dS
+
+
+def hamilton(L, u, theta, pp, rat, Phi, res2, am, imass, max_iters=50000):
+    v = [C.c_double(0) for _ in range(4)]
+    cnt = Counts()
+    rc = lib.orc_hamilton(C.byref(L), P(u), P(np.asfortranarray(theta, np.float32)),
+                          P(np.asfortranarray(pp, np.float32)), C.byref(rat), P(Phi), res2, am, imass, max_iters,
+                          *[C.byref(x) for x in v], C.byref(cnt))
+    assert rc == 0
+    return tuple(x.value for x in v)
+
+
+def initialise_phi(L, g, u, rat, am, imass, rescga=1e-8):
+    Phi = spinor(L)
+    cnt = Counts()
+    rc = lib.orc_initialise_phi(C.byref(L), g.h, P(u), C.byref(rat), P(Phi), am, imass, rescga, 50000, C.byref(cnt))
+    assert rc == 0
+    return Phi
+
+
+def initialise_pp(L, g):
+    pp = field3(L, np.float32)
+    lib.orc_initialise_pp(C.byref(L), g.h, P(pp))
+    return pp
+
+
+def trajectory(L, g, theta, rat, iterl, dt, am, imass, rescga, rescgg, use_sp, fixed_steps=0):
+    r = TrajResult()
+    cnt = Counts()
+    rc = lib.orc_trajectory(C.byref(L), g.h, P(theta), C.byref(rat), iterl, dt, am, imass, rescga, rescgg,
+                            int(use_sp), 50000, fixed_steps, C.byref(r), C.byref(cnt))
+    assert rc == 0
+    return r

@@ -76,6 +76,14 @@ int thr_ctx::use_links(const double* u_host) {
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
 
+// u = coef(theta) from a device theta[3][V3] (storage order); refreshes the FP32 copy
+int thr_ctx::coef_dev(const float* theta_dev) {
+  const size_t n3 = (size_t)g.v3 * 3;
+  k_coef<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(u64, theta_dev, g, p.ibound);
+  links_ok = true;
+  return use_links(nullptr);
+}
+
 int thr_ctx::sync() {
   THR_CUDA(cudaStreamSynchronize(st));
   return THR_OK;

@@ -56,8 +56,22 @@ struct thr_ctx {
     B_PHI0,     // qmrherm_module::Phi0 (FP64), ndiag fields
     B_DSDPI,    // gforce::dSdpi, [3][V3] FP64
     B_AUX,      // misc
+    B_MD,       // MD spinors: Phi, X2, Xresult, R
+    B_MDF,      // MD 3D fields: theta, thetat, pp (float) and dSdpi (double)
     B_COUNT = 16
   };
+  // rational approximations (remez.F90, remezg.F90): anum has n+1 entries
+  struct Rational {
+    bool set = false;
+    int ndiag = 0, ndiagg = 0;
+    std::vector<double> anum2, aden2, bnum2, bden2, anum4, aden4, bnum4, bden4;
+    std::vector<double> anum2g, aden2g, bnum2g, bden2g, anum4g, aden4g, bnum4g, bden4g;
+  } rat;
+  // inverter residuals and the guidance-precision switch (params.F90:60-64)
+  float rescga = 1e-8f, rescgg = 1e-6f;
+  int spmd = 1;             // 0: FP64 guidance solves; 1: single-precision (reference)
+  int max_qmr_iters = 50000;
+  double md_counts[8] = {};  // ancg, ancgpv, ancgf, ancgfpv, ancgh, ancghpv, ancgpf, ancgpfpv
   void* bufs[B_COUNT] = {};
   size_t buf_bytes[B_COUNT] = {};
   bool phi0_valid = false;
@@ -72,5 +86,6 @@ struct thr_ctx {
   int upload_spinor(double2* dst, const double* host);     // Fortran halo'd -> device
   int download_spinor(double* host, const double2* src);   // device -> Fortran halo'd
   int use_links(const double* u_host);                    // NULL keeps current links
+  int coef_dev(const float* theta_dev);                   // gauge.F90 coef on device theta
   int sync();
 };

@@ -1,0 +1,415 @@
+// md.cu -- the RHMC layer on device-resident fields: force (force_module.F90),
+// hamilton (dwf3d_lib.F90:511-616), initialise_phi_1flavour / initialise_pp
+// (evolution.F90:7-111), the leapfrog evolve_theta_pp (evolution.F90:113-179)
+// and one trajectory with its Metropolis test (dwf3d_lib.F90:265-323).
+//
+// Every field of a trajectory (theta, pp, u, Phi, dSdpi, solver vectors)
+// stays in HBM; the host only steers: it reads the trajectory-exit draw of
+// each MD step and the Hamiltonians.  theta and pp are single precision as
+// in the reference; the Hamiltonian sums are accumulated in FP64.
+#include <cmath>
+#include <cstring>
+
+#include "ctx.h"
+#include "md.h"
+#include "qmr.h"
+#include "rng.h"
+
+namespace thr {
+
+namespace {
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double sh[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  int nw = (blockDim.x + 31) >> 5;
+  v = (threadIdx.x < nw) ? sh[threadIdx.x] : 0.0;
+  if (w == 0) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+
+// force_module.F90:102-109: antiperiodic sign on the last t-slice, + beta*Nf*theta
+__global__ void k_force_finish(double* dS, const float* theta, Geom g, int ibound, float bnf) {
+  int n = g.v3 * 3;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int site = i % g.v3, mu = i / g.v3;
+    double v = dS[i];
+    if (ibound == -1 && mu == 2) {
+      int x, y, t;
+      site_coords(g, site, x, y, t);
+      if (t == g.lt - 1) v = -v;
+    }
+    dS[i] = v + (double)__fmul_rn(bnf, theta[i]);
+  }
+}
+
+// pp = pp - real(c*dSdpi): c = 0.5*dt or dt in single, product in double, rounded (evolution.F90:142,170,173)
+__global__ void k_pp_kick(float* pp, const double* dS, float c, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    pp[i] = __fsub_rn(pp[i], (float)((double)c * dS[i]));
+}
+// thetat = thetat + dt*pp (evolution.F90:157), single precision, no contraction
+__global__ void k_theta_drift(float* th, const float* pp, float dt, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    th[i] = __fadd_rn(th[i], __fmul_rn(dt, pp[i]));
+}
+// sum of squares of a float field in FP64
+__global__ void k_sumsq_f(const float* a, int n, double* partials) {
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double v = (double)a[i];
+    acc += v * v;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+// sum Re(conj(a) b) (dwf3d_lib.F90:594)
+__global__ void k_redot(const double2* a, const double2* b, size_t n, double* partials) {
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    acc += a[i].x * b[i].x + a[i].y * b[i].y;
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+__global__ void k_finish(const double* partials, int np, double* out) {
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) acc += partials[i];
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) *out = acc;
+}
+
+inline unsigned grid(size_t n) {
+  size_t b = (n + kThreads - 1) / kThreads;
+  if (b > 148 * 4) b = 148 * 4;
+  return (unsigned)(b ? b : 1);
+}
+}  // namespace
+
+int md_fields(thr_ctx* c, MdFields* f) {
+  const size_t n = c->n4();
+  const size_t n3 = (size_t)c->g.v3 * 3;
+  void *sp, *fp;
+  THR_TRY(c->buffer(thr_ctx::B_MD, 4 * n * sizeof(double2), &sp));
+  THR_TRY(c->buffer(thr_ctx::B_MDF, 3 * n3 * sizeof(float) + n3 * sizeof(double) + 64, &fp));
+  f->Phi = (double2*)sp;
+  f->X2 = f->Phi + n;
+  f->Xr = f->X2 + n;
+  f->R = f->Xr + n;
+  f->theta = (float*)fp;
+  f->thetat = f->theta + n3;
+  f->pp = f->thetat + n3;
+  f->dS = (double*)(f->pp + n3 + (n3 & 1));
+  return THR_OK;
+}
+
+static int reduce_to_host(thr_ctx* c, int np, double* out) {
+  k_finish<<<1, 1024, 0, c->st>>>(c->partials, np, c->dscal + 4000);
+  THR_CUDA(cudaMemcpyAsync(c->hscal + 4000, c->dscal + 4000, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  THR_CUDA(cudaStreamSynchronize(c->st));
+  *out = c->hscal[4000];
+  return THR_OK;
+}
+
+static int need_rat(thr_ctx* c) { return c->rat.set ? THR_OK : THR_ERR_BADARG; }
+
+// force_module.F90:9-113 on device theta; result in f->dS
+int force_dev(thr_ctx* c, MdFields* f, const float* theta, float res1, float am, int imass) {
+  THR_TRY(need_rat(c));
+  const size_t n = c->n4();
+  const size_t n3 = (size_t)c->g.v3 * 3;
+  auto& R = c->rat;
+  const int ng = R.ndiagg;
+  const int sp = c->spmd;
+  const float One = 1.0f;
+  int it = 0;
+  THR_CUDA(cudaMemsetAsync(f->dS, 0, n3 * sizeof(double), c->st));
+  THR_CUDA(cudaMemcpyAsync(f->X2, f->Phi, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
+  THR_TRY(qmrherm_dev(c, f->X2, f->Xr, res1, &it, One, 1, R.anum4g.data(), R.aden4g.data(), ng, 1, sp, nullptr,
+                      f->dS, c->max_qmr_iters));
+  c->md_counts[1] += it;  // ancgpv
+  THR_CUDA(cudaMemcpyAsync(f->X2, f->Xr, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
+  THR_TRY(qmrherm_dev(c, f->X2, f->Xr, res1, &it, am, imass, R.bnum2g.data(), R.bden2g.data(), ng, 0, sp, nullptr,
+                      f->dS, c->max_qmr_iters));
+  c->md_counts[0] += it;  // ancg
+  THR_CUDA(cudaMemcpyAsync(f->X2, f->Xr, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
+  THR_TRY(qmrherm_dev(c, f->X2, f->Xr, res1, &it, am, imass, R.anum2g.data(), R.aden2g.data(), ng, 2, sp, nullptr,
+                      f->dS, c->max_qmr_iters));
+  c->md_counts[2] += it;  // ancgf
+  THR_TRY(qmrherm_dev(c, f->X2, f->Xr, res1, &it, One, 1, R.anum4g.data(), R.aden4g.data(), ng, 3, sp, nullptr,
+                      f->dS, c->max_qmr_iters));
+  c->md_counts[3] += it;  // ancgfpv
+  const float bnf = c->p.beta * 1.0f;  // beta*Nf, Nf = 1 (params.F90:19)
+  k_force_finish<<<grid(n3), kThreads, 0, c->st>>>(f->dS, theta, c->g, c->p.ibound, bnf);
+  return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+
+// dwf3d_lib.F90:511-616 with the context's current links
+int hamilton_dev(thr_ctx* c, MdFields* f, const float* theta, const float* pp, float res2, float am, int imass,
+                 double* h, double* hg, double* hp, double* s) {
+  THR_TRY(need_rat(c));
+  const size_t n = c->n4();
+  const int n3 = c->g.v3 * 3;
+  double spp, sth;
+  k_sumsq_f<<<grid(n3), kThreads, 0, c->st>>>(pp, n3, c->partials);
+  THR_TRY(reduce_to_host(c, (int)grid(n3), &spp));
+  k_sumsq_f<<<grid(n3), kThreads, 0, c->st>>>(theta, n3, c->partials);
+  THR_TRY(reduce_to_host(c, (int)grid(n3), &sth));
+  *hp = 0.5 * spp;
+  *hg = 0.5 * 1.0 * (double)c->p.beta * sth;
+  auto& R = c->rat;
+  int it = 0;
+  THR_CUDA(cudaMemcpyAsync(f->R, f->Phi, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
+  THR_TRY(qmrherm_dev(c, f->R, f->Xr, res2, &it, 1.0f, 1, R.anum4.data(), R.aden4.data(), R.ndiag, 0, 0, nullptr,
+                      nullptr, c->max_qmr_iters));
+  c->md_counts[5] += it;  // ancghpv
+  if (it >= c->max_qmr_iters) return THR_ERR_MAXITER;  // check_qmr_iterations: dwf3d_lib.F90:860-881
+  THR_CUDA(cudaMemcpyAsync(f->R, f->Xr, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
+  THR_TRY(qmrherm_dev(c, f->R, f->Xr, res2, &it, am, imass, R.bnum2.data(), R.bden2.data(), R.ndiag, 0, 0, nullptr,
+                      nullptr, c->max_qmr_iters));
+  c->md_counts[4] += it;  // ancgh
+  if (it >= c->max_qmr_iters) return THR_ERR_MAXITER;
+  k_redot<<<grid(n), kThreads, 0, c->st>>>(f->R, f->Xr, n, c->partials);
+  double hf;
+  THR_TRY(reduce_to_host(c, (int)grid(n), &hf));
+  *h = *hg + *hp + hf;
+  *s = *hg + hf;
+  return THR_OK;
+}
+
+// evolution.F90:7-75 (Phi from a fresh Gaussian R) with the current links
+int initialise_phi_dev(thr_ctx* c, MdFields* f, float am, int imass) {
+  THR_TRY(need_rat(c));
+  const size_t n = c->n4();
+  auto& R = c->rat;
+  THR_TRY(rng_phi_draw(c, f->R));
+  int it = 0;
+  THR_TRY(qmrherm_dev(c, f->R, f->Xr, c->rescga, &it, am, imass, R.anum4.data(), R.aden4.data(), R.ndiag, 0, 0,
+                      nullptr, nullptr, c->max_qmr_iters));
+  c->md_counts[6] += it;  // ancgpf
+  THR_CUDA(cudaMemcpyAsync(f->R, f->Xr, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
+  THR_TRY(qmrherm_dev(c, f->R, f->Xr, c->rescga, &it, 1.0f, 1, R.bnum4.data(), R.bden4.data(), R.ndiag, 0, 0,
+                      nullptr, nullptr, c->max_qmr_iters));
+  c->md_counts[7] += it;  // ancgpfpv
+  THR_CUDA(cudaMemcpyAsync(f->Phi, f->Xr, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
+  return THR_OK;
+}
+
+// evolution.F90:113-179 on f->thetat / f->pp; links follow thetat.
+int evolve_dev(thr_ctx* c, MdFields* f, int iterl, float dt, float res, float am, int imass, int fixed_steps,
+               int* itot) {
+  const int n3 = c->g.v3 * 3;
+  THR_TRY(force_dev(c, f, f->thetat, res, am, imass));
+  const float hdt = 0.5f * dt;
+  k_pp_kick<<<grid(n3), kThreads, 0, c->st>>>(f->pp, f->dS, hdt, n3);
+  const float proby = 1.0f / (float)iterl;
+  const int nmax = fixed_steps > 0 ? fixed_steps : 4 * iterl;
+  int iter;
+  for (iter = 1; iter <= nmax; iter++) {
+    k_theta_drift<<<grid(n3), kThreads, 0, c->st>>>(f->thetat, f->pp, dt, n3);
+    THR_TRY(c->coef_dev(f->thetat));
+    THR_TRY(force_dev(c, f, f->thetat, res, am, imass));
+    float ytest = 0.0f;
+    THR_TRY(rng_rano_site(c, 1, 1, 1, nullptr, &ytest));  // evolution.F90:441
+    const bool last = fixed_steps > 0 ? (iter == fixed_steps) : (ytest < proby);
+    if (last) {
+      k_pp_kick<<<grid(n3), kThreads, 0, c->st>>>(f->pp, f->dS, hdt, n3);
+      break;
+    }
+    k_pp_kick<<<grid(n3), kThreads, 0, c->st>>>(f->pp, f->dS, dt, n3);
+  }
+  if (itot) *itot += iter < nmax ? iter : nmax;
+  return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+
+// one pass of dwf3d_lib.F90:265-323 on device theta (f->theta), accepted field left in f->theta
+int trajectory_dev(thr_ctx* c, MdFields* f, int iterl, float dt, float am, int imass, int fixed_steps,
+                   thr_traj_result* out) {
+  const int n3 = c->g.v3 * 3;
+  THR_CUDA(cudaMemcpyAsync(f->thetat, f->theta, n3 * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
+  THR_TRY(c->coef_dev(f->thetat));
+  THR_TRY(initialise_phi_dev(c, f, am, imass));
+  THR_TRY(rng_pp_draw(c, f->pp));
+  double h0, h1, hg, hp, s0, s1;
+  THR_TRY(hamilton_dev(c, f, f->thetat, f->pp, c->rescga, am, imass, &h0, &hg, &hp, &s0));
+  int itot = 0;
+  THR_TRY(evolve_dev(c, f, iterl, dt, c->rescgg, am, imass, fixed_steps, &itot));
+  THR_TRY(hamilton_dev(c, f, f->thetat, f->pp, c->rescga, am, imass, &h1, &hg, &hp, &s1));
+  const double dH = h0 - h1;
+  const float y = expf((float)dH);  // y = exp(real(dH)) (:304)
+  int accept = 1;
+  if (dH < 0.0) {
+    float x = 0.0f;
+    THR_TRY(rng_rano_site(c, 1, 1, 1, nullptr, &x));  // :309
+    if (x > y) accept = 0;
+  }
+  if (accept) THR_CUDA(cudaMemcpyAsync(f->theta, f->thetat, n3 * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
+  if (out) {
+    out->h0 = h0;
+    out->h1 = h1;
+    out->dh = dH;
+    out->ds = s0 - s1;
+    out->accepted = accept;
+    out->steps = itot;
+    out->y = y;
+  }
+  return c->sync();
+}
+
+}  // namespace thr
+
+using namespace thr;
+
+namespace {
+int up_f3(thr_ctx* c, float* dev, const float* host) {
+  const size_t n3 = (size_t)c->g.v3 * 3;
+  THR_CUDA(cudaMemcpyAsync(c->stage, host, n3 * sizeof(float), cudaMemcpyHostToDevice, c->st));
+  from_fortran_f3(c->g, dev, (const float*)c->stage, c->st);
+  return THR_OK;
+}
+int down_f3(thr_ctx* c, float* host, const float* dev) {
+  const size_t n3 = (size_t)c->g.v3 * 3;
+  to_fortran_f3(c->g, (float*)c->stage, dev, c->st);
+  THR_CUDA(cudaMemcpyAsync(host, c->stage, n3 * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  return THR_OK;
+}
+int down_d3(thr_ctx* c, double* host, const double* dev) {
+  const size_t n3 = (size_t)c->g.v3 * 3;
+  to_fortran_d3(c->g, (double*)c->stage, dev, c->st);
+  THR_CUDA(cudaMemcpyAsync(host, c->stage, n3 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  return THR_OK;
+}
+void copyv(std::vector<double>& v, const double* a, int n) { v.assign(a, a + n); }
+}  // namespace
+
+extern "C" {
+
+int thr_set_remez(thr_ctx* c, int ndiag, const double* anum2, const double* aden2, const double* bnum2,
+                  const double* bden2, const double* anum4, const double* aden4, const double* bnum4,
+                  const double* bden4, int ndiagg, const double* anum2g, const double* aden2g, const double* bnum2g,
+                  const double* bden2g, const double* anum4g, const double* aden4g, const double* bnum4g,
+                  const double* bden4g) {
+  if (!c || ndiag < 1 || ndiagg < 1 || ndiag > 64 || ndiagg > 64) return THR_ERR_BADARG;
+  if (ndiag > c->p.ndiag || ndiagg > c->p.ndiag) return THR_ERR_BADSHAPE;
+  auto& R = c->rat;
+  R.ndiag = ndiag;
+  R.ndiagg = ndiagg;
+  copyv(R.anum2, anum2, ndiag + 1); copyv(R.aden2, aden2, ndiag);
+  copyv(R.bnum2, bnum2, ndiag + 1); copyv(R.bden2, bden2, ndiag);
+  copyv(R.anum4, anum4, ndiag + 1); copyv(R.aden4, aden4, ndiag);
+  copyv(R.bnum4, bnum4, ndiag + 1); copyv(R.bden4, bden4, ndiag);
+  copyv(R.anum2g, anum2g, ndiagg + 1); copyv(R.aden2g, aden2g, ndiagg);
+  copyv(R.bnum2g, bnum2g, ndiagg + 1); copyv(R.bden2g, bden2g, ndiagg);
+  copyv(R.anum4g, anum4g, ndiagg + 1); copyv(R.aden4g, aden4g, ndiagg);
+  copyv(R.bnum4g, bnum4g, ndiagg + 1); copyv(R.bden4g, bden4g, ndiagg);
+  R.set = true;
+  return THR_OK;
+}
+
+int thr_set_residuals(thr_ctx* c, float rescga, float rescgg, int spmd, int max_qmr_iters) {
+  if (!c) return THR_ERR_BADARG;
+  c->rescga = rescga;
+  c->rescgg = rescgg;
+  c->spmd = spmd;
+  if (max_qmr_iters > 0) c->max_qmr_iters = max_qmr_iters;
+  return THR_OK;
+}
+
+int thr_force(thr_ctx* c, const double* Phi, float res1, float am, int imass, const float* theta, double* dSdpi) {
+  if (!c || !Phi || !theta || !dSdpi) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  MdFields f;
+  THR_TRY(md_fields(c, &f));
+  THR_TRY(c->use_links(nullptr));
+  THR_TRY(c->upload_spinor(f.Phi, Phi));
+  THR_TRY(up_f3(c, f.thetat, theta));
+  THR_TRY(force_dev(c, &f, f.thetat, res1, am, imass));
+  THR_TRY(down_d3(c, dSdpi, f.dS));
+  return c->sync();
+}
+
+int thr_hamilton(thr_ctx* c, const double* Phi, double* h, double* hg, double* hp, double* s, float res2, float am,
+                 int imass, const float* theta, const float* pp) {
+  if (!c || !Phi || !h || !hg || !hp || !s || !theta || !pp) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  MdFields f;
+  THR_TRY(md_fields(c, &f));
+  THR_TRY(c->use_links(nullptr));
+  THR_TRY(c->upload_spinor(f.Phi, Phi));
+  THR_TRY(up_f3(c, f.thetat, theta));
+  THR_TRY(up_f3(c, f.pp, pp));
+  THR_TRY(hamilton_dev(c, &f, f.thetat, f.pp, res2, am, imass, h, hg, hp, s));
+  return c->sync();
+}
+
+int thr_initialise_phi(thr_ctx* c, double* Phi, float am, int imass) {
+  if (!c || !Phi) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  MdFields f;
+  THR_TRY(md_fields(c, &f));
+  THR_TRY(c->use_links(nullptr));
+  THR_TRY(initialise_phi_dev(c, &f, am, imass));
+  THR_TRY(c->download_spinor(Phi, f.Phi));
+  return c->sync();
+}
+
+int thr_initialise_pp(thr_ctx* c, float* pp) {
+  if (!c || !pp) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  MdFields f;
+  THR_TRY(md_fields(c, &f));
+  THR_TRY(rng_pp_draw(c, f.pp));
+  THR_TRY(down_f3(c, pp, f.pp));
+  return c->sync();
+}
+
+int thr_evolve_theta_pp(thr_ctx* c, int iterl, float dt, float* pp, const double* Phi, float res, float am, int imass,
+                        int* itot, float* theta, double* u, double* dSdpi, int fixed_steps) {
+  if (!c || !pp || !Phi || !theta || iterl < 1) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  MdFields f;
+  THR_TRY(md_fields(c, &f));
+  THR_TRY(c->upload_spinor(f.Phi, Phi));
+  THR_TRY(up_f3(c, f.thetat, theta));
+  THR_TRY(up_f3(c, f.pp, pp));
+  THR_TRY(c->coef_dev(f.thetat));
+  int it = itot ? *itot : 0;
+  THR_TRY(evolve_dev(c, &f, iterl, dt, res, am, imass, fixed_steps, &it));
+  if (itot) *itot = it;
+  THR_TRY(down_f3(c, theta, f.thetat));
+  THR_TRY(down_f3(c, pp, f.pp));
+  if (dSdpi) THR_TRY(down_d3(c, dSdpi, f.dS));
+  if (u) {
+    to_fortran_links(c->g, c->stage, c->u64, c->st);
+    THR_CUDA(cudaMemcpyAsync(u, c->stage, c->nfl() * sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+  }
+  return c->sync();
+}
+
+int thr_trajectory(thr_ctx* c, float* theta, int iterl, float dt, float am, int imass, int fixed_steps,
+                   thr_traj_result* out) {
+  if (!c || !theta || iterl < 1) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  MdFields f;
+  THR_TRY(md_fields(c, &f));
+  THR_TRY(up_f3(c, f.theta, theta));
+  THR_TRY(trajectory_dev(c, &f, iterl, dt, am, imass, fixed_steps, out));
+  THR_TRY(down_f3(c, theta, f.theta));
+  return c->sync();
+}
+
+int thr_md_counters(thr_ctx* c, double* counts8, int reset) {
+  if (!c) return THR_ERR_BADARG;
+  if (counts8) memcpy(counts8, c->md_counts, sizeof(c->md_counts));
+  if (reset) memset(c->md_counts, 0, sizeof(c->md_counts));
+  return THR_OK;
+}
+
+}  // extern "C"

@@ -49,6 +49,15 @@ SIGNATURES = {
     "thr_gauss0": (_i, [_v, _v]),
     "thr_gaussp": (_i, [_v, _v]),
     "thr_rano": (_i, [_v, _i, _i, _i, C.POINTER(C.c_float)]),
+    "thr_set_remez": (_i, [_v, _i] + [_v] * 8 + [_i] + [_v] * 8),
+    "thr_set_residuals": (_i, [_v, _f, _f, _i, _i]),
+    "thr_force": (_i, [_v, _v, _f, _f, _i, _v, _v]),
+    "thr_hamilton": (_i, [_v, _v, _pd, _pd, _pd, _pd, _f, _f, _i, _v, _v]),
+    "thr_initialise_phi": (_i, [_v, _v, _f, _i]),
+    "thr_initialise_pp": (_i, [_v, _v]),
+    "thr_evolve_theta_pp": (_i, [_v, _i, _f, _v, _v, _f, _f, _i, _pi, _v, _v, _v, _i]),
+    "thr_trajectory": (_i, [_v, _v, _i, _f, _f, _i, _i, _v]),
+    "thr_md_counters": (_i, [_v, _v, _i]),
     "thr_field_create": (_i, [_v, _i, C.POINTER(_v)]),
     "thr_field_destroy": (_i, [_v, _v]),
     "thr_field_upload": (_i, [_v, _v, _i, _v]),

@@ -19,6 +19,39 @@ NATURAL, EVEN_ODD = 0, 1
 FP64, FP32_REF, MIXED_FP32, MIXED_BF16 = 0, 1, 2, 3
 
 
+class TrajResult(C.Structure):
+    _fields_ = [("h0", C.c_double), ("h1", C.c_double), ("dh", C.c_double), ("ds", C.c_double),
+                ("s0", C.c_double), ("s1", C.c_double), ("accepted", C.c_int), ("steps", C.c_int),
+                ("y", C.c_float)]
+
+
+def read_remez_file(path, maxidx):
+    """remez_common_subroutines.F90:20-35: returns two dicts-of-arrays pieces
+    (anumA, adenA, anumB, adenB) from a text file: a0 then `a_i, s_i` lines, twice."""
+    vals = []
+    with open(path) as f:
+        for line in f:
+            line = line.replace(",", " ").split()
+            if line:
+                vals.append([float(v) for v in line])
+    out = []
+    pos = 0
+    for _ in range(2):
+        a0 = vals[pos][0]
+        pairs = vals[pos + 1:pos + 1 + maxidx]
+        pos += 1 + maxidx
+        out.append((np.array([a0] + [p[0] for p in pairs]), np.array([p[1] for p in pairs])))
+    (anA, adA), (anB, adB) = out
+    return anA, adA, anB, adB
+
+
+def remez_set(path2, path4, n):
+    """The remez module arrays from the files `remez2` and `remez4` (dwf3d_lib.F90:205-209)."""
+    a2, d2, b2, e2 = read_remez_file(path2, n)
+    a4, d4, b4, e4 = read_remez_file(path4, n)
+    return dict(anum2=a2, aden2=d2, bnum2=b2, bden2=e2, anum4=a4, aden4=d4, bnum4=b4, bden4=e4)
+
+
 class ThirringError(RuntimeError):
     def __init__(self, status, where):
         self.status = status
@@ -213,6 +246,68 @@ class Lattice:
                                    _p(np.ascontiguousarray(aden, np.float64)), nq, iflag, int(use_sp), _p(cgr),
                                    _p(dSdpi), _p(Phi0), max_qmr_iters), "qmrherm")
         return x, it.value, cgr
+
+    # ---- RHMC layer
+    def set_remez(self, rat, ratg):
+        """rat / ratg: dicts with anum2, aden2, bnum2, bden2, anum4, aden4, bnum4, bden4
+        (remez.F90 with ndiag poles, remezg.F90 with ndiagg poles)."""
+        keys = ("anum2", "aden2", "bnum2", "bden2", "anum4", "aden4", "bnum4", "bden4")
+        self._keep = [np.ascontiguousarray(d[k], np.float64) for d in (rat, ratg) for k in keys]
+        nd, ndg = len(rat["aden2"]), len(ratg["aden2"])
+        args = [self.h, nd] + [_p(a) for a in self._keep[:8]] + [ndg] + [_p(a) for a in self._keep[8:]]
+        _check(self._L.thr_set_remez(*args), "set_remez")
+
+    def set_residuals(self, rescga=1e-8, rescgg=1e-6, spmd=1, max_qmr_iters=0):
+        _check(self._L.thr_set_residuals(self.h, rescga, rescgg, int(spmd), max_qmr_iters), "set_residuals")
+
+    def force(self, Phi, res1, am, imass, theta):
+        """dSdpi = force(Phi, res1, am, imass): force_module.F90:9-113 (current links)."""
+        _need(Phi, self.sshape, np.complex128, "Phi")
+        theta = np.asfortranarray(theta, np.float32)
+        dS = field3(self)
+        _check(self._L.thr_force(self.h, _p(Phi), res1, am, imass, _p(theta), _p(dS)), "force")
+        return dS
+
+    def hamilton(self, Phi, res2, am, imass, theta, pp):
+        """(h, hg, hp, s) = hamilton(Phi, …): dwf3d_lib.F90:511-616 (current links)."""
+        _need(Phi, self.sshape, np.complex128, "Phi")
+        theta = np.asfortranarray(theta, np.float32)
+        pp = np.asfortranarray(pp, np.float32)
+        v = [C.c_double(0) for _ in range(4)]
+        _check(self._L.thr_hamilton(self.h, _p(Phi), *[C.byref(x) for x in v], res2, am, imass, _p(theta), _p(pp)),
+               "hamilton")
+        return tuple(x.value for x in v)
+
+    def initialise_phi(self, am, imass):
+        Phi = spinor(self)
+        _check(self._L.thr_initialise_phi(self.h, _p(Phi), am, imass), "initialise_phi")
+        return Phi
+
+    def initialise_pp(self):
+        pp = field3(self, np.float32)
+        _check(self._L.thr_initialise_pp(self.h, _p(pp)), "initialise_pp")
+        return pp
+
+    def evolve_theta_pp(self, iterl, dt, pp, Phi, res, am, imass, theta, fixed_steps=0):
+        """Leapfrog (evolution.F90:113-179): theta, pp updated in place; returns (itot, u, dSdpi)."""
+        it = C.c_int(0)
+        u = links(self)
+        dS = field3(self)
+        _check(self._L.thr_evolve_theta_pp(self.h, iterl, dt, _p(pp), _p(Phi), res, am, imass, C.byref(it),
+                                           _p(theta), _p(u), _p(dS), fixed_steps), "evolve_theta_pp")
+        return it.value, u, dS
+
+    def trajectory(self, theta, iterl, dt, am, imass, fixed_steps=0):
+        """One trajectory (dwf3d_lib.F90:265-323); theta updated in place if accepted."""
+        r = TrajResult()
+        _check(self._L.thr_trajectory(self.h, _p(theta), iterl, dt, am, imass, fixed_steps, C.byref(r)),
+               "trajectory")
+        return r
+
+    def md_counters(self, reset=False):
+        a = np.zeros(8)
+        _check(self._L.thr_md_counters(self.h, _p(a), int(reset)), "md_counters")
+        return dict(zip(("ancg", "ancgpv", "ancgf", "ancgfpv", "ancgh", "ancghpv", "ancgpf", "ancgpfpv"), a))
 
     # ---- derivs_module.F90
     def derivs(self, R, X2, anum, iflag, am, imass, dSdpi):
