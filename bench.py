@@ -1,0 +1,442 @@
+#!/usr/bin/env python
+"""Headline benchmark: the rational-approximation multishift solve (qmrherm).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--mode fp64|mixed]
+
+Workload (one "step"): qmrherm iflag 0 -- x = sum_i a_i (M^dagger M + s_i)^-1 Phi --
+on a 32^2 x 32 lattice with Ls = 32 (Shamir kernel, am = 0.01, imass = 1,
+domain-wall height 1), 25 poles s_i log-spaced in [1e-5, 1e2] with positive
+residues of the x^-1/2 form, solved to the reference's residual 1e-9.
+theta is Gaussian with variance 1/beta (beta = 0.3) and Phi is a complex
+Gaussian source, both seeded (synthetic: the reference publishes no data
+set).  The working set (2 x 25 shift fields of 67 MB) is far larger than L2,
+so no flush is needed between steps.
+
+Reported: `value` = solves/s over all ranks with inputs resident in HBM;
+`e2e` = the same through the C-ABI call with host Fortran-layout arrays
+(pinned), host<->device copies inside the timed region; `roofline` for the
+dominant kernel, timed live with CUDA events on the library's stream;
+`cpu_baseline` = the oracle (C restatement of the reference) on this host's
+cores over a bounded sample of the same solve.  With N > 1 (torchrun), each
+rank solves its own replica lattice (no collective on the data path) and the
+timing is the max over ranks.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "thirring-rhmc_b200"))
+
+# ------------------------------------------------------------------ workload
+LX = LY = LT = 32
+LS = 32
+BETA, AM, IMASS, AM3, RES = 0.3, 0.01, 1, 1.0, 1e-9
+NPOLE = 25
+# iterations the FP64 multishift takes on this seeded input (used to scale
+# the CPU sample to whole solves; re-measured by every GPU run and printed)
+FP64_ITERS_REF = None
+METRIC = "multishift solve throughput (qmrherm, 25 poles, FP64 residual 1e-9)"
+UNIT = "solves/s"
+HBM_FALLBACK = 6650.0
+
+
+def rational():
+    s = np.logspace(-5.0, 2.0, NPOLE)
+    delta = 7.0 / (NPOLE - 1)  # decades between poles
+    a = np.sqrt(s) * delta * np.log(10.0) / np.pi  # x^-1/2 ~ (1/pi) int ds s^-1/2/(s+x)
+    return np.concatenate([[0.0], a]), s
+
+
+def inputs(rank):
+    rng = np.random.default_rng(20240 + rank)
+    theta = np.asfortranarray(rng.standard_normal((LX, LY, LT, 3)) / np.sqrt(BETA), np.float32)
+    phi = np.zeros((LS + 2, LX + 2, LY + 2, LT + 2, 4), np.complex128, order="F")
+    shp = phi[1:-1, 1:-1, 1:-1, 1:-1, :].shape
+    phi[1:-1, 1:-1, 1:-1, 1:-1, :] = rng.standard_normal(shp) + 1j * rng.standard_normal(shp)
+    return theta, phi
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK, "fallback"
+
+
+def ncu_traffic(kernel):
+    """per-launch DRAM bytes of `kernel` from the committed ncu summary, else None"""
+    p = os.path.join(REPO, "profiles", "roofline_traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        f = line.split()
+        if len(f) >= 3 and f[0] == "traffic" and f[1] == kernel:
+            return float(f[2])
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region"""
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.p = None
+        self.out = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.p = None
+        return self
+
+    def _read(self):
+        for line in self.p.stdout:
+            self.out.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import thirring
+    from thirring import _lib
+
+    torch.cuda.set_device(local_rank)
+    L = _lib.lib()
+    mode = {"fp64": 0, "sp": 1, "mixed": 2, "bf16": 3}[args.mode]
+    anum, aden = rational()
+    theta, phi = inputs(rank)
+    G = thirring.Lattice(LX, LY, LT, LS, kernel=0, beta=BETA, am3=AM3, device=local_rank)
+    G.coef(theta)
+    h = G.h
+    pd = C.c_void_p()
+    px = C.c_void_p()
+    assert L.thr_field_create(h, 0, C.byref(pd)) == 0 and L.thr_field_create(h, 0, C.byref(px)) == 0
+    assert L.thr_field_upload(h, pd, 0, phi.ctypes.data_as(C.c_void_p)) == 0
+    an = np.ascontiguousarray(anum)
+    ad = np.ascontiguousarray(aden)
+    it = C.c_int(0)
+    cgr = np.zeros(NPOLE, np.int32)
+
+    def solve(m):
+        rc = L.thr_qmrherm_dev(h, pd, px, RES, C.byref(it), AM, IMASS, an.ctypes.data_as(C.c_void_p),
+                               ad.ctypes.data_as(C.c_void_p), NPOLE, 0, m, cgr.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise RuntimeError(f"thr_qmrherm_dev failed: {rc}")
+        return it.value
+
+    sptr = C.c_void_p()
+    L.thr_get_stream(h, C.byref(sptr))
+    stream = torch.cuda.ExternalStream(sptr.value)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def tmax(x):
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([x], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    # ---- warm-up
+    iters = 0
+    for _ in range(args.warmup):
+        iters = solve(mode)
+    # ---- timed region (inputs resident), profiled kernels, sampled clocks
+    L.thr_profile(h, 1, 1)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local_rank) as clk:
+        e0.record(stream)
+        its = [solve(mode) for _ in range(args.steps)]
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = tmax(e0.elapsed_time(e1))
+    L.thr_profile(h, 0, 0)
+    prof = {}
+    for kind, name in ((0, "dslash"), (1, "multishift_update")):
+        n = C.c_int(0)
+        t = C.c_double(0)
+        b = C.c_double(0)
+        L.thr_profile_read(h, kind, C.byref(n), C.byref(t), C.byref(b))
+        prof[name] = (n.value, t.value, b.value)
+    # chunked loops enqueue 8 iterations at a time; every iteration is 8 kernels
+    launches = int(sum(3 + 8 * (8 * ((i + 7) // 8)) + 1 for i in its))
+
+    # ---- FP64 GPU path for comparison (same solver, FP64 everywhere)
+    fp64_s = None
+    if mode != 0:
+        solve(0)
+        torch.cuda.synchronize()
+        f0 = time.perf_counter()
+        e0.record(stream)
+        fp64_iters = solve(0)
+        e1.record(stream)
+        e1.synchronize()
+        fp64_s = e0.elapsed_time(e1) / 1e3
+    else:
+        fp64_iters = its[-1]
+
+    # ---- e2e through the host C ABI (pinned Fortran-layout arrays)
+    x = np.zeros_like(phi)
+    for a in (phi, x):
+        L.thr_host_register(a.ctypes.data_as(C.c_void_p), a.nbytes)
+    e2e_ms = None
+    if args.e2e_steps > 0:
+        G.qmrherm(phi, RES, AM, IMASS, anum, aden, 0, use_sp=mode)
+        barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            rc = L.thr_qmrherm(h, phi.ctypes.data_as(C.c_void_p), x.ctypes.data_as(C.c_void_p), RES, C.byref(it), AM,
+                               IMASS, an.ctypes.data_as(C.c_void_p), ad.ctypes.data_as(C.c_void_p), NPOLE, 0, mode,
+                               None, None, None, 0)
+            assert rc == 0, rc
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        e2e_ms = tmax(e0.elapsed_time(e1))
+    for a in (phi, x):
+        L.thr_host_unregister(a.ctypes.data_as(C.c_void_p))
+
+    # ---- stencil bandwidth at the largest config-2 lattice (extra figure)
+    dslash = dslash_bandwidth(args, local_rank) if (rank == 0 and not args.no_dslash) else None
+
+    res = dict(ms=ms, its=its, prof=prof, launches=launches, fp64_s=fp64_s, fp64_iters=fp64_iters,
+               e2e_ms=e2e_ms, clocks=clk.summary(), dslash=dslash, phi_bytes=phi.nbytes)
+    L.thr_field_destroy(h, pd)
+    L.thr_field_destroy(h, px)
+    G.close()
+    return res
+
+
+def dslash_bandwidth(args, dev, lx=48, ls=48, iters=20):
+    """FP64 Shamir M at 48^2 x 48, Ls = 48: algorithmic GB/s over `iters` launches."""
+    import torch
+    import thirring
+    from thirring import _lib
+    L = _lib.lib()
+    G = thirring.Lattice(lx, lx, lx, ls, device=dev)
+    rng = np.random.default_rng(7)
+    G.coef(np.asfortranarray(rng.standard_normal((lx, lx, lx, 3)) / np.sqrt(BETA), np.float32))
+    a, b = C.c_void_p(), C.c_void_p()
+    L.thr_field_create(G.h, 0, C.byref(a))
+    L.thr_field_create(G.h, 0, C.byref(b))
+    R = thirring.spinor(G)
+    R[1:-1, 1:-1, 1:-1, 1:-1, :] = rng.standard_normal(R[1:-1, 1:-1, 1:-1, 1:-1, :].shape)
+    L.thr_field_upload(G.h, a, 0, R.ctypes.data_as(C.c_void_p))
+    s = C.c_void_p()
+    L.thr_get_stream(G.h, C.byref(s))
+    st = torch.cuda.ExternalStream(s.value)
+    out = {}
+    for dag in (0, 1):
+        for _ in range(3):
+            L.thr_dslash_dev(G.h, b, a, 0, AM, IMASS, dag)
+        L.thr_sync(G.h)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(iters):
+            L.thr_dslash_dev(G.h, b, a, 0, AM, IMASS, dag)
+        e1.record(st)
+        e1.synchronize()
+        us = e0.elapsed_time(e1) / iters * 1e3
+        v3 = lx ** 3
+        byts = 2 * 4 * ls * v3 * 16 + 3 * v3 * 16
+        out["dslashd" if dag else "dslash"] = {"us": round(us, 2), "gbs": round(byts / us / 1e3, 1)}
+    L.thr_field_destroy(G.h, a)
+    L.thr_field_destroy(G.h, b)
+    G.close()
+    return out
+
+
+# ------------------------------------------------------------------ CPU arm
+def cpu_sample(iters_sample, threads=None):
+    """Seconds per multishift iteration of the oracle on this workload: FP64
+    multishift_solver restated in C, OpenMP over the host cores."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+    if threads:
+        O.lib.orc_set_num_threads(threads)
+    nthreads = O.lib.orc_num_threads()
+    anum, aden = rational()
+    theta, phi = inputs(0)
+    Lo = O.lat(LX, LY, LT, LS, beta=BETA, am3=AM3)
+    u = O.coef(Lo, theta)
+    t0 = time.perf_counter()
+    O.multishift(Lo, u, AM, IMASS, anum[1:], aden, phi, RES, iters_sample)
+    dt = time.perf_counter() - t0
+    return dt / iters_sample, nthreads
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+# ------------------------------------------------------------------ main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="fp64", choices=["fp64", "sp", "mixed", "bf16"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-iters", type=int, default=6, help="multishift iterations in the CPU sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-dslash", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    iters_for_cpu = FP64_ITERS_REF
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        t0 = time.perf_counter()
+        per_iter = []
+        nthreads = 0
+        for _ in range(args.warmup + args.steps):
+            s, nthreads = cpu_sample(max(1, args.cpu_iters // 2))
+            per_iter.append(s)
+        timed = per_iter[args.warmup:]
+        s_iter = float(np.mean(timed))
+        iters = iters_for_cpu or 0
+        value = 1.0 / (s_iter * iters) if iters else None
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": (s_iter * iters * 1e3) if iters else None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded Gaussian theta, complex Gaussian source)",
+                "config": workload_config(),
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
+                                 "sample": f"{max(1, args.cpu_iters // 2)} multishift iterations per step of the "
+                                           f"same solve, scaled by the {iters} iterations a full solve takes; "
+                                           f"{cpu_model()}"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "wall_s": round(time.perf_counter() - t0, 1)}
+        print(json.dumps(line), flush=True)
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    r = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    iters = r["its"][-1]
+    ms_step = r["ms"] / args.steps
+    value = world * args.steps / (r["ms"] / 1e3)
+    peak, peak_kind = peaks()
+    # dominant kernel of the timed region
+    name, (nl, tms, byts) = max(r["prof"].items(), key=lambda kv: kv[1][1])
+    achieved = byts / (tms / 1e3) / 1e9 if tms > 0 else None
+    kname = {"dslash": "k_dslash_shamir", "multishift_update": "k_ms_pshift"}[name]
+    traffic = ncu_traffic(kname)
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1) if achieved else None,
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
+                "peak_source": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": byts / max(nl, 1), "launches": nl,
+                "share_of_step": round(tms / r["ms"], 3)}
+    other = {k: {"launches": v[0], "ms": round(v[1], 3), "gbs": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] else None}
+             for k, v in r["prof"].items()}
+    cpu = None
+    if not args.no_cpu:
+        s_iter, nthreads = cpu_sample(args.cpu_iters)
+        cpu_val = 1.0 / (s_iter * iters)
+        cpu = {"value": cpu_val, "unit": UNIT, "cores": nthreads, "kind": "port",
+               "sample": f"{args.cpu_iters} FP64 multishift iterations of the same solve ({s_iter:.3f} s/iter), "
+                         f"scaled to the {iters} iterations the solve takes; {cpu_model()}"}
+    e2e = None
+    if r["e2e_ms"]:
+        e2e = {"value": world * args.e2e_steps / (r["e2e_ms"] / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": r["phi_bytes"], "d2h_bytes_per_step": r["phi_bytes"],
+               "path": "thr_qmrherm (C ABI) with page-locked Fortran-layout host arrays"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.mode == "fp64" else args.mode,
+            "data": "synthetic (seeded Gaussian theta, complex Gaussian source)",
+            "config": workload_config(), "iterations": iters, "e2e": e2e, "roofline": roofline,
+            "kernels": other, "cpu_baseline": cpu, "gpu_launches": r["launches"], "clocks": r["clocks"],
+            "fp64_gpu_solve_s": r["fp64_s"] if r["fp64_s"] is not None else ms_step / 1e3,
+            "fp64_gpu_iterations": r["fp64_iters"], "dslash_48x48x48_ls48_fp64": r["dslash"]}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config():
+    return {"workload": f"qmrherm multishift solve, {LX}^2x{LT} lattice, Ls={LS}, Shamir, {NPOLE} poles "
+                        f"log-spaced 1e-5..1e2, am={AM}, imass={IMASS}, beta={BETA}, res={RES}",
+            "lattice": [LX, LY, LT, LS], "poles": NPOLE, "l2_flush": "not needed: working set 3.4 GB > L2",
+            "parallelism": "replicas (one lattice per GPU)"}
+
+
+if __name__ == "__main__":
+    main()

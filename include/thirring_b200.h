@@ -222,9 +222,20 @@ int thr_field_upload(thr_ctx *ctx, void *field, int precision, const double *hos
 int thr_field_download(thr_ctx *ctx, double *host_spinor, const void *field, int precision);
 /* out = M in (dag = 0) or M^dagger in (dag = 1) with the current links */
 int thr_dslash_dev(thr_ctx *ctx, void *out, const void *in, int precision, float am, int imass, int dag);
+/* qmrherm on FP64 device fields (the device layout of thr_field_create with
+ * THR_FP64): same semantics as thr_qmrherm; dSdpi and Phi0 stay in the
+ * context.  Returns when the solve has converged (its scalars are polled). */
+int thr_qmrherm_dev(thr_ctx *ctx, const void *Phi, void *x, float res, int *itercg, float am, int imass,
+                    const double *anum, const double *aden, int ndiagq, int iflag, int use_sp, int *cg_returns);
 int thr_sync(thr_ctx *ctx);
 /* the context's cudaStream_t, for event timing by the caller */
 int thr_get_stream(thr_ctx *ctx, void **stream);
+/* Kernel timing: with profiling enabled the solvers bracket each launch of
+ * the stencil (kind 0) and of the multishift vector update (kind 1) with
+ * CUDA events; thr_profile_read returns the launches, their summed device
+ * time in ms and the algorithmic bytes those launches moved. */
+int thr_profile(thr_ctx *ctx, int enable, int reset);
+int thr_profile_read(thr_ctx *ctx, int kind, int *launches, double *ms, double *bytes);
 
 #ifdef __cplusplus
 }

@@ -14,7 +14,17 @@ import oracle as O
 import thirring
 
 
+def _faces(a):
+    """interior and the six face halos; edges/corners are never read by the reference"""
+    m = np.zeros(a.shape[:3], bool)
+    m[1:-1, 1:-1, :] = True
+    m[1:-1, :, 1:-1] = True
+    m[:, 1:-1, 1:-1] = True
+    return a[m]
+
+
 def _ulps(a, b):
+    a, b = _faces(a), _faces(b)
     ai = a.view(np.int32).astype(np.int64)
     bi = b.view(np.int32).astype(np.int64)
     return np.abs(ai - bi)

@@ -33,6 +33,25 @@ int thr_ctx::buffer(int id, size_t bytes, void** out) {
   return THR_OK;
 }
 
+int thr_ctx::prof_begin(int kind, double bytes) {
+  if (!prof_on) return -1;
+  const int idx = (int)prof_kind.size();
+  if (2 * idx + 2 > (int)prof_ev.size()) {
+    for (int k = 0; k < 256; k++) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      prof_ev.push_back(e);
+    }
+  }
+  prof_kind.push_back(kind);
+  prof_bytes.push_back(bytes);
+  cudaEventRecord(prof_ev[2 * idx], st);
+  return idx;
+}
+void thr_ctx::prof_end(int idx) {
+  if (idx >= 0) cudaEventRecord(prof_ev[2 * idx + 1], st);
+}
+
 int thr_ctx::upload_spinor(double2* dst, const double* host) {
   THR_CUDA(cudaMemcpyAsync(stage, host, nf5() * sizeof(double2), cudaMemcpyHostToDevice, st));
   from_fortran_spinor<double2>(g, dst, stage, st);
@@ -149,6 +168,7 @@ int thr_destroy(thr_ctx* c) {
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
   for (auto p : c->w64) cudaFree(p);
+  for (auto e : c->prof_ev) cudaEventDestroy(e);
   for (int i = 0; i < thr_ctx::B_COUNT; i++) cudaFree(c->bufs[i]);
   c->rng.release();
   cudaFree(c->u64);
@@ -314,6 +334,38 @@ int thr_dslash_dev(thr_ctx* c, void* out, const void* in, int precision, float a
 int thr_sync(thr_ctx* c) {
   if (!c) return THR_ERR_BADARG;
   return c->sync();
+}
+
+int thr_profile(thr_ctx* c, int enable, int reset) {
+  if (!c) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  if (reset) {
+    cudaStreamSynchronize(c->st);
+    c->prof_kind.clear();
+    c->prof_bytes.clear();
+    for (double& b : c->prof_eff_bytes) b = 0.0;
+  }
+  c->prof_on = enable != 0;
+  return THR_OK;
+}
+
+int thr_profile_read(thr_ctx* c, int kind, int* launches, double* ms, double* bytes) {
+  if (!c || kind < 0 || kind >= thr_ctx::P_COUNT) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  THR_CUDA(cudaStreamSynchronize(c->st));
+  int cnt = 0;
+  double tot = 0.0;
+  for (size_t i = 0; i < c->prof_kind.size(); i++) {
+    if (c->prof_kind[i] != kind) continue;
+    float e = 0.0f;
+    THR_CUDA(cudaEventElapsedTime(&e, c->prof_ev[2 * i], c->prof_ev[2 * i + 1]));
+    tot += e;
+    cnt++;
+  }
+  if (launches) *launches = cnt;
+  if (ms) *ms = tot;
+  if (bytes) *bytes = c->prof_eff_bytes[kind];
+  return THR_OK;
 }
 
 int thr_get_stream(thr_ctx* c, void** s) {

@@ -78,6 +78,16 @@ struct thr_ctx {
   thr::Rng rng;  // random's module state
   int buffer(int id, size_t bytes, void** out);  // contents preserved only if not regrown
 
+  // optional per-kernel timing: CUDA events around selected launches
+  enum ProfKernel { P_DSLASH = 0, P_SHIFTUPD = 1, P_COUNT = 4 };
+  bool prof_on = false;
+  std::vector<cudaEvent_t> prof_ev;  // pairs
+  std::vector<int> prof_kind;
+  std::vector<double> prof_bytes;
+  double prof_eff_bytes[P_COUNT] = {};  // algorithmic bytes of the launches that did work
+  int prof_begin(int kind, double bytes);  // returns pair index or -1
+  void prof_end(int idx);
+
   size_t n4() const { return (size_t)g.v5 * 4; }  // complex elements of one spinor
   size_t nf5() const { return (size_t)(g.ls + 2) * (g.lx + 2) * (g.ly + 2) * (g.lt + 2) * 4; }
   size_t nfl() const { return (size_t)(g.lx + 2) * (g.ly + 2) * (g.lt + 2) * 3; }

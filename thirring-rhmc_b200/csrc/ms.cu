@@ -118,6 +118,7 @@ __global__ void k_ms_lambda(MsState* ms, const double* partials, int np) {
   if (ms->done) return;
   const double lambda = sum_partials(partials, np);
   ms->lambda = lambda;
+  ms->active_sum += (double)(ms->hi - ms->lo + 1);
   ms->gammag = lambda / ms->delta;
   for (int k = ms->lo; k <= ms->hi; k++)
     ms->gammas[k] = ms->gammag * ms->zeta_iii[k] * ms->omegas[k] / (ms->zeta_ii[k] * ms->omega);
@@ -244,13 +245,19 @@ int multishift_dev(thr_ctx* c, const V* u_dummy, const V* in, V* out, V* sf, V* 
   int it_host = 0;
   for (;;) {
     for (int k = 0; k < chunk; k++) {
+      int pe = c->prof_begin(thr_ctx::P_DSLASH, 0);
       THR_TRY(launch_dslash_guarded<V>(c, false, hv, p, (const V*)u, am, imass, &ms->done));
+      c->prof_end(pe);
+      pe = c->prof_begin(thr_ctx::P_DSLASH, 0);
       THR_TRY(launch_dslash_guarded<V>(c, true, s, hv, (const V*)u, am, imass, &ms->done));
+      c->prof_end(pe);
       k_redot<V><<<gb, kThreads, 0, c->st>>>(ms, p, s, n, c->partials);
       k_ms_alpha<<<1, 1, 0, c->st>>>(ms, c->partials, gb);
       k_ms_rupdate<V><<<gb, kThreads, 0, c->st>>>(ms, r, s, n, c->partials);
       k_ms_lambda<<<1, 1, 0, c->st>>>(ms, c->partials, gb);
+      pe = c->prof_begin(thr_ctx::P_SHIFTUPD, 0);
       k_ms_pshift<V><<<gb, kThreads, 0, c->st>>>(ms, p, r, out, sf, n, stride);
+      c->prof_end(pe);
       k_ms_converge<<<1, 1, 0, c->st>>>(ms);
     }
     it_host += chunk;
@@ -258,6 +265,13 @@ int multishift_dev(thr_ctx* c, const V* u_dummy, const V* in, V* out, V* sf, V* 
     THR_CUDA(cudaStreamSynchronize(c->st));
     if (h->done) break;
     if (it_host > maxcg + 2 * chunk) return THR_ERR_CUDA;  // the device state stopped advancing
+  }
+  if (c->prof_on) {
+    // algorithmic traffic of the work done: dslash = read R + write Phi + read links;
+    // shift update = r, p read + p write + (out, sf) read + write per active shift
+    const double lb = sp ? sizeof(float2) : sizeof(double2);
+    c->prof_eff_bytes[thr_ctx::P_DSLASH] += 2.0 * h->it * (2.0 * n * sizeof(V) + 3.0 * c->g.v3 * lb);
+    c->prof_eff_bytes[thr_ctx::P_SHIFTUPD] += (3.0 * h->it + 4.0 * h->active_sum) * n * sizeof(V);
   }
   if (cg_return) *cg_return = h->it;
   if (cg_returns)

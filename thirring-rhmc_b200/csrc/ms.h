@@ -10,6 +10,7 @@ struct MsState {
   double omega, gammag, delta, alpha, lambda, omega_save;
   int it, maxcg, lo, hi, done, status, ndiagq;
   float res;
+  double active_sum;  // sum over iterations of the shifts updated (for traffic accounting)
   double zeta_i[kMaxShift], zeta_ii[kMaxShift], zeta_iii[kMaxShift];
   double omegas[kMaxShift], gammas[kMaxShift], correction[kMaxShift], aden[kMaxShift];
   int flags[kMaxShift], cg_returns[kMaxShift];

@@ -235,4 +235,19 @@ int thr_qmrherm(thr_ctx* c, const double* Phi, double* x, float res, int* itercg
   return c->sync();
 }
 
+int thr_qmrherm_dev(thr_ctx* c, const void* Phi, void* x, float res, int* itercg, float am, int imass,
+                    const double* anum, const double* aden, int ndiagq, int iflag, int use_sp, int* cg_returns) {
+  if (!c || !Phi || !x || !itercg || !anum || !aden) return THR_ERR_BADARG;
+  if (imass != 1 && imass != 3 && imass != 5) return THR_ERR_BADARG;
+  if (iflag >= 2) {
+    if (iflag == 3 && !c->phi0_valid) return THR_ERR_BADARG;
+  }
+  cudaSetDevice(c->dev);
+  if (!c->links_ok) return THR_ERR_BADARG;
+  double* dS = nullptr;
+  if (iflag >= 2) THR_TRY(dsdpi_dev(c, &dS));
+  return qmrherm_dev(c, (const double2*)Phi, (double2*)x, res, itercg, am, imass, anum, aden, ndiagq, iflag, use_sp,
+                     cg_returns, dS, c->max_qmr_iters);
+}
+
 }  // extern "C"
