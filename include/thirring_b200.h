@@ -122,6 +122,14 @@ int thr_multishift_solver_sp(thr_ctx *ctx, const double *u, float am, int imass,
                              const double *anum, double *output, const double *input, float res, int maxcg,
                              int *cg_return, int *cg_returns);
 
+/* Multishift organisation (no counterpart in the reference, which has one):
+ * 0 = every active shift field updated in every iteration, the reference's
+ *     loop structure (multishift_module.F90:155-176);
+ * 1 = (default) the per-shift updates of 16 iterations replayed in one pass
+ *     over the shift fields from a ring of the last residuals; the same
+ *     per-element arithmetic, about 8x less shift-field traffic. */
+int thr_set_solver(thr_ctx *ctx, int multishift_algo);
+
 /* ---- qmrherm_module.F90 -------------------------------------------------- */
 /* qmrherm(Phi, x, res, itercg, am, imass, anum, aden, ndiagq, iflag[, use_sp]
  * [, cg_returns]), qmrherm_module.F90:20-197, with the current links:

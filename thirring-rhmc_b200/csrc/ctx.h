@@ -58,6 +58,8 @@ struct thr_ctx {
     B_AUX,      // misc
     B_MD,       // MD spinors: Phi, X2, Xresult, R
     B_MDF,      // MD 3D fields: theta, thetat, pp (float) and dSdpi (double)
+    B_HIST,     // batched multishift coefficient history
+    B_RING,     // batched multishift residual ring
     B_COUNT = 16
   };
   // rational approximations (remez.F90, remezg.F90): anum has n+1 entries
@@ -71,6 +73,7 @@ struct thr_ctx {
   float rescga = 1e-8f, rescgg = 1e-6f;
   int spmd = 1;             // 0: FP64 guidance solves; 1: single-precision (reference)
   int max_qmr_iters = 50000;
+  int ms_algo = 1;          // multishift: 0 = per-iteration shift updates, 1 = batched
   double md_counts[8] = {};  // ancg, ancgpv, ancgf, ancgfpv, ancgh, ancghpv, ancgpf, ancgpfpv
   void* bufs[B_COUNT] = {};
   size_t buf_bytes[B_COUNT] = {};

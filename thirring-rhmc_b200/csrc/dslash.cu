@@ -30,18 +30,47 @@ struct SpinorView {
   }
 };
 
+// Re(conj(aux_i) v) in the working precision, accumulated in FP64 (for FP32
+// storage the term is an FP32 value summed in FP64, as reduce_real_dp5d does)
+template <class S>
+__device__ __forceinline__ double epi_redot(const S* aux, size_t i, typename Sto<S>::C v) {
+  using R = typename Sto<S>::R;
+  const typename Sto<S>::C a = Sto<S>::ld(aux, i);
+  const R t = a.x * v.x + a.y * v.y;
+  return (double)t;
+}
+
+// one FP64 partial per block, fixed reduction order
+__device__ __forceinline__ void block_partial(double v, double* partials) {
+  __shared__ double sh[32];
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int nthr = blockDim.x * blockDim.y;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((tid & 31) == 0) sh[tid >> 5] = v;
+  __syncthreads();
+  if (tid < 32) {
+    const int nw = (nthr + 31) >> 5;
+    v = tid < nw ? sh[tid] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (tid == 0) partials[blockIdx.x] = v;
+  }
+}
+
 // ---------------------------------------------------------------- Shamir
-template <class S, bool DAG>
+template <class S, bool DAG, int EPI>
 __global__ void __launch_bounds__(256) k_dslash_shamir(S* __restrict__ out, const S* __restrict__ in,
                                                        const typename Sto<S>::C* __restrict__ u, Geom g,
-                                                       float am, int imass, float am3, const int* skip) {
+                                                       float am, int imass, float am3, const int* skip,
+                                                       const S* __restrict__ aux, double* __restrict__ partials) {
   if (skip && *skip) return;
   using St = Sto<S>;
   using R = typename St::R;
   using C = typename St::C;
   const int s = threadIdx.x;
-  const int site = blockIdx.x * blockDim.y + threadIdx.y;
-  if (site >= g.v3) return;
+  double racc = 0.0;
+  for (int site = blockIdx.x * blockDim.y + threadIdx.y; site < g.v3; site += gridDim.x * blockDim.y) {
   int x, y, t;
   site_coords(g, site, x, y, t);
   const Nbr nb = neighbours(g, x, y, t);
@@ -119,7 +148,12 @@ __global__ void __launch_bounds__(256) k_dslash_shamir(S* __restrict__ out, cons
   if (!DAG) { hop(); shop(); mass(); }
   else { shop(); mass(); hop(); }
 #pragma unroll
-  for (int d = 0; d < 4; d++) St::st(out, sidx(g, s, site, d), acc[d]);
+  for (int d = 0; d < 4; d++) {
+    St::st(out, sidx(g, s, site, d), acc[d]);
+    if (EPI == 1) racc += epi_redot<S>(aux, sidx(g, s, site, d), acc[d]);
+  }
+  }
+  if (EPI == 1) block_partial(racc, partials);
 }
 
 // ---------------------------------------------------------------- Wilson
@@ -148,17 +182,18 @@ __device__ __forceinline__ void wilson_qd(const SpinorView<S>& Rv, int s, int si
   for (int d = 0; d < 4; d++) q[d] = inner ? Rv(s, site, d) + Rv(sn, site, d) : Rv(s, site, d) + cmul(z, Rv(swall, site, d));
 }
 
-template <class S, bool DAG>
+template <class S, bool DAG, int EPI>
 __global__ void __launch_bounds__(256) k_dslash_wilson(S* __restrict__ out, const S* __restrict__ in,
                                                        const typename Sto<S>::C* __restrict__ u, Geom g,
-                                                       float am, int imass, float am3, const int* skip) {
+                                                       float am, int imass, float am3, const int* skip,
+                                                       const S* __restrict__ aux, double* __restrict__ partials) {
   if (skip && *skip) return;
   using St = Sto<S>;
   using R = typename St::R;
   using C = typename St::C;
   const int s = threadIdx.x;
-  const int site = blockIdx.x * blockDim.y + threadIdx.y;
-  if (site >= g.v3) return;
+  double racc = 0.0;
+  for (int site = blockIdx.x * blockDim.y + threadIdx.y; site < g.v3; site += gridDim.x * blockDim.y) {
   int x, y, t;
   site_coords(g, site, x, y, t);
   const Nbr nb = neighbours(g, x, y, t);
@@ -228,7 +263,12 @@ __global__ void __launch_bounds__(256) k_dslash_wilson(S* __restrict__ out, cons
     }
   }
 #pragma unroll
-  for (int d = 0; d < 4; d++) St::st(out, sidx(g, s, site, d), res[d]);
+  for (int d = 0; d < 4; d++) {
+    St::st(out, sidx(g, s, site, d), res[d]);
+    if (EPI == 1) racc += epi_redot<S>(aux, sidx(g, s, site, d), res[d]);
+  }
+  }
+  if (EPI == 1) block_partial(racc, partials);
 }
 
 // ---------------------------------------------------------------- launch
@@ -238,30 +278,48 @@ dim3 stencil_block(const Geom& g) {
   return dim3(g.ls, spb, 1);
 }
 
+unsigned stencil_grid(const Geom& g) {
+  const dim3 blk = stencil_block(g);
+  unsigned need = (unsigned)((g.v3 + blk.y - 1) / blk.y);
+  const unsigned cap = 148 * 8;
+  return need < cap ? need : cap;
+}
+
 template <class S>
-int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
-                  int imass, float am3, cudaStream_t st, const int* skip) {
+int launch_dslash_epi(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
+                      int imass, float am3, cudaStream_t st, const int* skip, const S* aux, double* partials) {
   if (g.ls > 1024) return THR_ERR_BADSHAPE;
-  dim3 blk = stencil_block(g);
-  dim3 grd((g.v3 + blk.y - 1) / blk.y);
+  const dim3 blk = stencil_block(g);
+  const dim3 grd(stencil_grid(g));
+  const bool epi = aux != nullptr;
+#define THR_LAUNCH(KER, D, E) KER<S, D, E><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, partials)
   if (kernel == 1) {
     if (imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
-    if (dag) k_dslash_wilson<S, true><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip);
-    else k_dslash_wilson<S, false><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip);
+    if (dag) { if (epi) THR_LAUNCH(k_dslash_wilson, true, 1); else THR_LAUNCH(k_dslash_wilson, true, 0); }
+    else { if (epi) THR_LAUNCH(k_dslash_wilson, false, 1); else THR_LAUNCH(k_dslash_wilson, false, 0); }
   } else {
-    if (dag) k_dslash_shamir<S, true><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip);
-    else k_dslash_shamir<S, false><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip);
+    if (dag) { if (epi) THR_LAUNCH(k_dslash_shamir, true, 1); else THR_LAUNCH(k_dslash_shamir, true, 0); }
+    else { if (epi) THR_LAUNCH(k_dslash_shamir, false, 1); else THR_LAUNCH(k_dslash_shamir, false, 0); }
   }
+#undef THR_LAUNCH
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
 
-template int launch_dslash<double2>(const Geom&, int, bool, double2*, const double2*, const double2*, float, int, float,
-                                    cudaStream_t, const int*);
-template int launch_dslash<float2>(const Geom&, int, bool, float2*, const float2*, const float2*, float, int, float,
-                                   cudaStream_t, const int*);
-template int launch_dslash<__nv_bfloat162>(const Geom&, int, bool, __nv_bfloat162*, const __nv_bfloat162*,
-                                           const float2*, float, int, float, cudaStream_t, const int*);
-template int launch_dslash<__half2>(const Geom&, int, bool, __half2*, const __half2*, const float2*, float, int, float,
-                                    cudaStream_t, const int*);
+template <class S>
+int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
+                  int imass, float am3, cudaStream_t st, const int* skip) {
+  return launch_dslash_epi<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr);
+}
+
+#define THR_INST(S, L)                                                                                            \
+  template int launch_dslash<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float, cudaStream_t,   \
+                                const int*);                                                                      \
+  template int launch_dslash_epi<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,            \
+                                    cudaStream_t, const int*, const S*, double*);
+THR_INST(double2, double2)
+THR_INST(float2, float2)
+THR_INST(__nv_bfloat162, float2)
+THR_INST(__half2, float2)
+#undef THR_INST
 
 }  // namespace thr

@@ -13,6 +13,7 @@
 #include "ctx.h"
 #include "ms.h"
 #include "solver.h"
+#include "thr_reduce.cuh"
 
 namespace thr {
 
@@ -33,11 +34,6 @@ __device__ __forceinline__ double block_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   }
   return v;
-}
-__device__ double sum_partials(const double* p, int n) {
-  double a = 0.0;
-  for (int i = 0; i < n; i++) a += p[i];
-  return a;
 }
 
 template <class V> struct VT;
@@ -76,25 +72,18 @@ __global__ void k_redot(const MsState* ms, const V* a, const V* b, size_t n, dou
 }
 
 __global__ void k_ms_init(MsState* ms, const double* partials, int np) {
-  ms->delta = sum_partials(partials, np);  // :73
+  const double d = block_sum_partials(partials, np);  // :73
+  if (threadIdx.x == 0) ms->delta = d;
 }
 
-// iteration start + alpha: :104, :118-135
+// iteration start + alpha: :104, :118-135 (one block; shifts in parallel)
 __global__ void k_ms_alpha(MsState* ms, const double* partials, int np) {
   if (ms->done) return;
-  ms->it += 1;
-  const double alpha = sum_partials(partials, np);
-  ms->alpha = alpha;
-  const double omega_save = ms->omega;
-  const double omega = -ms->delta / alpha;
-  ms->omega_save = omega_save;
-  ms->omega = omega;
-  for (int k = ms->lo; k <= ms->hi; k++) {
-    ms->zeta_iii[k] = (ms->zeta_i[k] * ms->zeta_ii[k] * omega_save) /
-                      (omega * ms->gammag * (ms->zeta_i[k] - ms->zeta_ii[k]) +
-                       ms->zeta_i[k] * omega_save * (1.0 - ms->aden[k] * omega));
-    ms->omegas[k] = omega * ms->zeta_iii[k] / ms->zeta_ii[k];
-  }
+  const double alpha = block_sum_partials(partials, np);
+  if (threadIdx.x == 0) ms_alpha_scalar(ms, alpha);
+  __syncthreads();
+  const int k = ms->lo + threadIdx.x;
+  if (k <= ms->hi) ms_alpha_shift(ms, k);
 }
 
 // r = r + omega*s (:137) fused with lambda = |r|^2 (:138)
@@ -116,12 +105,11 @@ __global__ void k_ms_rupdate(const MsState* ms, V* r, const V* s, size_t n, doub
 // :143, :148-150
 __global__ void k_ms_lambda(MsState* ms, const double* partials, int np) {
   if (ms->done) return;
-  const double lambda = sum_partials(partials, np);
-  ms->lambda = lambda;
-  ms->active_sum += (double)(ms->hi - ms->lo + 1);
-  ms->gammag = lambda / ms->delta;
-  for (int k = ms->lo; k <= ms->hi; k++)
-    ms->gammas[k] = ms->gammag * ms->zeta_iii[k] * ms->omegas[k] / (ms->zeta_ii[k] * ms->omega);
+  const double lambda = block_sum_partials(partials, np);
+  if (threadIdx.x == 0) ms_lambda_scalar(ms, lambda);
+  __syncthreads();
+  const int k = ms->lo + threadIdx.x;
+  if (k <= ms->hi) ms_lambda_shift(ms, k);
 }
 
 // p = r + gammag*p (:145) and, for every shift in the window,
@@ -149,27 +137,7 @@ __global__ void k_ms_pshift(const MsState* ms, V* p, const V* r, V* out, V* sf, 
 // :178-180, :230-275
 __global__ void k_ms_converge(MsState* ms) {
   if (ms->done) return;
-  for (int k = ms->lo; k <= ms->hi; k++) ms->cg_returns[k] = ms->it;
-  int maxi = -1, mini = ms->ndiagq;
-  for (int k = 0; k < ms->ndiagq; k++) {
-    if (ms->flags[k]) {
-      if (sqrt(ms->delta * ms->zeta_ii[k] * ms->zeta_ii[k]) * ms->correction[k] < (double)ms->res) {
-        ms->flags[k] = 0;
-      } else {
-        maxi = k > maxi ? k : maxi;
-        mini = k < mini ? k : mini;
-      }
-    }
-  }
-  ms->lo = mini;
-  ms->hi = maxi;
-  for (int k = mini; k <= maxi; k++) {
-    ms->zeta_i[k] = ms->zeta_ii[k];
-    ms->zeta_ii[k] = ms->zeta_iii[k];
-  }
-  ms->delta = ms->lambda;
-  if (!(ms->lambda == ms->lambda)) ms->status = THR_ERR_NAN;
-  if (maxi < mini || ms->it >= ms->maxcg || ms->status) ms->done = 1;
+  ms_converge_step(ms);
 }
 
 template <class V>
@@ -236,7 +204,7 @@ int multishift_dev(thr_ctx* c, const V* u_dummy, const V* in, V* out, V* sf, V* 
   THR_CUDA(cudaMemcpyAsync(p, in, n * sizeof(V), cudaMemcpyDeviceToDevice, c->st));
   const unsigned gb = vec_grid(n);
   k_norm2<V><<<gb, kThreads, 0, c->st>>>(nullptr, r, n, c->partials);
-  k_ms_init<<<1, 1, 0, c->st>>>(ms, c->partials, gb);
+  k_ms_init<<<1, 256, 0, c->st>>>(ms, c->partials, gb);
   THR_CUDA(cudaMemsetAsync(out, 0, (size_t)ndiagq * stride * sizeof(V), c->st));
   k_fill_shifts<V><<<gb, kThreads, 0, c->st>>>(sf, in, n, stride, ndiagq);
   const bool sp = sizeof(V) == sizeof(float2);
@@ -252,9 +220,9 @@ int multishift_dev(thr_ctx* c, const V* u_dummy, const V* in, V* out, V* sf, V* 
       THR_TRY(launch_dslash_guarded<V>(c, true, s, hv, (const V*)u, am, imass, &ms->done));
       c->prof_end(pe);
       k_redot<V><<<gb, kThreads, 0, c->st>>>(ms, p, s, n, c->partials);
-      k_ms_alpha<<<1, 1, 0, c->st>>>(ms, c->partials, gb);
+      k_ms_alpha<<<1, 256, 0, c->st>>>(ms, c->partials, gb);
       k_ms_rupdate<V><<<gb, kThreads, 0, c->st>>>(ms, r, s, n, c->partials);
-      k_ms_lambda<<<1, 1, 0, c->st>>>(ms, c->partials, gb);
+      k_ms_lambda<<<1, 256, 0, c->st>>>(ms, c->partials, gb);
       pe = c->prof_begin(thr_ctx::P_SHIFTUPD, 0);
       k_ms_pshift<V><<<gb, kThreads, 0, c->st>>>(ms, p, r, out, sf, n, stride);
       c->prof_end(pe);

@@ -10,7 +10,8 @@ struct MsState {
   double omega, gammag, delta, alpha, lambda, omega_save;
   int it, maxcg, lo, hi, done, status, ndiagq;
   float res;
-  double active_sum;  // sum over iterations of the shifts updated (for traffic accounting)
+  double active_sum;    // sum over iterations of the shifts updated (for traffic accounting)
+  double flush_fields;  // fields moved by the batched shift updates (for traffic accounting)
   double zeta_i[kMaxShift], zeta_ii[kMaxShift], zeta_iii[kMaxShift];
   double omegas[kMaxShift], gammas[kMaxShift], correction[kMaxShift], aden[kMaxShift];
   int flags[kMaxShift], cg_returns[kMaxShift];
@@ -18,6 +19,71 @@ struct MsState {
 static_assert(sizeof(MsState) <= 4096 * sizeof(double), "MsState must fit the scalar block");
 
 int ms_prepare_state(thr_ctx* c, MsState* h, int ndiagq, const double* aden, const double* anum, float res, int maxcg);
+
+// ---- the scalar recurrences of multishift_module.F90, one statement group each
+// iteration start and omega (:104, :126-127); one thread
+__device__ __forceinline__ void ms_alpha_scalar(MsState* ms, double alpha) {
+  ms->it += 1;
+  ms->alpha = alpha;
+  ms->omega_save = ms->omega;
+  ms->omega = -ms->delta / alpha;
+}
+// zeta_iii and omegas of shift k (:129-135)
+__device__ __forceinline__ void ms_alpha_shift(MsState* ms, int k) {
+  const double omega = ms->omega, omega_save = ms->omega_save;
+  ms->zeta_iii[k] = (ms->zeta_i[k] * ms->zeta_ii[k] * omega_save) /
+                    (omega * ms->gammag * (ms->zeta_i[k] - ms->zeta_ii[k]) +
+                     ms->zeta_i[k] * omega_save * (1.0 - ms->aden[k] * omega));
+  ms->omegas[k] = omega * ms->zeta_iii[k] / ms->zeta_ii[k];
+}
+// lambda and gammag (:138-143); one thread
+__device__ __forceinline__ void ms_lambda_scalar(MsState* ms, double lambda) {
+  ms->lambda = lambda;
+  ms->active_sum += (double)(ms->hi - ms->lo + 1);
+  ms->gammag = lambda / ms->delta;
+}
+// gammas of shift k (:148-150)
+__device__ __forceinline__ void ms_lambda_shift(MsState* ms, int k) {
+  ms->gammas[k] = ms->gammag * ms->zeta_iii[k] * ms->omegas[k] / (ms->zeta_ii[k] * ms->omega);
+}
+// cg_returns, convergence test, window, zeta shift, delta (:178-180, :230-275); one thread
+__device__ __forceinline__ void ms_converge_step(MsState* ms) {
+  for (int k = ms->lo; k <= ms->hi; k++) ms->cg_returns[k] = ms->it;
+  int maxi = -1, mini = ms->ndiagq;
+  for (int k = 0; k < ms->ndiagq; k++) {
+    if (ms->flags[k]) {
+      if (sqrt(ms->delta * ms->zeta_ii[k] * ms->zeta_ii[k]) * ms->correction[k] < (double)ms->res) {
+        ms->flags[k] = 0;
+      } else {
+        maxi = k > maxi ? k : maxi;
+        mini = k < mini ? k : mini;
+      }
+    }
+  }
+  ms->lo = mini;
+  ms->hi = maxi;
+  for (int k = mini; k <= maxi; k++) {
+    ms->zeta_i[k] = ms->zeta_ii[k];
+    ms->zeta_ii[k] = ms->zeta_iii[k];
+  }
+  ms->delta = ms->lambda;
+  if (!(ms->lambda == ms->lambda)) ms->status = THR_ERR_NAN;
+  if (maxi < mini || ms->it >= ms->maxcg || ms->status) ms->done = 1;
+}
+
+// Batched variant: per-iteration coefficients of the shift update, applied
+// every kBatch iterations in one pass over the shift fields.
+constexpr int kBatch = 16;
+struct MsHist {
+  int nsteps;
+  int lo[kBatch], hi[kBatch];
+  double om[kBatch][kMaxShift], ga[kBatch][kMaxShift], ze[kBatch][kMaxShift];
+};
+
+template <class V>
+int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p, V* hv, V* s, int ndiagq,
+                           const double* aden, const double* anum, float res, float am, int imass, int maxcg,
+                           int* cg_return, int* cg_returns);
 
 template <class V>
 int multishift_dev(thr_ctx* c, const V* u_dummy, const V* in, V* out, V* sf, V* r, V* p, V* hv, V* s, int ndiagq,

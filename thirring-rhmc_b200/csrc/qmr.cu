@@ -47,10 +47,16 @@ __global__ void k_d2f(float2* d, const double2* s, size_t n) {
 int multishift_into(thr_ctx* c, const double2* Phi, double2* x1, int nq, const double* aden, const double* anum,
                     float res, float am, int imass, int maxcg, int sp, int* itercg, int* cg_returns) {
   const size_t n = c->n4();
+  const bool batched = c->ms_algo == 1;
   if (!sp) {
-    void* sf;
+    void *sf, *ring;
     THR_TRY(c->buffer(thr_ctx::B_SF64, (size_t)nq * n * sizeof(double2), &sf));
     THR_TRY(c->ensure_w64(8));
+    if (batched) {
+      THR_TRY(c->buffer(thr_ctx::B_RING, (size_t)(kBatch + 1) * n * sizeof(double2), &ring));
+      return multishift_batched_dev<double2>(c, Phi, x1, (double2*)sf, (double2*)ring, c->w64[5], c->w64[6],
+                                             c->w64[7], nq, aden, anum, res, am, imass, maxcg, itercg, cg_returns);
+    }
     return multishift_dev<double2>(c, nullptr, Phi, x1, (double2*)sf, c->w64[4], c->w64[5], c->w64[6], c->w64[7], nq,
                                    aden, anum, res, am, imass, maxcg, itercg, cg_returns);
   }
@@ -60,8 +66,16 @@ int multishift_into(thr_ctx* c, const double2* Phi, double2* x1, int nq, const d
   THR_TRY(c->buffer(thr_ctx::B_WORK32, 5 * n * sizeof(float2), &w32));
   float2* w = (float2*)w32;
   k_d2f<<<vec_grid(n), kThreads, 0, c->st>>>(w + 4 * n, Phi, n);  // input = cmplx(inputdp)
-  int rc = multishift_dev<float2>(c, nullptr, w + 4 * n, (float2*)out32, (float2*)sf32, w, w + n, w + 2 * n, w + 3 * n,
-                                  nq, aden, anum, res, am, imass, maxcg, itercg, cg_returns);
+  int rc;
+  if (batched) {
+    void* ring;
+    THR_TRY(c->buffer(thr_ctx::B_RING, (size_t)(kBatch + 1) * n * sizeof(double2), &ring));
+    rc = multishift_batched_dev<float2>(c, w + 4 * n, (float2*)out32, (float2*)sf32, (float2*)ring, w, w + n,
+                                        w + 2 * n, nq, aden, anum, res, am, imass, maxcg, itercg, cg_returns);
+  } else {
+    rc = multishift_dev<float2>(c, nullptr, w + 4 * n, (float2*)out32, (float2*)sf32, w, w + n, w + 2 * n, w + 3 * n,
+                                nq, aden, anum, res, am, imass, maxcg, itercg, cg_returns);
+  }
   k_f2d<<<vec_grid((size_t)nq * n), kThreads, 0, c->st>>>(x1, (const float2*)out32, (size_t)nq * n);
   return rc;
 }
@@ -233,6 +247,12 @@ int thr_qmrherm(thr_ctx* c, const double* Phi, double* x, float res, int* itercg
   }
   if (iflag >= 2 && dSdpi) THR_TRY(download_d3(c, dSdpi, dS));
   return c->sync();
+}
+
+int thr_set_solver(thr_ctx* c, int multishift_algo) {
+  if (!c || multishift_algo < 0 || multishift_algo > 1) return THR_ERR_BADARG;
+  c->ms_algo = multishift_algo;
+  return THR_OK;
 }
 
 int thr_qmrherm_dev(thr_ctx* c, const void* Phi, void* x, float res, int* itercg, float am, int imass,

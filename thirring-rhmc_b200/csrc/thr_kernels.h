@@ -9,11 +9,16 @@ namespace thr {
 constexpr int kMaxPartials = 4096;
 
 dim3 stencil_block(const Geom& g);
+unsigned stencil_grid(const Geom& g);  // bounded grid: the stencil kernels are grid-stride over sites
 
 // dslash.cu
 template <class S>
 int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
                   int imass, float am3, cudaStream_t st, const int* skip = nullptr);
+// same, and when aux != NULL also one FP64 partial per block of sum Re(conj(aux) out)
+template <class S>
+int launch_dslash_epi(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
+                      int imass, float am3, cudaStream_t st, const int* skip, const S* aux, double* partials);
 
 // layout.cu: Fortran halo'd host layout <-> device fields
 // spinor (0:Ls+1,0:Lx+1,0:Ly+1,0:Lt+1,4) complex(dp)  <-> S[4][V3][Ls]

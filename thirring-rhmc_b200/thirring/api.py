@@ -212,6 +212,10 @@ class Lattice:
             _check(rc, "congrad")
         return it.value, nx.value
 
+    def set_solver(self, multishift_algo):
+        """0: per-iteration shift updates (the reference's loop); 1: batched (default)."""
+        _check(self._L.thr_set_solver(self.h, int(multishift_algo)), "set_solver")
+
     # ---- multishift_module.F90
     def multishift_solver(self, u, am, imass, aden, anum, inp, res, maxcg, sp=False):
         """Returns (output (Ls,Lx,Ly,Lt,4,ndiag), cg_return, cg_returns)."""
