@@ -1,6 +1,7 @@
 // ctx.cu -- context lifetime, host<->device transfers, links, and the
 // dirac.F90 / gauge.F90 entry points of the C ABI.
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 
 #include "ctx.h"
@@ -148,7 +149,9 @@ int thr_create(const thr_params* p, thr_ctx** out) {
   if (!rc && cudaMalloc(&c->u32, (size_t)c->g.v3 * 3 * sizeof(float2)) != cudaSuccess) rc = THR_ERR_NOMEM;
   c->stage_elems = c->nf5();
   if (!rc && cudaMalloc(&c->stage, c->stage_elems * sizeof(double2)) != cudaSuccess) rc = THR_ERR_NOMEM;
-  if (!rc && cudaMalloc(&c->partials, kMaxPartials * 8 * sizeof(double)) != cudaSuccess) rc = THR_ERR_NOMEM;
+  // per-block partial sums: the stencil epilogue writes one per block of its grid
+  const size_t nparts = std::max<size_t>((size_t)kMaxPartials * 8, (size_t)stencil_grid(c->g) + 1024);
+  if (!rc && cudaMalloc(&c->partials, nparts * sizeof(double)) != cudaSuccess) rc = THR_ERR_NOMEM;
   if (!rc && cudaMalloc(&c->dscal, 4096 * sizeof(double)) != cudaSuccess) rc = THR_ERR_NOMEM;
   if (!rc && cudaMalloc(&c->iscal, 1024 * sizeof(int)) != cudaSuccess) rc = THR_ERR_NOMEM;
   if (!rc && cudaMallocHost(&c->hscal, 4096 * sizeof(double)) != cudaSuccess) rc = THR_ERR_NOMEM;

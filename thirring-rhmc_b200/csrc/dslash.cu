@@ -60,7 +60,7 @@ __device__ __forceinline__ void block_partial(double v, double* partials) {
 
 // ---------------------------------------------------------------- Shamir
 template <class S, bool DAG, int EPI>
-__global__ void __launch_bounds__(256) k_dslash_shamir(S* __restrict__ out, const S* __restrict__ in,
+__global__ void __launch_bounds__(256, 4) k_dslash_shamir(S* __restrict__ out, const S* __restrict__ in,
                                                        const typename Sto<S>::C* __restrict__ u, Geom g,
                                                        float am, int imass, float am3, const int* skip,
                                                        const S* __restrict__ aux, double* __restrict__ partials) {
@@ -70,7 +70,8 @@ __global__ void __launch_bounds__(256) k_dslash_shamir(S* __restrict__ out, cons
   using C = typename St::C;
   const int s = threadIdx.x;
   double racc = 0.0;
-  for (int site = blockIdx.x * blockDim.y + threadIdx.y; site < g.v3; site += gridDim.x * blockDim.y) {
+  const int site = blockIdx.x * blockDim.y + threadIdx.y;
+  if (site < g.v3) {
   int x, y, t;
   site_coords(g, site, x, y, t);
   const Nbr nb = neighbours(g, x, y, t);
@@ -82,23 +83,27 @@ __global__ void __launch_bounds__(256) k_dslash_shamir(S* __restrict__ out, cons
 #pragma unroll
   for (int d = 0; d < 4; d++) acc[d] = diag * Rv(s, site, d);
 
+  // Wilson and Dirac hopping terms.  The forward (U R(x+mu)) and backward
+  // (conj U(x-mu) R(x-mu)) halves are accumulated one after the other, so
+  // only one neighbour's four spins are live at a time (register pressure,
+  // hence occupancy): acc -= 1/2 T(d) +/- gamma(mu,d) T(gin) per half.
   auto hop = [&]() {
 #pragma unroll
     for (int mu = 0; mu < 3; mu++) {
-      const C U = __ldg(u + (size_t)mu * g.v3 + site);
-      const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
-      C A[4], B[4];
 #pragma unroll
-      for (int d = 0; d < 4; d++) {
-        A[d] = cmul(U, Rv(s, nb.f[mu], d));
-        B[d] = cmul(Ub, Rv(s, nb.b[mu], d));
-      }
+      for (int dir = 0; dir < 2; dir++) {
+        const int ns = dir == 0 ? nb.f[mu] : nb.b[mu];
+        const C W = dir == 0 ? __ldg(u + (size_t)mu * g.v3 + site) : cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
+        C T[4];
 #pragma unroll
-      for (int d = 0; d < 4; d++) {
-        const GammaEntry ge = gamma_entry(mu, d);
-        const C w = R(0.5) * (A[d] + B[d]);
-        const C dd = gmul<C, R>(ge, A[ge.gin] - B[ge.gin]);
-        acc[d] = DAG ? ((acc[d] - w) - dd) : ((acc[d] - w) + dd);
+        for (int d = 0; d < 4; d++) T[d] = cmul(W, Rv(s, ns, d));
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+          const GammaEntry ge = gamma_entry(mu, d);
+          const C gt = gmul<C, R>(ge, T[ge.gin]);
+          // forward: + gamma (M), - gamma (M^dagger); backward: the opposite sign
+          acc[d] = ((dir == 0) != DAG) ? (acc[d] - R(0.5) * T[d]) + gt : (acc[d] - R(0.5) * T[d]) - gt;
+        }
       }
     }
   };
@@ -145,8 +150,12 @@ __global__ void __launch_bounds__(256) k_dslash_shamir(S* __restrict__ out, cons
       }
     }
   };
-  if (!DAG) { hop(); shop(); mass(); }
-  else { shop(); mass(); hop(); }
+  // the reference adds the hopping terms before (M) or after (M^dagger) the
+  // fifth-dimension and mass terms; the order only affects rounding, and
+  // doing the short terms first keeps fewer registers live
+  shop();
+  mass();
+  hop();
 #pragma unroll
   for (int d = 0; d < 4; d++) {
     St::st(out, sidx(g, s, site, d), acc[d]);
@@ -193,7 +202,8 @@ __global__ void __launch_bounds__(256) k_dslash_wilson(S* __restrict__ out, cons
   using C = typename St::C;
   const int s = threadIdx.x;
   double racc = 0.0;
-  for (int site = blockIdx.x * blockDim.y + threadIdx.y; site < g.v3; site += gridDim.x * blockDim.y) {
+  const int site = blockIdx.x * blockDim.y + threadIdx.y;
+  if (site < g.v3) {
   int x, y, t;
   site_coords(g, site, x, y, t);
   const Nbr nb = neighbours(g, x, y, t);
@@ -278,11 +288,11 @@ dim3 stencil_block(const Geom& g) {
   return dim3(g.ls, spb, 1);
 }
 
+// one block row per site: ceil(V3 / sites per block) blocks (each writes one
+// partial when an epilogue reduction is requested)
 unsigned stencil_grid(const Geom& g) {
   const dim3 blk = stencil_block(g);
-  unsigned need = (unsigned)((g.v3 + blk.y - 1) / blk.y);
-  const unsigned cap = 148 * 8;
-  return need < cap ? need : cap;
+  return (unsigned)((g.v3 + blk.y - 1) / blk.y);
 }
 
 template <class S>

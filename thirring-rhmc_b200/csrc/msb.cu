@@ -219,7 +219,7 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
       THR_TRY(launch_dslash_epi<V>(c->g, c->p.kernel, true, s, hv, (const typename Sto<V>::C*)u, am, imass,
                                    c->p.am3, c->st, &ms->done, p, c->partials));
       c->prof_end(pe);
-      k_alpha<<<1, kThreads, 0, c->st>>>(ms, hist, c->partials, gs);
+      k_alpha<<<1, 1024, 0, c->st>>>(ms, hist, c->partials, gs);
       k_rupdate<V><<<gb, kThreads, 0, c->st>>>(ms, rnew, rold, s, n, c->partials);
       k_lambda<<<1, kThreads, 0, c->st>>>(ms, hist, c->partials, gb);
       k_pupdate<V><<<gb, kThreads, 0, c->st>>>(ms, p, rnew, n);
