@@ -119,7 +119,7 @@ __global__ void k_converge(MsState* ms) {
 
 // replay the recorded steps on every shift field (:155-176 for each step)
 template <class V>
-__global__ void __launch_bounds__(kThreads) k_flush(MsState* ms, const MsHist* hist, V* out, V* sf, const V* ring,
+__global__ void __launch_bounds__(kThreads, 3) k_flush(MsState* ms, const MsHist* hist, V* out, V* sf, const V* ring,
                                                    int base, int ring_len, size_t n, size_t stride) {
   using R = typename W<V>::R;
   __shared__ R s_om[kBatch][kMaxShift], s_ga[kBatch][kMaxShift], s_ze[kBatch][kMaxShift];
@@ -144,24 +144,46 @@ __global__ void __launch_bounds__(kThreads) k_flush(MsState* ms, const MsHist* h
     s_hi[threadIdx.x] = hist->hi[threadIdx.x];
   }
   __syncthreads();
+  // each thread keeps the batch's residuals at its element in its own column of
+  // shared memory (no sharing, so no barrier), leaving registers for the shift
+  // fields of two shifts whose loads are then in flight together
+  extern __shared__ unsigned char s_dyn[];
+  V* s_r = reinterpret_cast<V*>(s_dyn);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    V rj[kBatch];
 #pragma unroll
     for (int j = 0; j < kBatch; j++)
-      if (j < ns) rj[j] = ring[(size_t)((base + 1 + j) % ring_len) * n + i];
-    for (int k = lo_u; k <= hi_u; k++) {
-      V o = out[k * stride + i];
-      V f = sf[k * stride + i];
+      if (j < ns) s_r[j * blockDim.x + threadIdx.x] = ring[(size_t)((base + 1 + j) % ring_len) * n + i];
+#define rj(j) s_r[(j) * blockDim.x + threadIdx.x]
+    for (int k0 = lo_u; k0 <= hi_u; k0 += 2) {
+      const bool two = k0 + 1 <= hi_u;
+      V o0 = out[k0 * stride + i], f0 = sf[k0 * stride + i];
+      V o1 = o0, f1 = f0;
+      if (two) {
+        o1 = out[(k0 + 1) * stride + i];
+        f1 = sf[(k0 + 1) * stride + i];
+      }
 #pragma unroll
       for (int j = 0; j < kBatch; j++) {
-        if (j < ns && k >= s_lo[j] && k <= s_hi[j]) {
-          o = o - s_om[j][k] * f;
-          f = s_ga[j][k] * f + s_ze[j][k] * rj[j];
+        if (j < ns) {
+          const V r = rj(j);
+          if (k0 >= s_lo[j] && k0 <= s_hi[j]) {
+            o0 = o0 - s_om[j][k0] * f0;
+            f0 = s_ga[j][k0] * f0 + s_ze[j][k0] * r;
+          }
+          if (two && k0 + 1 >= s_lo[j] && k0 + 1 <= s_hi[j]) {
+            o1 = o1 - s_om[j][k0 + 1] * f1;
+            f1 = s_ga[j][k0 + 1] * f1 + s_ze[j][k0 + 1] * r;
+          }
         }
       }
-      out[k * stride + i] = o;
-      sf[k * stride + i] = f;
+      out[k0 * stride + i] = o0;
+      sf[k0 * stride + i] = f0;
+      if (two) {
+        out[(k0 + 1) * stride + i] = o1;
+        sf[(k0 + 1) * stride + i] = f1;
+      }
     }
+#undef rj
   }
 }
 __global__ void k_reset(MsHist* hist) { hist->nsteps = 0; }
@@ -205,6 +227,8 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
   const bool sp = sizeof(V) == sizeof(float2);
   const V* u = sp ? (const V*)(const void*)c->u32 : (const V*)(const void*)c->u64;
   const unsigned gs = stencil_grid(c->g);
+  const size_t flush_smem = (size_t)kBatch * kThreads * sizeof(V);
+  THR_CUDA(cudaFuncSetAttribute(k_flush<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flush_smem));
   long long k = 0;
   for (;;) {
     const long long base = k;
@@ -226,7 +250,8 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
       k_converge<<<1, 1, 0, c->st>>>(ms);
     }
     int pe = c->prof_begin(thr_ctx::P_SHIFTUPD, 0);
-    k_flush<V><<<gb, kThreads, 0, c->st>>>(ms, hist, out, sf, ring, (int)(base % ring_len), ring_len, n, stride);
+    k_flush<V><<<gb, kThreads, flush_smem, c->st>>>(ms, hist, out, sf, ring, (int)(base % ring_len), ring_len, n,
+                                                     stride);
     c->prof_end(pe);
     k_reset<<<1, 1, 0, c->st>>>(hist);
     THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
