@@ -107,6 +107,27 @@ int thr_dslashd(thr_ctx *ctx, double *Phi, const double *R, const double *u, flo
 int thr_congrad(thr_ctx *ctx, const double *Phi, double *X, float res, int *itercg, float am, int imass,
                 int *iterations);
 
+/* congrad with no allocation at all -- no counterpart in the reference.
+ * For callers that cannot allocate device memory when they solve (their
+ * device footprint is fixed once their fields are placed, e.g. memory owned
+ * by an OpenACC/OpenMP runtime or a pool of their own, or they solve where an
+ * allocation is not allowed).  Phi, X (initial guess in, solution out) and u
+ * are the caller's device arrays in the device layout of this library for
+ * the lattice `p` describes: spinors complex(dp) [4][Lt][Ly][Lx][Ls] (site
+ * order per p->layout), links complex(dp) [3][V3].  The CG work vectors, the
+ * partial sums and the scalars live in one 32 MiB array that belongs to the
+ * library image (every GPU that loads the library holds it until exit), so
+ * 4 * 4*Ls*Lx*Ly*Lt * 16 bytes plus a few KB must fit in 32 MiB (for
+ * example 12^3 x 24 or 16^3 x 24); larger lattices return THR_ERR_BADSHAPE
+ * before anything runs.  The first call on a device looks the array's device
+ * address up (once per device); make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * threads, other streams) race and must be serialised by the caller.
+ * `stream` is a cudaStream_t (NULL = the legacy default stream); the call
+ * returns when the solve has finished.  Semantics otherwise as thr_congrad. */
+int thr_congrad_static(const thr_params *p, const void *u, const void *Phi, void *X, float res, int *itercg,
+                       float am, int imass, int *iterations, void *stream);
+
 /* ---- multishift_module.F90 ----------------------------------------------- */
 /* multishift_solver(u, am, imass, ndiagq, aden, anum, output, input, res,
  * maxcg, cg_return[, cg_returns]), multishift_module.F90:13-284: solves

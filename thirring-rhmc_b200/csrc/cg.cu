@@ -6,6 +6,8 @@
 // return immediately (each kernel tests `done` first).  Vector work per
 // iteration: x1 = M p | |x1|^2 | x2 = M^dagger x1 | r -= alpha x2, |r|^2 |
 // x += alpha p, p = r + beta p.
+#include <mutex>
+
 #include "ctx.h"
 #include "solver.h"
 
@@ -153,9 +155,108 @@ int congrad_dev(thr_ctx* c, const double2* Phi, double2* X, float res, float am,
   return h.capped ? THR_ERR_MAXITER : THR_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free congrad.  Some callers cannot allocate device memory at the
+// point where they solve: a code that must keep its device footprint fixed
+// once its fields are placed (memory handed out by its own pool or by an
+// OpenACC/OpenMP runtime, with nothing left for a library to cudaMalloc), or
+// one that solves where an allocation would synchronise the device or is not
+// permitted.  thr_congrad_static takes the fields on the device from the
+// caller and keeps everything else it needs -- the four CG work vectors, the
+// per-block partial sums and the recurrence scalars -- in one array that is
+// part of the library's image (a file-scope __device__ array), so the call
+// itself allocates nothing.
+namespace {
+constexpr size_t kStaticScratchBytes = size_t(32) << 20;  // 32 MiB on every device that loads the library
+constexpr int kStaticMaxDevices = 64;
+__device__ __align__(256) unsigned char g_cg_scratch[kStaticScratchBytes];
+std::mutex g_scratch_mu;
+unsigned char* g_scratch_dev[kStaticMaxDevices] = {};  // device address of g_cg_scratch, per device
+
+// device address of the scratch array on the current device (set up once per device)
+int static_scratch(unsigned char** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kStaticMaxDevices) return THR_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_dev[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_cg_scratch) != cudaSuccess || !p) return THR_ERR_CUDA;
+    g_scratch_dev[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_scratch_dev[dev];
+  return THR_OK;
+}
+inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+}  // namespace
+
 }  // namespace thr
 
 using namespace thr;
+
+extern "C" int thr_congrad_static(const thr_params* prm, const void* u, const void* Phi, void* X, float res,
+                                  int* itercg, float am, int imass, int* iterations, void* stream) {
+  if (!prm || !u || !Phi || !X) return THR_ERR_BADARG;
+  if (imass != 1 && imass != 3 && imass != 5) return THR_ERR_BADARG;
+  if (prm->kernel != 0 && prm->kernel != 1) return THR_ERR_BADARG;
+  if (prm->lx < 2 || prm->ly < 2 || prm->lt < 2 || prm->ls < 1 || prm->ls > 1024) return THR_ERR_BADSHAPE;
+  if (prm->layout == 1 && prm->lx % 2 != 0) return THR_ERR_BADSHAPE;
+  Geom g;
+  g.lx = prm->lx; g.ly = prm->ly; g.lt = prm->lt; g.ls = prm->ls;
+  g.v3 = prm->lx * prm->ly * prm->lt;
+  g.v5 = (long long)g.v3 * prm->ls;
+  g.layout = prm->layout;
+  g.hv3 = g.v3 / 2;
+  const size_t n = (size_t)g.v5 * 4;
+  const unsigned gb = vec_grid(n);
+  // scratch layout: state | partials | p | r | x1 | x2
+  const size_t off_parts = align256(sizeof(CgState));
+  const size_t off_vec = off_parts + align256((size_t)gb * sizeof(double));
+  const size_t vbytes = align256(n * sizeof(double2));
+  if (off_vec + 4 * vbytes > kStaticScratchBytes) return THR_ERR_BADSHAPE;  // lattice too large for the fixed scratch
+  unsigned char* base = nullptr;
+  THR_TRY(static_scratch(&base));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  CgState* cs = reinterpret_cast<CgState*>(base);
+  double* partials = reinterpret_cast<double*>(base + off_parts);
+  double2* p = reinterpret_cast<double2*>(base + off_vec);
+  double2* r = reinterpret_cast<double2*>(base + off_vec + vbytes);
+  double2* x1 = reinterpret_cast<double2*>(base + off_vec + 2 * vbytes);
+  double2* x2 = reinterpret_cast<double2*>(base + off_vec + 3 * vbytes);
+  const double2* ud = static_cast<const double2*>(u);
+  double2* Xd = static_cast<double2*>(X);
+  // every call starts from a freshly written state (the array keeps the last call's contents)
+  CgState h{};
+  int ivol = 4 * g.lx * g.ly * g.lt * g.ls;
+  float resid = ((float)ivol * res) * res;  // measure_module.F90:41
+  h.resid = (double)resid;
+  h.alpha = 1.0;
+  h.alphan = 0.0;
+  h.betacgd = 1.0;
+  h.niterc = g.ls * g.v3;  // params.F90:57
+  THR_CUDA(cudaMemcpyAsync(cs, &h, sizeof(CgState), cudaMemcpyHostToDevice, st));
+  THR_CUDA(cudaMemcpyAsync(p, Xd, n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+  THR_CUDA(cudaMemcpyAsync(r, Phi, n * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+  const int chunk = 8;
+  for (int base_it = 0; base_it < h.niterc + chunk; base_it += chunk) {
+    for (int k = 0; k < chunk; k++) {
+      THR_TRY(launch_dslash<double2>(g, prm->kernel, false, x1, p, ud, am, imass, prm->am3, st, &cs->done));
+      k_cg_norm2<<<gb, kThreads, 0, st>>>(cs, x1, n, partials);
+      k_cg_alpha<<<1, 1, 0, st>>>(cs, partials, gb);
+      THR_TRY(launch_dslash<double2>(g, prm->kernel, true, x2, x1, ud, am, imass, prm->am3, st, &cs->done));
+      k_cg_rupdate<<<gb, kThreads, 0, st>>>(cs, r, x2, n, partials);
+      k_cg_beta<<<1, 1, 0, st>>>(cs, partials, gb);
+      k_cg_xp<<<gb, kThreads, 0, st>>>(cs, Xd, p, r, n);
+      k_cg_latch<<<1, 1, 0, st>>>(cs);
+    }
+    THR_CUDA(cudaMemcpyAsync(&h, cs, sizeof(CgState), cudaMemcpyDeviceToHost, st));
+    THR_CUDA(cudaStreamSynchronize(st));
+    if (h.done) break;
+  }
+  if (itercg) *itercg = h.itercg;
+  if (iterations) *iterations = h.capped ? h.nx + 1 : h.nx;
+  if (h.status) return h.status;
+  return h.capped ? THR_ERR_MAXITER : THR_OK;
+}
 
 extern "C" int thr_congrad(thr_ctx* c, const double* Phi, double* X, float res, int* itercg, float am, int imass,
                            int* iterations) {

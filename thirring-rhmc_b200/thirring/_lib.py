@@ -41,6 +41,7 @@ SIGNATURES = {
     "thr_dslash": (_i, [_v, _v, _v, _v, _f, _i]),
     "thr_dslashd": (_i, [_v, _v, _v, _v, _f, _i]),
     "thr_congrad": (_i, [_v, _v, _v, _f, _pi, _f, _i, _pi]),
+    "thr_congrad_static": (_i, [C.POINTER(Params), _v, _v, _v, _f, _pi, _f, _i, _pi, _v]),
     "thr_multishift_solver": (_i, [_v, _v, _f, _i, _i, _v, _v, _v, _v, _f, _i, _pi, _v]),
     "thr_multishift_solver_sp": (_i, [_v, _v, _f, _i, _i, _v, _v, _v, _v, _f, _i, _pi, _v]),
     "thr_qmrherm": (_i, [_v, _v, _v, _f, _pi, _f, _i, _v, _v, _i, _i, _i, _v, _v, _v, _i]),
