@@ -128,6 +128,32 @@ int thr_congrad(thr_ctx *ctx, const double *Phi, double *X, float res, int *iter
 int thr_congrad_static(const thr_params *p, const void *u, const void *Phi, void *X, float res, int *itercg,
                        float am, int imass, int *iterations, void *stream);
 
+/* ---- batched measurement solves (no counterpart: the reference calls
+ * congrad once per source, measure_module.F90:278,338,848,902,1230) ------- */
+/* nrhs right-hand sides Phi(…, k) and guesses/solutions X(…, k) (consecutive
+ * halo'd spinors) on the context's lattice and links, solved together: one
+ * launch per operation for all of them, each with congrad's stopping rule
+ * |r|^2 < 4*V*Ls*res^2 checked on its FP64 true residual.  precision:
+ * THR_FP64, THR_MIXED_FP32 (FP32 correction solves, FP64 defect correction)
+ * or THR_MIXED_BF16 (BF16 stencil operands, FP32 arithmetic).  itercg[k]
+ * counts CG steps plus the FP64 residual passes; *outer the correction rounds. */
+int thr_congrad_multi(thr_ctx *ctx, const double *Phi, double *X, int nrhs, float res, float am, int imass,
+                      int precision, int *itercg, int *outer);
+/* the same on FP64 device fields (nrhs consecutive fields of the device layout) */
+int thr_congrad_multi_dev(thr_ctx *ctx, const void *Phi, void *X, int nrhs, float res, float am, int imass,
+                          int precision, int *itercg, int *outer);
+/* Independent lattices of uneven sizes (each with its own links) packed into
+ * one persistent stencil launch per operation.  All share the operator kind
+ * (p[i].kernel) and am3 of p[0]. */
+typedef struct thr_pack thr_pack;
+int thr_pack_create(int n, const thr_params *p, int device, thr_pack **pack);
+int thr_pack_destroy(thr_pack *pack);
+int thr_pack_upload(thr_pack *pack, int i, const double *u, const double *Phi, const double *X);
+int thr_pack_congrad(thr_pack *pack, float res, float am, int imass, int precision, int *itercg, int *outer);
+int thr_pack_download(thr_pack *pack, int i, double *X);
+int thr_pack_zero_x(thr_pack *pack);
+int thr_pack_get_stream(thr_pack *pack, void **stream);
+
 /* ---- multishift_module.F90 ----------------------------------------------- */
 /* multishift_solver(u, am, imass, ndiagq, aden, anum, output, input, res,
  * maxcg, cg_return[, cg_returns]), multishift_module.F90:13-284: solves

@@ -14,10 +14,10 @@
     cudaError_t e_ = (call);                           \
     if (e_ != cudaSuccess) return THR_ERR_CUDA;   \
   } while (0)
-#define THR_TRY(call)                 \
+#define THR_TRY(...)                  \
   do {                                \
-    int rc_ = (call);                 \
-    if (rc_ != THR_OK) return rc_; \
+    int rc_ = (__VA_ARGS__);          \
+    if (rc_ != THR_OK) return rc_;    \
   } while (0)
 
 struct thr_ctx {
@@ -60,6 +60,7 @@ struct thr_ctx {
     B_MDF,      // MD 3D fields: theta, thetat, pp (float) and dSdpi (double)
     B_HIST,     // batched multishift coefficient history
     B_RING,     // batched multishift residual ring
+    B_COEF,     // batched multishift folded coefficients
     B_COUNT = 16
   };
   // rational approximations (remez.F90, remezg.F90): anum has n+1 entries

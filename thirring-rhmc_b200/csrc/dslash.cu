@@ -16,6 +16,11 @@
 //   M^dag:  Phi(s)[P-] = D_W^dag Qm(s) + 2 R(s) - Qm(s),  Qm = R(s) + R(s-1) (wall z R(Ls))
 //           Phi(s)[P+] = D_W^dag Qp(s) + 2 R(s) - Qp(s),  Qp = R(s) + R(s+1) (wall z' R(1))
 // so the whole operator is again one pass over memory.
+//
+// The per-site arithmetic lives in shamir_site / wilson_site; the single-
+// lattice kernels and the batched kernel (many right-hand sides or many
+// lattices of different shapes in one persistent launch) share it.
+#include "batch.h"
 #include "thr_common.cuh"
 #include "thr_kernels.h"
 
@@ -41,7 +46,7 @@ __device__ __forceinline__ double epi_redot(const S* aux, size_t i, typename Sto
 }
 
 // one FP64 partial per block, fixed reduction order
-__device__ __forceinline__ void block_partial(double v, double* partials) {
+__device__ __forceinline__ void block_partial(double v, double* out) {
   __shared__ double sh[32];
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
   const int nthr = blockDim.x * blockDim.y;
@@ -54,115 +59,89 @@ __device__ __forceinline__ void block_partial(double v, double* partials) {
     v = tid < nw ? sh[tid] : 0.0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (tid == 0) partials[blockIdx.x] = v;
+    if (tid == 0) *out = v;
   }
+  __syncthreads();
 }
 
 // ---------------------------------------------------------------- Shamir
-template <class S, bool DAG, int EPI>
-__global__ void __launch_bounds__(256, 4) k_dslash_shamir(S* __restrict__ out, const S* __restrict__ in,
-                                                       const typename Sto<S>::C* __restrict__ u, Geom g,
-                                                       float am, int imass, float am3, const int* skip,
-                                                       const S* __restrict__ aux, double* __restrict__ partials) {
-  if (skip && *skip) return;
-  using St = Sto<S>;
-  using R = typename St::R;
-  using C = typename St::C;
-  const int s = threadIdx.x;
-  double racc = 0.0;
-  const int site = blockIdx.x * blockDim.y + threadIdx.y;
-  if (site < g.v3) {
+template <class S, bool DAG>
+__device__ __forceinline__ void shamir_site(const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u,
+                                            const Geom& g, int s, int site, float am, int imass, float am3,
+                                            typename Sto<S>::C* acc) {
+  using R = typename Sto<S>::R;
+  using C = typename Sto<S>::C;
   int x, y, t;
   site_coords(g, site, x, y, t);
   const Nbr nb = neighbours(g, x, y, t);
   SpinorView<S> Rv{in, g};
   const int Ls = g.ls;
-
-  C acc[4];
   const R diag = (R)((3.0f - am3) + 1.0f);  // dirac.F90:45, default real
 #pragma unroll
   for (int d = 0; d < 4; d++) acc[d] = diag * Rv(s, site, d);
-
-  // Wilson and Dirac hopping terms.  The forward (U R(x+mu)) and backward
-  // (conj U(x-mu) R(x-mu)) halves are accumulated one after the other, so
-  // only one neighbour's four spins are live at a time (register pressure,
-  // hence occupancy): acc -= 1/2 T(d) +/- gamma(mu,d) T(gin) per half.
-  auto hop = [&]() {
-#pragma unroll
-    for (int mu = 0; mu < 3; mu++) {
-#pragma unroll
-      for (int dir = 0; dir < 2; dir++) {
-        const int ns = dir == 0 ? nb.f[mu] : nb.b[mu];
-        const C W = dir == 0 ? __ldg(u + (size_t)mu * g.v3 + site) : cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
-        C T[4];
-#pragma unroll
-        for (int d = 0; d < 4; d++) T[d] = cmul(W, Rv(s, ns, d));
-#pragma unroll
-        for (int d = 0; d < 4; d++) {
-          const GammaEntry ge = gamma_entry(mu, d);
-          const C gt = gmul<C, R>(ge, T[ge.gin]);
-          // forward: + gamma (M), - gamma (M^dagger); backward: the opposite sign
-          acc[d] = ((dir == 0) != DAG) ? (acc[d] - R(0.5) * T[d]) + gt : (acc[d] - R(0.5) * T[d]) - gt;
-        }
-      }
-    }
-  };
   // s-like term (np_third == 1): dirac.F90:80-87 (M), :317-324 (M^dagger)
-  auto shop = [&]() {
-    if (!DAG) {
-      if (s < Ls - 1) { acc[2] = acc[2] - Rv(s + 1, site, 2); acc[3] = acc[3] - Rv(s + 1, site, 3); }
-      if (s > 0) { acc[0] = acc[0] - Rv(s - 1, site, 0); acc[1] = acc[1] - Rv(s - 1, site, 1); }
-    } else {
-      if (s < Ls - 1) { acc[0] = acc[0] - Rv(s + 1, site, 0); acc[1] = acc[1] - Rv(s + 1, site, 1); }
-      if (s > 0) { acc[2] = acc[2] - Rv(s - 1, site, 2); acc[3] = acc[3] - Rv(s - 1, site, 3); }
-    }
-  };
+  if (!DAG) {
+    if (s < Ls - 1) { acc[2] = acc[2] - Rv(s + 1, site, 2); acc[3] = acc[3] - Rv(s + 1, site, 3); }
+    if (s > 0) { acc[0] = acc[0] - Rv(s - 1, site, 0); acc[1] = acc[1] - Rv(s - 1, site, 1); }
+  } else {
+    if (s < Ls - 1) { acc[0] = acc[0] - Rv(s + 1, site, 0); acc[1] = acc[1] - Rv(s + 1, site, 1); }
+    if (s > 0) { acc[2] = acc[2] - Rv(s - 1, site, 2); acc[3] = acc[3] - Rv(s - 1, site, 3); }
+  }
   // wall mass term: dirac.F90:119-176 (M), :356-402 (M^dagger)
-  auto mass = [&]() {
-    const R a = (R)am;
-    if (!DAG) {
-      if (imass == 1) {
-        const C zk = mk(a, R(0));
-        if (s == Ls - 1) { acc[2] = acc[2] + cmul(zk, Rv(0, site, 2)); acc[3] = acc[3] + cmul(zk, Rv(0, site, 3)); }
-        if (s == 0) { acc[0] = acc[0] + cmul(zk, Rv(Ls - 1, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(Ls - 1, site, 1)); }
-      } else if (imass == 3) {
-        const C zk = mk(R(0), -a);
-        if (s == Ls - 1) { acc[2] = acc[2] - cmul(zk, Rv(0, site, 2)); acc[3] = acc[3] - cmul(zk, Rv(0, site, 3)); }
-        if (s == 0) { acc[0] = acc[0] + cmul(zk, Rv(Ls - 1, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(Ls - 1, site, 1)); }
-      } else if (imass == 5) {
-        const C zk = mk(R(0), -a);
-        if (s == Ls - 1) { acc[2] = acc[2] - cmul(zk, Rv(Ls - 1, site, 0)); acc[3] = acc[3] - cmul(zk, Rv(Ls - 1, site, 1)); }
-        if (s == 0) { acc[0] = acc[0] - cmul(zk, Rv(0, site, 2)); acc[1] = acc[1] - cmul(zk, Rv(0, site, 3)); }
-      }
-    } else {
-      if (imass == 1) {
-        const C zk = mk(a, R(0));
-        if (s == Ls - 1) { acc[0] = acc[0] + cmul(zk, Rv(0, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(0, site, 1)); }
-        if (s == 0) { acc[2] = acc[2] + cmul(zk, Rv(Ls - 1, site, 2)); acc[3] = acc[3] + cmul(zk, Rv(Ls - 1, site, 3)); }
-      } else if (imass == 3) {
-        const C zk = mk(R(0), a);
-        if (s == Ls - 1) { acc[0] = acc[0] + cmul(zk, Rv(0, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(0, site, 1)); }
-        if (s == 0) { acc[2] = acc[2] - cmul(zk, Rv(Ls - 1, site, 2)); acc[3] = acc[3] - cmul(zk, Rv(Ls - 1, site, 3)); }
-      } else if (imass == 5) {
-        const C zk = mk(R(0), a);
-        if (s == Ls - 1) { acc[0] = acc[0] - cmul(zk, Rv(Ls - 1, site, 2)); acc[1] = acc[1] - cmul(zk, Rv(Ls - 1, site, 3)); }
-        if (s == 0) { acc[2] = acc[2] - cmul(zk, Rv(0, site, 0)); acc[3] = acc[3] - cmul(zk, Rv(0, site, 1)); }
+  const R a = (R)am;
+  if (!DAG) {
+    if (imass == 1) {
+      const C zk = mk(a, R(0));
+      if (s == Ls - 1) { acc[2] = acc[2] + cmul(zk, Rv(0, site, 2)); acc[3] = acc[3] + cmul(zk, Rv(0, site, 3)); }
+      if (s == 0) { acc[0] = acc[0] + cmul(zk, Rv(Ls - 1, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(Ls - 1, site, 1)); }
+    } else if (imass == 3) {
+      const C zk = mk(R(0), -a);
+      if (s == Ls - 1) { acc[2] = acc[2] - cmul(zk, Rv(0, site, 2)); acc[3] = acc[3] - cmul(zk, Rv(0, site, 3)); }
+      if (s == 0) { acc[0] = acc[0] + cmul(zk, Rv(Ls - 1, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(Ls - 1, site, 1)); }
+    } else if (imass == 5) {
+      const C zk = mk(R(0), -a);
+      if (s == Ls - 1) { acc[2] = acc[2] - cmul(zk, Rv(Ls - 1, site, 0)); acc[3] = acc[3] - cmul(zk, Rv(Ls - 1, site, 1)); }
+      if (s == 0) { acc[0] = acc[0] - cmul(zk, Rv(0, site, 2)); acc[1] = acc[1] - cmul(zk, Rv(0, site, 3)); }
+    }
+  } else {
+    if (imass == 1) {
+      const C zk = mk(a, R(0));
+      if (s == Ls - 1) { acc[0] = acc[0] + cmul(zk, Rv(0, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(0, site, 1)); }
+      if (s == 0) { acc[2] = acc[2] + cmul(zk, Rv(Ls - 1, site, 2)); acc[3] = acc[3] + cmul(zk, Rv(Ls - 1, site, 3)); }
+    } else if (imass == 3) {
+      const C zk = mk(R(0), a);
+      if (s == Ls - 1) { acc[0] = acc[0] + cmul(zk, Rv(0, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(0, site, 1)); }
+      if (s == 0) { acc[2] = acc[2] - cmul(zk, Rv(Ls - 1, site, 2)); acc[3] = acc[3] - cmul(zk, Rv(Ls - 1, site, 3)); }
+    } else if (imass == 5) {
+      const C zk = mk(R(0), a);
+      if (s == Ls - 1) { acc[0] = acc[0] - cmul(zk, Rv(Ls - 1, site, 2)); acc[1] = acc[1] - cmul(zk, Rv(Ls - 1, site, 3)); }
+      if (s == 0) { acc[2] = acc[2] - cmul(zk, Rv(0, site, 0)); acc[3] = acc[3] - cmul(zk, Rv(0, site, 1)); }
+    }
+  }
+  // Wilson and Dirac hopping terms (dirac.F90:49-76, :464-491).  The forward
+  // (U R(x+mu)) and backward (conj U(x-mu) R(x-mu)) halves are accumulated one
+  // after the other, so only one neighbour's four spins are live at a time
+  // (register pressure, hence occupancy): acc -= 1/2 T(d) +/- gamma(mu,d) T(gin).
+  // The reference adds these before (M) or after (M^dagger) the fifth-
+  // dimension and mass terms; the order only affects rounding.
+#pragma unroll
+  for (int mu = 0; mu < 3; mu++) {
+#pragma unroll
+    for (int dir = 0; dir < 2; dir++) {
+      const int ns = dir == 0 ? nb.f[mu] : nb.b[mu];
+      const C W = dir == 0 ? __ldg(u + (size_t)mu * g.v3 + site) : cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
+      C T[4];
+#pragma unroll
+      for (int d = 0; d < 4; d++) T[d] = cmul(W, Rv(s, ns, d));
+#pragma unroll
+      for (int d = 0; d < 4; d++) {
+        const GammaEntry ge = gamma_entry(mu, d);
+        const C gt = gmul<C, R>(ge, T[ge.gin]);
+        // forward: + gamma (M), - gamma (M^dagger); backward: the opposite sign
+        acc[d] = ((dir == 0) != DAG) ? (acc[d] - R(0.5) * T[d]) + gt : (acc[d] - R(0.5) * T[d]) - gt;
       }
     }
-  };
-  // the reference adds the hopping terms before (M) or after (M^dagger) the
-  // fifth-dimension and mass terms; the order only affects rounding, and
-  // doing the short terms first keeps fewer registers live
-  shop();
-  mass();
-  hop();
-#pragma unroll
-  for (int d = 0; d < 4; d++) {
-    St::st(out, sidx(g, s, site, d), acc[d]);
-    if (EPI == 1) racc += epi_redot<S>(aux, sidx(g, s, site, d), acc[d]);
   }
-  }
-  if (EPI == 1) block_partial(racc, partials);
 }
 
 // ---------------------------------------------------------------- Wilson
@@ -191,19 +170,12 @@ __device__ __forceinline__ void wilson_qd(const SpinorView<S>& Rv, int s, int si
   for (int d = 0; d < 4; d++) q[d] = inner ? Rv(s, site, d) + Rv(sn, site, d) : Rv(s, site, d) + cmul(z, Rv(swall, site, d));
 }
 
-template <class S, bool DAG, int EPI>
-__global__ void __launch_bounds__(256) k_dslash_wilson(S* __restrict__ out, const S* __restrict__ in,
-                                                       const typename Sto<S>::C* __restrict__ u, Geom g,
-                                                       float am, int imass, float am3, const int* skip,
-                                                       const S* __restrict__ aux, double* __restrict__ partials) {
-  if (skip && *skip) return;
-  using St = Sto<S>;
-  using R = typename St::R;
-  using C = typename St::C;
-  const int s = threadIdx.x;
-  double racc = 0.0;
-  const int site = blockIdx.x * blockDim.y + threadIdx.y;
-  if (site < g.v3) {
+template <class S, bool DAG>
+__device__ __forceinline__ void wilson_site(const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u,
+                                            const Geom& g, int s, int site, float am, int imass, float am3,
+                                            typename Sto<S>::C* res) {
+  using R = typename Sto<S>::R;
+  using C = typename Sto<S>::C;
   int x, y, t;
   site_coords(g, site, x, y, t);
   const Nbr nb = neighbours(g, x, y, t);
@@ -211,8 +183,6 @@ __global__ void __launch_bounds__(256) k_dslash_wilson(S* __restrict__ out, cons
   const int Ls = g.ls;
   const R a = (R)am;
   const R dgw = (R)(3.0f + (-am3));  // DWilson(…, -am3) diagonal: dirac.F90:191, :505
-  C res[4];
-
   if (!DAG) {
     // c1 = -am | -i am  (dirac.F90:274-278),  c2 = -am | +i am  (dirac.F90:287-291)
     const C c1 = imass == 1 ? mk(-a, R(0)) : mk(R(0), -a);
@@ -272,13 +242,73 @@ __global__ void __launch_bounds__(256) k_dslash_wilson(S* __restrict__ out, cons
       }
     }
   }
+}
+
+template <class S, int KER, bool DAG>
+__device__ __forceinline__ void apply_site(const S* in, const typename Sto<S>::C* u, const Geom& g, int s, int site,
+                                           float am, int imass, float am3, typename Sto<S>::C* acc) {
+  if (KER == 0) shamir_site<S, DAG>(in, u, g, s, site, am, imass, am3, acc);
+  else wilson_site<S, DAG>(in, u, g, s, site, am, imass, am3, acc);
+}
+
+// ---------------------------------------------------------------- kernels
+template <class S, int KER, bool DAG, int EPI>
+__global__ void __launch_bounds__(256, KER == 0 ? 4 : 1) k_dslash(S* __restrict__ out, const S* __restrict__ in,
+                                                                 const typename Sto<S>::C* __restrict__ u, Geom g,
+                                                                 float am, int imass, float am3, const int* skip,
+                                                                 const S* __restrict__ aux, double* __restrict__ partials) {
+  if (skip && *skip) return;
+  using C = typename Sto<S>::C;
+  const int s = threadIdx.x;
+  double racc = 0.0;
+  const int site = blockIdx.x * blockDim.y + threadIdx.y;
+  if (site < g.v3) {
+    C acc[4];
+    apply_site<S, KER, DAG>(in, u, g, s, site, am, imass, am3, acc);
 #pragma unroll
-  for (int d = 0; d < 4; d++) {
-    St::st(out, sidx(g, s, site, d), res[d]);
-    if (EPI == 1) racc += epi_redot<S>(aux, sidx(g, s, site, d), res[d]);
+    for (int d = 0; d < 4; d++) {
+      Sto<S>::st(out, sidx(g, s, site, d), acc[d]);
+      if (EPI == 1) racc += epi_redot<S>(aux, sidx(g, s, site, d), acc[d]);
+    }
   }
+  if (EPI == 1) block_partial(racc, partials + blockIdx.x);
+}
+
+// Batched stencil: a persistent grid walks the work blocks of all entries
+// (right-hand sides or lattices).  Work block wb belongs to the entry e with
+// blk0[e] <= wb < blk0[e+1]; inside it, thread tid handles s = tid % Ls of
+// site (wb - blk0) * spb + tid / Ls.  Entries with skip[e] set are passed over.
+template <class S, int KER, bool DAG, int EPI>
+__global__ void __launch_bounds__(256, KER == 0 ? 4 : 1)
+    k_dslash_batch(S* __restrict__ out, const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u,
+                   const BatchEntry* __restrict__ tab, int nent, int total_blocks, float am, int imass, float am3,
+                   const int* skip, const S* __restrict__ aux, double* __restrict__ partials) {
+  using C = typename Sto<S>::C;
+  for (int wb = blockIdx.x; wb < total_blocks; wb += gridDim.x) {
+    int lo = 0, hi = nent - 1;  // last entry with blk0 <= wb
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (tab[mid].blk0 <= wb) lo = mid;
+      else hi = mid - 1;
+    }
+    const BatchEntry& E = tab[lo];
+    if (skip && skip[lo]) continue;
+    const Geom g = E.g;
+    const int s = threadIdx.x % g.ls;
+    const int sub = threadIdx.x / g.ls;
+    const int site = (wb - E.blk0) * E.spb + sub;
+    double racc = 0.0;
+    if (sub < E.spb && site < g.v3) {
+      C acc[4];
+      apply_site<S, KER, DAG>(in + E.off, u + E.uoff, g, s, site, am, imass, am3, acc);
+#pragma unroll
+      for (int d = 0; d < 4; d++) {
+        Sto<S>::st(out + E.off, sidx(g, s, site, d), acc[d]);
+        if (EPI == 1) racc += epi_redot<S>(aux + E.off, sidx(g, s, site, d), acc[d]);
+      }
+    }
+    if (EPI == 1) block_partial(racc, partials + wb);
   }
-  if (EPI == 1) block_partial(racc, partials);
 }
 
 // ---------------------------------------------------------------- launch
@@ -299,19 +329,19 @@ template <class S>
 int launch_dslash_epi(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
                       int imass, float am3, cudaStream_t st, const int* skip, const S* aux, double* partials) {
   if (g.ls > 1024) return THR_ERR_BADSHAPE;
+  if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
   const dim3 blk = stencil_block(g);
   const dim3 grd(stencil_grid(g));
   const bool epi = aux != nullptr;
-#define THR_LAUNCH(KER, D, E) KER<S, D, E><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, partials)
+#define THR_L(K, D, E) k_dslash<S, K, D, E><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, partials)
   if (kernel == 1) {
-    if (imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
-    if (dag) { if (epi) THR_LAUNCH(k_dslash_wilson, true, 1); else THR_LAUNCH(k_dslash_wilson, true, 0); }
-    else { if (epi) THR_LAUNCH(k_dslash_wilson, false, 1); else THR_LAUNCH(k_dslash_wilson, false, 0); }
+    if (dag) { if (epi) THR_L(1, true, 1); else THR_L(1, true, 0); }
+    else { if (epi) THR_L(1, false, 1); else THR_L(1, false, 0); }
   } else {
-    if (dag) { if (epi) THR_LAUNCH(k_dslash_shamir, true, 1); else THR_LAUNCH(k_dslash_shamir, true, 0); }
-    else { if (epi) THR_LAUNCH(k_dslash_shamir, false, 1); else THR_LAUNCH(k_dslash_shamir, false, 0); }
+    if (dag) { if (epi) THR_L(0, true, 1); else THR_L(0, true, 0); }
+    else { if (epi) THR_L(0, false, 1); else THR_L(0, false, 0); }
   }
-#undef THR_LAUNCH
+#undef THR_L
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
 
@@ -321,11 +351,34 @@ int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, cons
   return launch_dslash_epi<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr);
 }
 
+template <class S>
+int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
+                        float am, int imass, float am3, cudaStream_t st, const int* skip, const S* aux,
+                        double* partials, int grid) {
+  if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;
+  const bool epi = aux != nullptr;
+  const int g = grid > 0 ? grid : (b.total_blocks < 148 * 8 ? b.total_blocks : 148 * 8);
+#define THR_L(K, D, E)                                                                                          \
+  k_dslash_batch<S, K, D, E><<<g, 256, 0, st>>>(out, in, u, b.dev, b.nent, b.total_blocks, am, imass, am3, skip, \
+                                                aux, partials)
+  if (kernel == 1) {
+    if (dag) { if (epi) THR_L(1, true, 1); else THR_L(1, true, 0); }
+    else { if (epi) THR_L(1, false, 1); else THR_L(1, false, 0); }
+  } else {
+    if (dag) { if (epi) THR_L(0, true, 1); else THR_L(0, true, 0); }
+    else { if (epi) THR_L(0, false, 1); else THR_L(0, false, 0); }
+  }
+#undef THR_L
+  return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+
 #define THR_INST(S, L)                                                                                            \
   template int launch_dslash<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float, cudaStream_t,   \
                                 const int*);                                                                      \
   template int launch_dslash_epi<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,            \
-                                    cudaStream_t, const int*, const S*, double*);
+                                    cudaStream_t, const int*, const S*, double*);                                 \
+  template int launch_dslash_batch<S>(const BatchTable&, int, bool, S*, const S*, const L*, float, int, float,    \
+                                      cudaStream_t, const int*, const S*, double*, int);
 THR_INST(double2, double2)
 THR_INST(float2, float2)
 THR_INST(__nv_bfloat162, float2)

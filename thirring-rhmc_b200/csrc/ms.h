@@ -80,6 +80,12 @@ struct MsHist {
   double om[kBatch][kMaxShift], ga[kBatch][kMaxShift], ze[kBatch][kMaxShift];
 };
 
+// a batch's recorded steps folded into one affine map per shift (see msb.cu)
+struct MsCoef {
+  int ns, lo, hi, pad;
+  double A[kMaxShift], P[kMaxShift], B[kMaxShift][kBatch], Q[kMaxShift][kBatch];
+};
+
 template <class V>
 int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p, V* hv, V* s, int ndiagq,
                            const double* aden, const double* anum, float res, float am, int imass, int maxcg,

@@ -6,14 +6,14 @@
 // :155-176).  Here each iteration only writes its new residual r_k into a
 // ring of kBatch+1 fields and records the iteration's per-shift
 // coefficients (omegas, gammas, zeta_iii and the active window); every
-// kBatch iterations one kernel replays those kBatch updates for all shifts
-// while each shift field is in registers:
+// kBatch iterations the recorded updates
 //     for j in batch:  out -= om_j * sf ;  sf = ga_j * sf + ze_j * r_j
-// which is the reference's per-element operation sequence, so the results
-// equal the per-iteration form.  Traffic per iteration drops from
-// (3 + 4 n_active) to about (1 + 4 n_active / kBatch) fields.  In addition
-// alpha = Re<p, M^dagger M p> is accumulated in the epilogue of the M^dagger
-// stencil, so s is not re-read.
+// are folded per shift into one affine map of the batch's start values
+// (k_flush_coef) and applied in one pass over the shift fields (k_flush).
+// The algebra is that of the per-iteration form; only the rounding order
+// differs.  Traffic per iteration drops from (3 + 4 n_active) to about
+// (1 + 4 n_active / kBatch) fields.  In addition alpha = Re<p, M^dagger M p>
+// is accumulated in the epilogue of the M^dagger stencil, so s is not re-read.
 #include <cmath>
 #include <cstring>
 
@@ -117,73 +117,93 @@ __global__ void k_converge(MsState* ms) {
   ms_converge_step(ms);
 }
 
-// replay the recorded steps on every shift field (:155-176 for each step)
-template <class V>
-__global__ void __launch_bounds__(kThreads, 3) k_flush(MsState* ms, const MsHist* hist, V* out, V* sf, const V* ring,
-                                                   int base, int ring_len, size_t n, size_t stride) {
-  using R = typename W<V>::R;
-  __shared__ R s_om[kBatch][kMaxShift], s_ga[kBatch][kMaxShift], s_ze[kBatch][kMaxShift];
-  __shared__ int s_lo[kBatch], s_hi[kBatch];
+// Fold each shift's recorded steps (:155-176 once per step) into one affine map
+// of the batch's start values: with f = sf, o = out,
+//   step j (if shift k is in that step's window):  o -= om_j f ;  f = ga_j f + ze_j r_j
+// gives  f_end = A f_0 + sum_i B_i r_i   and   o_end = o_0 - P f_0 - sum_i Q_i r_i.
+// One thread per shift; the map is exact algebra, only the rounding differs.
+__global__ void k_flush_coef(MsState* ms, const MsHist* hist, MsCoef* cf) {
   const int ns = hist->nsteps;
+  const int k = threadIdx.x;
+  if (k == 0) {
+    int lo_u = kMaxShift, hi_u = -1;
+    for (int j = 0; j < ns; j++) {
+      lo_u = min(lo_u, hist->lo[j]);
+      hi_u = max(hi_u, hist->hi[j]);
+    }
+    cf->ns = ns;
+    cf->lo = lo_u;
+    cf->hi = hi_u;
+    if (ns > 0) ms->flush_fields += (double)(ns + 4 * (hi_u - lo_u + 1));
+  }
+  if (k >= kMaxShift) return;
+  double A = 1.0, P = 0.0, B[kBatch], Q[kBatch];
+#pragma unroll
+  for (int i = 0; i < kBatch; i++) B[i] = Q[i] = 0.0;
+#pragma unroll
+  for (int j = 0; j < kBatch; j++) {
+    if (j < ns && k >= hist->lo[j] && k <= hist->hi[j]) {
+      const double om = hist->om[j][k], ga = hist->ga[j][k], ze = hist->ze[j][k];
+      P += om * A;
+#pragma unroll
+      for (int i = 0; i < kBatch; i++)
+        if (i < j) Q[i] += om * B[i];
+      A = ga * A;
+#pragma unroll
+      for (int i = 0; i < kBatch; i++)
+        if (i < j) B[i] = ga * B[i];
+      B[j] = ze;
+    }
+  }
+  cf->A[k] = A;
+  cf->P[k] = P;
+#pragma unroll
+  for (int i = 0; i < kBatch; i++) {
+    cf->B[k][i] = B[i];
+    cf->Q[k][i] = Q[i];
+  }
+}
+
+// apply the folded maps to every shift field of the batch's window
+template <class V>
+__global__ void __launch_bounds__(kThreads) k_flush(const MsCoef* cf, V* __restrict__ out, V* __restrict__ sf,
+                                                   const V* __restrict__ ring, int base, int ring_len, size_t n,
+                                                   size_t stride) {
+  using R = typename W<V>::R;
+  const int ns = cf->ns;
   if (ns == 0) return;
-  int lo_u = kMaxShift, hi_u = -1;
-  for (int j = 0; j < ns; j++) {
-    lo_u = min(lo_u, hist->lo[j]);
-    hi_u = max(hi_u, hist->hi[j]);
-  }
-  for (int t = threadIdx.x; t < ns * kMaxShift; t += blockDim.x) {
-    const int j = t / kMaxShift, k = t % kMaxShift;
-    const bool act = k >= hist->lo[j] && k <= hist->hi[j];
-    s_om[j][k] = act ? W<V>::cast(hist->om[j][k]) : R(0);
-    s_ga[j][k] = act ? W<V>::cast(hist->ga[j][k]) : R(0);
-    s_ze[j][k] = act ? W<V>::cast(hist->ze[j][k]) : R(0);
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) ms->flush_fields += (double)(ns + 4 * (hi_u - lo_u + 1));
-  if (threadIdx.x < ns) {
-    s_lo[threadIdx.x] = hist->lo[threadIdx.x];
-    s_hi[threadIdx.x] = hist->hi[threadIdx.x];
+  const int lo = cf->lo, hi = cf->hi;
+  __shared__ R s_A[kMaxShift], s_P[kMaxShift], s_B[kMaxShift][kBatch], s_Q[kMaxShift][kBatch];
+  for (int t = threadIdx.x; t < kMaxShift * kBatch; t += blockDim.x) {
+    const int k = t / kBatch, i = t % kBatch;
+    s_B[k][i] = (R)cf->B[k][i];
+    s_Q[k][i] = (R)cf->Q[k][i];
+    if (i == 0) {
+      s_A[k] = (R)cf->A[k];
+      s_P[k] = (R)cf->P[k];
+    }
   }
   __syncthreads();
-  // each thread keeps the batch's residuals at its element in its own column of
-  // shared memory (no sharing, so no barrier), leaving registers for the shift
-  // fields of two shifts whose loads are then in flight together
-  extern __shared__ unsigned char s_dyn[];
-  V* s_r = reinterpret_cast<V*>(s_dyn);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    V rj[kBatch];
 #pragma unroll
     for (int j = 0; j < kBatch; j++)
-      if (j < ns) s_r[j * blockDim.x + threadIdx.x] = ring[(size_t)((base + 1 + j) % ring_len) * n + i];
-#define rj(j) s_r[(j) * blockDim.x + threadIdx.x]
-    for (int k0 = lo_u; k0 <= hi_u; k0 += 2) {
-      const bool two = k0 + 1 <= hi_u;
-      V o0 = out[k0 * stride + i], f0 = sf[k0 * stride + i];
-      V o1 = o0, f1 = f0;
-      if (two) {
-        o1 = out[(k0 + 1) * stride + i];
-        f1 = sf[(k0 + 1) * stride + i];
-      }
+      if (j < ns) rj[j] = ring[(size_t)((base + 1 + j) % ring_len) * n + i];
+    for (int k = lo; k <= hi; k++) {
+      const V f0 = sf[k * stride + i];
+      const V o0 = out[k * stride + i];
+      V f = s_A[k] * f0;
+      V o = o0 - s_P[k] * f0;
 #pragma unroll
       for (int j = 0; j < kBatch; j++) {
         if (j < ns) {
-          const V r = rj(j);
-          if (k0 >= s_lo[j] && k0 <= s_hi[j]) {
-            o0 = o0 - s_om[j][k0] * f0;
-            f0 = s_ga[j][k0] * f0 + s_ze[j][k0] * r;
-          }
-          if (two && k0 + 1 >= s_lo[j] && k0 + 1 <= s_hi[j]) {
-            o1 = o1 - s_om[j][k0 + 1] * f1;
-            f1 = s_ga[j][k0 + 1] * f1 + s_ze[j][k0 + 1] * r;
-          }
+          f = f + s_B[k][j] * rj[j];
+          o = o - s_Q[k][j] * rj[j];
         }
       }
-      out[k0 * stride + i] = o0;
-      sf[k0 * stride + i] = f0;
-      if (two) {
-        out[(k0 + 1) * stride + i] = o1;
-        sf[(k0 + 1) * stride + i] = f1;
-      }
+      sf[k * stride + i] = f;
+      out[k * stride + i] = o;
     }
-#undef rj
   }
 }
 __global__ void k_reset(MsHist* hist) { hist->nsteps = 0; }
@@ -215,6 +235,9 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
   void* hv_;
   THR_TRY(c->buffer(thr_ctx::B_HIST, sizeof(MsHist), &hv_));
   MsHist* hist = (MsHist*)hv_;
+  void* cf_;
+  THR_TRY(c->buffer(thr_ctx::B_COEF, sizeof(MsCoef), &cf_));
+  MsCoef* cf = (MsCoef*)cf_;
   THR_TRY(ms_prepare_state(c, h, ndiagq, aden, anum, res, maxcg));
   THR_CUDA(cudaMemcpyAsync(ms, h, sizeof(MsState), cudaMemcpyHostToDevice, c->st));
   THR_CUDA(cudaMemcpyAsync(ring, in, n * sizeof(V), cudaMemcpyDeviceToDevice, c->st));  // r = input (slot 0)
@@ -227,8 +250,6 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
   const bool sp = sizeof(V) == sizeof(float2);
   const V* u = sp ? (const V*)(const void*)c->u32 : (const V*)(const void*)c->u64;
   const unsigned gs = stencil_grid(c->g);
-  const size_t flush_smem = (size_t)kBatch * kThreads * sizeof(V);
-  THR_CUDA(cudaFuncSetAttribute(k_flush<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flush_smem));
   long long k = 0;
   for (;;) {
     const long long base = k;
@@ -250,8 +271,8 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
       k_converge<<<1, 1, 0, c->st>>>(ms);
     }
     int pe = c->prof_begin(thr_ctx::P_SHIFTUPD, 0);
-    k_flush<V><<<gb, kThreads, flush_smem, c->st>>>(ms, hist, out, sf, ring, (int)(base % ring_len), ring_len, n,
-                                                     stride);
+    k_flush_coef<<<1, kMaxShift, 0, c->st>>>(ms, hist, cf);
+    k_flush<V><<<gb, kThreads, 0, c->st>>>(cf, out, sf, ring, (int)(base % ring_len), ring_len, n, stride);
     c->prof_end(pe);
     k_reset<<<1, 1, 0, c->st>>>(hist);
     THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));

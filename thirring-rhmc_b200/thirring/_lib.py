@@ -42,6 +42,15 @@ SIGNATURES = {
     "thr_dslashd": (_i, [_v, _v, _v, _v, _f, _i]),
     "thr_congrad": (_i, [_v, _v, _v, _f, _pi, _f, _i, _pi]),
     "thr_congrad_static": (_i, [C.POINTER(Params), _v, _v, _v, _f, _pi, _f, _i, _pi, _v]),
+    "thr_congrad_multi": (_i, [_v, _v, _v, _i, _f, _f, _i, _i, _v, _pi]),
+    "thr_congrad_multi_dev": (_i, [_v, _v, _v, _i, _f, _f, _i, _i, _v, _pi]),
+    "thr_pack_create": (_i, [_i, C.POINTER(Params), _i, C.POINTER(_v)]),
+    "thr_pack_destroy": (_i, [_v]),
+    "thr_pack_upload": (_i, [_v, _i, _v, _v, _v]),
+    "thr_pack_congrad": (_i, [_v, _f, _f, _i, _i, _v, _pi]),
+    "thr_pack_download": (_i, [_v, _i, _v]),
+    "thr_pack_zero_x": (_i, [_v]),
+    "thr_pack_get_stream": (_i, [_v, C.POINTER(_v)]),
     "thr_multishift_solver": (_i, [_v, _v, _f, _i, _i, _v, _v, _v, _v, _f, _i, _pi, _v]),
     "thr_multishift_solver_sp": (_i, [_v, _v, _f, _i, _i, _v, _v, _v, _v, _f, _i, _pi, _v]),
     "thr_qmrherm": (_i, [_v, _v, _v, _f, _pi, _f, _i, _v, _v, _i, _i, _i, _v, _v, _v, _i]),

@@ -52,6 +52,50 @@ def remez_set(path2, path4, n):
     return dict(anum2=a2, aden2=d2, bnum2=b2, bden2=e2, anum4=a4, aden4=d4, bnum4=b4, bden4=e4)
 
 
+class Pack:
+    """Independent lattices of uneven sizes solved together (thr_pack_*)."""
+
+    def __init__(self, shapes, kernel=SHAMIR, am3=1.0, device=0, layout=NATURAL):
+        self._L = _lib.lib()
+        self.shapes = list(shapes)
+        arr = (_lib.Params * len(shapes))(*[_lib.Params(lx, ly, lt, ls, kernel, layout, 25, am3, 0.4, -1, device)
+                                           for (lx, ly, lt, ls) in shapes])
+        h = C.c_void_p()
+        _check(self._L.thr_pack_create(len(shapes), arr, device, C.byref(h)), "thr_pack_create")
+        self.h = h
+
+    def upload(self, i, u, Phi, X):
+        _check(self._L.thr_pack_upload(self.h, i, _p(u), _p(Phi), _p(X)), "pack_upload")
+
+    def zero_x(self):
+        _check(self._L.thr_pack_zero_x(self.h), "pack_zero_x")
+
+    def congrad(self, res, am, imass, precision=FP64):
+        its = np.zeros(len(self.shapes), np.int32)
+        outer = C.c_int(0)
+        rc = self._L.thr_pack_congrad(self.h, res, am, imass, precision, _p(its), C.byref(outer))
+        if rc not in (0, 3):
+            _check(rc, "pack_congrad")
+        return its, outer.value
+
+    def download(self, i):
+        lx, ly, lt, ls = self.shapes[i]
+        X = np.zeros((ls + 2, lx + 2, ly + 2, lt + 2, 4), np.complex128, order="F")
+        _check(self._L.thr_pack_download(self.h, i, _p(X)), "pack_download")
+        return X
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.thr_pack_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class ThirringError(RuntimeError):
     def __init__(self, status, where):
         self.status = status
@@ -211,6 +255,20 @@ class Lattice:
         if rc not in (0, 3):
             _check(rc, "congrad")
         return it.value, nx.value
+
+    def congrad_multi(self, Phi, X, res, am, imass, precision=FP64):
+        """Batched congrad on the current links: Phi, X have a trailing rhs axis
+        (Ls+2, Lx+2, Ly+2, Lt+2, 4, nrhs).  X in/out.  Returns (itercg[nrhs], outer rounds)."""
+        nrhs = Phi.shape[-1]
+        _need(Phi, self.sshape + (nrhs,), np.complex128, "Phi")
+        _need(X, self.sshape + (nrhs,), np.complex128, "X")
+        its = np.zeros(nrhs, np.int32)
+        outer = C.c_int(0)
+        rc = self._L.thr_congrad_multi(self.h, _p(Phi), _p(X), nrhs, res, am, imass, precision, _p(its),
+                                       C.byref(outer))
+        if rc not in (0, 3):
+            _check(rc, "congrad_multi")
+        return its, outer.value
 
     def set_solver(self, multishift_algo):
         """0: per-iteration shift updates (the reference's loop); 1: batched (default)."""
