@@ -43,7 +43,7 @@ BETA, AM, IMASS, AM3, RES = 0.3, 0.01, 1, 1.0, 1e-9
 NPOLE = 25
 # iterations the FP64 multishift takes on this seeded input (used to scale
 # the CPU sample to whole solves; re-measured by every GPU run and printed)
-FP64_ITERS_REF = 17129  # measured on B200 for the seeded input below
+FP64_ITERS_REF = 17118  # measured on B200 for the seeded input below
 METRIC = "multishift solve throughput (qmrherm, 25 poles, FP64 residual 1e-9)"
 UNIT = "solves/s"
 HBM_FALLBACK = 6650.0
@@ -264,8 +264,9 @@ def run_ours(args, rank, world, local_rank):
     return res
 
 
-def dslash_bandwidth(args, dev, lx=48, ls=48, iters=20):
-    """FP64 Shamir M at 48^2 x 48, Ls = 48: algorithmic GB/s over `iters` launches."""
+def dslash_bandwidth(args, dev, lx=48, ls=48, iters=20, warmup=3):
+    """FP64 Shamir M at lx^2 x lx, Ls = ls: algorithmic GB/s over `iters` launches
+    (one read of the input spinor, one write of the output, three link fields)."""
     import torch
     import thirring
     from thirring import _lib
@@ -284,7 +285,7 @@ def dslash_bandwidth(args, dev, lx=48, ls=48, iters=20):
     st = torch.cuda.ExternalStream(s.value)
     out = {}
     for dag in (0, 1):
-        for _ in range(3):
+        for _ in range(warmup):
             L.thr_dslash_dev(G.h, b, a, 0, AM, IMASS, dag)
         L.thr_sync(G.h)
         e0 = torch.cuda.Event(enable_timing=True)
@@ -334,6 +335,149 @@ def cpu_model():
 
 
 # ------------------------------------------------------------------ main
+# ------------------------------------------------------------------ secondary workloads
+def run_measurement(args):
+    """Batched measurement solves: 24^2 x 24, Ls = 48, am = 0.02, 64 wall-noise
+    sources + 4 spins x 4 point sources (Phi = M^dagger xi as measure_shamir
+    builds them), congrad rule with res = 1e-8 (rescgm).  Compares one batched
+    launch per operation (FP64, and FP32 corrections with FP64 defect
+    correction) against one congrad call per source."""
+    import torch
+    import thirring
+    from thirring import _lib
+    L = _lib.lib()
+    lx, ls, am, imass, res = 24, 48, 0.02, 1, 1e-8
+    rng = np.random.default_rng(4)
+    G = thirring.Lattice(lx, lx, lx, ls, beta=BETA)
+    G.coef(np.asfortranarray(rng.standard_normal((lx, lx, lx, 3)) / np.sqrt(BETA), np.float32))
+    nsrc = 80
+    shp = (ls + 2, lx + 2, lx + 2, lx + 2, 4)
+    xi = np.zeros(shp + (nsrc,), np.complex128, order="F")
+    for k in range(64):
+        d = k % 4
+        s = 1 if d < 2 else ls
+        xi[s, 1:-1, 1:-1, 1:-1, d, k] = rng.standard_normal((lx, lx, lx)) + 1j * rng.standard_normal((lx, lx, lx))
+    pts = [(1, 1, 1), (7, 13, 5), (13, 7, 19), (19, 19, 11)]
+    for j, (x0, y0, t0) in enumerate(pts):
+        for d in range(4):
+            xi[1 if d < 2 else ls, x0, y0, t0, d, 64 + 4 * j + d] = 1.0
+    Phi = np.zeros_like(xi)
+    for k in range(nsrc):
+        Phi[..., k] = G.dslashd(np.asfortranarray(xi[..., k]), None, am, imass)
+    n = 4 * ls * lx ** 3
+    dev_phi = torch.zeros(nsrc * n, dtype=torch.complex128, device="cuda")
+    for k in range(nsrc):
+        i = Phi[1:-1, 1:-1, 1:-1, 1:-1, :, k]
+        dev_phi[k * n:(k + 1) * n] = torch.from_numpy(np.ascontiguousarray(i.transpose(4, 3, 2, 1, 0)).ravel())
+    out = {}
+    for name, prec in (("fp64", 0), ("mixed_fp32", 2), ("mixed_bf16", 3)):
+        best = None
+        for rep in range(2):
+            X = torch.zeros_like(dev_phi)
+            its = np.zeros(nsrc, np.int32)
+            outer = C.c_int(0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rc = L.thr_congrad_multi_dev(G.h, C.c_void_p(dev_phi.data_ptr()), C.c_void_p(X.data_ptr()), nsrc, res,
+                                         am, imass, prec, its.ctypes.data_as(C.c_void_p), C.byref(outer))
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        out[name] = {"s": round(best, 3), "rhs_per_s": round(nsrc / best, 2), "iters_mean": float(its.mean()),
+                     "outer_rounds": outer.value, "rc": rc}
+    # one congrad per source (FP64), on a sample of 8 sources
+    t0 = time.perf_counter()
+    for k in range(8):
+        X = np.zeros(shp, np.complex128, order="F")
+        G.congrad(np.asfortranarray(Phi[..., k]), X, res, am, imass)
+    dt = (time.perf_counter() - t0) / 8 * nsrc
+    out["sequential_fp64_congrad"] = {"s": round(dt, 3), "rhs_per_s": round(nsrc / dt, 2),
+                                      "sample": "8 of 80 sources, scaled"}
+    G.close()
+    return {"workload": "measurement solves 24^2x24 Ls48, 80 sources, res 1e-8, am 0.02", "results": out}
+
+
+def run_packed(args):
+    """32 independent lattices, L ~ U{8..20}, T = L, Ls ~ U{8,12,..,32},
+    beta ~ U[0.25, 0.5], seeds 1..32: one right-hand side each, solved
+    together in one persistent launch per operation vs one congrad each."""
+    import thirring
+    rng = np.random.default_rng(2024)
+    shapes, betas = [], []
+    for i in range(32):
+        lx = int(rng.integers(8, 21)) & ~1
+        shapes.append((lx, lx, lx, int(rng.choice(range(8, 33, 4)))))
+        betas.append(float(rng.uniform(0.25, 0.5)))
+    am, imass, res = 0.02, 1, 1e-8
+    pack = thirring.Pack(shapes)
+    data = []
+    for i, ((lx, ly, lt, ls), b) in enumerate(zip(shapes, betas)):
+        r = np.random.default_rng(i + 1)
+        th = np.asfortranarray(r.standard_normal((lx, ly, lt, 3)) / np.sqrt(b), np.float32)
+        with thirring.Lattice(lx, ly, lt, ls, beta=b) as G:
+            u = G.coef(th)
+        phi = np.zeros((ls + 2, lx + 2, ly + 2, lt + 2, 4), np.complex128, order="F")
+        sh = phi[1:-1, 1:-1, 1:-1, 1:-1, :].shape
+        phi[1:-1, 1:-1, 1:-1, 1:-1, :] = r.standard_normal(sh) + 1j * r.standard_normal(sh)
+        pack.upload(i, u, phi, np.zeros_like(phi))
+        data.append((u, phi))
+    out = {}
+    for name, prec in (("fp64", 0), ("mixed_fp32", 2)):
+        best = None
+        for rep in range(2):
+            pack.zero_x()
+            t0 = time.perf_counter()
+            its, outer = pack.congrad(res, am, imass, prec)
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        out[name] = {"s": round(best, 3), "lattices_per_s": round(32 / best, 2), "iters_max": int(its.max()),
+                     "outer_rounds": outer}
+    t0 = time.perf_counter()
+    for i, ((lx, ly, lt, ls), b) in enumerate(zip(shapes, betas)):
+        with thirring.Lattice(lx, ly, lt, ls, beta=b) as G:
+            G.set_links(data[i][0])
+            X = np.zeros_like(data[i][1])
+            G.congrad(data[i][1], X, res, am, imass)
+    dt = time.perf_counter() - t0
+    out["sequential_fp64_congrad"] = {"s": round(dt, 3), "lattices_per_s": round(32 / dt, 2)}
+    pack.close()
+    return {"workload": "32 packed lattices L 8..20, Ls 8..32, beta 0.25..0.5, res 1e-8", "shapes": shapes,
+            "results": out}
+
+
+def run_trajectory(args):
+    """RHMC trajectories on 12^2 x 12, Ls = 16 (beta 0.3, am 0.05, imass 3,
+    10 MD steps of dt 0.05) with the reference's remez2/remez4 (25 poles) and
+    remez2g/remez4g (12 poles) files; guidance solves single precision (spmd)
+    or FP64."""
+    import thirring
+    gold = os.path.join(REPO, "tests", "golden") + os.sep
+    rat = thirring.remez_set(gold + "remez2", gold + "remez4", 25)
+    ratg = thirring.remez_set(gold + "remez2g", gold + "remez4g", 12)
+    out = {}
+    for spmd in (1, 0):
+        G = thirring.Lattice(12, 12, 12, 16, beta=BETA)
+        G.set_remez(rat, ratg)
+        G.set_residuals(1e-8, 1e-6, spmd)
+        G.init_random(4139764973254.0)
+        rng = np.random.default_rng(1)
+        th = np.asfortranarray(rng.standard_normal((12, 12, 12, 3)) / np.sqrt(BETA), np.float32)
+        G.trajectory(th, 10, 0.05, 0.05, 3, fixed_steps=10)  # warm-up
+        t0 = time.perf_counter()
+        ntraj = 3
+        dh = []
+        acc = 0
+        for _ in range(ntraj):
+            r = G.trajectory(th, 10, 0.05, 0.05, 3, fixed_steps=10)
+            dh.append(r.dh)
+            acc += r.accepted
+        dt = (time.perf_counter() - t0) / ntraj
+        out["spmd_fp32_guidance" if spmd else "fp64_guidance"] = {
+            "s_per_traj": round(dt, 3), "traj_per_hr": round(3600 / dt, 1), "dH": dh, "accepted": acc}
+        G.close()
+    return {"workload": "RHMC 12^2x12 Ls16, 10 MD steps dt 0.05, remez2/4 + remez2g/4g", "results": out}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -341,9 +485,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="fp64", choices=["fp64", "sp", "mixed", "bf16"])
+    ap.add_argument("--workload", default="multishift",
+                    choices=["multishift", "measurement", "packed", "trajectory", "dslash"],
+                    help="secondary workloads print their own JSON line (not the headline contract)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-iters", type=int, default=6, help="multishift iterations in the CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--lx", type=int, default=0, help="profiling case: lattice extent (all three directions)")
+    ap.add_argument("--ls", type=int, default=0, help="profiling case: fifth-dimension extent")
     ap.add_argument("--no-dslash", action="store_true")
     ap.add_argument("--no-compare-plain", dest="compare_plain", action="store_false",
                     help="skip timing the plain FP64 path (reference loop structure)")
@@ -353,6 +502,22 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     iters_for_cpu = FP64_ITERS_REF
+
+    if args.lx or args.ls:
+        # a smaller (or larger) profiling case of the same solve; not the headline workload
+        global LX, LY, LT, LS
+        LX = LY = LT = args.lx or LX
+        LS = args.ls or LS
+    if args.workload == "dslash":
+        lx, ls = args.lx or 48, args.ls or 48
+        r = dslash_bandwidth(args, local_rank, lx, ls, args.steps, args.warmup)
+        print(json.dumps({"workload": f"FP64 Shamir M and M^dagger, {lx}^2x{lx}, Ls={ls}, "
+                                      f"{args.steps} launches each", "results": r}), flush=True)
+        return
+    if args.workload != "multishift":
+        fn = {"measurement": run_measurement, "packed": run_packed, "trajectory": run_trajectory}[args.workload]
+        print(json.dumps(fn(args)), flush=True)
+        return
 
     if args.impl == "reference":
         if rank != 0:
@@ -401,7 +566,8 @@ def main():
     # dominant kernel of the timed region
     name, (nl, tms, byts) = max(r["prof"].items(), key=lambda kv: kv[1][1])
     achieved = byts / (tms / 1e3) / 1e9 if tms > 0 else None
-    kname = {"dslash": "k_dslash_shamir", "multishift_update": "k_ms_pshift"}[name]
+    # the batched solver's shift-field update is the folded flush kernel
+    kname = {"dslash": "k_dslash", "multishift_update": "k_flush"}[name]
     traffic = ncu_traffic(kname)
     roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1) if achieved else None,
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
