@@ -141,6 +141,26 @@ class Clocks:
                 "samples": len(sm)}
 
 
+# ------------------------------------------------------------------ replicas
+def max_over_ranks(x, world):
+    """The slowest rank's time: one all-reduce(MAX) of a float64 scalar on the
+    process group's device (CUDA under NCCL, CPU under gloo)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, steps, ms_max):
+    """Whole-job solves/s: every rank solves its own replica lattice `steps`
+    times; the job takes as long as its slowest rank."""
+    return world * steps / (ms_max / 1e3)
+
+
 # ------------------------------------------------------------------ GPU arm
 def run_ours(args, rank, world, local_rank):
     import torch
@@ -181,12 +201,7 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
 
     def tmax(x):
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([x], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
+        return max_over_ranks(x, world)
 
     # ---- warm-up
     iters = 0
@@ -561,7 +576,7 @@ def main():
         return
     iters = r["its"][-1]
     ms_step = r["ms"] / args.steps
-    value = world * args.steps / (r["ms"] / 1e3)
+    value = job_throughput(world, args.steps, r["ms"])
     peak, peak_kind = peaks()
     # dominant kernel of the timed region
     name, (nl, tms, byts) = max(r["prof"].items(), key=lambda kv: kv[1][1])
@@ -585,7 +600,7 @@ def main():
                          f"scaled to the {iters} iterations the solve takes; {cpu_model()}"}
     e2e = None
     if r["e2e_ms"]:
-        e2e = {"value": world * args.e2e_steps / (r["e2e_ms"] / 1e3), "unit": UNIT,
+        e2e = {"value": job_throughput(world, args.e2e_steps, r["e2e_ms"]), "unit": UNIT,
                "h2d_bytes_per_step": r["phi_bytes"], "d2h_bytes_per_step": r["phi_bytes"],
                "path": "thr_qmrherm (C ABI) with page-locked Fortran-layout host arrays"}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
