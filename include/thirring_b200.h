@@ -154,6 +154,21 @@ int thr_pack_download(thr_pack *pack, int i, double *X);
 int thr_pack_zero_x(thr_pack *pack);
 int thr_pack_get_stream(thr_pack *pack, void **stream);
 
+/* measure(psibarpsi, res, aviter, am, imass[, isweep_total]),
+ * measure_module.F90:142-162: the noisy estimator of psibarpsi on the current
+ * links with the context's random numbers.  kernel_meas selects the
+ * measurement routine the reference picks at compile time: 0 = measure_shamir
+ * (:170-423, MEASURE_SHAMIR), 1 = measure_wilson (:431-670, MEASURE_WILSON;
+ * imass 1 or 3).  congrad runs on the context's (generation) kernel, as in the
+ * reference.  knoise = params.F90 knoise (10 in the reference).  All
+ * 4*knoise (Shamir) or 8*knoise (Wilson) solves run as one batched congrad
+ * (precision: thr_precision; THR_FP64 is the reference's arithmetic).
+ * Outputs: psibarpsi, susclsing (fort.200), aviter; optional parts[4*knoise] =
+ * Re/Im psibarpsi1, Re/Im psibarpsi2 per noise (fort.100) and itercg[] per
+ * solve in the reference's order. */
+int thr_measure(thr_ctx *ctx, int kernel_meas, float res, float am, int imass, int knoise, int precision,
+                float *psibarpsi, float *susclsing, float *aviter, double *parts, int *itercg);
+
 /* ---- multishift_module.F90 ----------------------------------------------- */
 /* multishift_solver(u, am, imass, ndiagq, aden, anum, output, input, res,
  * maxcg, cg_return[, cg_returns]), multishift_module.F90:13-284: solves

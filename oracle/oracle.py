@@ -98,6 +98,7 @@ for name, res, args in [
     ("orc_update_halo_5", None, [_L, _v]),
     ("orc_update_halo_4", None, [_L, C.c_int, _v]),
     ("orc_update_halo_4_real", None, [_L, C.c_int, _v]),
+    ("orc_dwilson", None, [_L, _v, _v, _v, C.c_float]),
     ("orc_coef", None, [_L, _v, _v]),
     ("orc_dslash", None, [_L, _v, _v, _v, C.c_float, C.c_int]),
     ("orc_dslashd", None, [_L, _v, _v, _v, C.c_float, C.c_int]),
@@ -332,3 +333,99 @@ def trajectory(L, g, theta, rat, iterl, dt, am, imass, rescga, rescgg, use_sp, f
                             int(use_sp), 50000, fixed_steps, C.byref(r), C.byref(cnt))
     assert rc == 0
     return r
+
+
+# ---------------------------------------------------------------- measurement
+def _with_kernel(L, kernel):
+    M = Lat()
+    C.memmove(C.byref(M), C.byref(L), C.sizeof(Lat))
+    M.kernel = kernel
+    return M
+
+
+def measure_solves(ls, imass, kernel_meas):
+    """The solves of one noise in the reference's order, 0-based:
+    (wall noise 0 = ps / 1 = pt, source s, source spin, source sign,
+     contraction s, contraction spin, post-projection 0 / 1 = P+ / 2 = P-, part 0 / 1).
+    measure_shamir: measure_module.F90:221-334; measure_wilson: :495-590."""
+    out = []
+    if kernel_meas == 0:
+        for i in range(2):
+            if imass != 5:
+                out.append((0, 0, i, 1.0, ls - 1, i, 0, 0))
+                out.append((1, ls - 1, i + 2, 1.0, 0, i + 2, 0, 1))
+            else:
+                out.append((0, 0, i, -1.0, 0, i + 2, 0, 0))
+                out.append((1, ls - 1, i + 2, -1.0, ls - 1, i, 0, 1))
+    else:
+        for i in range(4):
+            out.append((0, 0, i, 1.0, ls - 1, i, 1, 0))
+        for i in range(4):
+            out.append((1, ls - 1, i, 1.0, 0, i, 2, 1))
+    return out
+
+
+def measure(L, g, u, res, am, imass, kernel_meas=0, knoise=10):
+    """measure(psibarpsi, res, aviter, am, imass), measure_module.F90:142-162,
+    with the measurement kernel chosen at run time (MEASURE_SHAMIR -> 0,
+    MEASURE_WILSON -> 1):
+      measure_shamir :170-423 -- per noise gauss0(ps), gauss0(pt); for
+        idsource = 1, 2 a source on the wall s = 1 (from ps) and one on s = Ls
+        (from pt); Phi = M^dagger xi with the measurement kernel's dslashd
+        (:246), congrad(Phi) on the generation kernel with the source as the
+        initial guess (vector::X is xi, :173); psibarpsi1/2 += sum conj(eta) *
+        solution on the opposite wall (FP64 complex);
+      measure_wilson :431-670 -- idsource = 1..4 on each wall, and before the
+        contraction the wall slice of the solution becomes
+        DWilson(P xi, -am3) - P xi with P = P+ (spins 1,2) at s = Ls and
+        P- (spins 3,4) at s = 1.
+    Returns psibarpsi, susclsing, aviter (float32 as in the reference), the
+    per-noise (psibarpsi1, psibarpsi2) and each solve's itercg."""
+    Lm = _with_kernel(L, kernel_meas)
+    kvol = L.lx * L.ly * L.lt
+    pbp = np.zeros(knoise)
+    parts = []
+    its = []
+    it_total = 0
+    for n in range(knoise):
+        noise = [g.gauss0(), g.gauss0()]
+        etas = [p[1:-1, 1:-1, 1:-1, 0].astype(np.float64) + 1j * p[1:-1, 1:-1, 1:-1, 1].astype(np.float64)
+                for p in noise]
+        acc = [0j, 0j]
+        for (w, s_src, d_src, sign, s_c, d_c, post, part) in measure_solves(L.ls, imass, kernel_meas):
+            xi = spinor(L)
+            xi[s_src + 1, 1:-1, 1:-1, 1:-1, d_src] = sign * etas[w]
+            update_halo_5(L, xi)
+            Phi = update_halo_5(L, dslashd(Lm, xi, u, am, imass))
+            itercg, _ = congrad(L, Phi, xi, u, res, am, imass)
+            it_total += itercg
+            its.append(itercg)
+            if post:
+                isl = np.zeros((L.lx + 2, L.ly + 2, L.lt + 2, 4), np.complex128, order="F")
+                dd = (0, 1) if post == 1 else (2, 3)
+                for d in dd:
+                    isl[:, :, :, d] = xi[s_c + 1, :, :, :, d]
+                osl = np.zeros_like(isl)
+                lib.orc_dwilson(C.byref(L), P(osl), P(isl), P(u), -L.am3)
+                wall = (osl - isl)[1:-1, 1:-1, 1:-1, d_c]
+            else:
+                wall = xi[s_c + 1, 1:-1, 1:-1, 1:-1, d_c]
+            acc[part] = acc[part] + np.sum(np.conj(etas[w]) * wall)
+        p1, p2 = acc
+        if imass == 1:
+            p1, p2 = p1 / kvol, p2 / kvol
+        elif imass == 3:
+            p1, p2 = -1j * p1 / kvol, 1j * p2 / kvol
+        else:
+            p1, p2 = -1j * p1 / kvol, -1j * p2 / kvol
+        pbp[n] = (p1 + p2).real
+        parts.append((p1, p2))
+    psibarpsi = np.float32(np.sum(pbp))
+    sus = np.float32(0.0)
+    for n in range(knoise):
+        sus = np.float32(sus + np.float32(np.sum(pbp[n] * pbp[n + 1:])))
+    psibarpsi = np.float32(psibarpsi / np.float32(knoise))
+    sus = np.float32(np.float32(2 * kvol) * sus / np.float32(knoise * (knoise - 1)))
+    aviter = np.float32(np.float32(it_total) / np.float32(4 * knoise))
+    return dict(psibarpsi=float(psibarpsi), susclsing=float(sus), aviter=float(aviter), parts=parts,
+                pbp=pbp, itercg=its)

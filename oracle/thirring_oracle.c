@@ -342,6 +342,12 @@ static void acc_slice(const orc_lat *L, orc_zd *Phi, int il, int d0, int d1, con
         }
 }
 
+/* DWilson(Phi, R, u, mass) on one slice (dirac.F90:181-224): diag = (3.0 + mass)
+ * evaluated in default real and widened; R's halos must hold the periodic images. */
+void orc_dwilson(const orc_lat *L, orc_zd *Phi, const orc_zd *R, const orc_zd *u, float mass) {
+  dwilson(L, Phi, R, u, (double)(3.0f + mass), +1.0);
+}
+
 void orc_dslash_wilson(const orc_lat *L, orc_zd *Phi, const orc_zd *R, const orc_zd *u, float am, int imass) {
   size_t n4 = orc_n4(L) * 4, n5 = orc_n5(L);
   int Ls = L->ls;

@@ -64,6 +64,8 @@ void orc_gammas(int mu, int d, orc_zd *val, int *gin);
 void orc_update_halo_5(const orc_lat *L, orc_zd *a);
 void orc_update_halo_5_sp(const orc_lat *L, orc_zf *a);
 void orc_update_halo_4(const orc_lat *L, int n, orc_zd *u);
+/* DWilson on one (0:Lx+1,0:Ly+1,0:Lt+1,4) slice, dirac.F90:181-224 */
+void orc_dwilson(const orc_lat *L, orc_zd *Phi, const orc_zd *R, const orc_zd *u, float mass);
 void orc_update_halo_4_real(const orc_lat *L, int n, float *ps);
 
 /* gauge.F90:12-43 */

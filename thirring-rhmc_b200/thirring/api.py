@@ -270,6 +270,19 @@ class Lattice:
             _check(rc, "congrad_multi")
         return its, outer.value
 
+    def measure(self, res, am, imass, kernel_meas=SHAMIR, knoise=10, precision=FP64):
+        """measure(psibarpsi, res, aviter, am, imass), measure_module.F90:142-162,
+        on the current links and random numbers.  Returns a dict with psibarpsi,
+        susclsing, aviter (float32 values), parts (knoise x [Re p1, Im p1, Re p2,
+        Im p2], the fort.100 columns) and itercg (one per solve)."""
+        per = 4 if kernel_meas == SHAMIR else 8
+        pb, sus, av = C.c_float(0), C.c_float(0), C.c_float(0)
+        parts = np.zeros((knoise, 4), np.float64)
+        its = np.zeros(per * knoise, np.int32)
+        _check(self._L.thr_measure(self.h, kernel_meas, res, am, imass, knoise, precision, C.byref(pb), C.byref(sus),
+                                   C.byref(av), _p(parts), _p(its)), "measure")
+        return dict(psibarpsi=pb.value, susclsing=sus.value, aviter=av.value, parts=parts, itercg=its)
+
     def set_solver(self, multishift_algo):
         """0: per-iteration shift updates (the reference's loop); 1: batched (default)."""
         _check(self._L.thr_set_solver(self.h, int(multishift_algo)), "set_solver")
