@@ -233,6 +233,33 @@ int thr_gaussp(thr_ctx *ctx, float *ps);
  * site (ix,iy,it) (ignored for the global stream), random.f90:28-58. */
 int thr_rano(thr_ctx *ctx, int ix, int iy, int it, float *out);
 
+/* rranget(seed, 1, 1, 1), site_random.f90:74-80 / random.f90: the current
+ * 48-bit state of site (1,1,1)'s generator (site streams) or of the global
+ * generator, as the real(dp) the reference writes into checkpoints
+ * (dwf3d_lib.F90:373, :474, :498). */
+int thr_rranget(thr_ctx *ctx, double *seed);
+/* The whole generator state (every site's 48-bit state, shuffle table, y and
+ * idum, or the global stream's) as an opaque host image, so that a run can
+ * resume with the identical random sequence -- no counterpart in the
+ * reference, which reseeds from the checkpoint's seed on restart. */
+int thr_rng_state_bytes(thr_ctx *ctx, unsigned long long *bytes);
+int thr_rng_save(thr_ctx *ctx, void *host);
+int thr_rng_load(thr_ctx *ctx, const void *host);
+
+/* ---- checkpoints: dwf3d_lib.F90:618-767 (host only, no GPU) ----------- */
+enum thr_con_format {
+  THR_CON_SERIAL = 0,  /* unformatted sequential record: marker, theta, seed, marker (:651-653, :711-714) */
+  THR_CON_MPIIO = 1    /* MPI build: theta at offset 0, seed + record length at 12V+4 (:632-649, :683-704) */
+};
+/* sread: theta real(Lx,Ly,Lt,3) and seed from a `con` file of either layout
+ * (format returns which). */
+int thr_read_con(const char *path, int lx, int ly, int lt, float *theta, double *seed, int *format);
+/* swrite: write theta and seed in the given layout. */
+int thr_write_con(const char *path, int lx, int ly, int lt, const float *theta, double seed, int format);
+/* readseed / saveseed: the `random_seed` text file (one real(dp)). */
+int thr_readseed(const char *path, double *seed);
+int thr_saveseed(const char *path, double seed);
+
 /* ---- RHMC: remez.F90, force_module.F90, evolution.F90, dwf3d_lib.F90 ----- */
 /* The rational approximations read by dwf3d_lib.F90:205-209 (module remez:
  * anum2/aden2/bnum2/bden2/anum4/aden4/bnum4/bden4 with ndiag poles; module

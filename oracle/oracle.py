@@ -118,6 +118,7 @@ for name, res, args in [
     ("orc_init_random", C.c_int, [_v, C.c_double]),
     ("orc_rano", C.c_float, [_v, C.c_int, C.c_int, C.c_int]),
     ("orc_dranf", C.c_double, [_v, C.c_int, C.c_int, C.c_int]),
+    ("orc_rranget", C.c_double, [_v, C.c_int, C.c_int, C.c_int]),
     ("orc_gauss0", None, [_L, _v, _v]),
     ("orc_gaussp", None, [_L, _v, _v]),
     ("orc_read_remez_file", C.c_int, [C.c_char_p, C.c_int, _v, _v, _v, _v]),
@@ -246,6 +247,9 @@ class RNG:
 
     def rano(self, ix=1, iy=1, it=1):
         return lib.orc_rano(self.h, ix, iy, it)
+
+    def rranget(self, ix=1, iy=1, it=1):
+        return lib.orc_rranget(self.h, ix, iy, it)
 
     def gauss0(self):
         ps = ps_field(self.L)

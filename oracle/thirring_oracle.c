@@ -1065,6 +1065,8 @@ double orc_dranf(orc_rng *g, int ix, int iy, int it) {
   return (double)g->S[k] / 281474976710656.0;
 }
 static float rranf(orc_rng *g, int ix, int iy, int it) { return (float)orc_dranf(g, ix, iy, it); }
+/* RRANGET / G900GT: DS(2)*2^24 + DS(1), the 48-bit state as a double (site_random.f90:74-80, :114-118) */
+double orc_rranget(orc_rng *g, int ix, int iy, int it) { return (double)g->S[stream_of(g, ix, iy, it)]; }
 float orc_rano(orc_rng *g, int ix, int iy, int it) {
   int k = stream_of(g, ix, iy, it);
   float *v = g->v + (size_t)k * 97;

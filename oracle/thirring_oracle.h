@@ -124,6 +124,7 @@ void orc_rng_destroy(orc_rng *g);
 int orc_init_random(orc_rng *g, double seed);                 /* random.f90:119 / site_random.f90:133 */
 float orc_rano(orc_rng *g, int ix, int iy, int it);          /* 1-based site; ignored for global */
 double orc_dranf(orc_rng *g, int ix, int iy, int it);
+double orc_rranget(orc_rng *g, int ix, int iy, int it);
 void orc_gauss0(const orc_lat *L, orc_rng *g, float *ps);     /* gaussian.F90:63-104 */
 void orc_gaussp(const orc_lat *L, orc_rng *g, float *ps);     /* gaussian.F90:14-61 */
 

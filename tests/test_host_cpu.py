@@ -41,3 +41,41 @@ def test_remez_set_keys():
     assert sorted(rat) == sorted(["anum2", "aden2", "bnum2", "bden2", "anum4", "aden4", "bnum4", "bden4"])
     assert all(len(rat[k]) == 26 for k in ("anum2", "bnum2", "anum4", "bnum4"))
     assert all(len(rat[k]) == 25 for k in ("aden2", "bden2", "aden4", "bden4"))
+
+
+# ---- checkpoints (dwf3d_lib.F90:618-767); host code of the library, no GPU
+def test_read_con_kat():
+    # tests/broken_tests/test_load.F90:28-31 on the 12^3 sample configuration
+    import json
+    theta, seed, fmt = thirring.read_con(os.path.join(GOLD, "con_12x12x12"), 12, 12, 12)
+    kat = json.load(open(os.path.join(GOLD, "con_12x12x12.json")))
+    assert fmt == thirring.CON_SERIAL
+    assert seed == 196829593468928.0 == kat["seed"]
+    assert abs(theta.astype(np.float64).sum() - (-185.5681)) < 1e-3 * 185.5681
+    assert abs(float(theta.max()) - 5.015248) < 1e-6 and abs(float(theta.min()) - (-5.267587)) < 1e-6
+
+
+def test_con_round_trips(tmp_path):
+    src = os.path.join(GOLD, "con_12x12x12")
+    theta, seed, _ = thirring.read_con(src, 12, 12, 12)
+    a = str(tmp_path / "con_serial")
+    thirring.write_con(a, theta, seed, thirring.CON_SERIAL)
+    assert open(a, "rb").read() == open(src, "rb").read()  # byte-identical to the reference's file
+    b = str(tmp_path / "con_mpi")
+    thirring.write_con(b, theta, seed, thirring.CON_MPIIO)
+    raw = open(b, "rb").read()
+    assert len(raw) == 4 * theta.size + 16
+    assert raw[:4 * theta.size] == theta.tobytes(order="F")  # theta at offset 0
+    t2, s2, fmt = thirring.read_con(b, 12, 12, 12)
+    assert fmt == thirring.CON_MPIIO and s2 == seed and np.array_equal(t2, theta)
+    with pytest.raises(thirring.ThirringError):
+        thirring.read_con(src, 8, 8, 8)  # wrong lattice size
+
+
+def test_seed_file_round_trip(tmp_path):
+    p = str(tmp_path / "random_seed")
+    for v in (4139764973254.0, 196829593468928.0, 1.0):
+        thirring.saveseed(p, v)
+        assert thirring.readseed(p) == v
+    open(p, "w").write("   4139764973254.0000     \n")  # gfortran list-directed form
+    assert thirring.readseed(p) == 4139764973254.0

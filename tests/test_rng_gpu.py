@@ -76,3 +76,49 @@ def test_bad_seed_rejected():
             G.init_random(1.5)
         with pytest.raises(thirring.ThirringError):
             G.init_random(2.0 ** 49)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("site", [True, False])
+@pytest.mark.parametrize("layout", [0, 1])
+def test_rranget_and_reseed(site, layout):
+    # checkpoint semantics (dwf3d_lib.F90:373-376, :498-500): rranget(seed, 1, 1, 1)
+    # after some draws, then init_random(seed) on restart
+    L = O.lat(6, 4, 8, 8)
+    g = O.RNG(L, site).init(4139764973254.0)
+    with thirring.Lattice(6, 4, 8, 8, layout=layout) as G:
+        G.init_random(4139764973254.0, site=site)
+        assert G.rranget() == g.rranget()
+        for _ in range(3):
+            G.gauss0()
+            g.gauss0()
+        seed = G.rranget()
+        assert seed == g.rranget()
+        G.init_random(seed, site=site)
+        g.init(seed)
+        assert np.array_equal(_faces(G.gaussp()), _faces(g.gaussp()))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("site", [True, False])
+def test_rng_state_save_load(site):
+    # the full generator image resumes the identical sequence (no reseeding)
+    with thirring.Lattice(6, 4, 8, 8) as G:
+        G.init_random(12345.0, site=site)
+        G.gauss0()
+        state = G.rng_state()
+        a = G.gauss0()
+        b = G.gaussp()
+        r = G.rano(2, 3, 4)
+        G.gauss0()
+        G.set_rng_state(state)
+        assert np.array_equal(G.gauss0(), a)
+        assert np.array_equal(G.gaussp(), b)
+        assert G.rano(2, 3, 4) == r
+        with thirring.Lattice(6, 4, 8, 8) as H:  # into a fresh context
+            H.set_rng_state(state)
+            assert np.array_equal(H.gauss0(), a)
+        with thirring.Lattice(4, 4, 8, 8) as K:
+            if site:
+                with pytest.raises(thirring.ThirringError):
+                    K.set_rng_state(state)  # other lattice size

@@ -335,3 +335,99 @@ int thr_rano(thr_ctx* c, int ix, int iy, int it, float* out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- generator state
+namespace {
+// host image of the whole random state: a header, then the streams and tables
+struct RngImage {
+  uint32_t magic, version;
+  int32_t site, v3;
+  uint64_t hS;
+  float hy;
+  int32_t hidum;
+  float hv[97];
+};
+constexpr uint32_t kRngMagic = 0x54485252u;  // "RRHT"
+}  // namespace
+
+using namespace thr;
+
+extern "C" {
+
+int thr_rranget(thr_ctx* c, double* seed) {
+  if (!c || !seed) return THR_ERR_BADARG;
+  Rng& r = c->rng;
+  if (!r.ready) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  if (!r.site) {
+    *seed = (double)r.hS;
+    return THR_OK;
+  }
+  Stream h;
+  const int site = site_index(c->g, 0, 0, 0);  // rranget(seed, 1, 1, 1)
+  THR_CUDA(cudaMemcpyAsync(&h, (const Stream*)r.dev_streams + site, sizeof(Stream), cudaMemcpyDeviceToHost, c->st));
+  THR_CUDA(cudaStreamSynchronize(c->st));
+  *seed = (double)h.S;
+  return THR_OK;
+}
+
+int thr_rng_state_bytes(thr_ctx* c, unsigned long long* bytes) {
+  if (!c || !bytes) return THR_ERR_BADARG;
+  const size_t v3 = (size_t)c->g.v3;
+  *bytes = sizeof(RngImage) + (c->rng.site ? v3 * (sizeof(Stream) + 97 * sizeof(float)) : 0);
+  return THR_OK;
+}
+
+int thr_rng_save(thr_ctx* c, void* host) {
+  if (!c || !host) return THR_ERR_BADARG;
+  Rng& r = c->rng;
+  if (!r.ready) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  RngImage im{};
+  im.magic = kRngMagic;
+  im.version = 1;
+  im.site = r.site ? 1 : 0;
+  im.v3 = c->g.v3;
+  im.hS = r.hS;
+  im.hy = r.hy;
+  im.hidum = r.hidum;
+  std::memcpy(im.hv, r.hv, sizeof(im.hv));
+  std::memcpy(host, &im, sizeof(im));
+  if (r.site) {
+    char* p = (char*)host + sizeof(im);
+    const size_t v3 = (size_t)c->g.v3;
+    THR_CUDA(cudaMemcpyAsync(p, r.dev_streams, v3 * sizeof(Stream), cudaMemcpyDeviceToHost, c->st));
+    THR_CUDA(cudaMemcpyAsync(p + v3 * sizeof(Stream), r.dev_tables, v3 * 97 * sizeof(float), cudaMemcpyDeviceToHost,
+                             c->st));
+    THR_CUDA(cudaStreamSynchronize(c->st));
+  }
+  return THR_OK;
+}
+
+int thr_rng_load(thr_ctx* c, const void* host) {
+  if (!c || !host) return THR_ERR_BADARG;
+  RngImage im;
+  std::memcpy(&im, host, sizeof(im));
+  if (im.magic != kRngMagic || im.version != 1) return THR_ERR_BADARG;
+  if (im.site && im.v3 != c->g.v3) return THR_ERR_BADSHAPE;
+  cudaSetDevice(c->dev);
+  Rng& r = c->rng;
+  r.site = im.site != 0;
+  r.hS = im.hS;
+  r.hy = im.hy;
+  r.hidum = im.hidum;
+  std::memcpy(r.hv, im.hv, sizeof(im.hv));
+  if (r.site) {
+    THR_TRY(r.ensure(c));
+    const char* p = (const char*)host + sizeof(im);
+    const size_t v3 = (size_t)c->g.v3;
+    THR_CUDA(cudaMemcpyAsync(r.dev_streams, p, v3 * sizeof(Stream), cudaMemcpyHostToDevice, c->st));
+    THR_CUDA(cudaMemcpyAsync(r.dev_tables, p + v3 * sizeof(Stream), v3 * 97 * sizeof(float), cudaMemcpyHostToDevice,
+                             c->st));
+    THR_CUDA(cudaStreamSynchronize(c->st));
+  }
+  r.ready = true;
+  return THR_OK;
+}
+
+}  // extern "C"

@@ -8,5 +8,5 @@ reference's Fortran layout.  All compute runs in libthirring_b200.so on the
 GPU; errors are raised as ThirringError with the library's status code.
 """
 from ._lib import LibraryMissing, header_functions, lib  # noqa: F401
-from .api import (Lattice, Pack, ThirringError, TrajResult, field3, links, ps_field, read_remez_file,  # noqa: F401
-                  remez_set, shift_out, spinor)
+from .api import (CON_MPIIO, CON_SERIAL, Lattice, Pack, ThirringError, TrajResult, field3, links,  # noqa: F401
+                  ps_field, read_con, read_remez_file, readseed, remez_set, saveseed, shift_out, spinor, write_con)

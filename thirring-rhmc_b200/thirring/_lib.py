@@ -61,6 +61,14 @@ SIGNATURES = {
     "thr_gauss0": (_i, [_v, _v]),
     "thr_gaussp": (_i, [_v, _v]),
     "thr_rano": (_i, [_v, _i, _i, _i, C.POINTER(C.c_float)]),
+    "thr_rranget": (_i, [_v, _pd]),
+    "thr_rng_state_bytes": (_i, [_v, C.POINTER(C.c_ulonglong)]),
+    "thr_rng_save": (_i, [_v, _v]),
+    "thr_rng_load": (_i, [_v, _v]),
+    "thr_read_con": (_i, [C.c_char_p, _i, _i, _i, _v, _pd, _pi]),
+    "thr_write_con": (_i, [C.c_char_p, _i, _i, _i, _v, _d, _i]),
+    "thr_readseed": (_i, [C.c_char_p, _pd]),
+    "thr_saveseed": (_i, [C.c_char_p, _d]),
     "thr_set_remez": (_i, [_v, _i] + [_v] * 8 + [_i] + [_v] * 8),
     "thr_set_residuals": (_i, [_v, _f, _f, _i, _i]),
     "thr_force": (_i, [_v, _v, _f, _f, _i, _v, _v]),

@@ -9,6 +9,7 @@ Array shapes (numpy, order='F'), as declared in the reference:
   shifts  complex128 (Ls, Lx, Ly, Lt, 4, ndiag)       multishift_module.F90:29
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -50,6 +51,39 @@ def remez_set(path2, path4, n):
     a2, d2, b2, e2 = read_remez_file(path2, n)
     a4, d4, b4, e4 = read_remez_file(path4, n)
     return dict(anum2=a2, aden2=d2, bnum2=b2, bden2=e2, anum4=a4, aden4=d4, bnum4=b4, bden4=e4)
+
+
+CON_SERIAL, CON_MPIIO = 0, 1
+
+
+def read_con(path, lx, ly, lt):
+    """sread (dwf3d_lib.F90:618-667): returns (theta float32 (lx,ly,lt,3) in
+    Fortran order, seed, layout) from a `con` file of either layout."""
+    theta = np.zeros((lx, ly, lt, 3), np.float32, order="F")
+    seed = C.c_double(0)
+    fmt = C.c_int(-1)
+    _check(_lib.lib().thr_read_con(os.fsencode(path), lx, ly, lt, _p(theta), C.byref(seed), C.byref(fmt)), "read_con")
+    return theta, seed.value, fmt.value
+
+
+def write_con(path, theta, seed, layout=CON_SERIAL):
+    """swrite (dwf3d_lib.F90:669-717)."""
+    theta = np.asfortranarray(theta, np.float32)
+    lx, ly, lt, three = theta.shape
+    assert three == 3
+    _check(_lib.lib().thr_write_con(os.fsencode(path), lx, ly, lt, _p(theta), float(seed), layout), "write_con")
+
+
+def readseed(path):
+    """readseed (dwf3d_lib.F90:719-748): the seed in a `random_seed` file."""
+    v = C.c_double(0)
+    _check(_lib.lib().thr_readseed(os.fsencode(path), C.byref(v)), "readseed")
+    return v.value
+
+
+def saveseed(path, seed):
+    """saveseed (dwf3d_lib.F90:750-767)."""
+    _check(_lib.lib().thr_saveseed(os.fsencode(path), float(seed)), "saveseed")
 
 
 class Pack:
@@ -241,6 +275,24 @@ class Lattice:
         v = C.c_float(0)
         _check(self._L.thr_rano(self.h, ix, iy, it, C.byref(v)), "rano")
         return v.value
+
+    def rranget(self):
+        """rranget(seed, 1, 1, 1): the generator state written into checkpoints."""
+        v = C.c_double(0)
+        _check(self._L.thr_rranget(self.h, C.byref(v)), "rranget")
+        return v.value
+
+    def rng_state(self):
+        """The complete generator state as bytes (resume with the same sequence)."""
+        n = C.c_ulonglong(0)
+        _check(self._L.thr_rng_state_bytes(self.h, C.byref(n)), "rng_state_bytes")
+        buf = np.zeros(n.value, np.uint8)
+        _check(self._L.thr_rng_save(self.h, _p(buf)), "rng_save")
+        return buf.tobytes()
+
+    def set_rng_state(self, state):
+        buf = np.frombuffer(state, np.uint8).copy()
+        _check(self._L.thr_rng_load(self.h, _p(buf)), "rng_load")
 
     # ---- measure_module.F90
     def congrad(self, Phi, X, res, am, imass):
