@@ -45,6 +45,9 @@ NPOLE = 25
 # the CPU sample to whole solves; re-measured by every GPU run and printed)
 FP64_ITERS_REF = 17118  # measured on B200 for the seeded input below
 METRIC = "multishift solve throughput (qmrherm, 25 poles, FP64 residual 1e-9)"
+# kernel timing inside the timed region: every PROF_STRIDE-th launch of each kind
+PROF_STRIDE = 8
+PROF_KINDS = ((0, "k_dslash_M"), (2, "k_dslash_Mdag_dot"), (1, "k_flush"))
 UNIT = "solves/s"
 HBM_FALLBACK = 6650.0
 
@@ -74,15 +77,20 @@ def peaks():
         return HBM_FALLBACK, "fallback"
 
 
-def ncu_traffic(kernel):
-    """per-launch DRAM bytes of `kernel` from the committed ncu summary, else None"""
+def ncu_traffic(kernel, algorithmic_per_launch):
+    """per-launch DRAM bytes of `kernel` from the committed ncu summary: a measured
+    figure ("traffic <kernel> <bytes>") or a measured traffic/algorithmic ratio applied
+    to this launch ("ratio <kernel> <r>"); None if neither was recorded"""
     p = os.path.join(REPO, "profiles", "roofline_traffic.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
         f = line.split()
-        if len(f) >= 3 and f[0] == "traffic" and f[1] == kernel:
-            return float(f[2])
+        if len(f) >= 3 and f[1] == kernel:
+            if f[0] == "traffic":
+                return float(f[2])
+            if f[0] == "ratio":
+                return round(float(f[2]) * algorithmic_per_launch)
     return None
 
 
@@ -208,7 +216,8 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         iters = solve(mode)
     # ---- timed region (inputs resident), profiled kernels, sampled clocks
-    L.thr_profile(h, 1, 1)
+    # every PROF_STRIDE-th launch of each profiled kernel is bracketed by events
+    L.thr_profile(h, PROF_STRIDE, 1)
     barrier()
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -223,15 +232,16 @@ def run_ours(args, rank, world, local_rank):
     ms = tmax(e0.elapsed_time(e1))
     L.thr_profile(h, 0, 0)
     prof = {}
-    for kind, name in ((0, "dslash"), (1, "multishift_update")):
+    for kind, name in PROF_KINDS:
         n = C.c_int(0)
         t = C.c_double(0)
         b = C.c_double(0)
-        L.thr_profile_read(h, kind, C.byref(n), C.byref(t), C.byref(b))
-        prof[name] = (n.value, t.value, b.value)
-    # the batched solver enqueues 16 iterations of 7 kernels plus 2 per batch; 3 set-up
-    # kernels and the pole sum per solve
-    launches = int(sum(3 + ((i + 15) // 16) * (16 * 7 + 2) + 1 for i in its))
+        tot = C.c_double(0)
+        L.thr_profile_read(h, kind, C.byref(n), C.byref(t), C.byref(b), C.byref(tot))
+        prof[name] = dict(sampled=n.value, ms=t.value, bytes=b.value, launches=tot.value)
+    # the batched solver enqueues 16 iterations of 7 kernels plus 3 per batch (flush
+    # coefficients, flush, history reset); 3 set-up kernels and the pole sum per solve
+    launches = int(sum(3 + ((i + 15) // 16) * (16 * 7 + 3) + 1 for i in its))
 
     # ---- plain FP64 GPU path for comparison: FP64 everywhere and the reference's
     # loop structure (every shift field updated in every iteration)
@@ -508,6 +518,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--lx", type=int, default=0, help="profiling case: lattice extent (all three directions)")
     ap.add_argument("--ls", type=int, default=0, help="profiling case: fifth-dimension extent")
+    ap.add_argument("--poles", type=int, default=0, help="profiling case: number of poles")
     ap.add_argument("--no-dslash", action="store_true")
     ap.add_argument("--no-compare-plain", dest="compare_plain", action="store_false",
                     help="skip timing the plain FP64 path (reference loop structure)")
@@ -518,11 +529,12 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     iters_for_cpu = FP64_ITERS_REF
 
-    if args.lx or args.ls:
+    if args.lx or args.ls or args.poles:
         # a smaller (or larger) profiling case of the same solve; not the headline workload
-        global LX, LY, LT, LS
+        global LX, LY, LT, LS, NPOLE
         LX = LY = LT = args.lx or LX
         LS = args.ls or LS
+        NPOLE = args.poles or NPOLE
     if args.workload == "dslash":
         lx, ls = args.lx or 48, args.ls or 48
         r = dslash_bandwidth(args, local_rank, lx, ls, args.steps, args.warmup)
@@ -578,19 +590,28 @@ def main():
     ms_step = r["ms"] / args.steps
     value = job_throughput(world, args.steps, r["ms"])
     peak, peak_kind = peaks()
+    # per kernel: sampled launches give the mean duration and bytes per launch; the
+    # kernel's time in the step is that mean times its launches
+    kern = {}
+    for name, p in r["prof"].items():
+        if not p["sampled"] or p["ms"] <= 0:
+            continue
+        us = p["ms"] * 1e3 / p["sampled"]
+        bpl = p["bytes"] / p["sampled"]
+        kern[name] = {"launches": int(p["launches"]), "sampled": p["sampled"], "us_per_launch": round(us, 3),
+                      "algorithmic_bytes_per_launch": round(bpl), "gbs": round(bpl / us / 1e3, 1),
+                      "share_of_step": round(p["launches"] * us / 1e3 / r["ms"], 4)}
     # dominant kernel of the timed region
-    name, (nl, tms, byts) = max(r["prof"].items(), key=lambda kv: kv[1][1])
-    achieved = byts / (tms / 1e3) / 1e9 if tms > 0 else None
-    # the batched solver's shift-field update is the folded flush kernel
-    kname = {"dslash": "k_dslash", "multishift_update": "k_flush"}[name]
-    traffic = ncu_traffic(kname)
-    roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1) if achieved else None,
-                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
-                "peak_source": peak_kind, "traffic": traffic,
-                "algorithmic_bytes_per_launch": byts / max(nl, 1), "launches": nl,
-                "share_of_step": round(tms / r["ms"], 3)}
-    other = {k: {"launches": v[0], "ms": round(v[1], 3), "gbs": round(v[2] / (v[1] / 1e3) / 1e9, 1) if v[1] else None}
-             for k, v in r["prof"].items()}
+    name = max(kern, key=lambda k: kern[k]["share_of_step"])
+    k = kern[name]
+    achieved = k["gbs"]
+    traffic = ncu_traffic(name, k["algorithmic_bytes_per_launch"])
+    roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": k["algorithmic_bytes_per_launch"],
+                "us_per_launch": k["us_per_launch"], "launches": k["launches"], "sampled_launches": k["sampled"],
+                "share_of_step": k["share_of_step"]}
+    other = kern
     cpu = None
     if not args.no_cpu:
         s_iter, nthreads = cpu_sample(args.cpu_iters)

@@ -327,12 +327,16 @@ int thr_qmrherm_dev(thr_ctx *ctx, const void *Phi, void *x, float res, int *iter
 int thr_sync(thr_ctx *ctx);
 /* the context's cudaStream_t, for event timing by the caller */
 int thr_get_stream(thr_ctx *ctx, void **stream);
-/* Kernel timing: with profiling enabled the solvers bracket each launch of
- * the stencil (kind 0) and of the multishift vector update (kind 1) with
- * CUDA events; thr_profile_read returns the launches, their summed device
- * time in ms and the algorithmic bytes those launches moved. */
-int thr_profile(thr_ctx *ctx, int enable, int reset);
-int thr_profile_read(thr_ctx *ctx, int kind, int *launches, double *ms, double *bytes);
+/* Kernel timing inside the multishift solvers.  thr_profile(ctx, stride, reset):
+ * stride 0 turns it off; stride k >= 1 brackets every k-th launch of each kind
+ * with CUDA events on the context's stream -- kind 0 the stencil M, kind 2 the
+ * stencil M^dagger with its fused dot product, kind 1 the shift-field update
+ * (k_flush, or k_ms_pshift in the per-iteration solver).  thr_profile_read
+ * returns, for one kind, the sampled launches that did work, their summed
+ * device time in ms and their summed algorithmic bytes, and the number of
+ * launches of that kind that did work (sampled or not). */
+int thr_profile(thr_ctx *ctx, int stride, int reset);
+int thr_profile_read(thr_ctx *ctx, int kind, int *sampled, double *ms, double *bytes, double *launches);
 
 #ifdef __cplusplus
 }

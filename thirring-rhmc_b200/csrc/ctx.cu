@@ -34,8 +34,9 @@ int thr_ctx::buffer(int id, size_t bytes, void** out) {
   return THR_OK;
 }
 
-int thr_ctx::prof_begin(int kind, double bytes) {
+int thr_ctx::prof_begin(int kind, double bytes, long long tag) {
   if (!prof_on) return -1;
+  if (prof_seen[kind]++ % prof_stride) return -1;
   const int idx = (int)prof_kind.size();
   if (2 * idx + 2 > (int)prof_ev.size()) {
     for (int k = 0; k < 256; k++) {
@@ -46,11 +47,19 @@ int thr_ctx::prof_begin(int kind, double bytes) {
   }
   prof_kind.push_back(kind);
   prof_bytes.push_back(bytes);
+  prof_tag.push_back(tag);
   cudaEventRecord(prof_ev[2 * idx], st);
   return idx;
 }
 void thr_ctx::prof_end(int idx) {
   if (idx >= 0) cudaEventRecord(prof_ev[2 * idx + 1], st);
+}
+void thr_ctx::prof_set_bytes(int idx, double bytes) {
+  if (idx >= 0 && idx < (int)prof_bytes.size()) prof_bytes[idx] = bytes;
+}
+void thr_ctx::prof_trim(size_t first, long long iters) {
+  for (size_t i = first; i < prof_kind.size(); i++)
+    if (prof_tag[i] >= iters) prof_kind[i] = -1;
 }
 
 int thr_ctx::upload_spinor(double2* dst, const double* host) {
@@ -150,7 +159,7 @@ int thr_create(const thr_params* p, thr_ctx** out) {
   c->stage_elems = c->nf5();
   if (!rc && cudaMalloc(&c->stage, c->stage_elems * sizeof(double2)) != cudaSuccess) rc = THR_ERR_NOMEM;
   // per-block partial sums: the stencil epilogue writes one per block of its grid
-  const size_t nparts = std::max<size_t>((size_t)kMaxPartials * 8, (size_t)stencil_grid(c->g) + 1024);
+  const size_t nparts = std::max<size_t>((size_t)kMaxPartials * 8, (size_t)std::max(stencil_grid(c->g, 0), stencil_grid(c->g, 1)) + 1024);
   if (!rc && cudaMalloc(&c->partials, nparts * sizeof(double)) != cudaSuccess) rc = THR_ERR_NOMEM;
   if (!rc && cudaMalloc(&c->dscal, 4096 * sizeof(double)) != cudaSuccess) rc = THR_ERR_NOMEM;
   if (!rc && cudaMalloc(&c->iscal, 1024 * sizeof(int)) != cudaSuccess) rc = THR_ERR_NOMEM;
@@ -339,35 +348,40 @@ int thr_sync(thr_ctx* c) {
   return c->sync();
 }
 
-int thr_profile(thr_ctx* c, int enable, int reset) {
-  if (!c) return THR_ERR_BADARG;
+int thr_profile(thr_ctx* c, int stride, int reset) {
+  if (!c || stride < 0) return THR_ERR_BADARG;
   cudaSetDevice(c->dev);
   if (reset) {
     cudaStreamSynchronize(c->st);
     c->prof_kind.clear();
     c->prof_bytes.clear();
-    for (double& b : c->prof_eff_bytes) b = 0.0;
+    c->prof_tag.clear();
+    for (long long& n : c->prof_seen) n = 0;
+    for (double& n : c->prof_work) n = 0.0;
   }
-  c->prof_on = enable != 0;
+  c->prof_on = stride != 0;
+  if (stride > 0) c->prof_stride = stride;
   return THR_OK;
 }
 
-int thr_profile_read(thr_ctx* c, int kind, int* launches, double* ms, double* bytes) {
+int thr_profile_read(thr_ctx* c, int kind, int* sampled, double* ms, double* bytes, double* launches) {
   if (!c || kind < 0 || kind >= thr_ctx::P_COUNT) return THR_ERR_BADARG;
   cudaSetDevice(c->dev);
   THR_CUDA(cudaStreamSynchronize(c->st));
   int cnt = 0;
-  double tot = 0.0;
+  double tot = 0.0, byt = 0.0;
   for (size_t i = 0; i < c->prof_kind.size(); i++) {
     if (c->prof_kind[i] != kind) continue;
     float e = 0.0f;
     THR_CUDA(cudaEventElapsedTime(&e, c->prof_ev[2 * i], c->prof_ev[2 * i + 1]));
     tot += e;
+    byt += c->prof_bytes[i];
     cnt++;
   }
-  if (launches) *launches = cnt;
+  if (sampled) *sampled = cnt;
   if (ms) *ms = tot;
-  if (bytes) *bytes = c->prof_eff_bytes[kind];
+  if (bytes) *bytes = byt;
+  if (launches) *launches = c->prof_work[kind];
   return THR_OK;
 }
 

@@ -83,14 +83,21 @@ struct thr_ctx {
   int buffer(int id, size_t bytes, void** out);  // contents preserved only if not regrown
 
   // optional per-kernel timing: CUDA events around selected launches
-  enum ProfKernel { P_DSLASH = 0, P_SHIFTUPD = 1, P_COUNT = 4 };
+  // kernel timing: every prof_stride-th launch of each kind is bracketed by events
+  enum ProfKernel { P_DSLASH = 0, P_SHIFTUPD = 1, P_DSLASH_EPI = 2, P_COUNT = 4 };
   bool prof_on = false;
-  std::vector<cudaEvent_t> prof_ev;  // pairs
-  std::vector<int> prof_kind;
-  std::vector<double> prof_bytes;
-  double prof_eff_bytes[P_COUNT] = {};  // algorithmic bytes of the launches that did work
-  int prof_begin(int kind, double bytes);  // returns pair index or -1
+  int prof_stride = 1;
+  long long prof_seen[P_COUNT] = {};         // launches offered to prof_begin
+  double prof_work[P_COUNT] = {};            // launches that did work (guarded launches excluded)
+  std::vector<cudaEvent_t> prof_ev;          // pairs
+  std::vector<int> prof_kind;                // -1: dropped (a launch that skipped its work)
+  std::vector<double> prof_bytes;            // algorithmic bytes of the sampled launch
+  std::vector<long long> prof_tag;           // iteration of the sampled launch within its solve
+  int prof_begin(int kind, double bytes, long long tag = -1);  // returns pair index or -1
   void prof_end(int idx);
+  void prof_set_bytes(int idx, double bytes);
+  // drop the sampled launches since entry `first` whose tag is >= iters (skipped work)
+  void prof_trim(size_t first, long long iters);
 
   size_t n4() const { return (size_t)g.v5 * 4; }  // complex elements of one spinor
   size_t nf5() const { return (size_t)(g.ls + 2) * (g.lx + 2) * (g.ly + 2) * (g.lt + 2) * 4; }

@@ -65,7 +65,32 @@ __device__ __forceinline__ void block_partial(double v, double* out) {
 }
 
 // ---------------------------------------------------------------- Shamir
-template <class S, bool DAG>
+// One hop of the 3D Wilson-Dirac term, spin-projected.  The reference adds
+// -1/2 [T(d) -+ 2gamma(mu,d) T(gin)] with T = W R(neighbour) for each d
+// (dirac.F90:49-76, :464-491).  2gamma(mu,.) is a Hermitian unitary permutation
+// (entries +-1, +-i) pairing each upper spin with a lower one, so
+//   h(d) = R(d) -+ 2gamma(mu,d) R(gin)   for the upper spins d = 0, 1
+// carries the whole hop: W h(d) goes to spin d and -+2gamma(mu,gin) W h(d) to
+// spin gin.  Two complex multiplies per neighbour instead of four; the result
+// differs from the unprojected sum by rounding only.
+template <class C, class R>
+__device__ __forceinline__ void hop_projected(int mu, bool plus, C W, const C* r, C* acc) {
+#pragma unroll
+  for (int d = 0; d < 2; d++) {
+    const GammaEntry ge = gamma_entry(mu, d);
+    const int gi = ge.gin;
+    const C gr = gp(ge, r[gi]);
+    const C wh = cmul(W, plus ? r[d] - gr : r[d] + gr);
+    acc[d] = acc[d] - R(0.5) * wh;
+    const C gw = gp(gamma_entry(mu, gi), wh);
+    acc[gi] = plus ? acc[gi] + R(0.5) * gw : acc[gi] - R(0.5) * gw;
+  }
+}
+
+// SHFL: the fifth-dimension neighbours and wall values come from the lanes of
+// the same site (blockDim.x = Ls a power of two <= 32, so a site's Ls threads
+// are one aligned segment of a warp); every lane must call this.
+template <class S, bool DAG, bool SHFL>
 __device__ __forceinline__ void shamir_site(const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u,
                                             const Geom& g, int s, int site, float am, int imass, float am3,
                                             typename Sto<S>::C* acc) {
@@ -77,69 +102,70 @@ __device__ __forceinline__ void shamir_site(const S* __restrict__ in, const type
   SpinorView<S> Rv{in, g};
   const int Ls = g.ls;
   const R diag = (R)((3.0f - am3) + 1.0f);  // dirac.F90:45, default real
+  C rc[4];
 #pragma unroll
-  for (int d = 0; d < 4; d++) acc[d] = diag * Rv(s, site, d);
-  // s-like term (np_third == 1): dirac.F90:80-87 (M), :317-324 (M^dagger)
-  if (!DAG) {
-    if (s < Ls - 1) { acc[2] = acc[2] - Rv(s + 1, site, 2); acc[3] = acc[3] - Rv(s + 1, site, 3); }
-    if (s > 0) { acc[0] = acc[0] - Rv(s - 1, site, 0); acc[1] = acc[1] - Rv(s - 1, site, 1); }
-  } else {
-    if (s < Ls - 1) { acc[0] = acc[0] - Rv(s + 1, site, 0); acc[1] = acc[1] - Rv(s + 1, site, 1); }
-    if (s > 0) { acc[2] = acc[2] - Rv(s - 1, site, 2); acc[3] = acc[3] - Rv(s - 1, site, 3); }
+  for (int d = 0; d < 4; d++) {
+    rc[d] = Rv(s, site, d);
+    acc[d] = diag * rc[d];
   }
-  // wall mass term: dirac.F90:119-176 (M), :356-402 (M^dagger)
+  // fifth-dimension hop (np_third == 1), dirac.F90:80-87 (M), :317-324 (M^dagger):
+  // spins A take R(s+1), spins B take R(s-1); A = (2,3) for M, (0,1) for M^dagger
+  const int a0 = DAG ? 0 : 2, b0 = DAG ? 2 : 0;
+  C nxt[2], prv[2], w0[2], wl[2];
+  if (SHFL) {
+    const unsigned full = 0xffffffffu;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      nxt[k] = mk(__shfl_down_sync(full, rc[a0 + k].x, 1, Ls), __shfl_down_sync(full, rc[a0 + k].y, 1, Ls));
+      prv[k] = mk(__shfl_up_sync(full, rc[b0 + k].x, 1, Ls), __shfl_up_sync(full, rc[b0 + k].y, 1, Ls));
+      w0[k] = mk(__shfl_sync(full, rc[a0 + k].x, 0, Ls), __shfl_sync(full, rc[a0 + k].y, 0, Ls));
+      wl[k] = mk(__shfl_sync(full, rc[b0 + k].x, Ls - 1, Ls), __shfl_sync(full, rc[b0 + k].y, Ls - 1, Ls));
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    if (s < Ls - 1) acc[a0 + k] = acc[a0 + k] - (SHFL ? nxt[k] : Rv(s + 1, site, a0 + k));
+    if (s > 0) acc[b0 + k] = acc[b0 + k] - (SHFL ? prv[k] : Rv(s - 1, site, b0 + k));
+  }
+  // wall mass term: dirac.F90:119-176 (M), :356-402 (M^dagger).  imass 1, 3 couple
+  // R(1) into s = Ls (spins A) and R(Ls) into s = 1 (spins B); imass 5 mixes the
+  // chiralities at the same s.
   const R a = (R)am;
-  if (!DAG) {
-    if (imass == 1) {
-      const C zk = mk(a, R(0));
-      if (s == Ls - 1) { acc[2] = acc[2] + cmul(zk, Rv(0, site, 2)); acc[3] = acc[3] + cmul(zk, Rv(0, site, 3)); }
-      if (s == 0) { acc[0] = acc[0] + cmul(zk, Rv(Ls - 1, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(Ls - 1, site, 1)); }
-    } else if (imass == 3) {
-      const C zk = mk(R(0), -a);
-      if (s == Ls - 1) { acc[2] = acc[2] - cmul(zk, Rv(0, site, 2)); acc[3] = acc[3] - cmul(zk, Rv(0, site, 3)); }
-      if (s == 0) { acc[0] = acc[0] + cmul(zk, Rv(Ls - 1, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(Ls - 1, site, 1)); }
-    } else if (imass == 5) {
-      const C zk = mk(R(0), -a);
-      if (s == Ls - 1) { acc[2] = acc[2] - cmul(zk, Rv(Ls - 1, site, 0)); acc[3] = acc[3] - cmul(zk, Rv(Ls - 1, site, 1)); }
-      if (s == 0) { acc[0] = acc[0] - cmul(zk, Rv(0, site, 2)); acc[1] = acc[1] - cmul(zk, Rv(0, site, 3)); }
+  if (imass == 1 || imass == 3) {
+    const C zk = imass == 1 ? mk(a, R(0)) : mk(R(0), DAG ? a : -a);
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      if (s == Ls - 1) {
+        const C v = cmul(zk, SHFL ? w0[k] : Rv(0, site, a0 + k));
+        acc[a0 + k] = (imass == 3 && !DAG) ? acc[a0 + k] - v : acc[a0 + k] + v;
+      }
+      if (s == 0) {
+        const C v = cmul(zk, SHFL ? wl[k] : Rv(Ls - 1, site, b0 + k));
+        acc[b0 + k] = (imass == 3 && DAG) ? acc[b0 + k] - v : acc[b0 + k] + v;
+      }
     }
-  } else {
-    if (imass == 1) {
-      const C zk = mk(a, R(0));
-      if (s == Ls - 1) { acc[0] = acc[0] + cmul(zk, Rv(0, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(0, site, 1)); }
-      if (s == 0) { acc[2] = acc[2] + cmul(zk, Rv(Ls - 1, site, 2)); acc[3] = acc[3] + cmul(zk, Rv(Ls - 1, site, 3)); }
-    } else if (imass == 3) {
-      const C zk = mk(R(0), a);
-      if (s == Ls - 1) { acc[0] = acc[0] + cmul(zk, Rv(0, site, 0)); acc[1] = acc[1] + cmul(zk, Rv(0, site, 1)); }
-      if (s == 0) { acc[2] = acc[2] - cmul(zk, Rv(Ls - 1, site, 2)); acc[3] = acc[3] - cmul(zk, Rv(Ls - 1, site, 3)); }
-    } else if (imass == 5) {
-      const C zk = mk(R(0), a);
-      if (s == Ls - 1) { acc[0] = acc[0] - cmul(zk, Rv(Ls - 1, site, 2)); acc[1] = acc[1] - cmul(zk, Rv(Ls - 1, site, 3)); }
-      if (s == 0) { acc[2] = acc[2] - cmul(zk, Rv(0, site, 0)); acc[3] = acc[3] - cmul(zk, Rv(0, site, 1)); }
+  } else if (imass == 5) {
+    const C zk = mk(R(0), DAG ? a : -a);
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      if (s == Ls - 1) acc[a0 + k] = acc[a0 + k] - cmul(zk, rc[b0 + k]);
+      if (s == 0) acc[b0 + k] = acc[b0 + k] - cmul(zk, rc[a0 + k]);
     }
   }
-  // Wilson and Dirac hopping terms (dirac.F90:49-76, :464-491).  The forward
-  // (U R(x+mu)) and backward (conj U(x-mu) R(x-mu)) halves are accumulated one
-  // after the other, so only one neighbour's four spins are live at a time
-  // (register pressure, hence occupancy): acc -= 1/2 T(d) +/- gamma(mu,d) T(gin).
-  // The reference adds these before (M) or after (M^dagger) the fifth-
-  // dimension and mass terms; the order only affects rounding.
+  // Wilson and Dirac hopping terms, forward (U R(x+mu)) then backward
+  // (conj U(x-mu) R(x-mu)) per direction; +gamma forward and -gamma backward in
+  // M, the opposite in M^dagger.  The reference adds them before (M) or after
+  // (M^dagger) the fifth-dimension and mass terms; the order only affects rounding.
 #pragma unroll
   for (int mu = 0; mu < 3; mu++) {
 #pragma unroll
     for (int dir = 0; dir < 2; dir++) {
       const int ns = dir == 0 ? nb.f[mu] : nb.b[mu];
       const C W = dir == 0 ? __ldg(u + (size_t)mu * g.v3 + site) : cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
-      C T[4];
+      C r[4];
 #pragma unroll
-      for (int d = 0; d < 4; d++) T[d] = cmul(W, Rv(s, ns, d));
-#pragma unroll
-      for (int d = 0; d < 4; d++) {
-        const GammaEntry ge = gamma_entry(mu, d);
-        const C gt = gmul<C, R>(ge, T[ge.gin]);
-        // forward: + gamma (M), - gamma (M^dagger); backward: the opposite sign
-        acc[d] = ((dir == 0) != DAG) ? (acc[d] - R(0.5) * T[d]) + gt : (acc[d] - R(0.5) * T[d]) - gt;
-      }
+      for (int d = 0; d < 4; d++) r[d] = Rv(s, ns, d);
+      hop_projected<C, R>(mu, (dir == 0) != DAG, W, r, acc);
     }
   }
 }
@@ -191,20 +217,16 @@ __device__ __forceinline__ void wilson_site(const S* __restrict__ in, const type
     wilson_q<S>(Rv, s, site, Ls, c1, c2, q);
 #pragma unroll
     for (int d = 0; d < 4; d++) res[d] = (dgw - R(1)) * q[d] + R(2) * Rv(s, site, d);
+    // D_W hops of Q (dirac.F90:197-217), spin-projected as in the Shamir kernel
 #pragma unroll
     for (int mu = 0; mu < 3; mu++) {
       const C U = __ldg(u + (size_t)mu * g.v3 + site);
       const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
-      C qf[4], qb[4], A[4], B[4];
-      wilson_q<S>(Rv, s, nb.f[mu], Ls, c1, c2, qf);
-      wilson_q<S>(Rv, s, nb.b[mu], Ls, c1, c2, qb);
-#pragma unroll
-      for (int d = 0; d < 4; d++) { A[d] = cmul(U, qf[d]); B[d] = cmul(Ub, qb[d]); }
-#pragma unroll
-      for (int d = 0; d < 4; d++) {
-        const GammaEntry ge = gamma_entry(mu, d);
-        res[d] = (res[d] - R(0.5) * (A[d] + B[d])) + gmul<C, R>(ge, A[ge.gin] - B[ge.gin]);
-      }
+      C q[4];
+      wilson_q<S>(Rv, s, nb.f[mu], Ls, c1, c2, q);
+      hop_projected<C, R>(mu, true, U, q, res);
+      wilson_q<S>(Rv, s, nb.b[mu], Ls, c1, c2, q);
+      hop_projected<C, R>(mu, false, Ub, q, res);
     }
   } else {
     // z = -am | -i am (upper right, dirac.F90:602-606); z' = -am | +i am (lower left, :615-619)
@@ -224,51 +246,61 @@ __device__ __forceinline__ void wilson_site(const S* __restrict__ in, const type
         const int d = 2 * half + k;
         res[d] = (dgw - R(1)) * q[d] + R(2) * Rv(s, site, d);
       }
+      // D_W^dagger hops (dirac.F90:511-531): -1/2 W [q(d) +- 2gamma(mu,d) q(gin)], only
+      // the output spins of this half (their partners belong to the other half)
 #pragma unroll
       for (int mu = 0; mu < 3; mu++) {
         const C U = __ldg(u + (size_t)mu * g.v3 + site);
         const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
-        C qf[4], qb[4];
-        wilson_qd<S>(Rv, s, nb.f[mu], sn, inner, sw, zz, qf);
-        wilson_qd<S>(Rv, s, nb.b[mu], sn, inner, sw, zz, qb);
 #pragma unroll
-        for (int k = 0; k < 2; k++) {
-          const int d = 2 * half + k;
-          const GammaEntry ge = gamma_entry(mu, d);
-          const C w = R(0.5) * (cmul(U, qf[d]) + cmul(Ub, qb[d]));
-          const C dd = gmul<C, R>(ge, cmul(U, qf[ge.gin]) - cmul(Ub, qb[ge.gin]));
-          res[d] = (res[d] - w) - dd;
+        for (int dir = 0; dir < 2; dir++) {
+          C q[4];
+          wilson_qd<S>(Rv, s, dir == 0 ? nb.f[mu] : nb.b[mu], sn, inner, sw, zz, q);
+          const C W = dir == 0 ? U : Ub;
+#pragma unroll
+          for (int k = 0; k < 2; k++) {
+            const int d = 2 * half + k;
+            const GammaEntry ge = gamma_entry(mu, d);
+            const C gq = gp(ge, q[ge.gin]);
+            res[d] = res[d] - R(0.5) * cmul(W, dir == 0 ? q[d] + gq : q[d] - gq);
+          }
         }
       }
     }
   }
 }
 
-template <class S, int KER, bool DAG>
+template <class S, int KER, bool DAG, bool SHFL = false>
 __device__ __forceinline__ void apply_site(const S* in, const typename Sto<S>::C* u, const Geom& g, int s, int site,
                                            float am, int imass, float am3, typename Sto<S>::C* acc) {
-  if (KER == 0) shamir_site<S, DAG>(in, u, g, s, site, am, imass, am3, acc);
+  if (KER == 0) shamir_site<S, DAG, SHFL>(in, u, g, s, site, am, imass, am3, acc);
   else wilson_site<S, DAG>(in, u, g, s, site, am, imass, am3, acc);
 }
 
 // ---------------------------------------------------------------- kernels
-template <class S, int KER, bool DAG, int EPI>
-__global__ void __launch_bounds__(256, KER == 0 ? 4 : 1) k_dslash(S* __restrict__ out, const S* __restrict__ in,
-                                                                 const typename Sto<S>::C* __restrict__ u, Geom g,
-                                                                 float am, int imass, float am3, const int* skip,
-                                                                 const S* __restrict__ aux, double* __restrict__ partials) {
+// One thread per 5D site: blockDim = (Ls, sites per block), NT threads at most.
+// Shamir blocks are small (NT = 128, 8 resident per SM at <= 64 registers):
+// the kernel is latency-bound, and small blocks keep more loads in flight.
+template <class S, int KER, bool DAG, int EPI, int NT, bool SHFL>
+__global__ void __launch_bounds__(NT, (KER == 0 && NT <= 128) ? 1024 / NT : 1)
+    k_dslash(S* __restrict__ out, const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u, Geom g, float am,
+             int imass, float am3, const int* skip, const S* __restrict__ aux, double* __restrict__ partials) {
   if (skip && *skip) return;
   using C = typename Sto<S>::C;
   const int s = threadIdx.x;
   double racc = 0.0;
   const int site = blockIdx.x * blockDim.y + threadIdx.y;
-  if (site < g.v3) {
+  const bool live = site < g.v3;
+  if (SHFL || live) {  // with SHFL every lane takes part (the last block's spare rows on a clamped site)
+    const int st = live ? site : g.v3 - 1;
     C acc[4];
-    apply_site<S, KER, DAG>(in, u, g, s, site, am, imass, am3, acc);
+    apply_site<S, KER, DAG, SHFL>(in, u, g, s, st, am, imass, am3, acc);
+    if (live) {
 #pragma unroll
-    for (int d = 0; d < 4; d++) {
-      Sto<S>::st(out, sidx(g, s, site, d), acc[d]);
-      if (EPI == 1) racc += epi_redot<S>(aux, sidx(g, s, site, d), acc[d]);
+      for (int d = 0; d < 4; d++) {
+        Sto<S>::st(out, sidx(g, s, site, d), acc[d]);
+        if (EPI == 1) racc += epi_redot<S>(aux, sidx(g, s, site, d), acc[d]);
+      }
     }
   }
   if (EPI == 1) block_partial(racc, partials + blockIdx.x);
@@ -312,16 +344,24 @@ __global__ void __launch_bounds__(256, KER == 0 ? 4 : 1)
 }
 
 // ---------------------------------------------------------------- launch
-dim3 stencil_block(const Geom& g) {
-  int spb = 256 / g.ls;
+namespace {
+int stencil_threads(const Geom& g, int kernel) {
+  const int nt = kernel == 0 ? 128 : 256;
+  return g.ls <= nt ? nt : 1024;
+}
+bool stencil_shfl(const Geom& g, int kernel) { return kernel == 0 && g.ls <= 32 && (g.ls & (g.ls - 1)) == 0; }
+}  // namespace
+
+dim3 stencil_block(const Geom& g, int kernel) {
+  int spb = stencil_threads(g, kernel) / g.ls;
   if (spb < 1) spb = 1;
   return dim3(g.ls, spb, 1);
 }
 
 // one block row per site: ceil(V3 / sites per block) blocks (each writes one
 // partial when an epilogue reduction is requested)
-unsigned stencil_grid(const Geom& g) {
-  const dim3 blk = stencil_block(g);
+unsigned stencil_grid(const Geom& g, int kernel) {
+  const dim3 blk = stencil_block(g, kernel);
   return (unsigned)((g.v3 + blk.y - 1) / blk.y);
 }
 
@@ -330,17 +370,25 @@ int launch_dslash_epi(const Geom& g, int kernel, bool dag, S* out, const S* in, 
                       int imass, float am3, cudaStream_t st, const int* skip, const S* aux, double* partials) {
   if (g.ls > 1024) return THR_ERR_BADSHAPE;
   if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
-  const dim3 blk = stencil_block(g);
-  const dim3 grd(stencil_grid(g));
-  const bool epi = aux != nullptr;
-#define THR_L(K, D, E) k_dslash<S, K, D, E><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, partials)
+  const dim3 blk = stencil_block(g, kernel);
+  const dim3 grd(stencil_grid(g, kernel));
+  const int nt = stencil_threads(g, kernel);
+  const bool shfl = stencil_shfl(g, kernel);
+  const int e = aux != nullptr;
+#define THR_L(K, D, E, N, SH) \
+  k_dslash<S, K, D, E, N, SH><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, partials)
+#define THR_E(K, D, N, SH) \
+  do { if (e) THR_L(K, D, 1, N, SH); else THR_L(K, D, 0, N, SH); } while (0)
   if (kernel == 1) {
-    if (dag) { if (epi) THR_L(1, true, 1); else THR_L(1, true, 0); }
-    else { if (epi) THR_L(1, false, 1); else THR_L(1, false, 0); }
+    if (nt == 256) { if (dag) THR_E(1, true, 256, false); else THR_E(1, false, 256, false); }
+    else { if (dag) THR_E(1, true, 1024, false); else THR_E(1, false, 1024, false); }
+  } else if (nt == 128) {
+    if (shfl) { if (dag) THR_E(0, true, 128, true); else THR_E(0, false, 128, true); }
+    else { if (dag) THR_E(0, true, 128, false); else THR_E(0, false, 128, false); }
   } else {
-    if (dag) { if (epi) THR_L(0, true, 1); else THR_L(0, true, 0); }
-    else { if (epi) THR_L(0, false, 1); else THR_L(0, false, 0); }
+    if (dag) THR_E(0, true, 1024, false); else THR_E(0, false, 1024, false);
   }
+#undef THR_E
 #undef THR_L
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }

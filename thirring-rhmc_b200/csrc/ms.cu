@@ -211,19 +211,23 @@ int multishift_dev(thr_ctx* c, const V* u_dummy, const V* in, V* out, V* sf, V* 
   const void* u = sp ? (const void*)c->u32 : (const void*)c->u64;
   const int chunk = 8;
   int it_host = 0;
+  const double lb = sp ? sizeof(float2) : sizeof(double2);
+  const double b_m = 2.0 * n * sizeof(V) + 3.0 * c->g.v3 * lb;
+  const size_t prof_first = c->prof_kind.size();
   for (;;) {
     for (int k = 0; k < chunk; k++) {
-      int pe = c->prof_begin(thr_ctx::P_DSLASH, 0);
+      const long long tag = it_host + k;
+      int pe = c->prof_begin(thr_ctx::P_DSLASH, b_m, tag);
       THR_TRY(launch_dslash_guarded<V>(c, false, hv, p, (const V*)u, am, imass, &ms->done));
       c->prof_end(pe);
-      pe = c->prof_begin(thr_ctx::P_DSLASH, 0);
+      pe = c->prof_begin(thr_ctx::P_DSLASH, b_m, tag);
       THR_TRY(launch_dslash_guarded<V>(c, true, s, hv, (const V*)u, am, imass, &ms->done));
       c->prof_end(pe);
       k_redot<V><<<gb, kThreads, 0, c->st>>>(ms, p, s, n, c->partials);
       k_ms_alpha<<<1, 256, 0, c->st>>>(ms, c->partials, gb);
       k_ms_rupdate<V><<<gb, kThreads, 0, c->st>>>(ms, r, s, n, c->partials);
       k_ms_lambda<<<1, 256, 0, c->st>>>(ms, c->partials, gb);
-      pe = c->prof_begin(thr_ctx::P_SHIFTUPD, 0);
+      pe = c->prof_begin(thr_ctx::P_SHIFTUPD, 0.0, tag);
       k_ms_pshift<V><<<gb, kThreads, 0, c->st>>>(ms, p, r, out, sf, n, stride);
       c->prof_end(pe);
       k_ms_converge<<<1, 1, 0, c->st>>>(ms);
@@ -235,11 +239,14 @@ int multishift_dev(thr_ctx* c, const V* u_dummy, const V* in, V* out, V* sf, V* 
     if (it_host > maxcg + 2 * chunk) return THR_ERR_CUDA;  // the device state stopped advancing
   }
   if (c->prof_on) {
-    // algorithmic traffic of the work done: dslash = read R + write Phi + read links;
-    // shift update = r, p read + p write + (out, sf) read + write per active shift
-    const double lb = sp ? sizeof(float2) : sizeof(double2);
-    c->prof_eff_bytes[thr_ctx::P_DSLASH] += 2.0 * h->it * (2.0 * n * sizeof(V) + 3.0 * c->g.v3 * lb);
-    c->prof_eff_bytes[thr_ctx::P_SHIFTUPD] += (3.0 * h->it + 4.0 * h->active_sum) * n * sizeof(V);
+    // shift update = r, p read + p write + (out, sf) read + write per active shift; the
+    // active count of one iteration is not recorded, so each sampled launch gets the mean
+    c->prof_trim(prof_first, h->it);
+    const double per = h->it > 0 ? (3.0 + 4.0 * h->active_sum / h->it) * n * sizeof(V) : 0.0;
+    for (size_t i = prof_first; i < c->prof_kind.size(); i++)
+      if (c->prof_kind[i] == thr_ctx::P_SHIFTUPD) c->prof_bytes[i] = per;
+    c->prof_work[thr_ctx::P_DSLASH] += 2.0 * h->it;
+    c->prof_work[thr_ctx::P_SHIFTUPD] += h->it;
   }
   if (cg_return) *cg_return = h->it;
   if (cg_returns)

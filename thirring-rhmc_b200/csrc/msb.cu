@@ -249,18 +249,25 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
   k_fill<V><<<gb, kThreads, 0, c->st>>>(sf, in, n, stride, ndiagq);
   const bool sp = sizeof(V) == sizeof(float2);
   const V* u = sp ? (const V*)(const void*)c->u32 : (const V*)(const void*)c->u64;
-  const unsigned gs = stencil_grid(c->g);
+  const unsigned gs = stencil_grid(c->g, c->p.kernel);
+  // algorithmic bytes: M reads R, writes Phi, reads the links; M^dagger with the
+  // fused <p, M^dagger M p> also reads p
+  const double lb = sp ? sizeof(float2) : sizeof(double2);
+  const double b_m = 2.0 * n * sizeof(V) + 3.0 * c->g.v3 * lb, b_md = b_m + (double)n * sizeof(V);
+  const size_t prof_first = c->prof_kind.size();
+  double flushed = 0.0;
+  long long flushes = 0;
   long long k = 0;
   for (;;) {
     const long long base = k;
     for (int j = 0; j < kBatch; j++, k++) {
       V* rold = ring + (size_t)(k % ring_len) * n;
       V* rnew = ring + (size_t)((k + 1) % ring_len) * n;
-      int pe = c->prof_begin(thr_ctx::P_DSLASH, 0);
+      int pe = c->prof_begin(thr_ctx::P_DSLASH, b_m, k);
       THR_TRY(launch_dslash<V>(c->g, c->p.kernel, false, hv, p, (const typename Sto<V>::C*)u, am, imass, c->p.am3,
                                c->st, &ms->done));
       c->prof_end(pe);
-      pe = c->prof_begin(thr_ctx::P_DSLASH, 0);
+      pe = c->prof_begin(thr_ctx::P_DSLASH_EPI, b_md, k);
       THR_TRY(launch_dslash_epi<V>(c->g, c->p.kernel, true, s, hv, (const typename Sto<V>::C*)u, am, imass,
                                    c->p.am3, c->st, &ms->done, p, c->partials));
       c->prof_end(pe);
@@ -270,22 +277,26 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
       k_pupdate<V><<<gb, kThreads, 0, c->st>>>(ms, p, rnew, n);
       k_converge<<<1, 1, 0, c->st>>>(ms);
     }
-    int pe = c->prof_begin(thr_ctx::P_SHIFTUPD, 0);
+    int pe = c->prof_begin(thr_ctx::P_SHIFTUPD, 0.0, base);
     k_flush_coef<<<1, kMaxShift, 0, c->st>>>(ms, hist, cf);
     k_flush<V><<<gb, kThreads, 0, c->st>>>(cf, out, sf, ring, (int)(base % ring_len), ring_len, n, stride);
     c->prof_end(pe);
     k_reset<<<1, 1, 0, c->st>>>(hist);
     THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
     THR_CUDA(cudaStreamSynchronize(c->st));
+    // flush traffic: each recorded step's residual read once, each shift field of the
+    // batch's window read and written once (out and sf)
+    c->prof_set_bytes(pe, (h->flush_fields - flushed) * n * sizeof(V));
+    if (h->flush_fields > flushed) flushes++;
+    flushed = h->flush_fields;
     if (h->done) break;
     if (k > (long long)maxcg + 2 * kBatch) return THR_ERR_CUDA;  // the device state stopped advancing
   }
   if (c->prof_on) {
-    const double lb = sp ? sizeof(float2) : sizeof(double2);
-    c->prof_eff_bytes[thr_ctx::P_DSLASH] += 2.0 * h->it * (2.0 * n * sizeof(V) + 3.0 * c->g.v3 * lb);
-    // flush: each recorded step's residual read once, each shift field of the batch's
-    // window read and written once (out and sf)
-    c->prof_eff_bytes[thr_ctx::P_SHIFTUPD] += h->flush_fields * n * sizeof(V);
+    c->prof_trim(prof_first, h->it);  // launches after convergence skipped their work
+    c->prof_work[thr_ctx::P_DSLASH] += h->it;
+    c->prof_work[thr_ctx::P_DSLASH_EPI] += h->it;
+    c->prof_work[thr_ctx::P_SHIFTUPD] += flushes;
   }
   if (cg_return) *cg_return = h->it;
   if (cg_returns)

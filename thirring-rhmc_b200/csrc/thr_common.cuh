@@ -155,4 +155,11 @@ __device__ __forceinline__ C gmul(GammaEntry e, C z) {
   return (e.im > 0) ? mk(-(h * z.y), h * z.x) : mk(h * z.y, -(h * z.x));
 }
 
+// (2 gamma(mu,d)) * z, exact: a sign and possibly a swap (2 gamma entries are +-1, +-i)
+template <class C>
+__device__ __forceinline__ C gp(GammaEntry e, C z) {
+  if (e.re != 0) return e.re > 0 ? z : mk(-z.x, -z.y);
+  return e.im > 0 ? mk(-z.y, z.x) : mk(z.y, -z.x);
+}
+
 }  // namespace thr

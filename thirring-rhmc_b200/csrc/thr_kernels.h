@@ -8,8 +8,8 @@ namespace thr {
 // number of per-block partial sums a reduction may write (>= any grid used)
 constexpr int kMaxPartials = 4096;
 
-dim3 stencil_block(const Geom& g);
-unsigned stencil_grid(const Geom& g);  // bounded grid: the stencil kernels are grid-stride over sites
+dim3 stencil_block(const Geom& g, int kernel);
+unsigned stencil_grid(const Geom& g, int kernel);  // blocks of one stencil launch (= partials it writes)
 
 // dslash.cu
 template <class S>

@@ -86,7 +86,7 @@ SIGNATURES = {
     "thr_qmrherm_dev": (_i, [_v, _v, _v, _f, _pi, _f, _i, _v, _v, _i, _i, _i, _v]),
     "thr_set_solver": (_i, [_v, _i]),
     "thr_profile": (_i, [_v, _i, _i]),
-    "thr_profile_read": (_i, [_v, _i, _pi, _pd, _pd]),
+    "thr_profile_read": (_i, [_v, _i, _pi, _pd, _pd, _pd]),
     "thr_sync": (_i, [_v]),
     "thr_get_stream": (_i, [_v, C.POINTER(_v)]),
 }
