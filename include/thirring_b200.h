@@ -189,7 +189,11 @@ int thr_multishift_solver_sp(thr_ctx *ctx, const double *u, float am, int imass,
  *     loop structure (multishift_module.F90:155-176);
  * 1 = (default) the per-shift updates of 16 iterations replayed in one pass
  *     over the shift fields from a ring of the last residuals; the same
- *     per-element arithmetic, about 8x less shift-field traffic. */
+ *     per-element arithmetic, about 8x less shift-field traffic.  The loop over
+ *     batches runs on the device as one CUDA graph (a WHILE conditional node)
+ *     per solve, without host round trips;
+ * 2 = as 1, with the batches launched from the host one at a time (also what
+ *     1 does while kernel profiling is on). */
 int thr_set_solver(thr_ctx *ctx, int multishift_algo);
 
 /* ---- qmrherm_module.F90 -------------------------------------------------- */
@@ -329,8 +333,9 @@ int thr_sync(thr_ctx *ctx);
 int thr_get_stream(thr_ctx *ctx, void **stream);
 /* Kernel timing inside the multishift solvers.  thr_profile(ctx, stride, reset):
  * stride 0 turns it off; stride k >= 1 brackets every k-th launch of each kind
- * with CUDA events on the context's stream -- kind 0 the stencil M, kind 2 the
- * stencil M^dagger with its fused dot product, kind 1 the shift-field update
+ * with CUDA events on the context's stream -- kind 0 the stencil M (in the
+ * batched multishift with its fused |M p|^2), kind 2 the stencil M^dagger
+ * (kind 0 in the per-iteration multishift), kind 1 the shift-field update
  * (k_flush, or k_ms_pshift in the per-iteration solver).  thr_profile_read
  * returns, for one kind, the sampled launches that did work, their summed
  * device time in ms and their summed algorithmic bytes, and the number of

@@ -203,3 +203,27 @@ def test_derivs_reference_fixture():
     with thirring.Lattice(12, 12, 12, 24) as G:
         got = G.derivs(st["R"], st["X"], tau, 0, 0.05, 3, st["dSdpi"].copy(order="F"))
     assert rel_err(got, ref) <= 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sp", [False, True])
+@pytest.mark.parametrize("maxcg", [5000, 21])
+def test_multishift_graph_equals_host_launched(sp, maxcg):
+    """The graph-driven batch loop (WHILE node) runs exactly the kernels of the
+    host-launched loop: identical results, also when the iteration cap ends it."""
+    rng = np.random.default_rng(12)
+    L = O.lat(4, 4, 6, 8)
+    u = rand_links(L, rng)
+    inp = rand_spinor(L, rng)
+    an, ad, _, _ = remez("remez4g", 12)
+    res = 1e-6 if sp else 1e-9
+    outs = []
+    with thirring.Lattice(4, 4, 6, 8) as G:
+        for algo in (1, 2, 1):  # graph, host-launched, graph again (cached graph)
+            G.set_solver(algo)
+            outs.append(G.multishift_solver(u, 0.05, 3, ad, an[1:], inp, res, maxcg, sp=sp))
+    for o, it, cgr in outs[1:]:
+        assert it == outs[0][1] and np.array_equal(cgr, outs[0][2])
+        assert np.array_equal(o, outs[0][0])
+    if maxcg == 21:
+        assert outs[0][1] == 21

@@ -5,6 +5,7 @@
 #include <cstring>
 
 #include "ctx.h"
+#include "ms.h"
 
 using namespace thr;
 
@@ -179,6 +180,7 @@ int thr_destroy(thr_ctx* c) {
   if (!c) return THR_OK;
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
+  ms_graphs_release(c);
   for (auto p : c->w64) cudaFree(p);
   for (auto e : c->prof_ev) cudaEventDestroy(e);
   for (int i = 0; i < thr_ctx::B_COUNT; i++) cudaFree(c->bufs[i]);

@@ -75,6 +75,8 @@ struct thr_ctx {
   int spmd = 1;             // 0: FP64 guidance solves; 1: single-precision (reference)
   int max_qmr_iters = 50000;
   int ms_algo = 1;          // multishift: 0 = per-iteration shift updates, 1 = batched
+  bool use_graphs = true;   // batched solver loops as one CUDA graph (WHILE node) per solve
+  void* ms_graphs[2] = {};  // cached batched-multishift graphs (FP64, FP32 vectors)
   double md_counts[8] = {};  // ancg, ancgpv, ancgf, ancgfpv, ancgh, ancghpv, ancgpf, ancgpfpv
   void* bufs[B_COUNT] = {};
   size_t buf_bytes[B_COUNT] = {};
@@ -84,7 +86,7 @@ struct thr_ctx {
 
   // optional per-kernel timing: CUDA events around selected launches
   // kernel timing: every prof_stride-th launch of each kind is bracketed by events
-  enum ProfKernel { P_DSLASH = 0, P_SHIFTUPD = 1, P_DSLASH_EPI = 2, P_COUNT = 4 };
+  enum ProfKernel { P_DSLASH = 0, P_SHIFTUPD = 1, P_DSLASH_DAG = 2, P_COUNT = 4 };
   bool prof_on = false;
   int prof_stride = 1;
   long long prof_seen[P_COUNT] = {};         // launches offered to prof_begin

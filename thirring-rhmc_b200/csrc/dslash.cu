@@ -45,6 +45,14 @@ __device__ __forceinline__ double epi_redot(const S* aux, size_t i, typename Sto
   return (double)t;
 }
 
+// |v|^2 in the working precision, accumulated in FP64
+template <class S>
+__device__ __forceinline__ double epi_norm(typename Sto<S>::C v) {
+  using R = typename Sto<S>::R;
+  const R t = v.x * v.x + v.y * v.y;
+  return (double)t;
+}
+
 // one FP64 partial per block, fixed reduction order
 __device__ __forceinline__ void block_partial(double v, double* out) {
   __shared__ double sh[32];
@@ -300,10 +308,11 @@ __global__ void __launch_bounds__(NT, (KER == 0 && NT <= 128) ? 1024 / NT : 1)
       for (int d = 0; d < 4; d++) {
         Sto<S>::st(out, sidx(g, s, site, d), acc[d]);
         if (EPI == 1) racc += epi_redot<S>(aux, sidx(g, s, site, d), acc[d]);
+        if (EPI == 2) racc += epi_norm<S>(acc[d]);
       }
     }
   }
-  if (EPI == 1) block_partial(racc, partials + blockIdx.x);
+  if (EPI != 0) block_partial(racc, partials + blockIdx.x);
 }
 
 // Batched stencil: a persistent grid walks the work blocks of all entries
@@ -365,20 +374,25 @@ unsigned stencil_grid(const Geom& g, int kernel) {
   return (unsigned)((g.v3 + blk.y - 1) / blk.y);
 }
 
+// epi: 0 none, 1 Re<aux, out> per block, 2 |out|^2 per block (partials[blockIdx.x])
 template <class S>
-int launch_dslash_epi(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
-                      int imass, float am3, cudaStream_t st, const int* skip, const S* aux, double* partials) {
+int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
+                       int imass, float am3, cudaStream_t st, const int* skip, const S* aux, double* partials,
+                       int e) {
   if (g.ls > 1024) return THR_ERR_BADSHAPE;
   if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
   const dim3 blk = stencil_block(g, kernel);
   const dim3 grd(stencil_grid(g, kernel));
   const int nt = stencil_threads(g, kernel);
   const bool shfl = stencil_shfl(g, kernel);
-  const int e = aux != nullptr;
 #define THR_L(K, D, E, N, SH) \
   k_dslash<S, K, D, E, N, SH><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, partials)
-#define THR_E(K, D, N, SH) \
-  do { if (e) THR_L(K, D, 1, N, SH); else THR_L(K, D, 0, N, SH); } while (0)
+#define THR_E(K, D, N, SH)                 \
+  do {                                     \
+    if (e == 1) THR_L(K, D, 1, N, SH);     \
+    else if (e == 2) THR_L(K, D, 2, N, SH); \
+    else THR_L(K, D, 0, N, SH);            \
+  } while (0)
   if (kernel == 1) {
     if (nt == 256) { if (dag) THR_E(1, true, 256, false); else THR_E(1, false, 256, false); }
     else { if (dag) THR_E(1, true, 1024, false); else THR_E(1, false, 1024, false); }
@@ -391,6 +405,18 @@ int launch_dslash_epi(const Geom& g, int kernel, bool dag, S* out, const S* in, 
 #undef THR_E
 #undef THR_L
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+
+template <class S>
+int launch_dslash_epi(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
+                      int imass, float am3, cudaStream_t st, const int* skip, const S* aux, double* partials) {
+  return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, aux, partials, aux ? 1 : 0);
+}
+
+template <class S>
+int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
+                       float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials) {
+  return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, partials, 2);
 }
 
 template <class S>
@@ -425,6 +451,8 @@ int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const
                                 const int*);                                                                      \
   template int launch_dslash_epi<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,            \
                                     cudaStream_t, const int*, const S*, double*);                                 \
+  template int launch_dslash_norm<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
+                                     cudaStream_t, const int*, double*);                                          \
   template int launch_dslash_batch<S>(const BatchTable&, int, bool, S*, const S*, const L*, float, int, float,    \
                                       cudaStream_t, const int*, const S*, double*, int);
 THR_INST(double2, double2)

@@ -12,6 +12,8 @@ struct MsState {
   float res;
   double active_sum;    // sum over iterations of the shifts updated (for traffic accounting)
   double flush_fields;  // fields moved by the batched shift updates (for traffic accounting)
+  long long kbase;      // batched solver: first iteration of the current batch (ring slot base)
+  int batches, max_batches;  // batched solver: batches run, and the bound on them
   double zeta_i[kMaxShift], zeta_ii[kMaxShift], zeta_iii[kMaxShift];
   double omegas[kMaxShift], gammas[kMaxShift], correction[kMaxShift], aden[kMaxShift];
   int flags[kMaxShift], cg_returns[kMaxShift];
@@ -85,6 +87,9 @@ struct MsCoef {
   int ns, lo, hi, pad;
   double A[kMaxShift], P[kMaxShift], B[kMaxShift][kBatch], Q[kMaxShift][kBatch];
 };
+
+// destroys the cached graphs of the batched solver (context teardown)
+void ms_graphs_release(thr_ctx* c);
 
 template <class V>
 int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p, V* hv, V* s, int ndiagq,

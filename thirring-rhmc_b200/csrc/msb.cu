@@ -13,7 +13,8 @@
 // The algebra is that of the per-iteration form; only the rounding order
 // differs.  Traffic per iteration drops from (3 + 4 n_active) to about
 // (1 + 4 n_active / kBatch) fields.  In addition alpha = Re<p, M^dagger M p>
-// is accumulated in the epilogue of the M^dagger stencil, so s is not re-read.
+// (= |M p|^2) is accumulated in the epilogue of the M stencil from the values
+// it writes, so neither p nor s is re-read for it.
 #include <cmath>
 #include <cstring>
 
@@ -72,11 +73,18 @@ __global__ void k_alpha(MsState* ms, MsHist* hist, const double* partials, int n
   }
 }
 
+// ring slots of iteration kbase + j: r_old in slot (k mod ring_len), r_new in the next
+__device__ __forceinline__ size_t ring_slot(const MsState* ms, int j, int ring_len) {
+  return (size_t)((ms->kbase + j) % ring_len);
+}
+
 // r_new = r_old + omega*s (:137), lambda partials (:138)
 template <class V>
-__global__ void k_rupdate(const MsState* ms, V* rnew, const V* rold, const V* s, size_t n, double* partials) {
+__global__ void k_rupdate(const MsState* ms, V* ring, int j, int ring_len, const V* s, size_t n, double* partials) {
   if (ms->done) return;
   using R = typename W<V>::R;
+  const V* rold = ring + ring_slot(ms, j, ring_len) * n;
+  V* rnew = ring + ring_slot(ms, j + 1, ring_len) * n;
   const R om = W<V>::cast(ms->omega);
   double acc = 0.0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -99,22 +107,21 @@ __global__ void k_lambda(MsState* ms, MsHist* hist, const double* partials, int 
     hist->ga[hist->nsteps][k] = ms->gammas[k];
   }
   __syncthreads();
-  if (threadIdx.x == 0) hist->nsteps += 1;
+  if (threadIdx.x == 0) {
+    hist->nsteps += 1;
+    ms_converge_step(ms);  // :240-258, after the step's gammas are recorded
+  }
 }
 
 // p = r + gammag*p (:145)
 template <class V>
-__global__ void k_pupdate(const MsState* ms, V* p, const V* r, size_t n) {
+__global__ void k_pupdate(const MsState* ms, V* p, const V* ring, int j, int ring_len, size_t n) {
   if (ms->done) return;
   using R = typename W<V>::R;
+  const V* r = ring + ring_slot(ms, j + 1, ring_len) * n;
   const R gg = W<V>::cast(ms->gammag);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     p[i] = r[i] + gg * p[i];
-}
-
-__global__ void k_converge(MsState* ms) {
-  if (ms->done) return;
-  ms_converge_step(ms);
 }
 
 // Fold each shift's recorded steps (:155-176 once per step) into one affine map
@@ -166,12 +173,13 @@ __global__ void k_flush_coef(MsState* ms, const MsHist* hist, MsCoef* cf) {
 
 // apply the folded maps to every shift field of the batch's window
 template <class V>
-__global__ void __launch_bounds__(kThreads) k_flush(const MsCoef* cf, V* __restrict__ out, V* __restrict__ sf,
-                                                   const V* __restrict__ ring, int base, int ring_len, size_t n,
-                                                   size_t stride) {
+__global__ void __launch_bounds__(kThreads) k_flush(const MsCoef* cf, const MsState* ms, V* __restrict__ out,
+                                                   V* __restrict__ sf, const V* __restrict__ ring, int ring_len,
+                                                   size_t n, size_t stride) {
   using R = typename W<V>::R;
   const int ns = cf->ns;
   if (ns == 0) return;
+  const int base = (int)(ms->kbase % ring_len);
   const int lo = cf->lo, hi = cf->hi;
   __shared__ R s_A[kMaxShift], s_P[kMaxShift], s_B[kMaxShift][kBatch], s_Q[kMaxShift][kBatch];
   for (int t = threadIdx.x; t < kMaxShift * kBatch; t += blockDim.x) {
@@ -206,7 +214,28 @@ __global__ void __launch_bounds__(kThreads) k_flush(const MsCoef* cf, V* __restr
     }
   }
 }
-__global__ void k_reset(MsHist* hist) { hist->nsteps = 0; }
+// close a batch: the next one starts kBatch iterations later (launches of
+// iterations after convergence are skipped but still counted, as on the host)
+__global__ void k_reset(MsHist* hist, MsState* ms) {
+  hist->nsteps = 0;
+  ms->kbase += kBatch;
+  ms->batches += 1;
+}
+
+// Loop control of the graph-driven solve: run another batch unless the solve is
+// done.  max_batches bounds the loop whatever the device state holds (the
+// recurrences stop at maxcg iterations; this is the backstop).
+__global__ void k_loop_ctl(MsState* ms, cudaGraphConditionalHandle h) {
+  unsigned more = 1u;
+  if (ms->done) {
+    more = 0u;
+  } else if (ms->batches >= ms->max_batches) {
+    ms->status = THR_ERR_MAXITER;
+    ms->done = 1;
+    more = 0u;
+  }
+  cudaGraphSetConditional(h, more);
+}
 
 template <class V>
 __global__ void k_fill(V* sf, const V* in, size_t n, size_t stride, int nq) {
@@ -223,13 +252,130 @@ inline unsigned vec_grid(size_t n) {
 }
 }  // namespace
 
+namespace {
+// everything one batch of kBatch iterations enqueues (stream order); prof: sample
+// kernel timings with events (stream-launched solves only)
+template <class V>
+int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V* ring, V* p, V* hv, V* s,
+                  float am, int imass, long long k0, bool prof, int* prof_flush) {
+  const size_t n = c->n4();
+  const int ring_len = kBatch + 1;
+  const unsigned gb = vec_grid(n);
+  const unsigned gs = stencil_grid(c->g, c->p.kernel);
+  const bool sp = sizeof(V) == sizeof(float2);
+  const typename Sto<V>::C* u =
+      sp ? (const typename Sto<V>::C*)(const void*)c->u32 : (const typename Sto<V>::C*)(const void*)c->u64;
+  const double lb = sp ? sizeof(float2) : sizeof(double2);
+  // algorithmic bytes: M reads R, writes Phi, reads the links (its |M p|^2 comes
+  // from registers), and so does M^dagger
+  const double b_m = 2.0 * n * sizeof(V) + 3.0 * c->g.v3 * lb;
+  for (int j = 0; j < kBatch; j++) {
+    // alpha = Re<p, M^dagger M p> (:104) evaluated as |M p|^2 in the M epilogue
+    int pe = prof ? c->prof_begin(thr_ctx::P_DSLASH, b_m, k0 + j) : -1;
+    THR_TRY(launch_dslash_norm<V>(c->g, c->p.kernel, false, hv, p, u, am, imass, c->p.am3, c->st, &ms->done,
+                                  c->partials));
+    c->prof_end(pe);
+    pe = prof ? c->prof_begin(thr_ctx::P_DSLASH_DAG, b_m, k0 + j) : -1;
+    THR_TRY(launch_dslash<V>(c->g, c->p.kernel, true, s, hv, u, am, imass, c->p.am3, c->st, &ms->done));
+    c->prof_end(pe);
+    k_alpha<<<1, 1024, 0, c->st>>>(ms, hist, c->partials, gs);
+    k_rupdate<V><<<gb, kThreads, 0, c->st>>>(ms, ring, j, ring_len, s, n, c->partials);
+    k_lambda<<<1, kThreads, 0, c->st>>>(ms, hist, c->partials, gb);
+    k_pupdate<V><<<gb, kThreads, 0, c->st>>>(ms, p, ring, j, ring_len, n);
+  }
+  const int pe = prof ? c->prof_begin(thr_ctx::P_SHIFTUPD, 0.0, k0) : -1;
+  k_flush_coef<<<1, kMaxShift, 0, c->st>>>(ms, hist, cf);
+  k_flush<V><<<gb, kThreads, 0, c->st>>>(cf, ms, out, sf, ring, ring_len, n, n);
+  c->prof_end(pe);
+  if (prof_flush) *prof_flush = pe;
+  k_reset<<<1, 1, 0, c->st>>>(hist, ms);
+  return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+
+// The whole batch loop as one CUDA graph: a WHILE conditional node whose body is
+// one batch followed by k_loop_ctl.  The body reads every per-solve value from
+// device memory (MsState, the ring base), so one instantiated graph serves every
+// solve with the same buffers and operator; it is rebuilt when they change.
+struct MsGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const void *out = nullptr, *sf = nullptr, *ring = nullptr, *p = nullptr, *hv = nullptr, *s = nullptr;
+  const void *u = nullptr, *partials = nullptr, *ms = nullptr, *hist = nullptr, *cf = nullptr;
+  float am = 0.f, am3 = 0.f;
+  int imass = 0, kernel = -1;
+  size_t n = 0;
+  void release() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+};
+
+template <class V>
+int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V* ring, V* p, V* hv, V* s, float am,
+             int imass, cudaGraphExec_t* exec_out) {
+  const int slot = sizeof(V) == sizeof(float2) ? 1 : 0;
+  if (!c->ms_graphs[slot]) c->ms_graphs[slot] = new MsGraph();
+  MsGraph& G = *static_cast<MsGraph*>(c->ms_graphs[slot]);
+  const void* u = sizeof(V) == sizeof(float2) ? (const void*)c->u32 : (const void*)c->u64;
+  if (G.exec && G.out == out && G.sf == sf && G.ring == ring && G.p == p && G.hv == hv && G.s == s && G.u == u &&
+      G.partials == c->partials && G.ms == ms && G.hist == hist && G.cf == cf && G.am == am && G.am3 == c->p.am3 && G.imass == imass &&
+      G.kernel == c->p.kernel && G.n == c->n4()) {
+    *exec_out = G.exec;
+    return THR_OK;
+  }
+  G.release();
+  THR_CUDA(cudaGraphCreate(&G.graph, 0));
+  cudaGraphConditionalHandle handle;
+  THR_CUDA(cudaGraphConditionalHandleCreate(&handle, G.graph, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  THR_CUDA(cudaGraphAddNode(&node, G.graph, nullptr, 0, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  THR_CUDA(cudaStreamBeginCaptureToGraph(c->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_batch<V>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 0, false, nullptr);
+  if (rc == THR_OK) k_loop_ctl<<<1, 1, 0, c->st>>>(ms, handle);
+  cudaGraph_t captured = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(c->st, &captured);
+  if (rc != THR_OK || ce != cudaSuccess) {
+    G.release();
+    cudaGetLastError();
+    return rc != THR_OK ? rc : THR_ERR_CUDA;
+  }
+  if (cudaGraphInstantiate(&G.exec, G.graph, 0) != cudaSuccess) {
+    G.release();
+    cudaGetLastError();
+    return THR_ERR_CUDA;
+  }
+  G.out = out; G.sf = sf; G.ring = ring; G.p = p; G.hv = hv; G.s = s; G.u = u;
+  G.partials = c->partials; G.ms = ms; G.hist = hist; G.cf = cf; G.am = am; G.am3 = c->p.am3; G.imass = imass;
+  G.kernel = c->p.kernel; G.n = c->n4();
+  *exec_out = G.exec;
+  return THR_OK;
+}
+}  // namespace
+
+void ms_graphs_release(thr_ctx* c) {
+  for (void*& g : c->ms_graphs) {
+    if (g) {
+      static_cast<MsGraph*>(g)->release();
+      delete static_cast<MsGraph*>(g);
+      g = nullptr;
+    }
+  }
+}
+
 template <class V>
 int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p, V* hv, V* s, int ndiagq,
                            const double* aden, const double* anum, float res, float am, int imass, int maxcg,
                            int* cg_return, int* cg_returns) {
   const size_t n = c->n4();
   const size_t stride = n;
-  const int ring_len = kBatch + 1;
   MsState* ms = reinterpret_cast<MsState*>(c->dscal);
   MsState* h = reinterpret_cast<MsState*>(c->hscal);
   void* hv_;
@@ -239,6 +385,9 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
   THR_TRY(c->buffer(thr_ctx::B_COEF, sizeof(MsCoef), &cf_));
   MsCoef* cf = (MsCoef*)cf_;
   THR_TRY(ms_prepare_state(c, h, ndiagq, aden, anum, res, maxcg));
+  h->kbase = 0;
+  h->batches = 0;
+  h->max_batches = (maxcg > 0 ? maxcg : 0) / kBatch + 3;
   THR_CUDA(cudaMemcpyAsync(ms, h, sizeof(MsState), cudaMemcpyHostToDevice, c->st));
   THR_CUDA(cudaMemcpyAsync(ring, in, n * sizeof(V), cudaMemcpyDeviceToDevice, c->st));  // r = input (slot 0)
   THR_CUDA(cudaMemcpyAsync(p, in, n * sizeof(V), cudaMemcpyDeviceToDevice, c->st));     // p = r
@@ -247,56 +396,37 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
   k_init<<<1, kThreads, 0, c->st>>>(ms, hist, c->partials, gb);
   THR_CUDA(cudaMemsetAsync(out, 0, (size_t)ndiagq * stride * sizeof(V), c->st));
   k_fill<V><<<gb, kThreads, 0, c->st>>>(sf, in, n, stride, ndiagq);
-  const bool sp = sizeof(V) == sizeof(float2);
-  const V* u = sp ? (const V*)(const void*)c->u32 : (const V*)(const void*)c->u64;
-  const unsigned gs = stencil_grid(c->g, c->p.kernel);
-  // algorithmic bytes: M reads R, writes Phi, reads the links; M^dagger with the
-  // fused <p, M^dagger M p> also reads p
-  const double lb = sp ? sizeof(float2) : sizeof(double2);
-  const double b_m = 2.0 * n * sizeof(V) + 3.0 * c->g.v3 * lb, b_md = b_m + (double)n * sizeof(V);
-  const size_t prof_first = c->prof_kind.size();
-  double flushed = 0.0;
-  long long flushes = 0;
-  long long k = 0;
-  for (;;) {
-    const long long base = k;
-    for (int j = 0; j < kBatch; j++, k++) {
-      V* rold = ring + (size_t)(k % ring_len) * n;
-      V* rnew = ring + (size_t)((k + 1) % ring_len) * n;
-      int pe = c->prof_begin(thr_ctx::P_DSLASH, b_m, k);
-      THR_TRY(launch_dslash<V>(c->g, c->p.kernel, false, hv, p, (const typename Sto<V>::C*)u, am, imass, c->p.am3,
-                               c->st, &ms->done));
-      c->prof_end(pe);
-      pe = c->prof_begin(thr_ctx::P_DSLASH_EPI, b_md, k);
-      THR_TRY(launch_dslash_epi<V>(c->g, c->p.kernel, true, s, hv, (const typename Sto<V>::C*)u, am, imass,
-                                   c->p.am3, c->st, &ms->done, p, c->partials));
-      c->prof_end(pe);
-      k_alpha<<<1, 1024, 0, c->st>>>(ms, hist, c->partials, gs);
-      k_rupdate<V><<<gb, kThreads, 0, c->st>>>(ms, rnew, rold, s, n, c->partials);
-      k_lambda<<<1, kThreads, 0, c->st>>>(ms, hist, c->partials, gb);
-      k_pupdate<V><<<gb, kThreads, 0, c->st>>>(ms, p, rnew, n);
-      k_converge<<<1, 1, 0, c->st>>>(ms);
-    }
-    int pe = c->prof_begin(thr_ctx::P_SHIFTUPD, 0.0, base);
-    k_flush_coef<<<1, kMaxShift, 0, c->st>>>(ms, hist, cf);
-    k_flush<V><<<gb, kThreads, 0, c->st>>>(cf, out, sf, ring, (int)(base % ring_len), ring_len, n, stride);
-    c->prof_end(pe);
-    k_reset<<<1, 1, 0, c->st>>>(hist);
+  if (c->use_graphs && !c->prof_on) {
+    // one graph launch runs every batch until convergence; one synchronisation
+    cudaGraphExec_t exec = nullptr;
+    THR_TRY(ms_graph<V>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, &exec));
+    THR_CUDA(cudaGraphLaunch(exec, c->st));
     THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
     THR_CUDA(cudaStreamSynchronize(c->st));
-    // flush traffic: each recorded step's residual read once, each shift field of the
-    // batch's window read and written once (out and sf)
-    c->prof_set_bytes(pe, (h->flush_fields - flushed) * n * sizeof(V));
-    if (h->flush_fields > flushed) flushes++;
-    flushed = h->flush_fields;
-    if (h->done) break;
-    if (k > (long long)maxcg + 2 * kBatch) return THR_ERR_CUDA;  // the device state stopped advancing
-  }
-  if (c->prof_on) {
-    c->prof_trim(prof_first, h->it);  // launches after convergence skipped their work
-    c->prof_work[thr_ctx::P_DSLASH] += h->it;
-    c->prof_work[thr_ctx::P_DSLASH_EPI] += h->it;
-    c->prof_work[thr_ctx::P_SHIFTUPD] += flushes;
+  } else {
+    // stream-launched batches, one synchronisation per batch (and kernel timing)
+    const size_t prof_first = c->prof_kind.size();
+    double flushed = 0.0;
+    long long flushes = 0;
+    for (long long k = 0;; k += kBatch) {
+      int pf = -1;
+      THR_TRY(enqueue_batch<V>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, k, c->prof_on, &pf));
+      THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
+      THR_CUDA(cudaStreamSynchronize(c->st));
+      // flush traffic: each recorded step's residual read once, each shift field of the
+      // batch's window read and written once (out and sf)
+      c->prof_set_bytes(pf, (h->flush_fields - flushed) * n * sizeof(V));
+      if (h->flush_fields > flushed) flushes++;
+      flushed = h->flush_fields;
+      if (h->done) break;
+      if (h->batches >= h->max_batches) return THR_ERR_CUDA;  // the device state stopped advancing
+    }
+    if (c->prof_on) {
+      c->prof_trim(prof_first, h->it);  // launches after convergence skipped their work
+      c->prof_work[thr_ctx::P_DSLASH] += h->it;
+      c->prof_work[thr_ctx::P_DSLASH_DAG] += h->it;
+      c->prof_work[thr_ctx::P_SHIFTUPD] += flushes;
+    }
   }
   if (cg_return) *cg_return = h->it;
   if (cg_returns)

@@ -250,8 +250,9 @@ int thr_qmrherm(thr_ctx* c, const double* Phi, double* x, float res, int* itercg
 }
 
 int thr_set_solver(thr_ctx* c, int multishift_algo) {
-  if (!c || multishift_algo < 0 || multishift_algo > 1) return THR_ERR_BADARG;
-  c->ms_algo = multishift_algo;
+  if (!c || multishift_algo < 0 || multishift_algo > 2) return THR_ERR_BADARG;
+  c->ms_algo = multishift_algo == 0 ? 0 : 1;
+  c->use_graphs = multishift_algo == 1;
   return THR_OK;
 }
 
