@@ -10,6 +10,7 @@
 
 #include "ctx.h"
 #include "solver.h"
+#include "thr_reduce.cuh"
 
 namespace thr {
 
@@ -32,13 +33,6 @@ __device__ __forceinline__ double block_sum(double v) {
   return v;
 }
 
-__device__ double sum_partials(const double* p, int n) {
-  // one thread, fixed order (n <= a few thousand)
-  double a = 0.0;
-  for (int i = 0; i < n; i++) a += p[i];
-  return a;
-}
-
 __global__ void k_cg_norm2(const CgState* cs, const double2* a, size_t n, double* partials) {
   if (cs->done) return;
   double acc = 0.0;
@@ -50,15 +44,14 @@ __global__ void k_cg_norm2(const CgState* cs, const double2* a, size_t n, double
   if (threadIdx.x == 0) partials[blockIdx.x] = acc;
 }
 
-// measure_module.F90:57, :66-75
+// measure_module.F90:57, :66-75 (one block; fixed-order reduction of the partials)
 __global__ void k_cg_alpha(CgState* cs, const double* partials, int np) {
   if (cs->done) return;
+  const double alphad = block_sum_partials(partials, np);
+  if (threadIdx.x != 0) return;
   cs->nx += 1;
   cs->itercg += 1;
-  if (cs->nx != 1) {
-    double alphad = sum_partials(partials, np);
-    cs->alpha = cs->alphan / alphad;
-  }
+  if (cs->nx != 1) cs->alpha = cs->alphan / alphad;
 }
 
 // r = r - alpha*x2 (:92) fused with betacgn = |r|^2 (:102)
@@ -75,10 +68,11 @@ __global__ void k_cg_rupdate(CgState* cs, double2* r, const double2* x2, size_t 
   if (threadIdx.x == 0) partials[blockIdx.x] = acc;
 }
 
-// :102-110, :120
+// :102-110, :120 (one block)
 __global__ void k_cg_beta(CgState* cs, const double* partials, int np) {
   if (cs->done) return;
-  double betacgn = sum_partials(partials, np);
+  const double betacgn = block_sum_partials(partials, np);
+  if (threadIdx.x != 0) return;
   double betacg = betacgn / cs->betacgd;
   cs->betacgd = betacgn;
   cs->alphan = betacgn;
@@ -105,12 +99,110 @@ __global__ void k_cg_latch(CgState* cs) {
   if (cs->pending_done) cs->done = 1;
 }
 
+// graph-driven loop: another chunk unless done; max_chunks bounds the loop
+// whatever the device state holds (congrad itself stops at niterc)
+__global__ void k_cg_loop(CgState* cs, cudaGraphConditionalHandle h) {
+  cs->chunks += 1;
+  unsigned more = cs->done ? 0u : 1u;
+  if (more && cs->chunks >= cs->max_chunks) {
+    cs->status = THR_ERR_MAXITER;
+    cs->done = 1;
+    more = 0u;
+  }
+  cudaGraphSetConditional(h, more);
+}
+
 inline unsigned vec_grid(size_t n) {
   size_t b = (n + kThreads - 1) / kThreads;
   if (b > 148 * 8) b = 148 * 8;
   return (unsigned)(b ? b : 1);
 }
+
+constexpr int kCgChunk = 8;
+
+// one chunk of kCgChunk iterations (stream order)
+int cg_enqueue_chunk(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r, double2* x1, double2* x2, float am,
+                     int imass) {
+  const size_t n = c->n4();
+  const unsigned gb = vec_grid(n);
+  const unsigned gs = stencil_grid(c->g, c->p.kernel);
+  for (int k = 0; k < kCgChunk; k++) {
+    // x1 = M p with alphad = |x1|^2 (:60, :70) from the stencil's epilogue
+    THR_TRY(launch_dslash_norm<double2>(c->g, c->p.kernel, false, x1, p, c->u64, am, imass, c->p.am3, c->st,
+                                        &cs->done, c->partials));
+    k_cg_alpha<<<1, 1024, 0, c->st>>>(cs, c->partials, gs);
+    THR_TRY(launch_dslash_guarded<double2>(c, true, x2, x1, c->u64, am, imass, &cs->done));
+    k_cg_rupdate<<<gb, kThreads, 0, c->st>>>(cs, r, x2, n, c->partials);
+    k_cg_beta<<<1, 1024, 0, c->st>>>(cs, c->partials, gb);
+    k_cg_xp<<<gb, kThreads, 0, c->st>>>(cs, X, p, r, n);
+    k_cg_latch<<<1, 1, 0, c->st>>>(cs);
+  }
+  return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+
+// The chunk loop as one CUDA graph (WHILE node), cached per buffers and operator.
+struct CgGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const void *X = nullptr, *p = nullptr, *r = nullptr, *x1 = nullptr, *x2 = nullptr, *cs = nullptr;
+  const void *u = nullptr, *partials = nullptr;
+  float am = 0.f, am3 = 0.f;
+  int imass = 0, kernel = -1;
+  size_t n = 0;
+  void release() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+};
+
+int cg_graph(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r, double2* x1, double2* x2, float am,
+             int imass, cudaGraphExec_t* exec_out) {
+  if (!c->cg_graph) c->cg_graph = new CgGraph();
+  CgGraph& G = *static_cast<CgGraph*>(c->cg_graph);
+  if (G.exec && G.X == X && G.p == p && G.r == r && G.x1 == x1 && G.x2 == x2 && G.cs == cs && G.u == c->u64 &&
+      G.partials == c->partials && G.am == am && G.am3 == c->p.am3 && G.imass == imass && G.kernel == c->p.kernel &&
+      G.n == c->n4()) {
+    *exec_out = G.exec;
+    return THR_OK;
+  }
+  G.release();
+  THR_CUDA(cudaGraphCreate(&G.graph, 0));
+  cudaGraphConditionalHandle handle;
+  THR_CUDA(cudaGraphConditionalHandleCreate(&handle, G.graph, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  THR_CUDA(cudaGraphAddNode(&node, G.graph, nullptr, 0, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  THR_CUDA(cudaStreamBeginCaptureToGraph(c->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  int rc = cg_enqueue_chunk(c, cs, X, p, r, x1, x2, am, imass);
+  if (rc == THR_OK) k_cg_loop<<<1, 1, 0, c->st>>>(cs, handle);
+  cudaGraph_t captured = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(c->st, &captured);
+  if (rc != THR_OK || ce != cudaSuccess || cudaGraphInstantiate(&G.exec, G.graph, 0) != cudaSuccess) {
+    G.release();
+    cudaGetLastError();
+    return rc != THR_OK ? rc : THR_ERR_CUDA;
+  }
+  G.X = X; G.p = p; G.r = r; G.x1 = x1; G.x2 = x2; G.cs = cs; G.u = c->u64; G.partials = c->partials;
+  G.am = am; G.am3 = c->p.am3; G.imass = imass; G.kernel = c->p.kernel; G.n = c->n4();
+  *exec_out = G.exec;
+  return THR_OK;
+}
 }  // namespace
+
+void cg_graph_release(thr_ctx* c) {
+  if (c->cg_graph) {
+    static_cast<CgGraph*>(c->cg_graph)->release();
+    delete static_cast<CgGraph*>(c->cg_graph);
+    c->cg_graph = nullptr;
+  }
+}
 
 // Runs congrad on device fields: Phi (rhs), X (guess in, solution out).
 int congrad_dev(thr_ctx* c, const double2* Phi, double2* X, float res, float am, int imass, int niterc, int* itercg,
@@ -128,25 +220,23 @@ int congrad_dev(thr_ctx* c, const double2* Phi, double2* X, float res, float am,
   h.alphan = 0.0;
   h.betacgd = 1.0;
   h.niterc = niterc;
+  h.max_chunks = niterc / kCgChunk + 3;
   THR_CUDA(cudaMemcpyAsync(cs, &h, sizeof(CgState), cudaMemcpyHostToDevice, c->st));
   THR_CUDA(cudaMemcpyAsync(p, X, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
   THR_CUDA(cudaMemcpyAsync(r, Phi, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
-  const unsigned gb = vec_grid(n);
-  const int chunk = 8;
-  for (int base = 0; base < niterc + chunk; base += chunk) {
-    for (int k = 0; k < chunk; k++) {
-      THR_TRY(launch_dslash_guarded<double2>(c, false, x1, p, c->u64, am, imass, &cs->done));
-      k_cg_norm2<<<gb, kThreads, 0, c->st>>>(cs, x1, n, c->partials);
-      k_cg_alpha<<<1, 1, 0, c->st>>>(cs, c->partials, gb);
-      THR_TRY(launch_dslash_guarded<double2>(c, true, x2, x1, c->u64, am, imass, &cs->done));
-      k_cg_rupdate<<<gb, kThreads, 0, c->st>>>(cs, r, x2, n, c->partials);
-      k_cg_beta<<<1, 1, 0, c->st>>>(cs, c->partials, gb);
-      k_cg_xp<<<gb, kThreads, 0, c->st>>>(cs, X, p, r, n);
-      k_cg_latch<<<1, 1, 0, c->st>>>(cs);
-    }
+  if (c->use_graphs) {
+    cudaGraphExec_t exec = nullptr;
+    THR_TRY(cg_graph(c, cs, X, p, r, x1, x2, am, imass, &exec));
+    THR_CUDA(cudaGraphLaunch(exec, c->st));
     THR_CUDA(cudaMemcpyAsync(&h, cs, sizeof(CgState), cudaMemcpyDeviceToHost, c->st));
     THR_CUDA(cudaStreamSynchronize(c->st));
-    if (h.done) break;
+  } else {
+    for (int base = 0; base < niterc + kCgChunk; base += kCgChunk) {
+      THR_TRY(cg_enqueue_chunk(c, cs, X, p, r, x1, x2, am, imass));
+      THR_CUDA(cudaMemcpyAsync(&h, cs, sizeof(CgState), cudaMemcpyDeviceToHost, c->st));
+      THR_CUDA(cudaStreamSynchronize(c->st));
+      if (h.done) break;
+    }
   }
   if (itercg) *itercg = h.itercg;
   // Fortran DO semantics: nx ends at niterc+1 when the loop runs out (:124)
@@ -241,10 +331,10 @@ extern "C" int thr_congrad_static(const thr_params* prm, const void* u, const vo
     for (int k = 0; k < chunk; k++) {
       THR_TRY(launch_dslash<double2>(g, prm->kernel, false, x1, p, ud, am, imass, prm->am3, st, &cs->done));
       k_cg_norm2<<<gb, kThreads, 0, st>>>(cs, x1, n, partials);
-      k_cg_alpha<<<1, 1, 0, st>>>(cs, partials, gb);
+      k_cg_alpha<<<1, 1024, 0, st>>>(cs, partials, gb);
       THR_TRY(launch_dslash<double2>(g, prm->kernel, true, x2, x1, ud, am, imass, prm->am3, st, &cs->done));
       k_cg_rupdate<<<gb, kThreads, 0, st>>>(cs, r, x2, n, partials);
-      k_cg_beta<<<1, 1, 0, st>>>(cs, partials, gb);
+      k_cg_beta<<<1, 1024, 0, st>>>(cs, partials, gb);
       k_cg_xp<<<gb, kThreads, 0, st>>>(cs, Xd, p, r, n);
       k_cg_latch<<<1, 1, 0, st>>>(cs);
     }

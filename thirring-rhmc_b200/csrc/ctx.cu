@@ -6,6 +6,7 @@
 
 #include "ctx.h"
 #include "ms.h"
+#include "solver.h"
 
 using namespace thr;
 
@@ -181,6 +182,7 @@ int thr_destroy(thr_ctx* c) {
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
   ms_graphs_release(c);
+  cg_graph_release(c);
   for (auto p : c->w64) cudaFree(p);
   for (auto e : c->prof_ev) cudaEventDestroy(e);
   for (int i = 0; i < thr_ctx::B_COUNT; i++) cudaFree(c->bufs[i]);

@@ -77,6 +77,7 @@ struct thr_ctx {
   int ms_algo = 1;          // multishift: 0 = per-iteration shift updates, 1 = batched
   bool use_graphs = true;   // batched solver loops as one CUDA graph (WHILE node) per solve
   void* ms_graphs[2] = {};  // cached batched-multishift graphs (FP64, FP32 vectors)
+  void* cg_graph = nullptr;  // cached congrad graph
   double md_counts[8] = {};  // ancg, ancgpv, ancgf, ancgfpv, ancgh, ancghpv, ancgpf, ancgpfpv
   void* bufs[B_COUNT] = {};
   size_t buf_bytes[B_COUNT] = {};

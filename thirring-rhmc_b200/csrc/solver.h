@@ -7,7 +7,7 @@ namespace thr {
 // congrad scalars (measure_module.F90:29-31), kept in device memory
 struct CgState {
   double alpha, alphan, betacg, betacgd, betacgn, resid;
-  int nx, itercg, niterc, done, pending_done, capped, status, pad;
+  int nx, itercg, niterc, done, pending_done, capped, status, chunks, max_chunks, pad;
 };
 
 template <class S>
@@ -18,5 +18,7 @@ inline int launch_dslash_guarded(thr_ctx* c, bool dag, S* out, const S* in, cons
 
 int congrad_dev(thr_ctx* c, const double2* Phi, double2* X, float res, float am, int imass, int niterc, int* itercg,
                 int* iterations);
+// destroys the cached congrad graph (context teardown)
+void cg_graph_release(thr_ctx* c);
 
 }  // namespace thr
