@@ -299,7 +299,11 @@ def run_ours(args, rank, world, local_rank):
     # ---- stencil bandwidth at the largest config-2 lattice (extra figure)
     dslash = dslash_bandwidth(args, local_rank) if (rank == 0 and not args.no_dslash) else None
 
+    buf = C.create_string_buffer(8192)
+    L.thr_tune_report(buf, len(buf))
+    tune = [ln for ln in buf.value.decode().splitlines() if ln]
     res = dict(ms=ms, its=its, prof=prof, launches=launches, fp64_s=fp64_s, fp64_iters=fp64_iters, stream_s=stream_s,
+               tune=tune,
                e2e_ms=e2e_ms, clocks=clk.summary(), dslash=dslash, phi_bytes=phi.nbytes)
     L.thr_field_destroy(h, pd)
     L.thr_field_destroy(h, px)
@@ -618,7 +622,7 @@ def main():
         bpl = p["bytes"] / p["sampled"]
         kern[name] = {"launches": int(p["launches"]), "sampled": p["sampled"], "us_per_launch": round(us, 3),
                       "algorithmic_bytes_per_launch": round(bpl), "gbs": round(bpl / us / 1e3, 1),
-                      "share_of_step": round(p["launches"] * us / 1e3 / r["ms"], 4)}
+                      "share_of_step": round(p["launches"] * us / 1e3 / ms_step, 4)}
     # dominant kernel of the timed region
     name = max(kern, key=lambda k: kern[k]["share_of_step"])
     k = kern[name]
@@ -652,6 +656,7 @@ def main():
             "plain_fp64_gpu_solve_s": r["fp64_s"], "plain_fp64_gpu_iterations": r["fp64_iters"],
             "speedup_vs_plain_fp64_gpu": (r["fp64_s"] / (ms_step / 1e3)) if r["fp64_s"] else None,
             "batched_host_launched_solve_s": r["stream_s"],
+            "autotune": r["tune"],
             "dslash_48x48x48_ls48_fp64": r["dslash"]}
     print(json.dumps(line), flush=True)
 

@@ -343,6 +343,12 @@ int thr_get_stream(thr_ctx *ctx, void **stream);
 int thr_profile(thr_ctx *ctx, int stride, int reset);
 int thr_profile_read(thr_ctx *ctx, int kind, int *sampled, double *ms, double *bytes, double *launches);
 
+/* The stencil autotuner's choices so far (process-wide), as text: one line per
+ * tuned case with the candidates' mean launch times.  The tuner picks the
+ * register budget of the Shamir stencil per lattice on first use (results are
+ * identical for every choice); THR_TUNE=0 in the environment disables it. */
+int thr_tune_report(char *buf, int len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -82,3 +82,34 @@ def test_wilson_imass5_rejected():
         with pytest.raises(thirring.ThirringError) as ei:
             G.dslash(R, u, 0.1, 5)
         assert ei.value.status == 7
+
+
+@pytest.mark.gpu
+def test_autotuner_keeps_results_bit_identical(tmp_path):
+    """The stencil autotuner (register budget per lattice) runs on first use; its
+    candidates share block shape and arithmetic, so the output is the same bits
+    before and after tuning and equal to a THR_TUNE=0 process."""
+    import ctypes as C
+    import os
+    import subprocess
+    import sys
+    rng = np.random.default_rng(99)
+    L = O.lat(8, 6, 4, 16)
+    u = rand_links(L, rng)
+    R = rand_spinor(L, rng)
+    with thirring.Lattice(8, 6, 4, 16) as G:
+        a = G.dslash(R, u, 0.05, 3)
+        b = G.dslash(R, u, 0.05, 3)
+        buf = C.create_string_buffer(8192)
+        thirring.lib().thr_tune_report(buf, len(buf))
+    assert np.array_equal(a, b)
+    assert "8x6x4 Ls=16" in buf.value.decode()
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "thirring-rhmc_b200")
+    np.save(tmp_path / "R.npy", R)
+    np.save(tmp_path / "u.npy", u)
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import thirring; d = %r;"
+            "R = np.asfortranarray(np.load(d + '/R.npy')); u = np.asfortranarray(np.load(d + '/u.npy'));"
+            "G = thirring.Lattice(8, 6, 4, 16); np.save(d + '/out.npy', G.dslash(R, u, 0.05, 3)); G.close()"
+            % (pkg, str(tmp_path)))
+    subprocess.run([sys.executable, "-c", code], check=True, env=dict(os.environ, THR_TUNE="0"))
+    assert np.array_equal(a, np.load(tmp_path / "out.npy"))

@@ -168,6 +168,11 @@ int cg_graph(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r, double
     return THR_OK;
   }
   G.release();
+  // the iteration's two stencils once outside the capture, so that the autotuner
+  // settles their configuration first (x1, x2 and the partials are scratch here)
+  THR_TRY(launch_dslash_norm<double2>(c->g, c->p.kernel, false, x1, p, c->u64, am, imass, c->p.am3, c->st, &cs->done,
+                                      c->partials));
+  THR_TRY(launch_dslash_guarded<double2>(c, true, x2, x1, c->u64, am, imass, &cs->done));
   THR_CUDA(cudaGraphCreate(&G.graph, 0));
   cudaGraphConditionalHandle handle;
   THR_CUDA(cudaGraphConditionalHandleCreate(&handle, G.graph, 1, cudaGraphCondAssignDefault));

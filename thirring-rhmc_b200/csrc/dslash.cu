@@ -20,6 +20,12 @@
 // The per-site arithmetic lives in shamir_site / wilson_site; the single-
 // lattice kernels and the batched kernel (many right-hand sides or many
 // lattices of different shapes in one persistent launch) share it.
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
+
 #include "batch.h"
 #include "thr_common.cuh"
 #include "thr_kernels.h"
@@ -289,8 +295,11 @@ __device__ __forceinline__ void apply_site(const S* in, const typename Sto<S>::C
 // One thread per 5D site: blockDim = (Ls, sites per block), NT threads at most.
 // Shamir blocks are small (NT = 128, 8 resident per SM at <= 64 registers):
 // the kernel is latency-bound, and small blocks keep more loads in flight.
-template <class S, int KER, bool DAG, int EPI, int NT, bool SHFL>
-__global__ void __launch_bounds__(NT, (KER == 0 && NT <= 128) ? 1024 / NT : 1)
+// MINB (resident blocks per SM the register budget is cut for) is chosen per
+// lattice by the autotuner below; it changes register allocation only, so the
+// results are bit-identical whichever value runs.
+template <class S, int KER, bool DAG, int EPI, int NT, bool SHFL, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
     k_dslash(S* __restrict__ out, const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u, Geom g, float am,
              int imass, float am3, const int* skip, const S* __restrict__ aux, double* __restrict__ partials) {
   if (skip && *skip) return;
@@ -374,6 +383,50 @@ unsigned stencil_grid(const Geom& g, int kernel) {
   return (unsigned)((g.v3 + blk.y - 1) / blk.y);
 }
 
+// ---------------------------------------------------------------- autotuner
+// For the Shamir stencil in FP64 and FP32 storage the register budget (blocks
+// per SM the compiler may assume: 8, 7 or 6 for 128-thread blocks) is tuned
+// per (storage, M or M^dagger, epilogue, lattice, layout, device) on first use:
+// each candidate runs 1 + 3 times on the call's own fields (the launches are
+// idempotent: out and partials are overwritten), the fastest is kept for the
+// process.  Block shape and reduction order do not change, so neither do the
+// results.  THR_TUNE=0 in the environment keeps the default (8).  Launches
+// made while the stream is being captured into a graph use the default until
+// a tuned value exists.
+namespace {
+constexpr int kTuneMinb[3] = {8, 7, 6};
+struct TuneKey {
+  int dev, sid, dag, epi, lx, ly, lt, ls, layout;
+  bool operator<(const TuneKey& o) const {
+    const int a[9] = {dev, sid, dag, epi, lx, ly, lt, ls, layout};
+    const int b[9] = {o.dev, o.sid, o.dag, o.epi, o.lx, o.ly, o.lt, o.ls, o.layout};
+    for (int i = 0; i < 9; i++)
+      if (a[i] != b[i]) return a[i] < b[i];
+    return false;
+  }
+};
+struct TuneVal {
+  int pick;
+  float us[3];
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune;
+int g_tune_mode = -1;  // -1: not read yet, 0 off, 1 on
+bool tune_on() {
+  if (g_tune_mode < 0) {
+    const char* e = std::getenv("THR_TUNE");
+    g_tune_mode = (e && e[0] == '0') ? 0 : 1;
+  }
+  return g_tune_mode == 1;
+}
+bool capturing(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return true;
+  return cs != cudaStreamCaptureStatusNone;
+}
+template <class S> constexpr int storage_id() { return sizeof(S) == sizeof(double2) ? 0 : sizeof(S) == sizeof(float2) ? 1 : 2; }
+}  // namespace
+
 // epi: 0 none, 1 Re<aux, out> per block, 2 |out|^2 per block (partials[blockIdx.x])
 template <class S>
 int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
@@ -385,23 +438,81 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   const dim3 grd(stencil_grid(g, kernel));
   const int nt = stencil_threads(g, kernel);
   const bool shfl = stencil_shfl(g, kernel);
-#define THR_L(K, D, E, N, SH) \
-  k_dslash<S, K, D, E, N, SH><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, partials)
-#define THR_E(K, D, N, SH)                 \
-  do {                                     \
-    if (e == 1) THR_L(K, D, 1, N, SH);     \
-    else if (e == 2) THR_L(K, D, 2, N, SH); \
-    else THR_L(K, D, 0, N, SH);            \
+#define THR_L(K, D, E, N, SH, MB) \
+  k_dslash<S, K, D, E, N, SH, MB><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, partials)
+#define THR_E(K, D, N, SH, MB)                 \
+  do {                                         \
+    if (e == 1) THR_L(K, D, 1, N, SH, MB);     \
+    else if (e == 2) THR_L(K, D, 2, N, SH, MB); \
+    else THR_L(K, D, 0, N, SH, MB);            \
+  } while (0)
+#define THR_D(K, N, SH, MB)                        \
+  do {                                             \
+    if (dag) THR_E(K, true, N, SH, MB);            \
+    else THR_E(K, false, N, SH, MB);               \
   } while (0)
   if (kernel == 1) {
-    if (nt == 256) { if (dag) THR_E(1, true, 256, false); else THR_E(1, false, 256, false); }
-    else { if (dag) THR_E(1, true, 1024, false); else THR_E(1, false, 1024, false); }
+    if (nt == 256) THR_D(1, 256, false, 1);
+    else THR_D(1, 1024, false, 1);
   } else if (nt == 128) {
-    if (shfl) { if (dag) THR_E(0, true, 128, true); else THR_E(0, false, 128, true); }
-    else { if (dag) THR_E(0, true, 128, false); else THR_E(0, false, 128, false); }
+    // the Shamir fast path: 128-thread blocks, register budget from the tuner
+    auto launch = [&](int minb) {
+      if (shfl) {
+        if (minb == 8) THR_D(0, 128, true, 8);
+        else if (minb == 7) THR_D(0, 128, true, 7);
+        else THR_D(0, 128, true, 6);
+      } else {
+        if (minb == 8) THR_D(0, 128, false, 8);
+        else if (minb == 7) THR_D(0, 128, false, 7);
+        else THR_D(0, 128, false, 6);
+      }
+    };
+    int minb = 8;
+    if (storage_id<S>() < 2) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      const TuneKey key{dev, storage_id<S>(), dag ? 1 : 0, e, g.lx, g.ly, g.lt, g.ls, g.layout};
+      bool found = false;
+      {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+          minb = it->second.pick;
+          found = true;
+        }
+      }
+      if (!found && tune_on() && !capturing(st)) {
+        TuneVal tv{8, {0.f, 0.f, 0.f}};
+        cudaEvent_t e0, e1;
+        if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
+          float best = 1e30f;
+          for (int c = 0; c < 3; c++) {
+            launch(kTuneMinb[c]);
+            cudaEventRecord(e0, st);
+            for (int r = 0; r < 3; r++) launch(kTuneMinb[c]);
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            tv.us[c] = ms * 1e3f / 3.f;
+            if (tv.us[c] < best) {
+              best = tv.us[c];
+              tv.pick = kTuneMinb[c];
+            }
+          }
+          cudaEventDestroy(e0);
+          cudaEventDestroy(e1);
+          std::lock_guard<std::mutex> lock(g_tune_mu);
+          g_tune[key] = tv;
+          minb = tv.pick;
+        }
+      }
+    }
+    launch(minb);
   } else {
-    if (dag) THR_E(0, true, 1024, false); else THR_E(0, false, 1024, false);
+    THR_D(0, 1024, false, 1);
   }
+#undef THR_D
 #undef THR_E
 #undef THR_L
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
@@ -462,3 +573,24 @@ THR_INST(__half2, float2)
 #undef THR_INST
 
 }  // namespace thr
+
+// The autotuner's choices so far, one line each:
+//   <storage> <M|Mdag> epi=<e> <lx>x<ly>x<lt> Ls=<ls> layout=<l> dev=<d> minb=<pick> us=<8>/<7>/<6>
+extern "C" int thr_tune_report(char* buf, int len) {
+  using namespace thr;
+  if (!buf || len < 1) return THR_ERR_BADARG;
+  std::string r;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    for (const auto& kv : g_tune) {
+      const TuneKey& k = kv.first;
+      char line[256];
+      std::snprintf(line, sizeof(line), "%s %s epi=%d %dx%dx%d Ls=%d layout=%d dev=%d minb=%d us=%.2f/%.2f/%.2f\n",
+                    k.sid == 0 ? "fp64" : "fp32", k.dag ? "Mdag" : "M", k.epi, k.lx, k.ly, k.lt, k.ls, k.layout,
+                    k.dev, kv.second.pick, kv.second.us[0], kv.second.us[1], kv.second.us[2]);
+      r += line;
+    }
+  }
+  std::snprintf(buf, (size_t)len, "%s", r.c_str());
+  return THR_OK;
+}

@@ -326,6 +326,15 @@ int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V
     return THR_OK;
   }
   G.release();
+  // run the two stencils of an iteration once outside the capture, so that the
+  // autotuner settles their configuration before it is baked into the graph
+  // (hv, s and the partials are scratch at this point; p holds the source)
+  {
+    const typename Sto<V>::C* uu = (const typename Sto<V>::C*)u;
+    THR_TRY(launch_dslash_norm<V>(c->g, c->p.kernel, false, hv, p, uu, am, imass, c->p.am3, c->st, &ms->done,
+                                  c->partials));
+    THR_TRY(launch_dslash<V>(c->g, c->p.kernel, true, s, hv, uu, am, imass, c->p.am3, c->st, &ms->done));
+  }
   THR_CUDA(cudaGraphCreate(&G.graph, 0));
   cudaGraphConditionalHandle handle;
   THR_CUDA(cudaGraphConditionalHandleCreate(&handle, G.graph, 1, cudaGraphCondAssignDefault));
