@@ -298,12 +298,19 @@ __device__ __forceinline__ void apply_site(const S* in, const typename Sto<S>::C
 // MINB (resident blocks per SM the register budget is cut for) is chosen per
 // lattice by the autotuner below; it changes register allocation only, so the
 // results are bit-identical whichever value runs.
+//
+// Epilogues (EPI): 0 store out = M in; 2 also one FP64 partial per block of
+// |out|^2; 1 the residual update of the multishift solver fused in -- out =
+// aux + (*coef) * (M in), with M in never stored, and a partial of |out|^2.
 template <class S, int KER, bool DAG, int EPI, int NT, bool SHFL, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     k_dslash(S* __restrict__ out, const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u, Geom g, float am,
-             int imass, float am3, const int* skip, const S* __restrict__ aux, double* __restrict__ partials) {
+             int imass, float am3, const int* skip, const S* __restrict__ aux, const double* __restrict__ coef,
+             double* __restrict__ partials) {
   if (skip && *skip) return;
   using C = typename Sto<S>::C;
+  using R = typename Sto<S>::R;
+  const R om = EPI == 1 ? (R)(*coef) : R(0);
   const int s = threadIdx.x;
   double racc = 0.0;
   const int site = blockIdx.x * blockDim.y + threadIdx.y;
@@ -315,9 +322,15 @@ __global__ void __launch_bounds__(NT, MINB)
     if (live) {
 #pragma unroll
       for (int d = 0; d < 4; d++) {
-        Sto<S>::st(out, sidx(g, s, site, d), acc[d]);
-        if (EPI == 1) racc += epi_redot<S>(aux, sidx(g, s, site, d), acc[d]);
-        if (EPI == 2) racc += epi_norm<S>(acc[d]);
+        const size_t i = sidx(g, s, site, d);
+        if (EPI == 1) {
+          const C rn = Sto<S>::ld(aux, i) + om * acc[d];  // r = r + omega*s (multishift_module.F90:137)
+          Sto<S>::st(out, i, rn);
+          racc += epi_norm<S>(rn);
+        } else {
+          Sto<S>::st(out, i, acc[d]);
+          if (EPI == 2) racc += epi_norm<S>(acc[d]);
+        }
       }
     }
   }
@@ -427,11 +440,11 @@ bool capturing(cudaStream_t st) {
 template <class S> constexpr int storage_id() { return sizeof(S) == sizeof(double2) ? 0 : sizeof(S) == sizeof(float2) ? 1 : 2; }
 }  // namespace
 
-// epi: 0 none, 1 Re<aux, out> per block, 2 |out|^2 per block (partials[blockIdx.x])
+// epi: 0 none, 1 out = aux + (*coef) M in with |out|^2 per block, 2 |out|^2 per block
 template <class S>
 int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
-                       int imass, float am3, cudaStream_t st, const int* skip, const S* aux, double* partials,
-                       int e) {
+                       int imass, float am3, cudaStream_t st, const int* skip, const S* aux, const double* coef,
+                       double* partials, int e) {
   if (g.ls > 1024) return THR_ERR_BADSHAPE;
   if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
   const dim3 blk = stencil_block(g, kernel);
@@ -439,7 +452,7 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   const int nt = stencil_threads(g, kernel);
   const bool shfl = stencil_shfl(g, kernel);
 #define THR_L(K, D, E, N, SH, MB) \
-  k_dslash<S, K, D, E, N, SH, MB><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, partials)
+  k_dslash<S, K, D, E, N, SH, MB><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, coef, partials)
 #define THR_E(K, D, N, SH, MB)                 \
   do {                                         \
     if (e == 1) THR_L(K, D, 1, N, SH, MB);     \
@@ -519,21 +532,22 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
 }
 
 template <class S>
-int launch_dslash_epi(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
-                      int imass, float am3, cudaStream_t st, const int* skip, const S* aux, double* partials) {
-  return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, aux, partials, aux ? 1 : 0);
+int launch_dslash_axpy(const Geom& g, int kernel, bool dag, S* rnew, const S* in, const typename Sto<S>::C* u,
+                       float am, int imass, float am3, cudaStream_t st, const int* skip, const S* rold,
+                       const double* coef, double* partials) {
+  return launch_dslash_mode<S>(g, kernel, dag, rnew, in, u, am, imass, am3, st, skip, rold, coef, partials, 1);
 }
 
 template <class S>
 int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
                        float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials) {
-  return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, partials, 2);
+  return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr, partials, 2);
 }
 
 template <class S>
 int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
                   int imass, float am3, cudaStream_t st, const int* skip) {
-  return launch_dslash_epi<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr);
+  return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr, nullptr, 0);
 }
 
 template <class S>
@@ -560,8 +574,8 @@ int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const
 #define THR_INST(S, L)                                                                                            \
   template int launch_dslash<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float, cudaStream_t,   \
                                 const int*);                                                                      \
-  template int launch_dslash_epi<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,            \
-                                    cudaStream_t, const int*, const S*, double*);                                 \
+  template int launch_dslash_axpy<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
+                                     cudaStream_t, const int*, const S*, const double*, double*);                 \
   template int launch_dslash_norm<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
                                      cudaStream_t, const int*, double*);                                          \
   template int launch_dslash_batch<S>(const BatchTable&, int, bool, S*, const S*, const L*, float, int, float,    \

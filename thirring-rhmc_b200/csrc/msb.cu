@@ -73,28 +73,6 @@ __global__ void k_alpha(MsState* ms, MsHist* hist, const double* partials, int n
   }
 }
 
-// ring slots of iteration kbase + j: r_old in slot (k mod ring_len), r_new in the next
-__device__ __forceinline__ size_t ring_slot(const MsState* ms, int j, int ring_len) {
-  return (size_t)((ms->kbase + j) % ring_len);
-}
-
-// r_new = r_old + omega*s (:137), lambda partials (:138)
-template <class V>
-__global__ void k_rupdate(const MsState* ms, V* ring, int j, int ring_len, const V* s, size_t n, double* partials) {
-  if (ms->done) return;
-  using R = typename W<V>::R;
-  const V* rold = ring + ring_slot(ms, j, ring_len) * n;
-  V* rnew = ring + ring_slot(ms, j + 1, ring_len) * n;
-  const R om = W<V>::cast(ms->omega);
-  double acc = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const V v = rold[i] + om * s[i];
-    rnew[i] = v;
-    acc += W<V>::abs2(v);
-  }
-  block_write_partial(acc, partials);
-}
-
 // :143, :148-150, recording gammas; closes the step's record
 __global__ void k_lambda(MsState* ms, MsHist* hist, const double* partials, int np) {
   if (ms->done) return;
@@ -115,10 +93,9 @@ __global__ void k_lambda(MsState* ms, MsHist* hist, const double* partials, int 
 
 // p = r + gammag*p (:145)
 template <class V>
-__global__ void k_pupdate(const MsState* ms, V* p, const V* ring, int j, int ring_len, size_t n) {
+__global__ void k_pupdate(const MsState* ms, V* p, const V* r, size_t n) {
   if (ms->done) return;
   using R = typename W<V>::R;
-  const V* r = ring + ring_slot(ms, j + 1, ring_len) * n;
   const R gg = W<V>::cast(ms->gammag);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     p[i] = r[i] + gg * p[i];
@@ -172,14 +149,14 @@ __global__ void k_flush_coef(MsState* ms, const MsHist* hist, MsCoef* cf) {
 }
 
 // apply the folded maps to every shift field of the batch's window
+// (ring slot j+1 holds the residual of the batch's step j; the last one is copied
+// to slot 0, where the next batch starts)
 template <class V>
-__global__ void __launch_bounds__(kThreads) k_flush(const MsCoef* cf, const MsState* ms, V* __restrict__ out,
-                                                   V* __restrict__ sf, const V* __restrict__ ring, int ring_len,
-                                                   size_t n, size_t stride) {
+__global__ void __launch_bounds__(kThreads) k_flush(const MsCoef* cf, V* __restrict__ out, V* __restrict__ sf,
+                                                   V* __restrict__ ring, size_t n, size_t stride) {
   using R = typename W<V>::R;
   const int ns = cf->ns;
   if (ns == 0) return;
-  const int base = (int)(ms->kbase % ring_len);
   const int lo = cf->lo, hi = cf->hi;
   __shared__ R s_A[kMaxShift], s_P[kMaxShift], s_B[kMaxShift][kBatch], s_Q[kMaxShift][kBatch];
   for (int t = threadIdx.x; t < kMaxShift * kBatch; t += blockDim.x) {
@@ -196,7 +173,7 @@ __global__ void __launch_bounds__(kThreads) k_flush(const MsCoef* cf, const MsSt
     V rj[kBatch];
 #pragma unroll
     for (int j = 0; j < kBatch; j++)
-      if (j < ns) rj[j] = ring[(size_t)((base + 1 + j) % ring_len) * n + i];
+      if (j < ns) rj[j] = ring[(size_t)(1 + j) * n + i];
     for (int k = lo; k <= hi; k++) {
       const V f0 = sf[k * stride + i];
       const V o0 = out[k * stride + i];
@@ -212,13 +189,14 @@ __global__ void __launch_bounds__(kThreads) k_flush(const MsCoef* cf, const MsSt
       sf[k * stride + i] = f;
       out[k * stride + i] = o;
     }
+#pragma unroll
+    for (int j = 0; j < kBatch; j++)
+      if (j == ns - 1) ring[i] = rj[j];
   }
 }
-// close a batch: the next one starts kBatch iterations later (launches of
-// iterations after convergence are skipped but still counted, as on the host)
+// close a batch
 __global__ void k_reset(MsHist* hist, MsState* ms) {
   hist->nsteps = 0;
-  ms->kbase += kBatch;
   ms->batches += 1;
 }
 
@@ -259,33 +237,36 @@ template <class V>
 int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V* ring, V* p, V* hv, V* s,
                   float am, int imass, long long k0, bool prof, int* prof_flush) {
   const size_t n = c->n4();
-  const int ring_len = kBatch + 1;
   const unsigned gb = vec_grid(n);
   const unsigned gs = stencil_grid(c->g, c->p.kernel);
   const bool sp = sizeof(V) == sizeof(float2);
   const typename Sto<V>::C* u =
       sp ? (const typename Sto<V>::C*)(const void*)c->u32 : (const typename Sto<V>::C*)(const void*)c->u64;
   const double lb = sp ? sizeof(float2) : sizeof(double2);
-  // algorithmic bytes: M reads R, writes Phi, reads the links (its |M p|^2 comes
-  // from registers), and so does M^dagger
-  const double b_m = 2.0 * n * sizeof(V) + 3.0 * c->g.v3 * lb;
+  // algorithmic bytes: M reads p, writes h, reads the links (|M p|^2 comes from
+  // registers); the M^dagger launch reads h, the links and r_old and writes r_new
+  const double b_m = 2.0 * n * sizeof(V) + 3.0 * c->g.v3 * lb, b_md = b_m + (double)n * sizeof(V);
   for (int j = 0; j < kBatch; j++) {
+    V* rold = ring + (size_t)j * n;
+    V* rnew = ring + (size_t)(j + 1) * n;
     // alpha = Re<p, M^dagger M p> (:104) evaluated as |M p|^2 in the M epilogue
     int pe = prof ? c->prof_begin(thr_ctx::P_DSLASH, b_m, k0 + j) : -1;
     THR_TRY(launch_dslash_norm<V>(c->g, c->p.kernel, false, hv, p, u, am, imass, c->p.am3, c->st, &ms->done,
                                   c->partials));
     c->prof_end(pe);
-    pe = prof ? c->prof_begin(thr_ctx::P_DSLASH_DAG, b_m, k0 + j) : -1;
-    THR_TRY(launch_dslash<V>(c->g, c->p.kernel, true, s, hv, u, am, imass, c->p.am3, c->st, &ms->done));
-    c->prof_end(pe);
     k_alpha<<<1, 1024, 0, c->st>>>(ms, hist, c->partials, gs);
-    k_rupdate<V><<<gb, kThreads, 0, c->st>>>(ms, ring, j, ring_len, s, n, c->partials);
-    k_lambda<<<1, kThreads, 0, c->st>>>(ms, hist, c->partials, gb);
-    k_pupdate<V><<<gb, kThreads, 0, c->st>>>(ms, p, ring, j, ring_len, n);
+    // s = M^dagger h is never stored: the epilogue forms r = r + omega*s (:137) and |r|^2 (:138)
+    pe = prof ? c->prof_begin(thr_ctx::P_DSLASH_DAG, b_md, k0 + j) : -1;
+    THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, rnew, hv, u, am, imass, c->p.am3, c->st, &ms->done, rold,
+                                  &ms->omega, c->partials));
+    c->prof_end(pe);
+    k_lambda<<<1, 1024, 0, c->st>>>(ms, hist, c->partials, gs);
+    k_pupdate<V><<<gb, kThreads, 0, c->st>>>(ms, p, rnew, n);
   }
+  (void)s;
   const int pe = prof ? c->prof_begin(thr_ctx::P_SHIFTUPD, 0.0, k0) : -1;
   k_flush_coef<<<1, kMaxShift, 0, c->st>>>(ms, hist, cf);
-  k_flush<V><<<gb, kThreads, 0, c->st>>>(cf, ms, out, sf, ring, ring_len, n, n);
+  k_flush<V><<<gb, kThreads, 0, c->st>>>(cf, out, sf, ring, n, n);
   c->prof_end(pe);
   if (prof_flush) *prof_flush = pe;
   k_reset<<<1, 1, 0, c->st>>>(hist, ms);
@@ -333,7 +314,8 @@ int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V
     const typename Sto<V>::C* uu = (const typename Sto<V>::C*)u;
     THR_TRY(launch_dslash_norm<V>(c->g, c->p.kernel, false, hv, p, uu, am, imass, c->p.am3, c->st, &ms->done,
                                   c->partials));
-    THR_TRY(launch_dslash<V>(c->g, c->p.kernel, true, s, hv, uu, am, imass, c->p.am3, c->st, &ms->done));
+    THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, s, hv, uu, am, imass, c->p.am3, c->st, &ms->done, ring,
+                                  &ms->omega, c->partials));
   }
   THR_CUDA(cudaGraphCreate(&G.graph, 0));
   cudaGraphConditionalHandle handle;

@@ -15,10 +15,12 @@ unsigned stencil_grid(const Geom& g, int kernel);  // blocks of one stencil laun
 template <class S>
 int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
                   int imass, float am3, cudaStream_t st, const int* skip = nullptr);
-// same, and when aux != NULL also one FP64 partial per block of sum Re(conj(aux) out)
+// rnew = rold + (*coef) * (M or M^dagger) in, without storing the stencil's output,
+// and one FP64 partial per block of |rnew|^2
 template <class S>
-int launch_dslash_epi(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
-                      int imass, float am3, cudaStream_t st, const int* skip, const S* aux, double* partials);
+int launch_dslash_axpy(const Geom& g, int kernel, bool dag, S* rnew, const S* in, const typename Sto<S>::C* u,
+                       float am, int imass, float am3, cudaStream_t st, const int* skip, const S* rold,
+                       const double* coef, double* partials);
 // same, with one FP64 partial per block of sum |out|^2
 template <class S>
 int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
