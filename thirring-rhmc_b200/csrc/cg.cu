@@ -52,6 +52,7 @@ __global__ void k_cg_alpha(CgState* cs, const double* partials, int np) {
   cs->nx += 1;
   cs->itercg += 1;
   if (cs->nx != 1) cs->alpha = cs->alphan / alphad;
+  cs->nalpha = -cs->alpha;
 }
 
 // r = r - alpha*x2 (:92) fused with betacgn = |r|^2 (:102)
@@ -131,9 +132,11 @@ int cg_enqueue_chunk(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r
     THR_TRY(launch_dslash_norm<double2>(c->g, c->p.kernel, false, x1, p, c->u64, am, imass, c->p.am3, c->st,
                                         &cs->done, c->partials));
     k_cg_alpha<<<1, 1024, 0, c->st>>>(cs, c->partials, gs);
-    THR_TRY(launch_dslash_guarded<double2>(c, true, x2, x1, c->u64, am, imass, &cs->done));
-    k_cg_rupdate<<<gb, kThreads, 0, c->st>>>(cs, r, x2, n, c->partials);
-    k_cg_beta<<<1, 1024, 0, c->st>>>(cs, c->partials, gb);
+    // x2 = M^dagger x1 is never stored: the epilogue forms r = r - alpha*x2 (:92) and
+    // betacgn = |r|^2 (:102)
+    THR_TRY(launch_dslash_axpy<double2>(c->g, c->p.kernel, true, r, x1, c->u64, am, imass, c->p.am3, c->st, &cs->done,
+                                        r, &cs->nalpha, c->partials));
+    k_cg_beta<<<1, 1024, 0, c->st>>>(cs, c->partials, gs);
     k_cg_xp<<<gb, kThreads, 0, c->st>>>(cs, X, p, r, n);
     k_cg_latch<<<1, 1, 0, c->st>>>(cs);
   }
@@ -172,7 +175,8 @@ int cg_graph(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r, double
   // settles their configuration first (x1, x2 and the partials are scratch here)
   THR_TRY(launch_dslash_norm<double2>(c->g, c->p.kernel, false, x1, p, c->u64, am, imass, c->p.am3, c->st, &cs->done,
                                       c->partials));
-  THR_TRY(launch_dslash_guarded<double2>(c, true, x2, x1, c->u64, am, imass, &cs->done));
+  THR_TRY(launch_dslash_axpy<double2>(c->g, c->p.kernel, true, x2, x1, c->u64, am, imass, c->p.am3, c->st, &cs->done,
+                                      x2, &cs->nalpha, c->partials));
   THR_CUDA(cudaGraphCreate(&G.graph, 0));
   cudaGraphConditionalHandle handle;
   THR_CUDA(cudaGraphConditionalHandleCreate(&handle, G.graph, 1, cudaGraphCondAssignDefault));

@@ -6,7 +6,7 @@ namespace thr {
 
 // congrad scalars (measure_module.F90:29-31), kept in device memory
 struct CgState {
-  double alpha, alphan, betacg, betacgd, betacgn, resid;
+  double alpha, alphan, betacg, betacgd, betacgn, resid, nalpha;  // nalpha = -alpha for the fused r update
   int nx, itercg, niterc, done, pending_done, capped, status, chunks, max_chunks, pad;
 };
 
