@@ -345,8 +345,9 @@ int thr_profile_read(thr_ctx *ctx, int kind, int *sampled, double *ms, double *b
 
 /* The stencil autotuner's choices so far (process-wide), as text: one line per
  * tuned case with the candidates' mean launch times.  The tuner picks the
- * register budget of the Shamir stencil per lattice on first use (results are
- * identical for every choice); THR_TUNE=0 in the environment disables it. */
+ * register budget (resident blocks per SM) of the Shamir and Wilson stencils
+ * per lattice on first use (results are identical for every choice);
+ * THR_TUNE=0 in the environment disables it. */
 int thr_tune_report(char *buf, int len);
 
 #ifdef __cplusplus

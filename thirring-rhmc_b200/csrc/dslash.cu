@@ -397,29 +397,31 @@ unsigned stencil_grid(const Geom& g, int kernel) {
 }
 
 // ---------------------------------------------------------------- autotuner
-// For the Shamir stencil in FP64 and FP32 storage the register budget (blocks
-// per SM the compiler may assume: 8, 7 or 6 for 128-thread blocks) is tuned
-// per (storage, M or M^dagger, epilogue, lattice, layout, device) on first use:
+// For the stencils in FP64 and FP32 storage the register budget (blocks per SM
+// the compiler may assume: 8, 7 or 6 for the Shamir kernel's 128-thread blocks,
+// 2 or 1 for the Wilson kernel's 256-thread blocks) is tuned per (storage,
+// kernel, M or M^dagger, epilogue, lattice, layout, device) on first use:
 // each candidate runs 1 + 3 times on the call's own fields (the launches are
 // idempotent: out and partials are overwritten), the fastest is kept for the
 // process.  Block shape and reduction order do not change, so neither do the
-// results.  THR_TUNE=0 in the environment keeps the default (8).  Launches
+// results.  THR_TUNE=0 in the environment keeps the defaults (8, 2).  Launches
 // made while the stream is being captured into a graph use the default until
 // a tuned value exists.
 namespace {
-constexpr int kTuneMinb[3] = {8, 7, 6};
+constexpr int kTuneShamir[3] = {8, 7, 6};
+constexpr int kTuneWilson[2] = {2, 1};
 struct TuneKey {
-  int dev, sid, dag, epi, lx, ly, lt, ls, layout;
+  int dev, sid, ker, dag, epi, lx, ly, lt, ls, layout;
   bool operator<(const TuneKey& o) const {
-    const int a[9] = {dev, sid, dag, epi, lx, ly, lt, ls, layout};
-    const int b[9] = {o.dev, o.sid, o.dag, o.epi, o.lx, o.ly, o.lt, o.ls, o.layout};
-    for (int i = 0; i < 9; i++)
+    const int a[10] = {dev, sid, ker, dag, epi, lx, ly, lt, ls, layout};
+    const int b[10] = {o.dev, o.sid, o.ker, o.dag, o.epi, o.lx, o.ly, o.lt, o.ls, o.layout};
+    for (int i = 0; i < 10; i++)
       if (a[i] != b[i]) return a[i] < b[i];
     return false;
   }
 };
 struct TuneVal {
-  int pick;
+  int pick, ncand;
   float us[3];
 };
 std::mutex g_tune_mu;
@@ -464,67 +466,70 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
     if (dag) THR_E(K, true, N, SH, MB);            \
     else THR_E(K, false, N, SH, MB);               \
   } while (0)
-  if (kernel == 1) {
-    if (nt == 256) THR_D(1, 256, false, 1);
-    else THR_D(1, 1024, false, 1);
-  } else if (nt == 128) {
-    // the Shamir fast path: 128-thread blocks, register budget from the tuner
-    auto launch = [&](int minb) {
-      if (shfl) {
-        if (minb == 8) THR_D(0, 128, true, 8);
-        else if (minb == 7) THR_D(0, 128, true, 7);
-        else THR_D(0, 128, true, 6);
-      } else {
-        if (minb == 8) THR_D(0, 128, false, 8);
-        else if (minb == 7) THR_D(0, 128, false, 7);
-        else THR_D(0, 128, false, 6);
-      }
-    };
-    int minb = 8;
-    if (storage_id<S>() < 2) {
-      int dev = 0;
-      cudaGetDevice(&dev);
-      const TuneKey key{dev, storage_id<S>(), dag ? 1 : 0, e, g.lx, g.ly, g.lt, g.ls, g.layout};
-      bool found = false;
-      {
-        std::lock_guard<std::mutex> lock(g_tune_mu);
-        auto it = g_tune.find(key);
-        if (it != g_tune.end()) {
-          minb = it->second.pick;
-          found = true;
-        }
-      }
-      if (!found && tune_on() && !capturing(st)) {
-        TuneVal tv{8, {0.f, 0.f, 0.f}};
-        cudaEvent_t e0, e1;
-        if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
-          float best = 1e30f;
-          for (int c = 0; c < 3; c++) {
-            launch(kTuneMinb[c]);
-            cudaEventRecord(e0, st);
-            for (int r = 0; r < 3; r++) launch(kTuneMinb[c]);
-            cudaEventRecord(e1, st);
-            cudaEventSynchronize(e1);
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            tv.us[c] = ms * 1e3f / 3.f;
-            if (tv.us[c] < best) {
-              best = tv.us[c];
-              tv.pick = kTuneMinb[c];
-            }
-          }
-          cudaEventDestroy(e0);
-          cudaEventDestroy(e1);
-          std::lock_guard<std::mutex> lock(g_tune_mu);
-          g_tune[key] = tv;
-          minb = tv.pick;
-        }
+  // the register budget (resident blocks per SM) of the common configurations is
+  // tuned: Shamir 128-thread blocks {8, 7, 6}, Wilson 256-thread blocks {2, 1}
+  auto launch = [&](int minb) {
+    if (kernel == 1) {
+      if (nt != 256) THR_D(1, 1024, false, 1);
+      else if (minb == 2) THR_D(1, 256, false, 2);
+      else THR_D(1, 256, false, 1);
+    } else if (nt != 128) {
+      THR_D(0, 1024, false, 1);
+    } else if (shfl) {
+      if (minb == 8) THR_D(0, 128, true, 8);
+      else if (minb == 7) THR_D(0, 128, true, 7);
+      else THR_D(0, 128, true, 6);
+    } else {
+      if (minb == 8) THR_D(0, 128, false, 8);
+      else if (minb == 7) THR_D(0, 128, false, 7);
+      else THR_D(0, 128, false, 6);
+    }
+  };
+  const bool tunable = storage_id<S>() < 2 && nt == (kernel == 0 ? 128 : 256);
+  const int* cand = kernel == 0 ? kTuneShamir : kTuneWilson;
+  const int ncand = kernel == 0 ? 3 : 2;
+  int minb = cand[0];
+  if (tunable) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const TuneKey key{dev, storage_id<S>(), kernel, dag ? 1 : 0, e, g.lx, g.ly, g.lt, g.ls, g.layout};
+    bool found = false;
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      auto it = g_tune.find(key);
+      if (it != g_tune.end()) {
+        minb = it->second.pick;
+        found = true;
       }
     }
-    launch(minb);
-  } else {
-    THR_D(0, 1024, false, 1);
+    if (!found && tune_on() && !capturing(st)) {
+      TuneVal tv{cand[0], ncand, {0.f, 0.f, 0.f}};
+      cudaEvent_t e0, e1;
+      if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
+        float best = 1e30f;
+        for (int c = 0; c < ncand; c++) {
+          launch(cand[c]);
+          cudaEventRecord(e0, st);
+          for (int r = 0; r < 3; r++) launch(cand[c]);
+          cudaEventRecord(e1, st);
+          cudaEventSynchronize(e1);
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, e0, e1);
+          tv.us[c] = ms * 1e3f / 3.f;
+          if (tv.us[c] < best) {
+            best = tv.us[c];
+            tv.pick = cand[c];
+          }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune[key] = tv;
+        minb = tv.pick;
+      }
+    }
   }
+  launch(minb);
 #undef THR_D
 #undef THR_E
 #undef THR_L
@@ -589,7 +594,7 @@ THR_INST(__half2, float2)
 }  // namespace thr
 
 // The autotuner's choices so far, one line each:
-//   <storage> <M|Mdag> epi=<e> <lx>x<ly>x<lt> Ls=<ls> layout=<l> dev=<d> minb=<pick> us=<8>/<7>/<6>
+//   <storage> <shamir|wilson> <M|Mdag> epi=<e> <lx>x<ly>x<lt> Ls=<ls> layout=<l> dev=<d> minb=<pick> us=<per candidate>
 extern "C" int thr_tune_report(char* buf, int len) {
   using namespace thr;
   if (!buf || len < 1) return THR_ERR_BADARG;
@@ -599,10 +604,13 @@ extern "C" int thr_tune_report(char* buf, int len) {
     for (const auto& kv : g_tune) {
       const TuneKey& k = kv.first;
       char line[256];
-      std::snprintf(line, sizeof(line), "%s %s epi=%d %dx%dx%d Ls=%d layout=%d dev=%d minb=%d us=%.2f/%.2f/%.2f\n",
-                    k.sid == 0 ? "fp64" : "fp32", k.dag ? "Mdag" : "M", k.epi, k.lx, k.ly, k.lt, k.ls, k.layout,
-                    k.dev, kv.second.pick, kv.second.us[0], kv.second.us[1], kv.second.us[2]);
+      int w = std::snprintf(line, sizeof(line), "%s %s %s epi=%d %dx%dx%d Ls=%d layout=%d dev=%d minb=%d us=",
+                            k.sid == 0 ? "fp64" : "fp32", k.ker ? "wilson" : "shamir", k.dag ? "Mdag" : "M", k.epi,
+                            k.lx, k.ly, k.lt, k.ls, k.layout, k.dev, kv.second.pick);
+      for (int c = 0; c < kv.second.ncand && w > 0 && w < (int)sizeof(line); c++)
+        w += std::snprintf(line + w, sizeof(line) - w, c ? "/%.2f" : "%.2f", kv.second.us[c]);
       r += line;
+      r += "\n";
     }
   }
   std::snprintf(buf, (size_t)len, "%s", r.c_str());
