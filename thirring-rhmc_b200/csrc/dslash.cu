@@ -143,28 +143,18 @@ __device__ __forceinline__ void shamir_site(const S* __restrict__ in, const type
   }
   // wall mass term: dirac.F90:119-176 (M), :356-402 (M^dagger).  imass 1, 3 couple
   // R(1) into s = Ls (spins A) and R(Ls) into s = 1 (spins B); imass 5 mixes the
-  // chiralities at the same s.
+  // chiralities at the same s.  Written as acc += c * v with one coefficient per
+  // wall: imass 1: am; imass 3: +i am (A), -i am (B); imass 5: +-i am (M / M^dagger).
   const R a = (R)am;
-  if (imass == 1 || imass == 3) {
-    const C zk = imass == 1 ? mk(a, R(0)) : mk(R(0), DAG ? a : -a);
+  const bool five = imass == 5;
+  const C cA = imass == 1 ? mk(a, R(0)) : mk(R(0), (five && DAG) ? -a : a);
+  const C cB = imass == 1 ? mk(a, R(0)) : mk(R(0), five ? (DAG ? -a : a) : -a);
 #pragma unroll
-    for (int k = 0; k < 2; k++) {
-      if (s == Ls - 1) {
-        const C v = cmul(zk, SHFL ? w0[k] : Rv(0, site, a0 + k));
-        acc[a0 + k] = (imass == 3 && !DAG) ? acc[a0 + k] - v : acc[a0 + k] + v;
-      }
-      if (s == 0) {
-        const C v = cmul(zk, SHFL ? wl[k] : Rv(Ls - 1, site, b0 + k));
-        acc[b0 + k] = (imass == 3 && DAG) ? acc[b0 + k] - v : acc[b0 + k] + v;
-      }
-    }
-  } else if (imass == 5) {
-    const C zk = mk(R(0), DAG ? a : -a);
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-      if (s == Ls - 1) acc[a0 + k] = acc[a0 + k] - cmul(zk, rc[b0 + k]);
-      if (s == 0) acc[b0 + k] = acc[b0 + k] - cmul(zk, rc[a0 + k]);
-    }
+  for (int k = 0; k < 2; k++) {
+    if (s == Ls - 1)
+      acc[a0 + k] = acc[a0 + k] + cmul(cA, five ? rc[b0 + k] : (SHFL ? w0[k] : Rv(0, site, a0 + k)));
+    if (s == 0)
+      acc[b0 + k] = acc[b0 + k] + cmul(cB, five ? rc[a0 + k] : (SHFL ? wl[k] : Rv(Ls - 1, site, b0 + k)));
   }
   // Wilson and Dirac hopping terms, forward (U R(x+mu)) then backward
   // (conj U(x-mu) R(x-mu)) per direction; +gamma forward and -gamma backward in
@@ -334,7 +324,23 @@ __global__ void __launch_bounds__(NT, MINB)
       }
     }
   }
-  if (EPI != 0) block_partial(racc, partials + blockIdx.x);
+  if (EPI != 0) {
+    // one FP64 partial per block in a fixed order.  Blocks of Ls x sites need not be
+    // whole warps (Ls = 12: 120 threads), so the values go through shared memory and
+    // the first warp -- always complete: every configuration has >= 32 threads -- sums them.
+    __shared__ double red[NT];
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int nthr = blockDim.x * blockDim.y;
+    red[tid] = racc;
+    __syncthreads();
+    if (tid < 32) {
+      double v = 0.0;
+      for (int i = tid; i < nthr; i += 32) v += red[i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (tid == 0) partials[blockIdx.x] = v;
+    }
+  }
 }
 
 // Batched stencil: a persistent grid walks the work blocks of all entries

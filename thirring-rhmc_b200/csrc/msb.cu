@@ -174,6 +174,7 @@ __global__ void __launch_bounds__(kThreads) k_flush(const MsCoef* cf, V* __restr
 #pragma unroll
     for (int j = 0; j < kBatch; j++)
       if (j < ns) rj[j] = ring[(size_t)(1 + j) * n + i];
+    ring[i] = ring[(size_t)ns * n + i];  // the next batch starts from the last residual (just read: cached)
     for (int k = lo; k <= hi; k++) {
       const V f0 = sf[k * stride + i];
       const V o0 = out[k * stride + i];
@@ -189,9 +190,6 @@ __global__ void __launch_bounds__(kThreads) k_flush(const MsCoef* cf, V* __restr
       sf[k * stride + i] = f;
       out[k * stride + i] = o;
     }
-#pragma unroll
-    for (int j = 0; j < kBatch; j++)
-      if (j == ns - 1) ring[i] = rj[j];
   }
 }
 // close a batch
