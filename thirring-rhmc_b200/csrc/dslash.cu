@@ -37,7 +37,7 @@ struct SpinorView {
   const S* p;
   Geom g;
   __device__ __forceinline__ typename Sto<S>::C operator()(int s, int site, int d) const {
-    return Sto<S>::ld(p, sidx(g, s, site, d));
+    return Sto<S>::ld(p, sidx32(g, s, site, d));
   }
 };
 
@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(NT, MINB)
     if (live) {
 #pragma unroll
       for (int d = 0; d < 4; d++) {
-        const size_t i = sidx(g, s, site, d);
+        const unsigned i = sidx32(g, s, site, d);
         if (EPI == 1) {
           const C rn = Sto<S>::ld(aux, i) + om * acc[d];  // r = r + omega*s (multishift_module.F90:137)
           Sto<S>::st(out, i, rn);
@@ -454,6 +454,7 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
                        int imass, float am3, cudaStream_t st, const int* skip, const S* aux, const double* coef,
                        double* partials, int e) {
   if (g.ls > 1024) return THR_ERR_BADSHAPE;
+  if (4ULL * (unsigned long long)g.v5 >= (1ULL << 32)) return THR_ERR_BADSHAPE;  // 32-bit element offsets
   if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
   const dim3 blk = stencil_block(g, kernel);
   const dim3 grd(stencil_grid(g, kernel));
