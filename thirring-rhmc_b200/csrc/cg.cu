@@ -135,7 +135,7 @@ int cg_enqueue_chunk(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r
     // x2 = M^dagger x1 is never stored: the epilogue forms r = r - alpha*x2 (:92) and
     // betacgn = |r|^2 (:102)
     THR_TRY(launch_dslash_axpy<double2>(c->g, c->p.kernel, true, r, x1, c->u64, am, imass, c->p.am3, c->st, &cs->done,
-                                        r, &cs->nalpha, c->partials));
+                                        r, &cs->nalpha, c->partials, c->rev_sweep));
     k_cg_beta<<<1, 1024, 0, c->st>>>(cs, c->partials, gs);
     k_cg_xp<<<gb, kThreads, 0, c->st>>>(cs, X, p, r, n);
     k_cg_latch<<<1, 1, 0, c->st>>>(cs);
@@ -176,7 +176,7 @@ int cg_graph(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r, double
   THR_TRY(launch_dslash_norm<double2>(c->g, c->p.kernel, false, x1, p, c->u64, am, imass, c->p.am3, c->st, &cs->done,
                                       c->partials));
   THR_TRY(launch_dslash_axpy<double2>(c->g, c->p.kernel, true, x2, x1, c->u64, am, imass, c->p.am3, c->st, &cs->done,
-                                      x2, &cs->nalpha, c->partials));
+                                      x2, &cs->nalpha, c->partials, c->rev_sweep));
   THR_CUDA(cudaGraphCreate(&G.graph, 0));
   cudaGraphConditionalHandle handle;
   THR_CUDA(cudaGraphConditionalHandleCreate(&handle, G.graph, 1, cudaGraphCondAssignDefault));

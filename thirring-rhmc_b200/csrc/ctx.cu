@@ -152,6 +152,10 @@ int thr_create(const thr_params* p, thr_ctx** out) {
   c->g.layout = p->layout;
   c->g.hv3 = c->g.v3 / 2;
   c->dev = p->device;
+  {
+    const char* e = std::getenv("THR_REVERSE");
+    if (e && e[0] == '0') c->rev_sweep = 0;
+  }
   int rc = THR_OK;
   if (cudaSetDevice(c->dev) != cudaSuccess) rc = THR_ERR_CUDA;
   if (!rc && cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) rc = THR_ERR_CUDA;

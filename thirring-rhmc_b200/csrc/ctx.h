@@ -78,6 +78,7 @@ struct thr_ctx {
   bool use_graphs = true;   // batched solver loops as one CUDA graph (WHILE node) per solve
   void* ms_graphs[2] = {};  // cached batched-multishift graphs (FP64, FP32 vectors)
   void* cg_graph = nullptr;  // cached congrad graph
+  int rev_sweep = 1;         // M^dagger-with-update stencil walks the sites top down (THR_REVERSE=0: bottom up)
   double md_counts[8] = {};  // ancg, ancgpv, ancgf, ancgfpv, ancgh, ancghpv, ancgpf, ancgpfpv
   void* bufs[B_COUNT] = {};
   size_t buf_bytes[B_COUNT] = {};

@@ -296,14 +296,17 @@ template <class S, int KER, bool DAG, int EPI, int NT, bool SHFL, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     k_dslash(S* __restrict__ out, const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u, Geom g, float am,
              int imass, float am3, const int* skip, const S* __restrict__ aux, const double* __restrict__ coef,
-             double* __restrict__ partials) {
+             double* __restrict__ partials, int rev) {
   if (skip && *skip) return;
   using C = typename Sto<S>::C;
   using R = typename Sto<S>::R;
   const R om = EPI == 1 ? (R)(*coef) : R(0);
   const int s = threadIdx.x;
   double racc = 0.0;
-  const int site = blockIdx.x * blockDim.y + threadIdx.y;
+  // rev: blocks walk the sites from the top, so that the first blocks find the
+  // end of a field the previous kernel has just written still in L2
+  const int bid = rev ? (int)gridDim.x - 1 - (int)blockIdx.x : (int)blockIdx.x;
+  const int site = bid * blockDim.y + threadIdx.y;
   const bool live = site < g.v3;
   if (SHFL || live) {  // with SHFL every lane takes part (the last block's spare rows on a clamped site)
     const int st = live ? site : g.v3 - 1;
@@ -338,7 +341,7 @@ __global__ void __launch_bounds__(NT, MINB)
       for (int i = tid; i < nthr; i += 32) v += red[i];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-      if (tid == 0) partials[blockIdx.x] = v;
+      if (tid == 0) partials[bid] = v;
     }
   }
 }
@@ -452,7 +455,7 @@ template <class S> constexpr int storage_id() { return sizeof(S) == sizeof(doubl
 template <class S>
 int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
                        int imass, float am3, cudaStream_t st, const int* skip, const S* aux, const double* coef,
-                       double* partials, int e) {
+                       double* partials, int e, int rev) {
   if (g.ls > 1024) return THR_ERR_BADSHAPE;
   if (4ULL * (unsigned long long)g.v5 >= (1ULL << 32)) return THR_ERR_BADSHAPE;  // 32-bit element offsets
   if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
@@ -461,7 +464,7 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   const int nt = stencil_threads(g, kernel);
   const bool shfl = stencil_shfl(g, kernel);
 #define THR_L(K, D, E, N, SH, MB) \
-  k_dslash<S, K, D, E, N, SH, MB><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, coef, partials)
+  k_dslash<S, K, D, E, N, SH, MB><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, coef, partials, rev)
 #define THR_E(K, D, N, SH, MB)                 \
   do {                                         \
     if (e == 1) THR_L(K, D, 1, N, SH, MB);     \
@@ -546,20 +549,22 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
 template <class S>
 int launch_dslash_axpy(const Geom& g, int kernel, bool dag, S* rnew, const S* in, const typename Sto<S>::C* u,
                        float am, int imass, float am3, cudaStream_t st, const int* skip, const S* rold,
-                       const double* coef, double* partials) {
-  return launch_dslash_mode<S>(g, kernel, dag, rnew, in, u, am, imass, am3, st, skip, rold, coef, partials, 1);
+                       const double* coef, double* partials, int rev) {
+  return launch_dslash_mode<S>(g, kernel, dag, rnew, in, u, am, imass, am3, st, skip, rold, coef, partials, 1, rev);
 }
 
 template <class S>
 int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
                        float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials) {
-  return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr, partials, 2);
+  return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr, partials, 2,
+                               0);
 }
 
 template <class S>
 int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
                   int imass, float am3, cudaStream_t st, const int* skip) {
-  return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr, nullptr, 0);
+  return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr, nullptr, 0,
+                               0);
 }
 
 template <class S>
@@ -587,7 +592,7 @@ int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const
   template int launch_dslash<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float, cudaStream_t,   \
                                 const int*);                                                                      \
   template int launch_dslash_axpy<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
-                                     cudaStream_t, const int*, const S*, const double*, double*);                 \
+                                     cudaStream_t, const int*, const S*, const double*, double*, int);            \
   template int launch_dslash_norm<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
                                      cudaStream_t, const int*, double*);                                          \
   template int launch_dslash_batch<S>(const BatchTable&, int, bool, S*, const S*, const L*, float, int, float,    \

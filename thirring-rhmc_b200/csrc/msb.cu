@@ -256,7 +256,7 @@ int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* 
     // s = M^dagger h is never stored: the epilogue forms r = r + omega*s (:137) and |r|^2 (:138)
     pe = prof ? c->prof_begin(thr_ctx::P_DSLASH_DAG, b_md, k0 + j) : -1;
     THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, rnew, hv, u, am, imass, c->p.am3, c->st, &ms->done, rold,
-                                  &ms->omega, c->partials));
+                                  &ms->omega, c->partials, c->rev_sweep));
     c->prof_end(pe);
     k_lambda<<<1, 1024, 0, c->st>>>(ms, hist, c->partials, gs);
     k_pupdate<V><<<gb, kThreads, 0, c->st>>>(ms, p, rnew, n);
@@ -313,7 +313,7 @@ int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V
     THR_TRY(launch_dslash_norm<V>(c->g, c->p.kernel, false, hv, p, uu, am, imass, c->p.am3, c->st, &ms->done,
                                   c->partials));
     THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, s, hv, uu, am, imass, c->p.am3, c->st, &ms->done, ring,
-                                  &ms->omega, c->partials));
+                                  &ms->omega, c->partials, c->rev_sweep));
   }
   THR_CUDA(cudaGraphCreate(&G.graph, 0));
   cudaGraphConditionalHandle handle;

@@ -16,11 +16,12 @@ template <class S>
 int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
                   int imass, float am3, cudaStream_t st, const int* skip = nullptr);
 // rnew = rold + (*coef) * (M or M^dagger) in, without storing the stencil's output,
-// and one FP64 partial per block of |rnew|^2
+// and one FP64 partial per block of |rnew|^2.  rev != 0: blocks take the sites from
+// the top down (same results; better L2 reuse of a field written just before)
 template <class S>
 int launch_dslash_axpy(const Geom& g, int kernel, bool dag, S* rnew, const S* in, const typename Sto<S>::C* u,
                        float am, int imass, float am3, cudaStream_t st, const int* skip, const S* rold,
-                       const double* coef, double* partials);
+                       const double* coef, double* partials, int rev = 0);
 // same, with one FP64 partial per block of sum |out|^2
 template <class S>
 int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
