@@ -169,6 +169,23 @@ int thr_pack_get_stream(thr_pack *pack, void **stream);
 int thr_measure(thr_ctx *ctx, int kernel_meas, float res, float am, int imass, int knoise, int precision,
                 float *psibarpsi, float *susclsing, float *aviter, double *parts, int *itercg);
 
+/* meson(res, itercg, aviter, am, imass[, isweep_total]), measure_module.F90:684-1085
+ * (SITE_RANDOM source positions, no smearing): nsource point sources on the
+ * wall s = 1 (spins 3, 4), at positions drawn with rano at site (1,1,1); for
+ * imass != 1 also the propagators with -am.  Outputs per time separation t =
+ * 0..Lt-1 (fort.302/320/321): cpm[t], cmm[t], cpmn[2t..2t+1], cmmn[2t..2t+1]
+ * (real, imaginary), chim (fort.400), itercg of the last solve, aviter.
+ * nsource = 5 in the reference. */
+int thr_meson(thr_ctx *ctx, float res, float am, int imass, int nsource, int precision, double *cpm, double *cmm,
+              double *cpmn, double *cmmn, double *chim, int *itercg, float *aviter);
+
+/* fermion(res, itercg, aviter, am, imass[, isweep_total]), measure_module.F90:1100-1376
+ * (SITE_RANDOM source times): wall sources 1/ksize2 on a time slice at s = 1,
+ * spins 3, 4.  Outputs cferm1[2t..2t+1], cferm2[2t..2t+1] (fort.500/501),
+ * itercg of the last solve, aviter. */
+int thr_fermion(thr_ctx *ctx, float res, float am, int imass, int nsource, int precision, double *cferm1,
+                double *cferm2, int *itercg, float *aviter);
+
 /* ---- multishift_module.F90 ----------------------------------------------- */
 /* multishift_solver(u, am, imass, ndiagq, aden, anum, output, input, res,
  * maxcg, cg_return[, cg_returns]), multishift_module.F90:13-284: solves

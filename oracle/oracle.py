@@ -433,3 +433,104 @@ def measure(L, g, u, res, am, imass, kernel_meas=0, knoise=10):
     aviter = np.float32(np.float32(it_total) / np.float32(4 * knoise))
     return dict(psibarpsi=float(psibarpsi), susclsing=float(sus), aviter=float(aviter), parts=parts,
                 pbp=pbp, itercg=its)
+
+
+def _wall_props(L, u, xi_src, res, am, imass):
+    """measure_module.F90:811-826 (and :1162-1177): Phi = M^dagger xi, the initial
+    guess M^dagger Phi, congrad; returns (itercg, solution)."""
+    Phi = update_halo_5(L, dslashd(L, xi_src, u, am, imass))
+    X = update_halo_5(L, dslashd(L, Phi, u, am, imass))
+    itercg, _ = congrad(L, Phi, X, u, res, am, imass)
+    return itercg, X
+
+
+def meson(L, g, u, res, am, imass, nsource=5):
+    """meson(res, itercg, aviter, am, imass), measure_module.F90:684-1085 with
+    SITE_RANDOM source positions (three rano draws at site (1,1,1) per source)
+    and nsmear = 0: point sources on the wall s = 1, spins 3 and 4; propagators
+    to s = 1 (spins 1,2) and s = Ls (spins 3,4); for imass != 1 also with -am.
+    Returns cpm, cmm (real(dp)), cpmn, cmmn (complex(dp)) per time separation,
+    chim, the last itercg and aviter."""
+    lx, ly, lt, ls = L.lx, L.ly, L.lt, L.ls
+    cpm = np.zeros(lt); cmm = np.zeros(lt)
+    cpmn = np.zeros(lt, complex); cmmn = np.zeros(lt, complex)
+    it_total = 0
+    itercg = 0
+    for _ in range(nsource):
+        ix = int(np.float32(lx) * np.float32(g.rano(1, 1, 1))) + 1
+        iy = int(np.float32(lx) * np.float32(g.rano(1, 1, 1))) + 1  # ksize for x and y
+        itt0 = int(np.float32(lt) * np.float32(g.rano(1, 1, 1))) + 1
+        p00 = np.zeros((lx, ly, lt, 2, 2), complex); p0L = np.zeros_like(p00)
+        p00n = np.zeros_like(p00); p0Ln = np.zeros_like(p00)
+        for k, ids in enumerate((3, 4)):
+            xi = spinor(L)
+            xi[1, ix, iy, itt0, ids - 1] = 1.0
+            update_halo_5(L, xi)
+            itercg, X = _wall_props(L, u, xi, res, am, imass)
+            it_total += itercg
+            p00[..., k, :] = X[1, 1:-1, 1:-1, 1:-1, 0:2]
+            p0L[..., k, :] = X[ls, 1:-1, 1:-1, 1:-1, 2:4]
+            if imass != 1:
+                itercg, Xn = _wall_props(L, u, xi, res, -am, imass)
+                it_total += itercg
+                p00n[..., k, :] = Xn[1, 1:-1, 1:-1, 1:-1, 0:2]
+                p0Ln[..., k, :] = Xn[ls, 1:-1, 1:-1, 1:-1, 2:4]
+            else:
+                p00n[..., k, :] = p00[..., k, :]
+                p0Ln[..., k, :] = p0L[..., k, :]
+        for it in range(lt):
+            t = (itt0 - 1 + it) % lt
+            cpm[it] += np.sum(np.abs(p00[:, :, t]) ** 2)
+            cpmn[it] += np.sum(p00[:, :, t] * np.conj(p00n[:, :, t]))
+            cmm[it] += np.sum(np.abs(p0L[:, :, t]) ** 2)
+            cmmn[it] += np.sum(p0L[:, :, t] * np.conj(p0Ln[:, :, t]))
+    cpm /= nsource; cmm /= nsource; cpmn /= nsource; cmmn /= nsource
+    chim = 0.0
+    for it in range(lt):
+        chim += 2 * (cpm[it] + cmm[it])
+    aviter = np.float32(np.float32(it_total) / np.float32(2 * nsource))
+    return dict(cpm=cpm, cmm=cmm, cpmn=cpmn, cmmn=cmmn, chim=chim, itercg=itercg, aviter=float(aviter))
+
+
+# 2 gamma(3, d) (gammamatrices.F90: mu = 3 row, already times akappa = 1/2 there)
+_GAMVAL3 = {3: 0.5j, 4: -0.5j}
+_GAMIN3 = {3: 1, 4: 2}
+
+
+def fermion(L, g, u, res, am, imass, nsource=5, ibound=-1):
+    """fermion(res, itercg, aviter, am, imass), measure_module.F90:1100-1376 with
+    SITE_RANDOM source times: wall sources 1/ksize2 on a whole time slice at
+    s = 1, spins 3 and 4; cferm1(t) = sum isign akappa prop0L(.,t,d,d),
+    cferm2(t) = sum isign gamval(3,d) prop00(.,t,d,gamin(3,d)), isign = ibound
+    across the time boundary.  Returns cferm1, cferm2, the last itercg, aviter."""
+    lx, ly, lt, ls = L.lx, L.ly, L.lt, L.ls
+    cf1 = np.zeros(lt, complex); cf2 = np.zeros(lt, complex)
+    it_total = 0
+    itercg = 0
+    for _ in range(nsource):
+        itt0 = int(np.float32(lt) * np.float32(g.rano(1, 1, 1))) + 1
+        p00 = {}; p0L = {}
+        for ids in (3, 4):
+            xi = spinor(L)
+            # cmplx(1.0, 0.0) / ksize2: a default-real complex, widened
+            xi[1, 1:-1, 1:-1, itt0, ids - 1] = float(np.float32(1.0) / np.float32(lx * lx))
+            update_halo_5(L, xi)
+            itercg, X = _wall_props(L, u, xi, res, am, imass)
+            it_total += itercg
+            p00[ids] = X[1, 1:-1, 1:-1, 1:-1, :]
+            p0L[ids] = X[ls, 1:-1, 1:-1, 1:-1, :]
+        t1 = np.zeros(lt, complex); t2 = np.zeros(lt, complex)
+        for idd in (3, 4):
+            for it in range(lt):
+                itt = (itt0 - 1 + it) % lt + 1
+                isign = 1 if itt >= itt0 else ibound
+                t1[it] += isign * 0.5 * np.sum(p0L[idd][:, :, itt - 1, idd - 1])
+        for idd in (3, 4):
+            for it in range(lt):
+                itt = (itt0 - 1 + it) % lt + 1
+                isign = 1 if itt >= itt0 else ibound
+                t2[it] += isign * _GAMVAL3[idd] * np.sum(p00[idd][:, :, itt - 1, _GAMIN3[idd] - 1])
+        cf1 += t1; cf2 += t2
+    cf1 /= nsource; cf2 /= nsource
+    aviter = np.float32(np.float32(it_total) / np.float32(2 * nsource))
+    return dict(cferm1=cf1, cferm2=cf2, itercg=itercg, aviter=float(aviter))

@@ -88,3 +88,43 @@ def test_measure_rejects():
         G.init_random(1.0)
         with pytest.raises(thirring.ThirringError):
             G.measure(0.1, 0.05, 5, kernel_meas=1)  # measure_wilson has no imass 5 branch
+
+
+@pytest.mark.gpu
+def test_meson_fixture_kat():
+    # tests/test_meson.F90: itercg == 3, aviter (3, 6, 6), and the correlators of the oracle
+    dims = (12, 12, 12, 24)
+    L = O.lat(*dims)
+    u = O.starting_state(L)["u"]
+    g = O.RNG(L, True).init(4139764973254.0)
+    with thirring.Lattice(*dims) as G:
+        G.set_links(u)
+        G.init_random(4139764973254.0)
+        for imass, aviter in ((1, 3.0), (3, 6.0), (5, 6.0)):
+            ref = O.meson(L, g, u, 0.1, 0.05, imass)
+            got = G.meson(0.1, 0.05, imass)
+            assert got["itercg"] == 3 and got["aviter"] == aviter
+            for k in ("cpm", "cmm", "cpmn", "cmmn"):
+                np.testing.assert_allclose(got[k], ref[k], rtol=1e-9, atol=1e-14)
+            assert abs(got["chim"] - ref["chim"]) <= 1e-9 * abs(ref["chim"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel,imass", [(0, 1), (0, 3), (0, 5), (1, 3)])
+def test_meson_and_fermion_converged(kernel, imass):
+    dims = (6, 6, 8, 8)
+    L = O.lat(*dims, kernel=kernel)
+    u = rand_links(L, np.random.default_rng(60 + imass), beta=2.0)
+    g = O.RNG(L, True).init(24680.0)
+    with thirring.Lattice(*dims, kernel=kernel) as G:
+        G.set_links(u)
+        G.init_random(24680.0)
+        ref = O.meson(L, g, u, 1e-8, 0.1, imass, nsource=3)
+        got = G.meson(1e-8, 0.1, imass, nsource=3)
+        assert abs(got["itercg"] - ref["itercg"]) <= 2
+        for k in ("cpm", "cmm", "cpmn", "cmmn"):
+            np.testing.assert_allclose(got[k], ref[k], rtol=1e-6, atol=1e-10 * np.max(np.abs(ref[k])))
+        ref = O.fermion(L, g, u, 1e-8, 0.1, imass, nsource=3)
+        got = G.fermion(1e-8, 0.1, imass, nsource=3)
+        for k in ("cferm1", "cferm2"):
+            np.testing.assert_allclose(got[k], ref[k], rtol=1e-6, atol=1e-9 * np.max(np.abs(ref[k])))

@@ -94,3 +94,15 @@ def test_measure_wilson_kat():
     r = _measure_fixture(0, 1)
     assert abs(r["aviter"] - 10.95) < 1e-6
     assert abs(abs(r["psibarpsi"]) - 5.422668e-2) < 5e-3 * 5.422668e-2
+
+
+def test_meson_kat():
+    # tests/test_meson.F90:22-58: seed 4139764973254 at site (1,1,1), the analytic
+    # fixture, res 0.1, am 0.05; itercg == 3 and aviter (3, 6, 6) for imass (1, 3, 5),
+    # one random-number stream carried across the three calls
+    L = O.lat(12, 12, 12, 24)
+    g = O.RNG(L, True).init(4139764973254.0)
+    u = O.starting_state(L)["u"]
+    for imass, aviter in ((1, 3.0), (3, 6.0), (5, 6.0)):
+        r = O.meson(L, g, u, 0.1, 0.05, imass)
+        assert r["itercg"] == 3 and r["aviter"] == aviter, (imass, r["itercg"], r["aviter"])

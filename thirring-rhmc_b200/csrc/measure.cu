@@ -128,7 +128,68 @@ __global__ void __launch_bounds__(kMeasThreads) k_meas_contract(const double2* _
   }
 }
 
+// propagator sources on the wall s = 1 (0-based s = 0), spin d: a point source at
+// storage site `site` (site >= 0) or a wall on the time slice t (site < 0), value v
+__global__ void k_prop_source(double2* X, Geom g, size_t n4, int d, int site, int t, double v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.v3) return;
+  if (site >= 0) {
+    if (i == 0) X[sidx(g, 0, site, d)] = make_double2(v, 0.0);
+    return;
+  }
+  int x, y, tt;
+  site_coords(g, i, x, y, tt);
+  if (tt == t) X[sidx(g, 0, i, d)] = make_double2(v, 0.0);
+}
+
+// the two walls of a propagator: W[0..1][site] = X(s = 1, spins 1,2),
+// W[2..3][site] = X(s = Ls, spins 3,4) (storage site order)
+__global__ void k_prop_walls(double2* W, const double2* X, Geom g) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.v3) return;
+  for (int k = 0; k < 2; k++) {
+    W[(size_t)k * g.v3 + i] = X[sidx(g, 0, i, k)];
+    W[(size_t)(2 + k) * g.v3 + i] = X[sidx(g, g.ls - 1, i, 2 + k)];
+  }
+}
 }  // namespace
+
+// Solves the propagators of `src` (one wall-s = 1 source each, built by the caller
+// on X) as measure_module.F90:811-826 does: Phi = M^dagger xi, initial guess
+// M^dagger Phi, congrad; returns the two walls of every solution on the host
+// (W: per solve 4 x V3 double2) and the iteration counts.
+static int prop_walls(thr_ctx* c, double2* X, int nsol, float res, float am, int imass, int precision,
+               std::vector<double2>& W, int* its) {
+  const Geom& g = c->g;
+  const size_t n4 = c->n4();
+  double2 *Phi = nullptr, *Wd = nullptr;
+  int rc = THR_OK;
+  if (cudaMalloc(&Phi, sizeof(double2) * n4 * nsol) != cudaSuccess ||
+      cudaMalloc(&Wd, sizeof(double2) * 4 * (size_t)g.v3 * nsol) != cudaSuccess)
+    rc = THR_ERR_NOMEM;
+  for (int j = 0; !rc && j < nsol; j++) {
+    rc = launch_dslash<double2>(g, c->p.kernel, true, Phi + j * n4, X + j * n4, c->u64, am, imass, c->p.am3, c->st,
+                                nullptr);
+    if (!rc)
+      rc = launch_dslash<double2>(g, c->p.kernel, true, X + j * n4, Phi + j * n4, c->u64, am, imass, c->p.am3,
+                                  c->st, nullptr);
+  }
+  int outer = 0;
+  if (!rc) rc = thr_congrad_multi_dev(c, Phi, X, nsol, res, am, imass, precision, its, &outer);
+  if (rc == THR_ERR_MAXITER) rc = THR_OK;  // congrad only writes a notice at niterc
+  const unsigned nb = (unsigned)((g.v3 + 255) / 256);
+  for (int j = 0; !rc && j < nsol; j++) k_prop_walls<<<nb, 256, 0, c->st>>>(Wd + (size_t)j * 4 * g.v3, X + j * n4, g);
+  if (!rc) {
+    W.resize((size_t)4 * g.v3 * nsol);
+    if (cudaMemcpyAsync(W.data(), Wd, sizeof(double2) * W.size(), cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
+        cudaStreamSynchronize(c->st) != cudaSuccess)
+      rc = THR_ERR_CUDA;
+  }
+  cudaFree(Phi);
+  cudaFree(Wd);
+  return rc;
+}
+
 }  // namespace thr
 
 using namespace thr;
@@ -251,6 +312,200 @@ int thr_measure(thr_ctx* c, int kernel_meas, float res, float am, int imass, int
   *susclsing = sus;
   *aviter = (float)iter / (float)(4 * knoise);
   if (itercg) std::copy(its.begin(), its.end(), itercg);
+  return THR_OK;
+}
+
+// meson(res, itercg, aviter, am, imass), measure_module.F90:684-1085 (SITE_RANDOM,
+// nsmear = 0).  Per source three rano draws at site (1,1,1) place a point
+// source on the wall s = 1 with spin 3 and 4; the propagators to s = 1 (spins
+// 1,2) and s = Ls (spins 3,4) are contracted per time separation from the
+// source time.  For imass != 1 the same with -am gives the "n" propagators.
+// All solves of one mass go through one batched congrad.
+int thr_meson(thr_ctx* c, float res, float am, int imass, int nsource, int precision, double* cpm, double* cmm,
+              double* cpmn, double* cmmn, double* chim, int* itercg, float* aviter) {
+  if (!c || !cpm || !cmm || !cpmn || !cmmn || !chim || !itercg || !aviter || nsource < 1) return THR_ERR_BADARG;
+  if (imass != 1 && imass != 3 && imass != 5) return THR_ERR_BADARG;
+  if (c->p.kernel == 1 && imass == 5) return THR_ERR_UNSUPPORTED;
+  if (!c->links_ok || !c->rng.ready) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  const Geom& g = c->g;
+  const size_t n4 = c->n4();
+  const int nsol = 2 * nsource;
+  std::vector<int> tsrc(nsource);
+  double2* X = nullptr;
+  if (cudaMalloc(&X, sizeof(double2) * n4 * nsol) != cudaSuccess) return THR_ERR_NOMEM;
+  auto build = [&](std::vector<int>& sites) -> int {
+    THR_CUDA(cudaMemsetAsync(X, 0, sizeof(double2) * n4 * nsol, c->st));
+    for (int k = 0; k < nsource; k++)
+      for (int ids = 0; ids < 2; ids++)
+        k_prop_source<<<1, 32, 0, c->st>>>(X + (size_t)(2 * k + ids) * n4, g, n4, 2 + ids, sites[k], 0, 1.0);
+    return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+  };
+  // source positions: int(ksize * rano) + 1 in default real (:756-758; ksize = Lx for x and y)
+  std::vector<int> sites(nsource);
+  int rc = THR_OK;
+  for (int k = 0; !rc && k < nsource; k++) {
+    float r[3];
+    for (int q = 0; !rc && q < 3; q++) rc = rng_rano_site(c, 1, 1, 1, nullptr, &r[q]);
+    if (rc) break;
+    const int ix = (int)((float)g.lx * r[0]), iy = (int)((float)g.lx * r[1]), it = (int)((float)g.lt * r[2]);
+    if (ix >= g.lx || iy >= g.ly || it >= g.lt) { rc = THR_ERR_BADSHAPE; break; }
+    sites[k] = site_index(g, ix, iy, it);
+    tsrc[k] = it;
+  }
+  std::vector<double2> W, Wn;
+  std::vector<int> its(nsol), itsn(nsol, 0);
+  if (!rc) rc = build(sites);
+  if (!rc) rc = prop_walls(c, X, nsol, res, am, imass, precision, W, its.data());
+  if (!rc && imass != 1) {
+    rc = build(sites);
+    if (!rc) rc = prop_walls(c, X, nsol, res, -am, imass, precision, Wn, itsn.data());
+  }
+  cudaFree(X);
+  if (rc) return rc;
+  if (imass == 1) Wn = W;
+  // contractions (:900-967): per source, per time separation, sums over x, y, both
+  // source spins and the two sink spins, in the Fortran element order
+  const int lt = g.lt;
+  // natural-order site lists per time slice (x fastest, then y)
+  std::vector<std::vector<int>> slice(lt);
+  for (int t = 0; t < lt; t++)
+    for (int y = 0; y < g.ly; y++)
+      for (int x = 0; x < g.lx; x++) slice[t].push_back(site_index(g, x, y, t));
+  for (int t = 0; t < lt; t++) {
+    cpm[t] = cmm[t] = 0.0;
+    cpmn[2 * t] = cpmn[2 * t + 1] = cmmn[2 * t] = cmmn[2 * t + 1] = 0.0;
+  }
+  const size_t v3 = g.v3;
+  for (int k = 0; k < nsource; k++) {
+    for (int it = 0; it < lt; it++) {
+      const int t = (tsrc[k] + it) % lt;
+      double r00 = 0.0, rL = 0.0, c00r = 0.0, c00i = 0.0, cLr = 0.0, cLi = 0.0;
+      for (int wall = 0; wall < 2; wall++)       // prop00 (spins 1,2 at s = 1), prop0L (spins 3,4 at s = Ls)
+        for (int sp = 0; sp < 2; sp++)           // sink spin (slowest index of the Fortran slice)
+          for (int ids = 0; ids < 2; ids++)      // source spin 3, 4
+            for (int q : slice[t]) {
+              const size_t o = (size_t)(2 * k + ids) * 4 * v3 + (size_t)(2 * wall + sp) * v3 + q;
+              const double2 a = W[o], b = Wn[o];
+              const double ab2 = a.x * a.x + a.y * a.y;
+              const double pr = a.x * b.x + a.y * b.y, pi = a.y * b.x - a.x * b.y;  // a * conj(b)
+              if (wall == 0) { r00 += ab2; c00r += pr; c00i += pi; }
+              else { rL += ab2; cLr += pr; cLi += pi; }
+            }
+      cpm[it] += r00;
+      cmm[it] += rL;
+      cpmn[2 * it] += c00r;
+      cpmn[2 * it + 1] += c00i;
+      cmmn[2 * it] += cLr;
+      cmmn[2 * it + 1] += cLi;
+    }
+  }
+  double ch = 0.0;
+  for (int it = 0; it < lt; it++) {
+    cpm[it] /= nsource;
+    cmm[it] /= nsource;
+    for (int q = 0; q < 2; q++) {
+      cpmn[2 * it + q] /= nsource;
+      cmmn[2 * it + q] /= nsource;
+    }
+    ch += 2 * (cpm[it] + cmm[it]);
+  }
+  *chim = ch;
+  long long iter = 0;
+  for (int j = 0; j < nsol; j++) iter += its[j] + itsn[j];
+  *itercg = imass != 1 ? itsn[nsol - 1] : its[nsol - 1];
+  *aviter = (float)iter / (float)(2 * nsource);
+  return THR_OK;
+}
+
+// fermion(res, itercg, aviter, am, imass), measure_module.F90:1100-1376
+// (SITE_RANDOM): per source one rano draw picks a time slice; wall sources
+// 1/ksize2 (default real) on it at s = 1 with spin 3 and 4;
+//   cferm1(t) = sum isign akappa prop0L(x,y,t,d,d),
+//   cferm2(t) = sum isign gamval(3,d) prop00(x,y,t,d,gamin(3,d)),
+// isign = ibound for sink times before the source time.
+int thr_fermion(thr_ctx* c, float res, float am, int imass, int nsource, int precision, double* cferm1,
+                double* cferm2, int* itercg, float* aviter) {
+  if (!c || !cferm1 || !cferm2 || !itercg || !aviter || nsource < 1) return THR_ERR_BADARG;
+  if (imass != 1 && imass != 3 && imass != 5) return THR_ERR_BADARG;
+  if (c->p.kernel == 1 && imass == 5) return THR_ERR_UNSUPPORTED;
+  if (!c->links_ok || !c->rng.ready) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  const Geom& g = c->g;
+  const size_t n4 = c->n4();
+  const int nsol = 2 * nsource;
+  std::vector<int> tsrc(nsource);
+  int rc = THR_OK;
+  for (int k = 0; !rc && k < nsource; k++) {
+    float r = 0.f;
+    rc = rng_rano_site(c, 1, 1, 1, nullptr, &r);
+    tsrc[k] = (int)((float)g.lt * r);
+    if (!rc && tsrc[k] >= g.lt) rc = THR_ERR_BADSHAPE;
+  }
+  if (rc) return rc;
+  double2* X = nullptr;
+  if (cudaMalloc(&X, sizeof(double2) * n4 * nsol) != cudaSuccess) return THR_ERR_NOMEM;
+  const double v = (double)(1.0f / (float)(g.lx * g.lx));  // cmplx(1.0,0.0) / ksize2 in default real
+  const unsigned nb = (unsigned)((g.v3 + 255) / 256);
+  if (cudaMemsetAsync(X, 0, sizeof(double2) * n4 * nsol, c->st) != cudaSuccess) rc = THR_ERR_CUDA;
+  for (int k = 0; !rc && k < nsource; k++)
+    for (int ids = 0; ids < 2; ids++)
+      k_prop_source<<<nb, 256, 0, c->st>>>(X + (size_t)(2 * k + ids) * n4, g, n4, 2 + ids, -1, tsrc[k], v);
+  std::vector<double2> W;
+  std::vector<int> its(nsol);
+  if (!rc) rc = prop_walls(c, X, nsol, res, am, imass, precision, W, its.data());
+  cudaFree(X);
+  if (rc) return rc;
+  const int lt = g.lt;
+  std::vector<std::vector<int>> slice(lt);
+  for (int t = 0; t < lt; t++)
+    for (int y = 0; y < g.ly; y++)
+      for (int x = 0; x < g.lx; x++) slice[t].push_back(site_index(g, x, y, t));
+  for (int q = 0; q < 2 * lt; q++) cferm1[q] = cferm2[q] = 0.0;
+  const size_t v3 = g.v3;
+  const double gim[2] = {0.5, -0.5};  // gamval(3, 3:4) = +-i akappa (gammamatrices.F90, mu = 3)
+  for (int k = 0; k < nsource; k++) {
+    std::vector<double> t1(2 * lt, 0.0), t2(2 * lt, 0.0);
+    for (int idd = 0; idd < 2; idd++)
+      for (int it = 0; it < lt; it++) {
+        const int t = (tsrc[k] + it) % lt;
+        const double isign = t >= tsrc[k] ? 1.0 : (double)c->p.ibound;
+        double sr = 0.0, si = 0.0;
+        for (int q : slice[t]) {  // prop0L(:, :, t, d, d): wall s = Ls, sink spin d = 3 + idd
+          const double2 a = W[(size_t)(2 * k + idd) * 4 * v3 + (size_t)(2 + idd) * v3 + q];
+          sr += a.x;
+          si += a.y;
+        }
+        t1[2 * it] += isign * 0.5 * sr;
+        t1[2 * it + 1] += isign * 0.5 * si;
+      }
+    for (int idd = 0; idd < 2; idd++)
+      for (int it = 0; it < lt; it++) {
+        const int t = (tsrc[k] + it) % lt;
+        const double isign = t >= tsrc[k] ? 1.0 : (double)c->p.ibound;
+        double sr = 0.0, si = 0.0;
+        for (int q : slice[t]) {  // prop00(:, :, t, d, gamin(3, d)): wall s = 1, sink spin gamin(3,d) = 1 + idd
+          const double2 a = W[(size_t)(2 * k + idd) * 4 * v3 + (size_t)idd * v3 + q];
+          sr += a.x;
+          si += a.y;
+        }
+        // isign * (i * gim) * (sr + i si)
+        t2[2 * it] += isign * (-gim[idd] * si);
+        t2[2 * it + 1] += isign * (gim[idd] * sr);
+      }
+    for (int q = 0; q < 2 * lt; q++) {
+      cferm1[q] += t1[q];
+      cferm2[q] += t2[q];
+    }
+  }
+  for (int q = 0; q < 2 * lt; q++) {
+    cferm1[q] /= nsource;
+    cferm2[q] /= nsource;
+  }
+  long long iter = 0;
+  for (int j = 0; j < nsol; j++) iter += its[j];
+  *itercg = its[nsol - 1];
+  *aviter = (float)iter / (float)(2 * nsource);
   return THR_OK;
 }
 

@@ -51,6 +51,8 @@ SIGNATURES = {
     "thr_pack_download": (_i, [_v, _i, _v]),
     "thr_pack_zero_x": (_i, [_v]),
     "thr_pack_get_stream": (_i, [_v, C.POINTER(_v)]),
+    "thr_meson": (_i, [_v, _f, _f, _i, _i, _i, _v, _v, _v, _v, _pd, _pi, C.POINTER(C.c_float)]),
+    "thr_fermion": (_i, [_v, _f, _f, _i, _i, _i, _v, _v, _pi, C.POINTER(C.c_float)]),
     "thr_measure": (_i, [_v, _i, _f, _f, _i, _i, _i, C.POINTER(C.c_float), C.POINTER(C.c_float),
                          C.POINTER(C.c_float), _v, _v]),
     "thr_multishift_solver": (_i, [_v, _v, _f, _i, _i, _v, _v, _v, _v, _f, _i, _pi, _v]),

@@ -276,6 +276,30 @@ class Lattice:
         _check(self._L.thr_rano(self.h, ix, iy, it, C.byref(v)), "rano")
         return v.value
 
+    def meson(self, res, am, imass, nsource=5, precision=FP64):
+        """meson(res, itercg, aviter, am, imass), measure_module.F90:684-1085."""
+        lt = self.lt
+        cpm, cmm = np.zeros(lt), np.zeros(lt)
+        cpmn, cmmn = np.zeros(2 * lt), np.zeros(2 * lt)
+        chim = C.c_double(0)
+        it = C.c_int(0)
+        av = C.c_float(0)
+        _check(self._L.thr_meson(self.h, res, am, imass, nsource, precision, _p(cpm), _p(cmm), _p(cpmn), _p(cmmn),
+                                 C.byref(chim), C.byref(it), C.byref(av)), "meson")
+        return dict(cpm=cpm, cmm=cmm, cpmn=cpmn[0::2] + 1j * cpmn[1::2], cmmn=cmmn[0::2] + 1j * cmmn[1::2],
+                    chim=chim.value, itercg=it.value, aviter=av.value)
+
+    def fermion(self, res, am, imass, nsource=5, precision=FP64):
+        """fermion(res, itercg, aviter, am, imass), measure_module.F90:1100-1376."""
+        lt = self.lt
+        c1, c2 = np.zeros(2 * lt), np.zeros(2 * lt)
+        it = C.c_int(0)
+        av = C.c_float(0)
+        _check(self._L.thr_fermion(self.h, res, am, imass, nsource, precision, _p(c1), _p(c2), C.byref(it),
+                                   C.byref(av)), "fermion")
+        return dict(cferm1=c1[0::2] + 1j * c1[1::2], cferm2=c2[0::2] + 1j * c2[1::2], itercg=it.value,
+                    aviter=av.value)
+
     def rranget(self):
         """rranget(seed, 1, 1, 1): the generator state written into checkpoints."""
         v = C.c_double(0)
