@@ -525,6 +525,43 @@ def run_trajectory(args):
     return {"workload": "RHMC 12^2x12 Ls16, 10 MD steps dt 0.05, remez2/4 + remez2g/4g", "results": out}
 
 
+def run_trajectory48(args):
+    """A sample of the config-5 run: 48^2 x 48, Ls = 48, beta 0.28, am 0.005,
+    imass 3, dt 0.02, remez2/remez4 (25 poles) for the action and remez2g/4g
+    (12 poles) for the guidance force, FP32 guidance solves (spmd), acceptance
+    residual 1e-9.  Two trajectories of 1 and 2 fixed MD steps give the cost of
+    one MD step and the fixed cost per trajectory (pseudofermion and momentum
+    refresh, the two Hamiltonians); the 50-step trajectory time is extrapolated
+    from them and labelled so."""
+    import thirring
+    gold = os.path.join(REPO, "tests", "golden") + os.sep
+    rat = thirring.remez_set(gold + "remez2", gold + "remez4", 25)
+    ratg = thirring.remez_set(gold + "remez2g", gold + "remez4g", 12)
+    lx, ls, beta, am, dt = 48, 48, 0.28, 0.005, 0.02
+    G = thirring.Lattice(lx, lx, lx, ls, beta=beta)
+    G.set_remez(rat, ratg)
+    G.set_residuals(1e-9, 1e-6, 1)
+    G.init_random(4139764973254.0)
+    rng = np.random.default_rng(5)
+    th = np.asfortranarray(rng.standard_normal((lx, lx, lx, 3)) / np.sqrt(beta), np.float32)
+    times, res = [], []
+    for nsteps in (1, 2):
+        G.md_counters(reset=True)
+        t0 = time.perf_counter()
+        r = G.trajectory(th, 50, dt, am, 3, fixed_steps=nsteps)
+        times.append(time.perf_counter() - t0)
+        res.append({"md_steps": nsteps, "s": round(times[-1], 2), "dH": r.dh, "accepted": r.accepted,
+                    "iterations": {k: v for k, v in G.md_counters().items() if v}})
+    step = times[1] - times[0]
+    fixed = times[0] - step
+    t50 = fixed + 50 * step
+    G.close()
+    return {"workload": "RHMC 48^2x48 Ls48 (config 5 shape), beta 0.28, am 0.005, dt 0.02; trajectories of 1 and 2 "
+                        "fixed MD steps", "results": res, "s_per_md_step": round(step, 3),
+            "s_fixed_per_traj": round(fixed, 2), "extrapolated_50_step_traj_s": round(t50, 1),
+            "extrapolated_traj_per_hr": round(3600 / t50, 2)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -533,7 +570,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="fp64", choices=["fp64", "sp", "mixed", "bf16"])
     ap.add_argument("--workload", default="multishift",
-                    choices=["multishift", "measurement", "packed", "trajectory", "dslash"],
+                    choices=["multishift", "measurement", "packed", "trajectory", "trajectory48", "dslash"],
                     help="secondary workloads print their own JSON line (not the headline contract)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-iters", type=int, default=6, help="multishift iterations in the CPU sample")
@@ -564,7 +601,8 @@ def main():
                                       f"{args.steps} launches each", "results": r}), flush=True)
         return
     if args.workload != "multishift":
-        fn = {"measurement": run_measurement, "packed": run_packed, "trajectory": run_trajectory}[args.workload]
+        fn = {"measurement": run_measurement, "packed": run_packed, "trajectory": run_trajectory,
+              "trajectory48": run_trajectory48}[args.workload]
         print(json.dumps(fn(args)), flush=True)
         return
 
