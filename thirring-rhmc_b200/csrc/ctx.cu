@@ -155,6 +155,10 @@ int thr_create(const thr_params* p, thr_ctx** out) {
   {
     const char* e = std::getenv("THR_REVERSE");
     if (e && e[0] == '0') c->rev_sweep = 0;
+    // THR_GRAPHS=0: solver loops launched from the host (profilers cannot look inside
+    // graphs with conditional nodes)
+    e = std::getenv("THR_GRAPHS");
+    if (e && e[0] == '0') c->use_graphs = false;
   }
   int rc = THR_OK;
   if (cudaSetDevice(c->dev) != cudaSuccess) rc = THR_ERR_CUDA;

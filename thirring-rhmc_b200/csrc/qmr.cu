@@ -1,5 +1,6 @@
 // qmr.cu -- qmrherm (qmrherm_module.F90:20-197), the multishift entry points
 // and derivs, on device fields, plus their C ABI wrappers.
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -252,7 +253,8 @@ int thr_qmrherm(thr_ctx* c, const double* Phi, double* x, float res, int* itercg
 int thr_set_solver(thr_ctx* c, int multishift_algo) {
   if (!c || multishift_algo < 0 || multishift_algo > 2) return THR_ERR_BADARG;
   c->ms_algo = multishift_algo == 0 ? 0 : 1;
-  c->use_graphs = multishift_algo == 1;
+  const char* e = std::getenv("THR_GRAPHS");
+  c->use_graphs = multishift_algo == 1 && !(e && e[0] == '0');
   return THR_OK;
 }
 
