@@ -227,3 +227,22 @@ def test_multishift_graph_equals_host_launched(sp, maxcg):
         assert np.array_equal(o, outs[0][0])
     if maxcg == 21:
         assert outs[0][1] == 21
+
+
+@pytest.mark.gpu
+def test_congrad_graph_equals_host_launched():
+    """congrad's chunk loop as a CUDA graph gives the bits of the host-launched loop."""
+    rng = np.random.default_rng(21)
+    L = O.lat(4, 4, 6, 8)
+    u = rand_links(L, rng, beta=2.0)
+    Phi = rand_spinor(L, rng)
+    outs = []
+    with thirring.Lattice(4, 4, 6, 8) as G:
+        G.set_links(u)
+        for algo in (1, 2, 1):
+            G.set_solver(algo)
+            X = O.spinor(L)
+            it, nx = G.congrad(Phi, X, 1e-9, 0.1, 3)
+            outs.append((it, nx, X))
+    for it, nx, X in outs[1:]:
+        assert (it, nx) == outs[0][:2] and np.array_equal(X, outs[0][2])
