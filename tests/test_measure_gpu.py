@@ -121,10 +121,12 @@ def test_meson_and_fermion_converged(kernel, imass):
         G.init_random(24680.0)
         ref = O.meson(L, g, u, 1e-8, 0.1, imass, nsource=3)
         got = G.meson(1e-8, 0.1, imass, nsource=3)
+        # both solutions meet congrad's absolute rule |r|^2 < 4 V Ls res^2; point and wall
+        # sources have |xi| ~ 1, so they agree to ~1e-6 relative of the largest entry
         assert abs(got["itercg"] - ref["itercg"]) <= 2
         for k in ("cpm", "cmm", "cpmn", "cmmn"):
-            np.testing.assert_allclose(got[k], ref[k], rtol=1e-6, atol=1e-10 * np.max(np.abs(ref[k])))
+            np.testing.assert_allclose(got[k], ref[k], rtol=1e-5, atol=1e-6 * np.max(np.abs(ref[k])))
         ref = O.fermion(L, g, u, 1e-8, 0.1, imass, nsource=3)
         got = G.fermion(1e-8, 0.1, imass, nsource=3)
         for k in ("cferm1", "cferm2"):
-            np.testing.assert_allclose(got[k], ref[k], rtol=1e-6, atol=1e-9 * np.max(np.abs(ref[k])))
+            np.testing.assert_allclose(got[k], ref[k], rtol=1e-5, atol=1e-6 * np.max(np.abs(ref[k])))
