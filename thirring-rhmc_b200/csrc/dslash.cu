@@ -346,6 +346,106 @@ __global__ void __launch_bounds__(NT, MINB)
   }
 }
 
+// FP32 storage, Shamir kernel, even Ls: one thread owns two consecutive s of a
+// site (s0 = 2 threadIdx.x and s0 + 1), so every spinor access is one 16-byte
+// load or store (float4) instead of two 8-byte ones; the arithmetic per element
+// is that of shamir_site.  blockDim = (Ls / 2, sites per block) with the sites
+// per block of the one-s kernel, so the grid -- and the partials of the
+// epilogues -- are the same; blocks have about 64 threads, 16 per SM.
+__device__ __forceinline__ void ld_pair(const float2* p, unsigned i, float2& a, float2& b) {
+  const float4 v = __ldg(reinterpret_cast<const float4*>(p + i));
+  a = make_float2(v.x, v.y);
+  b = make_float2(v.z, v.w);
+}
+template <bool DAG, int EPI, int MINB>
+__global__ void __launch_bounds__(64, MINB)
+    k_dslash_pair(float2* __restrict__ out, const float2* __restrict__ in, const float2* __restrict__ u, Geom g, float am,
+                  int imass, float am3, const int* skip, const float2* __restrict__ aux, const double* __restrict__ coef,
+                  double* __restrict__ partials, int rev) {
+  if (skip && *skip) return;
+  using C = float2;
+  using R = float;
+  const R om = EPI == 1 ? (R)(*coef) : R(0);
+  const int s0 = 2 * threadIdx.x;
+  const int bid = rev ? (int)gridDim.x - 1 - (int)blockIdx.x : (int)blockIdx.x;
+  const int site0 = bid * blockDim.y + threadIdx.y;
+  const bool live = site0 < g.v3;
+  double racc = 0.0;
+  if (live) {
+    const int site = site0;
+    int x, y, t;
+    site_coords(g, site, x, y, t);
+    const Nbr nb = neighbours(g, x, y, t);
+    SpinorView<float2> Rv{in, g};
+    const int Ls = g.ls;
+    const R diag = (R)((3.0f - am3) + 1.0f);
+    C c0[4], c1[4], a0c[4], a1c[4];
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+      ld_pair(in, sidx32(g, s0, site, d), c0[d], c1[d]);
+      a0c[d] = diag * c0[d];
+      a1c[d] = diag * c1[d];
+    }
+    const int A = DAG ? 0 : 2, B = DAG ? 2 : 0;  // spins taking R(s+1) / R(s-1)
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      a0c[A + k] = a0c[A + k] - c1[A + k];                                   // s0 + 1 = s1 < Ls
+      if (s0 + 1 < Ls - 1) a1c[A + k] = a1c[A + k] - Rv(s0 + 2, site, A + k);
+      if (s0 > 0) a0c[B + k] = a0c[B + k] - Rv(s0 - 1, site, B + k);
+      a1c[B + k] = a1c[B + k] - c0[B + k];                                   // s1 - 1 = s0
+    }
+    const R a = (R)am;
+    const bool five = imass == 5;
+    const C cA = imass == 1 ? mk(a, R(0)) : mk(R(0), (five && DAG) ? -a : a);
+    const C cB = imass == 1 ? mk(a, R(0)) : mk(R(0), five ? (DAG ? -a : a) : -a);
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      if (s0 + 1 == Ls - 1) a1c[A + k] = a1c[A + k] + cmul(cA, five ? c1[B + k] : Rv(0, site, A + k));
+      if (s0 == 0) a0c[B + k] = a0c[B + k] + cmul(cB, five ? c0[A + k] : Rv(Ls - 1, site, B + k));
+    }
+#pragma unroll
+    for (int mu = 0; mu < 3; mu++) {
+#pragma unroll
+      for (int dir = 0; dir < 2; dir++) {
+        const int ns = dir == 0 ? nb.f[mu] : nb.b[mu];
+        const C W = dir == 0 ? __ldg(u + (size_t)mu * g.v3 + site) : cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
+        C r0[4], r1[4];
+#pragma unroll
+        for (int d = 0; d < 4; d++) ld_pair(in, sidx32(g, s0, ns, d), r0[d], r1[d]);
+        hop_projected<C, R>(mu, (dir == 0) != DAG, W, r0, a0c);
+        hop_projected<C, R>(mu, (dir == 0) != DAG, W, r1, a1c);
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+      const unsigned i = sidx32(g, s0, site, d);
+      C v0 = a0c[d], v1 = a1c[d];
+      if (EPI == 1) {
+        C q0, q1;
+        ld_pair(aux, i, q0, q1);
+        v0 = q0 + om * v0;  // r = r + omega*s (multishift_module.F90:137)
+        v1 = q1 + om * v1;
+      }
+      *reinterpret_cast<float4*>(out + i) = make_float4(v0.x, v0.y, v1.x, v1.y);
+      if (EPI != 0) racc += epi_norm<float2>(v0) + epi_norm<float2>(v1);
+    }
+  }
+  if (EPI != 0) {
+    __shared__ double red[64];
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int nthr = blockDim.x * blockDim.y;
+    red[tid] = racc;
+    __syncthreads();
+    if (tid < 32) {
+      double v = 0.0;
+      for (int i = tid; i < nthr; i += 32) v += red[i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (tid == 0) partials[bid] = v;
+    }
+  }
+}
+
 // Batched stencil: a persistent grid walks the work blocks of all entries
 // (right-hand sides or lattices).  Work block wb belongs to the entry e with
 // blk0[e] <= wb < blk0[e+1]; inside it, thread tid handles s = tid % Ls of
@@ -476,9 +576,40 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
     if (dag) THR_E(K, true, N, SH, MB);            \
     else THR_E(K, false, N, SH, MB);               \
   } while (0)
+  // FP32 Shamir with even Ls: two s per thread (k_dslash_pair), same grid
+  const bool pair = storage_id<S>() == 1 && kernel == 0 && nt == 128 && g.ls % 2 == 0;
   // the register budget (resident blocks per SM) of the common configurations is
-  // tuned: Shamir 128-thread blocks {8, 7, 6}, Wilson 256-thread blocks {2, 1}
+  // tuned: Shamir 128-thread blocks {8, 7, 6} (pair kernel: 64-thread blocks {16, 14, 12}),
+  // Wilson 256-thread blocks {2, 1}
   auto launch = [&](int minb) {
+    if (pair) {
+      const dim3 pblk(g.ls / 2, blk.y, 1);
+      const float2* in2 = reinterpret_cast<const float2*>(in);
+      float2* out2 = reinterpret_cast<float2*>(out);
+      const float2* aux2 = reinterpret_cast<const float2*>(aux);
+      const float2* u2 = reinterpret_cast<const float2*>(u);
+#define THR_P(D, E, MB) \
+  k_dslash_pair<D, E, MB><<<grd, pblk, 0, st>>>(out2, in2, u2, g, am, imass, am3, skip, aux2, coef, partials, rev)
+#define THR_PE(D, MB)                    \
+  do {                                   \
+    if (e == 1) THR_P(D, 1, MB);         \
+    else if (e == 2) THR_P(D, 2, MB);    \
+    else THR_P(D, 0, MB);                \
+  } while (0)
+      const int mb = minb == 8 ? 16 : minb == 7 ? 14 : 12;
+      if (dag) {
+        if (mb == 16) THR_PE(true, 16);
+        else if (mb == 14) THR_PE(true, 14);
+        else THR_PE(true, 12);
+      } else {
+        if (mb == 16) THR_PE(false, 16);
+        else if (mb == 14) THR_PE(false, 14);
+        else THR_PE(false, 12);
+      }
+#undef THR_PE
+#undef THR_P
+      return;
+    }
     if (kernel == 1) {
       if (nt != 256) THR_D(1, 1024, false, 1);
       else if (minb == 2) THR_D(1, 256, false, 2);
