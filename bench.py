@@ -498,15 +498,18 @@ def run_packed(args):
 def run_trajectory(args):
     """RHMC trajectories on 12^2 x 12, Ls = 16 (beta 0.3, am 0.05, imass 3,
     10 MD steps of dt 0.05) with the reference's remez2/remez4 (25 poles) and
-    remez2g/remez4g (12 poles) files; guidance solves single precision (spmd)
-    or FP64."""
+    remez2g/remez4g (12 poles) files: guidance solves single precision (spmd)
+    or FP64 with the batched, graph-driven multishift, and the plain FP64 GPU
+    path (the reference's multishift loop structure, host-launched, FP64
+    guidance) for comparison."""
     import thirring
     gold = os.path.join(REPO, "tests", "golden") + os.sep
     rat = thirring.remez_set(gold + "remez2", gold + "remez4", 25)
     ratg = thirring.remez_set(gold + "remez2g", gold + "remez4g", 12)
     out = {}
-    for spmd in (1, 0):
+    for name, spmd, algo in (("spmd_fp32_guidance", 1, 1), ("fp64_guidance", 0, 1), ("plain_fp64_gpu", 0, 0)):
         G = thirring.Lattice(12, 12, 12, 16, beta=BETA)
+        G.set_solver(algo)
         G.set_remez(rat, ratg)
         G.set_residuals(1e-8, 1e-6, spmd)
         G.init_random(4139764973254.0)
@@ -522,9 +525,9 @@ def run_trajectory(args):
             dh.append(r.dh)
             acc += r.accepted
         dt = (time.perf_counter() - t0) / ntraj
-        out["spmd_fp32_guidance" if spmd else "fp64_guidance"] = {
-            "s_per_traj": round(dt, 3), "traj_per_hr": round(3600 / dt, 1), "dH": dh, "accepted": acc}
+        out[name] = {"s_per_traj": round(dt, 3), "traj_per_hr": round(3600 / dt, 1), "dH": dh, "accepted": acc}
         G.close()
+    out["speedup_vs_plain_fp64_gpu"] = round(out["plain_fp64_gpu"]["s_per_traj"] / out["spmd_fp32_guidance"]["s_per_traj"], 2)
     return {"workload": "RHMC 12^2x12 Ls16, 10 MD steps dt 0.05, remez2/4 + remez2g/4g", "results": out}
 
 
