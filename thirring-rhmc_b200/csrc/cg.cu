@@ -9,7 +9,6 @@
 #include <mutex>
 
 #include "ctx.h"
-#include "finish.cuh"
 #include "solver.h"
 #include "thr_reduce.cuh"
 
@@ -128,20 +127,16 @@ int cg_enqueue_chunk(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r
   const size_t n = c->n4();
   const unsigned gb = vec_grid(n);
   const unsigned gs = stencil_grid(c->g, c->p.kernel);
-  FinArgs fa_alpha, fa_beta;
-  fa_alpha.kind = FIN_CG_ALPHA;
-  fa_beta.kind = FIN_CG_BETA;
-  fa_alpha.state = fa_beta.state = cs;
-  fa_alpha.counter = fa_beta.counter = fin_counter(c);
-  (void)gs;
   for (int k = 0; k < kCgChunk; k++) {
-    // x1 = M p with alphad = |x1|^2 (:60, :70) from the stencil's epilogue, alpha in its last block
+    // x1 = M p with alphad = |x1|^2 (:60, :70) from the stencil's epilogue
     THR_TRY(launch_dslash_norm<double2>(c->g, c->p.kernel, false, x1, p, c->u64, am, imass, c->p.am3, c->st,
-                                        &cs->done, c->partials, &fa_alpha));
+                                        &cs->done, c->partials));
+    k_cg_alpha<<<1, 1024, 0, c->st>>>(cs, c->partials, gs);
     // x2 = M^dagger x1 is never stored: the epilogue forms r = r - alpha*x2 (:92) and
-    // betacgn = |r|^2 (:102); beta and the stopping rule (:102-120) in its last block
+    // betacgn = |r|^2 (:102)
     THR_TRY(launch_dslash_axpy<double2>(c->g, c->p.kernel, true, r, x1, c->u64, am, imass, c->p.am3, c->st, &cs->done,
-                                        r, &cs->nalpha, c->partials, c->rev_sweep, &fa_beta));
+                                        r, &cs->nalpha, c->partials, c->rev_sweep));
+    k_cg_beta<<<1, 1024, 0, c->st>>>(cs, c->partials, gs);
     k_cg_xp<<<gb, kThreads, 0, c->st>>>(cs, X, p, r, n);
     k_cg_latch<<<1, 1, 0, c->st>>>(cs);
   }
@@ -236,7 +231,6 @@ int congrad_dev(thr_ctx* c, const double2* Phi, double2* X, float res, float am,
   h.niterc = niterc;
   h.max_chunks = niterc / kCgChunk + 3;
   THR_CUDA(cudaMemcpyAsync(cs, &h, sizeof(CgState), cudaMemcpyHostToDevice, c->st));
-  THR_CUDA(cudaMemsetAsync(fin_counter(c), 0, sizeof(unsigned), c->st));
   THR_CUDA(cudaMemcpyAsync(p, X, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
   THR_CUDA(cudaMemcpyAsync(r, Phi, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
   if (c->use_graphs) {

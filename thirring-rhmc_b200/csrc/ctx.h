@@ -114,6 +114,3 @@ struct thr_ctx {
   int coef_dev(const float* theta_dev);                   // gauge.F90 coef on device theta
   int sync();
 };
-
-// the ticket counter of the stencil launches whose last block runs a solver's scalar step
-inline unsigned* fin_counter(thr_ctx* c) { return reinterpret_cast<unsigned*>(c->iscal + 640); }

@@ -27,7 +27,6 @@
 #include <string>
 
 #include "batch.h"
-#include "finish.cuh"
 #include "thr_common.cuh"
 #include "thr_kernels.h"
 
@@ -297,7 +296,7 @@ template <class S, int KER, bool DAG, int EPI, int NT, bool SHFL, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     k_dslash(S* __restrict__ out, const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u, Geom g, float am,
              int imass, float am3, const int* skip, const S* __restrict__ aux, const double* __restrict__ coef,
-             double* __restrict__ partials, int rev, FinArgs fa) {
+             double* __restrict__ partials, int rev) {
   if (skip && *skip) return;
   using C = typename Sto<S>::C;
   using R = typename Sto<S>::R;
@@ -344,10 +343,6 @@ __global__ void __launch_bounds__(NT, MINB)
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
       if (tid == 0) partials[bid] = v;
     }
-    if (fa.kind != FIN_NONE) {
-      __syncthreads();  // red is reused by the finisher
-      block_finish(fa, partials, (int)gridDim.x, red, tid, nthr);
-    }
   }
 }
 
@@ -366,7 +361,7 @@ template <bool DAG, int EPI, int MINB>
 __global__ void __launch_bounds__(64, MINB)
     k_dslash_pair(float2* __restrict__ out, const float2* __restrict__ in, const float2* __restrict__ u, Geom g, float am,
                   int imass, float am3, const int* skip, const float2* __restrict__ aux, const double* __restrict__ coef,
-                  double* __restrict__ partials, int rev, FinArgs fa) {
+                  double* __restrict__ partials, int rev) {
   if (skip && *skip) return;
   using C = float2;
   using R = float;
@@ -447,10 +442,6 @@ __global__ void __launch_bounds__(64, MINB)
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
       if (tid == 0) partials[bid] = v;
-    }
-    if (fa.kind != FIN_NONE) {
-      __syncthreads();  // red is reused by the finisher
-      block_finish(fa, partials, (int)gridDim.x, red, tid, nthr);
     }
   }
 }
@@ -564,7 +555,7 @@ template <class S> constexpr int storage_id() { return sizeof(S) == sizeof(doubl
 template <class S>
 int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
                        int imass, float am3, cudaStream_t st, const int* skip, const S* aux, const double* coef,
-                       double* partials, int e, int rev, FinArgs fa = FinArgs()) {
+                       double* partials, int e, int rev) {
   if (g.ls > 1024) return THR_ERR_BADSHAPE;
   if (4ULL * (unsigned long long)g.v5 >= (1ULL << 32)) return THR_ERR_BADSHAPE;  // 32-bit element offsets
   if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
@@ -573,8 +564,7 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   const int nt = stencil_threads(g, kernel);
   const bool shfl = stencil_shfl(g, kernel);
 #define THR_L(K, D, E, N, SH, MB) \
-  k_dslash<S, K, D, E, N, SH, MB><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, coef, partials, rev, \
-                                                       fa)
+  k_dslash<S, K, D, E, N, SH, MB><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, coef, partials, rev)
 #define THR_E(K, D, N, SH, MB)                 \
   do {                                         \
     if (e == 1) THR_L(K, D, 1, N, SH, MB);     \
@@ -591,10 +581,7 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   // the register budget (resident blocks per SM) of the common configurations is
   // tuned: Shamir 128-thread blocks {8, 7, 6} (pair kernel: 64-thread blocks {16, 14, 12}),
   // Wilson 256-thread blocks {2, 1}
-  // tuning launches run without the finisher (it advances solver state); the real one with it
-  const FinArgs fa_real = fa;
-  auto launch = [&](int minb, bool real) {
-    const FinArgs fa = real ? fa_real : FinArgs();
+  auto launch = [&](int minb) {
     if (pair) {
       const dim3 pblk(g.ls / 2, blk.y, 1);
       const float2* in2 = reinterpret_cast<const float2*>(in);
@@ -602,7 +589,7 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
       const float2* aux2 = reinterpret_cast<const float2*>(aux);
       const float2* u2 = reinterpret_cast<const float2*>(u);
 #define THR_P(D, E, MB) \
-  k_dslash_pair<D, E, MB><<<grd, pblk, 0, st>>>(out2, in2, u2, g, am, imass, am3, skip, aux2, coef, partials, rev, fa)
+  k_dslash_pair<D, E, MB><<<grd, pblk, 0, st>>>(out2, in2, u2, g, am, imass, am3, skip, aux2, coef, partials, rev)
 #define THR_PE(D, MB)                    \
   do {                                   \
     if (e == 1) THR_P(D, 1, MB);         \
@@ -662,9 +649,9 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
       if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
         float best = 1e30f;
         for (int c = 0; c < ncand; c++) {
-          launch(cand[c], false);
+          launch(cand[c]);
           cudaEventRecord(e0, st);
-          for (int r = 0; r < 3; r++) launch(cand[c], false);
+          for (int r = 0; r < 3; r++) launch(cand[c]);
           cudaEventRecord(e1, st);
           cudaEventSynchronize(e1);
           float ms = 0.f;
@@ -683,7 +670,7 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
       }
     }
   }
-  launch(minb, true);
+  launch(minb);
 #undef THR_D
 #undef THR_E
 #undef THR_L
@@ -693,17 +680,15 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
 template <class S>
 int launch_dslash_axpy(const Geom& g, int kernel, bool dag, S* rnew, const S* in, const typename Sto<S>::C* u,
                        float am, int imass, float am3, cudaStream_t st, const int* skip, const S* rold,
-                       const double* coef, double* partials, int rev, const FinArgs* fin) {
-  return launch_dslash_mode<S>(g, kernel, dag, rnew, in, u, am, imass, am3, st, skip, rold, coef, partials, 1, rev,
-                               fin ? *fin : FinArgs());
+                       const double* coef, double* partials, int rev) {
+  return launch_dslash_mode<S>(g, kernel, dag, rnew, in, u, am, imass, am3, st, skip, rold, coef, partials, 1, rev);
 }
 
 template <class S>
 int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
-                       float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials,
-                       const FinArgs* fin) {
+                       float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials) {
   return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr, partials, 2,
-                               0, fin ? *fin : FinArgs());
+                               0);
 }
 
 template <class S>
@@ -738,10 +723,9 @@ int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const
   template int launch_dslash<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float, cudaStream_t,   \
                                 const int*);                                                                      \
   template int launch_dslash_axpy<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
-                                     cudaStream_t, const int*, const S*, const double*, double*, int,             \
-                                     const FinArgs*);                                                              \
+                                     cudaStream_t, const int*, const S*, const double*, double*, int);            \
   template int launch_dslash_norm<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
-                                     cudaStream_t, const int*, double*, const FinArgs*);                          \
+                                     cudaStream_t, const int*, double*);                                          \
   template int launch_dslash_batch<S>(const BatchTable&, int, bool, S*, const S*, const L*, float, int, float,    \
                                       cudaStream_t, const int*, const S*, double*, int);
 THR_INST(double2, double2)

@@ -19,7 +19,6 @@
 #include <cstring>
 
 #include "ctx.h"
-#include "finish.cuh"
 #include "ms.h"
 #include "solver.h"
 #include "thr_reduce.cuh"
@@ -245,29 +244,21 @@ int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* 
   // algorithmic bytes: M reads p, writes h, reads the links (|M p|^2 comes from
   // registers); the M^dagger launch reads h, the links and r_old and writes r_new
   const double b_m = 2.0 * n * sizeof(V) + 3.0 * c->g.v3 * lb, b_md = b_m + (double)n * sizeof(V);
-  // the scalar steps run in the last block of the stencil launch that produces their sum
-  FinArgs fa_alpha, fa_lambda;
-  fa_alpha.kind = FIN_MS_ALPHA;
-  fa_lambda.kind = FIN_MS_LAMBDA;
-  fa_alpha.state = fa_lambda.state = ms;
-  fa_alpha.hist = fa_lambda.hist = hist;
-  fa_alpha.counter = fa_lambda.counter = fin_counter(c);
-  (void)gs;
   for (int j = 0; j < kBatch; j++) {
     V* rold = ring + (size_t)j * n;
     V* rnew = ring + (size_t)(j + 1) * n;
-    // alpha = Re<p, M^dagger M p> (:104) evaluated as |M p|^2 in the M epilogue; the
-    // alpha step (:118-135) in its last block
+    // alpha = Re<p, M^dagger M p> (:104) evaluated as |M p|^2 in the M epilogue
     int pe = prof ? c->prof_begin(thr_ctx::P_DSLASH, b_m, k0 + j) : -1;
     THR_TRY(launch_dslash_norm<V>(c->g, c->p.kernel, false, hv, p, u, am, imass, c->p.am3, c->st, &ms->done,
-                                  c->partials, &fa_alpha));
+                                  c->partials));
     c->prof_end(pe);
-    // s = M^dagger h is never stored: the epilogue forms r = r + omega*s (:137) and |r|^2
-    // (:138); the lambda step and the convergence test (:143-150, :240-258) in its last block
+    k_alpha<<<1, 1024, 0, c->st>>>(ms, hist, c->partials, gs);
+    // s = M^dagger h is never stored: the epilogue forms r = r + omega*s (:137) and |r|^2 (:138)
     pe = prof ? c->prof_begin(thr_ctx::P_DSLASH_DAG, b_md, k0 + j) : -1;
     THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, rnew, hv, u, am, imass, c->p.am3, c->st, &ms->done, rold,
-                                  &ms->omega, c->partials, c->rev_sweep, &fa_lambda));
+                                  &ms->omega, c->partials, c->rev_sweep));
     c->prof_end(pe);
+    k_lambda<<<1, 1024, 0, c->st>>>(ms, hist, c->partials, gs);
     k_pupdate<V><<<gb, kThreads, 0, c->st>>>(ms, p, rnew, n);
   }
   (void)s;
@@ -387,7 +378,6 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
   h->batches = 0;
   h->max_batches = (maxcg > 0 ? maxcg : 0) / kBatch + 3;
   THR_CUDA(cudaMemcpyAsync(ms, h, sizeof(MsState), cudaMemcpyHostToDevice, c->st));
-  THR_CUDA(cudaMemsetAsync(fin_counter(c), 0, sizeof(unsigned), c->st));
   THR_CUDA(cudaMemcpyAsync(ring, in, n * sizeof(V), cudaMemcpyDeviceToDevice, c->st));  // r = input (slot 0)
   THR_CUDA(cudaMemcpyAsync(p, in, n * sizeof(V), cudaMemcpyDeviceToDevice, c->st));     // p = r
   const unsigned gb = vec_grid(n);

@@ -18,18 +18,14 @@ int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, cons
 // rnew = rold + (*coef) * (M or M^dagger) in, without storing the stencil's output,
 // and one FP64 partial per block of |rnew|^2.  rev != 0: blocks take the sites from
 // the top down (same results; better L2 reuse of a field written just before)
-// fin: optional scalar step run by the launch's last block on the sum of the partials
-// (finish.cuh); the partials are still written
-struct FinArgs;
 template <class S>
 int launch_dslash_axpy(const Geom& g, int kernel, bool dag, S* rnew, const S* in, const typename Sto<S>::C* u,
                        float am, int imass, float am3, cudaStream_t st, const int* skip, const S* rold,
-                       const double* coef, double* partials, int rev = 0, const FinArgs* fin = nullptr);
+                       const double* coef, double* partials, int rev = 0);
 // same, with one FP64 partial per block of sum |out|^2
 template <class S>
 int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
-                       float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials,
-                       const FinArgs* fin = nullptr);
+                       float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials);
 
 // layout.cu: Fortran halo'd host layout <-> device fields
 // spinor (0:Ls+1,0:Lx+1,0:Ly+1,0:Lt+1,4) complex(dp)  <-> S[4][V3][Ls]
