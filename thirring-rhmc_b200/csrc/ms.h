@@ -75,7 +75,7 @@ __device__ __forceinline__ void ms_converge_step(MsState* ms) {
 
 // Batched variant: per-iteration coefficients of the shift update, applied
 // every kBatch iterations in one pass over the shift fields.
-constexpr int kBatch = 16;
+constexpr int kBatch = 32;
 struct MsHist {
   int nsteps;
   int lo[kBatch], hi[kBatch];

@@ -150,14 +150,19 @@ __global__ void k_flush_coef(MsState* ms, const MsHist* hist, MsCoef* cf) {
 
 // apply the folded maps to every shift field of the batch's window
 // (ring slot j+1 holds the residual of the batch's step j; the last one is copied
-// to slot 0, where the next batch starts)
+// to slot 0, where the next batch starts).  One thread per element holds the
+// batch's residuals in registers (kBatch values) and walks the window; the next
+// shift's two fields are loaded while the current one is combined.
+constexpr int kFlushThreads = 128;
+constexpr int kFlushBlocks = 3;  // resident per SM at the register budget of kBatch residuals
 template <class V>
-__global__ void __launch_bounds__(kThreads) k_flush(const MsCoef* cf, V* __restrict__ out, V* __restrict__ sf,
-                                                   V* __restrict__ ring, size_t n, size_t stride) {
+__global__ void __launch_bounds__(kFlushThreads, kFlushBlocks)
+    k_flush(const MsCoef* cf, V* __restrict__ out, V* __restrict__ sf, V* __restrict__ ring, size_t n,
+            size_t stride) {
   using R = typename W<V>::R;
   const int ns = cf->ns;
   if (ns == 0) return;
-  const int lo = cf->lo, hi = cf->hi;
+  const int lo = cf->lo, hi = cf->hi;  // lo > hi: no shift active in the batch (only the ring carry)
   __shared__ R s_A[kMaxShift], s_P[kMaxShift], s_B[kMaxShift][kBatch], s_Q[kMaxShift][kBatch];
   for (int t = threadIdx.x; t < kMaxShift * kBatch; t += blockDim.x) {
     const int k = t / kBatch, i = t % kBatch;
@@ -175,9 +180,17 @@ __global__ void __launch_bounds__(kThreads) k_flush(const MsCoef* cf, V* __restr
     for (int j = 0; j < kBatch; j++)
       if (j < ns) rj[j] = ring[(size_t)(1 + j) * n + i];
     ring[i] = ring[(size_t)ns * n + i];  // the next batch starts from the last residual (just read: cached)
+    V f0n, o0n;
+    if (lo <= hi) {
+      f0n = sf[lo * stride + i];
+      o0n = out[lo * stride + i];
+    }
     for (int k = lo; k <= hi; k++) {
-      const V f0 = sf[k * stride + i];
-      const V o0 = out[k * stride + i];
+      const V f0 = f0n, o0 = o0n;
+      if (k < hi) {
+        f0n = sf[(k + 1) * stride + i];
+        o0n = out[(k + 1) * stride + i];
+      }
       V f = s_A[k] * f0;
       V o = o0 - s_P[k] * f0;
 #pragma unroll
@@ -191,6 +204,11 @@ __global__ void __launch_bounds__(kThreads) k_flush(const MsCoef* cf, V* __restr
       out[k * stride + i] = o;
     }
   }
+}
+inline unsigned flush_grid(size_t n) {
+  size_t b = (n + kFlushThreads - 1) / kFlushThreads;
+  if (b > 148 * kFlushBlocks) b = 148 * kFlushBlocks;
+  return (unsigned)(b ? b : 1);
 }
 // close a batch
 __global__ void k_reset(MsHist* hist, MsState* ms) {
@@ -264,7 +282,7 @@ int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* 
   (void)s;
   const int pe = prof ? c->prof_begin(thr_ctx::P_SHIFTUPD, 0.0, k0) : -1;
   k_flush_coef<<<1, kMaxShift, 0, c->st>>>(ms, hist, cf);
-  k_flush<V><<<gb, kThreads, 0, c->st>>>(cf, out, sf, ring, n, n);
+  k_flush<V><<<flush_grid(n), kFlushThreads, 0, c->st>>>(cf, out, sf, ring, n, n);
   c->prof_end(pe);
   if (prof_flush) *prof_flush = pe;
   k_reset<<<1, 1, 0, c->st>>>(hist, ms);
