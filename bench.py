@@ -248,11 +248,14 @@ def run_ours(args, rank, world, local_rank):
         tot = C.c_double(0)
         L.thr_profile_read(h, kind, C.byref(n), C.byref(t), C.byref(b), C.byref(tot))
         prof[name] = dict(sampled=n.value, ms=t.value, bytes=b.value, launches=tot.value)
-    # the batched solver enqueues batches of 32 iterations of 5 kernels (M with |Mp|^2,
-    # alpha, M^dagger with the residual update, lambda, p update) plus 4 per batch (flush
-    # coefficients, flush, history reset, loop control); 3 set-up kernels and the pole
-    # sum per solve
-    launches = int(sum(3 + ((i + 31) // 32) * (32 * 5 + 4) + 1 for i in its))
+    # the batched solver's graph runs batches in pairs: a batch is 32 iterations of 5
+    # kernels (M with |Mp|^2, alpha, M^dagger with the residual update, lambda, p update)
+    # plus the previous batch's flush (coefficients, flush, history reset), a pair ends in
+    # the loop control; per solve 3 set-up kernels, the last batch's flush and the pole sum
+    def batch_launches(i):
+        pairs = (i + 63) // 64
+        return 3 + pairs * (2 * (32 * 5 + 3) + 1) + 3 + 1
+    launches = int(sum(batch_launches(i) for i in its))
 
     # ---- plain FP64 GPU path for comparison: FP64 everywhere and the reference's
     # loop structure (every shift field updated in every iteration)

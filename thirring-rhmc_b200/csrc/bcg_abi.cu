@@ -73,13 +73,7 @@ struct thr_pack {
 
 namespace {
 Geom geom_of(const thr_params& p) {
-  Geom g;
-  g.lx = p.lx; g.ly = p.ly; g.lt = p.lt; g.ls = p.ls;
-  g.v3 = p.lx * p.ly * p.lt;
-  g.v5 = (long long)g.v3 * p.ls;
-  g.layout = p.layout;
-  g.hv3 = g.v3 / 2;
-  return g;
+  return geom_make(p.lx, p.ly, p.lt, p.ls, p.layout);
 }
 size_t nf5_of(const Geom& g) { return (size_t)(g.ls + 2) * (g.lx + 2) * (g.ly + 2) * (g.lt + 2) * 4; }
 

@@ -86,14 +86,21 @@ __global__ void k_cg_beta(CgState* cs, const double* partials, int np) {
 }
 
 // x = x + alpha*p (:77, skipped at nx == 1); p = r + betacg*p (:119); then latch done
-__global__ void k_cg_xp(CgState* cs, double2* x, double2* p, const double2* r, size_t n) {
+// in site order: a thread takes the four spin planes of one (s, site) element of
+// the plane (np = n / 4 elements); rev: from the top site down
+__global__ void k_cg_xp(CgState* cs, double2* x, double2* p, const double2* r, size_t np, int rev) {
   if (cs->done) return;
   const double alpha = cs->alpha, beta = cs->betacg;
   const bool upd = cs->nx != 1;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    double2 pv = p[i];
-    if (upd) x[i] = x[i] + alpha * pv;
-    p[i] = r[i] + beta * pv;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < np; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t i0 = rev ? np - 1 - e : e;
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+      const size_t i = i0 + d * np;
+      const double2 pv = p[i];
+      if (upd) x[i] = x[i] + alpha * pv;
+      p[i] = r[i] + beta * pv;
+    }
   }
 }
 __global__ void k_cg_latch(CgState* cs) {
@@ -125,19 +132,23 @@ constexpr int kCgChunk = 8;
 int cg_enqueue_chunk(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r, double2* x1, double2* x2, float am,
                      int imass) {
   const size_t n = c->n4();
-  const unsigned gb = vec_grid(n);
+  const unsigned gb = vec_grid(n / 4);
   const unsigned gs = stencil_grid(c->g, c->p.kernel);
   for (int k = 0; k < kCgChunk; k++) {
+    // sweep directions alternate with the iteration's parity (kCgChunk is even): each
+    // kernel starts on the sites its predecessor wrote last (results do not depend on it)
+    const int odd = c->rev_sweep == 2 ? (k & 1) : 0;
+    const int rev_m = odd, rev_md = c->rev_sweep ? 1 - odd : 0, rev_p = odd;
     // x1 = M p with alphad = |x1|^2 (:60, :70) from the stencil's epilogue
     THR_TRY(launch_dslash_norm<double2>(c->g, c->p.kernel, false, x1, p, c->u64, am, imass, c->p.am3, c->st,
-                                        &cs->done, c->partials));
+                                        &cs->done, c->partials, rev_m));
     k_cg_alpha<<<1, 1024, 0, c->st>>>(cs, c->partials, gs);
     // x2 = M^dagger x1 is never stored: the epilogue forms r = r - alpha*x2 (:92) and
     // betacgn = |r|^2 (:102)
     THR_TRY(launch_dslash_axpy<double2>(c->g, c->p.kernel, true, r, x1, c->u64, am, imass, c->p.am3, c->st, &cs->done,
-                                        r, &cs->nalpha, c->partials, c->rev_sweep));
+                                        r, &cs->nalpha, c->partials, rev_md));
     k_cg_beta<<<1, 1024, 0, c->st>>>(cs, c->partials, gs);
-    k_cg_xp<<<gb, kThreads, 0, c->st>>>(cs, X, p, r, n);
+    k_cg_xp<<<gb, kThreads, 0, c->st>>>(cs, X, p, r, n / 4, rev_p);
     k_cg_latch<<<1, 1, 0, c->st>>>(cs);
   }
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
@@ -176,7 +187,7 @@ int cg_graph(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r, double
   THR_TRY(launch_dslash_norm<double2>(c->g, c->p.kernel, false, x1, p, c->u64, am, imass, c->p.am3, c->st, &cs->done,
                                       c->partials));
   THR_TRY(launch_dslash_axpy<double2>(c->g, c->p.kernel, true, x2, x1, c->u64, am, imass, c->p.am3, c->st, &cs->done,
-                                      x2, &cs->nalpha, c->partials, c->rev_sweep));
+                                      x2, &cs->nalpha, c->partials, c->rev_sweep ? 1 : 0));
   THR_CUDA(cudaGraphCreate(&G.graph, 0));
   cudaGraphConditionalHandle handle;
   THR_CUDA(cudaGraphConditionalHandleCreate(&handle, G.graph, 1, cudaGraphCondAssignDefault));
@@ -299,12 +310,7 @@ extern "C" int thr_congrad_static(const thr_params* prm, const void* u, const vo
   if (prm->kernel != 0 && prm->kernel != 1) return THR_ERR_BADARG;
   if (prm->lx < 2 || prm->ly < 2 || prm->lt < 2 || prm->ls < 1 || prm->ls > 1024) return THR_ERR_BADSHAPE;
   if (prm->layout == 1 && prm->lx % 2 != 0) return THR_ERR_BADSHAPE;
-  Geom g;
-  g.lx = prm->lx; g.ly = prm->ly; g.lt = prm->lt; g.ls = prm->ls;
-  g.v3 = prm->lx * prm->ly * prm->lt;
-  g.v5 = (long long)g.v3 * prm->ls;
-  g.layout = prm->layout;
-  g.hv3 = g.v3 / 2;
+  const Geom g = geom_make(prm->lx, prm->ly, prm->lt, prm->ls, prm->layout);
   const size_t n = (size_t)g.v5 * 4;
   const unsigned gb = vec_grid(n);
   // scratch layout: state | partials | p | r | x1 | x2
@@ -344,7 +350,7 @@ extern "C" int thr_congrad_static(const thr_params* prm, const void* u, const vo
       THR_TRY(launch_dslash<double2>(g, prm->kernel, true, x2, x1, ud, am, imass, prm->am3, st, &cs->done));
       k_cg_rupdate<<<gb, kThreads, 0, st>>>(cs, r, x2, n, partials);
       k_cg_beta<<<1, 1024, 0, st>>>(cs, partials, gb);
-      k_cg_xp<<<gb, kThreads, 0, st>>>(cs, Xd, p, r, n);
+      k_cg_xp<<<vec_grid(n / 4), kThreads, 0, st>>>(cs, Xd, p, r, n / 4, 0);
       k_cg_latch<<<1, 1, 0, st>>>(cs);
     }
     THR_CUDA(cudaMemcpyAsync(&h, cs, sizeof(CgState), cudaMemcpyDeviceToHost, st));

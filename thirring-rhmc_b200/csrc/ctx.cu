@@ -36,7 +36,7 @@ int thr_ctx::buffer(int id, size_t bytes, void** out) {
   return THR_OK;
 }
 
-int thr_ctx::prof_begin(int kind, double bytes, long long tag) {
+int thr_ctx::prof_begin(int kind, double bytes, long long tag, cudaStream_t on) {
   if (!prof_on) return -1;
   if (prof_seen[kind]++ % prof_stride) return -1;
   const int idx = (int)prof_kind.size();
@@ -50,11 +50,11 @@ int thr_ctx::prof_begin(int kind, double bytes, long long tag) {
   prof_kind.push_back(kind);
   prof_bytes.push_back(bytes);
   prof_tag.push_back(tag);
-  cudaEventRecord(prof_ev[2 * idx], st);
+  cudaEventRecord(prof_ev[2 * idx], on ? on : st);
   return idx;
 }
-void thr_ctx::prof_end(int idx) {
-  if (idx >= 0) cudaEventRecord(prof_ev[2 * idx + 1], st);
+void thr_ctx::prof_end(int idx, cudaStream_t on) {
+  if (idx >= 0) cudaEventRecord(prof_ev[2 * idx + 1], on ? on : st);
 }
 void thr_ctx::prof_set_bytes(int idx, double bytes) {
   if (idx >= 0 && idx < (int)prof_bytes.size()) prof_bytes[idx] = bytes;
@@ -146,15 +146,13 @@ int thr_create(const thr_params* p, thr_ctx** out) {
   thr_ctx* c = new thr_ctx();
   c->p = *p;
   if (c->p.ndiag <= 0) c->p.ndiag = 25;
-  c->g.lx = p->lx; c->g.ly = p->ly; c->g.lt = p->lt; c->g.ls = p->ls;
-  c->g.v3 = p->lx * p->ly * p->lt;
-  c->g.v5 = (long long)c->g.v3 * p->ls;
-  c->g.layout = p->layout;
-  c->g.hv3 = c->g.v3 / 2;
+  c->g = thr::geom_make(p->lx, p->ly, p->lt, p->ls, p->layout);
   c->dev = p->device;
   {
     const char* e = std::getenv("THR_REVERSE");
-    if (e && e[0] == '0') c->rev_sweep = 0;
+    if (e && (e[0] == '0' || e[0] == '1')) c->rev_sweep = e[0] - '0';
+    e = std::getenv("THR_OVERLAP");
+    if (e && e[0] == '0') c->overlap_flush = 0;
     // THR_GRAPHS=0: solver loops launched from the host (profilers cannot look inside
     // graphs with conditional nodes)
     e = std::getenv("THR_GRAPHS");
@@ -162,8 +160,15 @@ int thr_create(const thr_params* p, thr_ctx** out) {
   }
   int rc = THR_OK;
   if (cudaSetDevice(c->dev) != cudaSuccess) rc = THR_ERR_CUDA;
-  if (!rc && cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) rc = THR_ERR_CUDA;
+  int prio_lo = 0, prio_hi = 0;  // numerically: lo >= hi
+  if (!rc && cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess) rc = THR_ERR_CUDA;
+  if (!rc && cudaStreamCreateWithPriority(&c->st, cudaStreamNonBlocking, prio_hi) != cudaSuccess) rc = THR_ERR_CUDA;
+  if (!rc && cudaStreamCreateWithPriority(&c->st2, cudaStreamNonBlocking, prio_lo) != cudaSuccess) rc = THR_ERR_CUDA;
   if (!rc && (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)) rc = THR_ERR_CUDA;
+  for (int i = 0; i < 2 && !rc; i++)
+    if (cudaEventCreateWithFlags(&c->ev_fork[i], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join[i], cudaEventDisableTiming) != cudaSuccess)
+      rc = THR_ERR_CUDA;
   if (!rc && cudaMalloc(&c->u64, (size_t)c->g.v3 * 3 * sizeof(double2)) != cudaSuccess) rc = THR_ERR_NOMEM;
   if (!rc && cudaMalloc(&c->u32, (size_t)c->g.v3 * 3 * sizeof(float2)) != cudaSuccess) rc = THR_ERR_NOMEM;
   c->stage_elems = c->nf5();
@@ -189,6 +194,7 @@ int thr_destroy(thr_ctx* c) {
   if (!c) return THR_OK;
   cudaSetDevice(c->dev);
   if (c->st) cudaStreamSynchronize(c->st);
+  if (c->st2) cudaStreamSynchronize(c->st2);
   ms_graphs_release(c);
   cg_graph_release(c);
   for (auto p : c->w64) cudaFree(p);
@@ -206,6 +212,11 @@ int thr_destroy(thr_ctx* c) {
   if (c->hiscal) cudaFreeHost(c->hiscal);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
+  for (int i = 0; i < 2; i++) {
+    if (c->ev_fork[i]) cudaEventDestroy(c->ev_fork[i]);
+    if (c->ev_join[i]) cudaEventDestroy(c->ev_join[i]);
+  }
+  if (c->st2) cudaStreamDestroy(c->st2);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return THR_OK;

@@ -25,7 +25,11 @@ struct thr_ctx {
   thr::Geom g;
   int dev = 0;
   cudaStream_t st = nullptr;
+  // side stream (lowest priority; st has the highest) for work that overlaps the
+  // solver's main chain: the batched multishift's shift-field flushes
+  cudaStream_t st2 = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_fork[2] = {}, ev_join[2] = {};  // fork / join of st2 work, one pair per ring half
 
   // current links (trial::u) in FP64 and FP32
   double2* u64 = nullptr;
@@ -78,7 +82,11 @@ struct thr_ctx {
   bool use_graphs = true;   // batched solver loops as one CUDA graph (WHILE node) per solve
   void* ms_graphs[2] = {};  // cached batched-multishift graphs (FP64, FP32 vectors)
   void* cg_graph = nullptr;  // cached congrad graph
-  int rev_sweep = 1;         // M^dagger-with-update stencil walks the sites top down (THR_REVERSE=0: bottom up)
+  // sweep directions of the solver kernels (THR_REVERSE=0|1|2): 0 all bottom up; 1 the
+  // M^dagger-with-update stencil top down; 2 (default) directions alternate per iteration
+  // so each kernel starts on the sites its predecessor wrote last
+  int rev_sweep = 2;
+  int overlap_flush = 1;     // batched multishift flushes on the side stream (THR_OVERLAP=0: in line)
   double md_counts[8] = {};  // ancg, ancgpv, ancgf, ancgfpv, ancgh, ancghpv, ancgpf, ancgpfpv
   void* bufs[B_COUNT] = {};
   size_t buf_bytes[B_COUNT] = {};
@@ -97,8 +105,9 @@ struct thr_ctx {
   std::vector<int> prof_kind;                // -1: dropped (a launch that skipped its work)
   std::vector<double> prof_bytes;            // algorithmic bytes of the sampled launch
   std::vector<long long> prof_tag;           // iteration of the sampled launch within its solve
-  int prof_begin(int kind, double bytes, long long tag = -1);  // returns pair index or -1
-  void prof_end(int idx);
+  // events go on stream `on` (nullptr: st)
+  int prof_begin(int kind, double bytes, long long tag = -1, cudaStream_t on = nullptr);  // pair index or -1
+  void prof_end(int idx, cudaStream_t on = nullptr);
   void prof_set_bytes(int idx, double bytes);
   // drop the sampled launches since entry `first` whose tag is >= iters (skipped work)
   void prof_trim(size_t first, long long iters);

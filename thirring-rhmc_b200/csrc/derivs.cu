@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(256) k_derivs(double* __restrict__ dS, const d
   const int site = warp;
   int x, y, t;
   site_coords(g, site, x, y, t);
-  const Nbr nb = neighbours(g, x, y, t);
+  const Nbr nb = neighbours(g, site, x, y, t);
   const double sg = (iflag == 0) ? 1.0 : -1.0;
   double accm[3] = {0.0, 0.0, 0.0};
   const int Ls = g.ls;

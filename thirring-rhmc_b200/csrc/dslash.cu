@@ -112,7 +112,7 @@ __device__ __forceinline__ void shamir_site(const S* __restrict__ in, const type
   using C = typename Sto<S>::C;
   int x, y, t;
   site_coords(g, site, x, y, t);
-  const Nbr nb = neighbours(g, x, y, t);
+  const Nbr nb = neighbours(g, site, x, y, t);
   SpinorView<S> Rv{in, g};
   const int Ls = g.ls;
   const R diag = (R)((3.0f - am3) + 1.0f);  // dirac.F90:45, default real
@@ -208,7 +208,7 @@ __device__ __forceinline__ void wilson_site(const S* __restrict__ in, const type
   using C = typename Sto<S>::C;
   int x, y, t;
   site_coords(g, site, x, y, t);
-  const Nbr nb = neighbours(g, x, y, t);
+  const Nbr nb = neighbours(g, site, x, y, t);
   SpinorView<S> Rv{in, g};
   const int Ls = g.ls;
   const R a = (R)am;
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(64, MINB)
     const int site = site0;
     int x, y, t;
     site_coords(g, site, x, y, t);
-    const Nbr nb = neighbours(g, x, y, t);
+    const Nbr nb = neighbours(g, site, x, y, t);
     SpinorView<float2> Rv{in, g};
     const int Ls = g.ls;
     const R diag = (R)((3.0f - am3) + 1.0f);
@@ -686,9 +686,9 @@ int launch_dslash_axpy(const Geom& g, int kernel, bool dag, S* rnew, const S* in
 
 template <class S>
 int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
-                       float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials) {
+                       float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials, int rev) {
   return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr, partials, 2,
-                               0);
+                               rev);
 }
 
 template <class S>
@@ -725,7 +725,7 @@ int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const
   template int launch_dslash_axpy<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
                                      cudaStream_t, const int*, const S*, const double*, double*, int);            \
   template int launch_dslash_norm<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
-                                     cudaStream_t, const int*, double*);                                          \
+                                     cudaStream_t, const int*, double*, int);                                     \
   template int launch_dslash_batch<S>(const BatchTable&, int, bool, S*, const S*, const L*, float, int, float,    \
                                       cudaStream_t, const int*, const S*, double*, int);
 THR_INST(double2, double2)

@@ -83,7 +83,7 @@ __device__ __forceinline__ double2 wall_value(const double2* __restrict__ X, con
   };
   int x, y, t;
   site_coords(g, site, x, y, t);
-  const Nbr nb = neighbours(g, x, y, t);
+  const Nbr nb = neighbours(g, site, x, y, t);
   const int d = m.d_c;
   double2 out = dgw * is(site, d);  // DWilson: Phi = diag * R (dirac.F90:191-192)
 #pragma unroll

@@ -4,17 +4,21 @@
 // vectors), reorganised for HBM traffic.  The reference updates every
 // active shift field in every iteration (4 passes per shift per iteration,
 // :155-176).  Here each iteration only writes its new residual r_k into a
-// ring of kBatch+1 fields and records the iteration's per-shift
+// circular ring of 2 kBatch fields and records the iteration's per-shift
 // coefficients (omegas, gammas, zeta_iii and the active window); every
-// kBatch iterations the recorded updates
+// kBatch iterations (a batch, one half of the ring) the recorded updates
 //     for j in batch:  out -= om_j * sf ;  sf = ga_j * sf + ze_j * r_j
 // are folded per shift into one affine map of the batch's start values
 // (k_flush_coef) and applied in one pass over the shift fields (k_flush).
 // The algebra is that of the per-iteration form; only the rounding order
 // differs.  Traffic per iteration drops from (3 + 4 n_active) to about
-// (1 + 4 n_active / kBatch) fields.  In addition alpha = Re<p, M^dagger M p>
-// (= |M p|^2) is accumulated in the epilogue of the M stencil from the values
-// it writes, so neither p nor s is re-read for it.
+// (1 + 4 n_active / kBatch) fields.  A batch's flush runs on the context's
+// low-priority side stream while the next batch iterates on the main stream
+// (it reads the other half of the ring and the other of two histories), so
+// the bandwidth-bound flush fills the time the latency-bound stencils and the
+// one-block scalar kernels leave unused.  In addition alpha =
+// Re<p, M^dagger M p> (= |M p|^2) is accumulated in the epilogue of the M
+// stencil from the values it writes, so neither p nor s is re-read for it.
 #include <cmath>
 #include <cstring>
 
@@ -47,11 +51,13 @@ __global__ void k_norm2(const V* a, size_t n, double* partials) {
     acc += W<V>::abs2(a[i]);
   block_write_partial(acc, partials);
 }
+// hist: the two batch histories (both start empty)
 __global__ void k_init(MsState* ms, MsHist* hist, const double* partials, int np) {
   const double d = block_sum_partials(partials, np);
   if (threadIdx.x == 0) {
     ms->delta = d;
-    hist->nsteps = 0;
+    hist[0].nsteps = 0;
+    hist[1].nsteps = 0;
   }
 }
 
@@ -91,14 +97,19 @@ __global__ void k_lambda(MsState* ms, MsHist* hist, const double* partials, int 
   }
 }
 
-// p = r + gammag*p (:145)
+// p = r + gammag*p (:145), in site order: a thread takes the four spin planes of
+// one (s, site) element of the plane (np = n / 4 elements), so the sweep moves
+// through the sites like the stencils do; rev: from the top site down
 template <class V>
-__global__ void k_pupdate(const MsState* ms, V* p, const V* r, size_t n) {
+__global__ void k_pupdate(const MsState* ms, V* p, const V* r, size_t np, int rev) {
   if (ms->done) return;
   using R = typename W<V>::R;
   const R gg = W<V>::cast(ms->gammag);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    p[i] = r[i] + gg * p[i];
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < np; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = rev ? np - 1 - e : e;
+#pragma unroll
+    for (int d = 0; d < 4; d++) p[i + d * np] = r[i + d * np] + gg * p[i + d * np];
+  }
 }
 
 // Fold each shift's recorded steps (:155-176 once per step) into one affine map
@@ -148,24 +159,26 @@ __global__ void k_flush_coef(MsState* ms, const MsHist* hist, MsCoef* cf) {
   }
 }
 
-// apply the folded maps to every shift field of the batch's window
-// (ring slot j+1 holds the residual of the batch's step j; the last one is copied
-// to slot 0, where the next batch starts).  One thread per element holds the
-// batch's residuals in registers (kBatch values) and walks the window; the next
-// shift's two fields are loaded while the current one is combined.
+// apply the folded maps to every shift field of the batch's window (the
+// residual of the batch's step j is in ring slot (first + j) mod 2 kBatch).  One
+// thread per element holds the batch's residuals in registers (kBatch values)
+// and walks the window; the next shift's two fields are loaded while the
+// current one is combined.
 constexpr int kFlushThreads = 128;
 constexpr int kFlushBlocks = 3;  // resident per SM at the register budget of kBatch residuals
 template <class V>
 __global__ void __launch_bounds__(kFlushThreads, kFlushBlocks)
-    k_flush(const MsCoef* cf, V* __restrict__ out, V* __restrict__ sf, V* __restrict__ ring, size_t n,
-            size_t stride) {
+    k_flush(const MsCoef* cf, V* __restrict__ out, V* __restrict__ sf, const V* __restrict__ ring, size_t n,
+            size_t stride, int first) {
   using R = typename W<V>::R;
   const int ns = cf->ns;
   if (ns == 0) return;
-  const int lo = cf->lo, hi = cf->hi;  // lo > hi: no shift active in the batch (only the ring carry)
+  const int lo = cf->lo, hi = cf->hi;  // lo > hi: no shift active in the batch
+  if (lo > hi) return;
+  // the maps of the window's shifts (the only rows read below)
   __shared__ R s_A[kMaxShift], s_P[kMaxShift], s_B[kMaxShift][kBatch], s_Q[kMaxShift][kBatch];
-  for (int t = threadIdx.x; t < kMaxShift * kBatch; t += blockDim.x) {
-    const int k = t / kBatch, i = t % kBatch;
+  for (int t = threadIdx.x; t < (hi - lo + 1) * kBatch; t += blockDim.x) {
+    const int k = lo + t / kBatch, i = t % kBatch;
     s_B[k][i] = (R)cf->B[k][i];
     s_Q[k][i] = (R)cf->Q[k][i];
     if (i == 0) {
@@ -177,14 +190,11 @@ __global__ void __launch_bounds__(kFlushThreads, kFlushBlocks)
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     V rj[kBatch];
 #pragma unroll
-    for (int j = 0; j < kBatch; j++)
-      if (j < ns) rj[j] = ring[(size_t)(1 + j) * n + i];
-    ring[i] = ring[(size_t)ns * n + i];  // the next batch starts from the last residual (just read: cached)
-    V f0n, o0n;
-    if (lo <= hi) {
-      f0n = sf[lo * stride + i];
-      o0n = out[lo * stride + i];
+    for (int j = 0; j < kBatch; j++) {
+      const int slot = first + j < 2 * kBatch ? first + j : first + j - 2 * kBatch;
+      if (j < ns) rj[j] = ring[(size_t)slot * n + i];
     }
+    V f0n = sf[lo * stride + i], o0n = out[lo * stride + i];
     for (int k = lo; k <= hi; k++) {
       const V f0 = f0n, o0 = o0n;
       if (k < hi) {
@@ -205,9 +215,12 @@ __global__ void __launch_bounds__(kFlushThreads, kFlushBlocks)
     }
   }
 }
+// short-lived blocks (at most kFlushPerThread elements per thread), so that a
+// flush running beside the main chain interleaves with its kernels block by block
+constexpr int kFlushPerThread = 4;
 inline unsigned flush_grid(size_t n) {
-  size_t b = (n + kFlushThreads - 1) / kFlushThreads;
-  if (b > 148 * kFlushBlocks) b = 148 * kFlushBlocks;
+  const size_t per = (size_t)kFlushThreads * kFlushPerThread;
+  const size_t b = (n + per - 1) / per;
   return (unsigned)(b ? b : 1);
 }
 // close a batch
@@ -247,52 +260,83 @@ inline unsigned vec_grid(size_t n) {
 }  // namespace
 
 namespace {
-// everything one batch of kBatch iterations enqueues (stream order); prof: sample
-// kernel timings with events (stream-launched solves only)
+// flush of the batch recorded in hist (ring half `half`) on stream `on`
+template <class V>
+void enqueue_flush(thr_ctx* c, cudaStream_t on, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, const V* ring,
+                   int half, bool prof, long long tag, int* prof_flush) {
+  const size_t n = c->n4();
+  const int pe = prof ? c->prof_begin(thr_ctx::P_SHIFTUPD, 0.0, tag, on) : -1;
+  k_flush_coef<<<1, kMaxShift, 0, on>>>(ms, hist, cf);
+  k_flush<V><<<flush_grid(n), kFlushThreads, 0, on>>>(cf, out, sf, ring, n, n, half * kBatch + 1);
+  c->prof_end(pe, on);
+  if (prof_flush) *prof_flush = pe;
+  k_reset<<<1, 1, 0, on>>>(hist, ms);
+}
+
+// One batch of kBatch iterations on ring half `half` (stream order on c->st),
+// recording into hist[half]; alongside it, on c->st2, the flush of the batch
+// before (hist[1 - half], the other half).  Ring slots: iteration j of the batch
+// reads r from slot half*kBatch + j and writes the new r to the next slot (mod
+// 2 kBatch), so each half's batch starts from the other half's last residual.
+// prof: sample kernel timings with events (stream-launched solves only).
 template <class V>
 int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V* ring, V* p, V* hv, V* s,
-                  float am, int imass, long long k0, bool prof, int* prof_flush) {
+                  float am, int imass, int half, long long k0, bool prof, int* prof_flush) {
   const size_t n = c->n4();
-  const unsigned gb = vec_grid(n);
+  const unsigned gb = vec_grid(n / 4);
   const unsigned gs = stencil_grid(c->g, c->p.kernel);
   const bool sp = sizeof(V) == sizeof(float2);
   const typename Sto<V>::C* u =
       sp ? (const typename Sto<V>::C*)(const void*)c->u32 : (const typename Sto<V>::C*)(const void*)c->u64;
   const double lb = sp ? sizeof(float2) : sizeof(double2);
+  // the previous batch's flush, forked onto the side stream (c->overlap_flush 0: in line)
+  const bool fork = c->overlap_flush != 0;
+  if (fork) {
+    THR_CUDA(cudaEventRecord(c->ev_fork[half], c->st));
+    THR_CUDA(cudaStreamWaitEvent(c->st2, c->ev_fork[half], 0));
+  }
+  enqueue_flush<V>(c, fork ? c->st2 : c->st, ms, hist + (1 - half), cf + (1 - half), out, sf, ring, 1 - half, prof,
+                   k0 - kBatch, prof_flush);
+  if (fork) THR_CUDA(cudaEventRecord(c->ev_join[half], c->st2));
   // algorithmic bytes: M reads p, writes h, reads the links (|M p|^2 comes from
   // registers); the M^dagger launch reads h, the links and r_old and writes r_new
   const double b_m = 2.0 * n * sizeof(V) + 3.0 * c->g.v3 * lb, b_md = b_m + (double)n * sizeof(V);
+  MsHist* rec = hist + half;
+  // sweep directions alternate with the iteration's parity (kBatch is even) so that
+  // every kernel starts on the sites its predecessor wrote last, still in L2:
+  //   even: M forward, M^dagger top down, p update forward; odd: the reverse
+  // (partials are indexed by site block, so the direction does not change results)
   for (int j = 0; j < kBatch; j++) {
-    V* rold = ring + (size_t)j * n;
-    V* rnew = ring + (size_t)(j + 1) * n;
+    const int odd = c->rev_sweep == 2 ? (j & 1) : 0;
+    const int rev_m = odd, rev_md = c->rev_sweep ? 1 - odd : 0, rev_p = odd;
+    const int so = half * kBatch + j, sn = so + 1 == 2 * kBatch ? 0 : so + 1;
+    V* rold = ring + (size_t)so * n;
+    V* rnew = ring + (size_t)sn * n;
     // alpha = Re<p, M^dagger M p> (:104) evaluated as |M p|^2 in the M epilogue
     int pe = prof ? c->prof_begin(thr_ctx::P_DSLASH, b_m, k0 + j) : -1;
     THR_TRY(launch_dslash_norm<V>(c->g, c->p.kernel, false, hv, p, u, am, imass, c->p.am3, c->st, &ms->done,
-                                  c->partials));
+                                  c->partials, rev_m));
     c->prof_end(pe);
-    k_alpha<<<1, 1024, 0, c->st>>>(ms, hist, c->partials, gs);
+    k_alpha<<<1, 1024, 0, c->st>>>(ms, rec, c->partials, gs);
     // s = M^dagger h is never stored: the epilogue forms r = r + omega*s (:137) and |r|^2 (:138)
     pe = prof ? c->prof_begin(thr_ctx::P_DSLASH_DAG, b_md, k0 + j) : -1;
     THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, rnew, hv, u, am, imass, c->p.am3, c->st, &ms->done, rold,
-                                  &ms->omega, c->partials, c->rev_sweep));
+                                  &ms->omega, c->partials, rev_md));
     c->prof_end(pe);
-    k_lambda<<<1, 1024, 0, c->st>>>(ms, hist, c->partials, gs);
-    k_pupdate<V><<<gb, kThreads, 0, c->st>>>(ms, p, rnew, n);
+    k_lambda<<<1, 1024, 0, c->st>>>(ms, rec, c->partials, gs);
+    k_pupdate<V><<<gb, kThreads, 0, c->st>>>(ms, p, rnew, n / 4, rev_p);
   }
   (void)s;
-  const int pe = prof ? c->prof_begin(thr_ctx::P_SHIFTUPD, 0.0, k0) : -1;
-  k_flush_coef<<<1, kMaxShift, 0, c->st>>>(ms, hist, cf);
-  k_flush<V><<<flush_grid(n), kFlushThreads, 0, c->st>>>(cf, out, sf, ring, n, n);
-  c->prof_end(pe);
-  if (prof_flush) *prof_flush = pe;
-  k_reset<<<1, 1, 0, c->st>>>(hist, ms);
+  if (fork) THR_CUDA(cudaStreamWaitEvent(c->st, c->ev_join[half], 0));
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
 
 // The whole batch loop as one CUDA graph: a WHILE conditional node whose body is
-// one batch followed by k_loop_ctl.  The body reads every per-solve value from
-// device memory (MsState, the ring base), so one instantiated graph serves every
-// solve with the same buffers and operator; it is rebuilt when they change.
+// two batches (ring halves 0 and 1, each with the other half's flush alongside)
+// followed by k_loop_ctl, then the flush of the last half-1 batch.  The body reads
+// every per-solve value from device memory (MsState), so one instantiated graph
+// serves every solve with the same buffers and operator; it is rebuilt when they
+// change.
 struct MsGraph {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -331,7 +375,7 @@ int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V
     THR_TRY(launch_dslash_norm<V>(c->g, c->p.kernel, false, hv, p, uu, am, imass, c->p.am3, c->st, &ms->done,
                                   c->partials));
     THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, s, hv, uu, am, imass, c->p.am3, c->st, &ms->done, ring,
-                                  &ms->omega, c->partials, c->rev_sweep));
+                                  &ms->omega, c->partials, c->rev_sweep ? 1 : 0));
   }
   THR_CUDA(cudaGraphCreate(&G.graph, 0));
   cudaGraphConditionalHandle handle;
@@ -345,16 +389,26 @@ int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V
   THR_CUDA(cudaGraphAddNode(&node, G.graph, nullptr, 0, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   THR_CUDA(cudaStreamBeginCaptureToGraph(c->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  int rc = enqueue_batch<V>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 0, false, nullptr);
+  int rc = enqueue_batch<V>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 0, 0, false, nullptr);
+  if (rc == THR_OK) rc = enqueue_batch<V>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 1, 0, false, nullptr);
   if (rc == THR_OK) k_loop_ctl<<<1, 1, 0, c->st>>>(ms, handle);
   cudaGraph_t captured = nullptr;
-  const cudaError_t ce = cudaStreamEndCapture(c->st, &captured);
+  cudaError_t ce = cudaStreamEndCapture(c->st, &captured);
+  if (rc == THR_OK && ce == cudaSuccess) {
+    // after the loop: the flush of the last batch (ring half 1)
+    ce = cudaStreamBeginCaptureToGraph(c->st, G.graph, &node, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+    if (ce == cudaSuccess) {
+      enqueue_flush<V>(c, c->st, ms, hist + 1, cf + 1, out, sf, ring, 1, false, 0, nullptr);
+      ce = cudaStreamEndCapture(c->st, &captured);
+    }
+  }
   if (rc != THR_OK || ce != cudaSuccess) {
     G.release();
     cudaGetLastError();
     return rc != THR_OK ? rc : THR_ERR_CUDA;
   }
-  if (cudaGraphInstantiate(&G.exec, G.graph, 0) != cudaSuccess) {
+  // node priorities: the flush nodes captured from the side stream yield to the main chain
+  if (cudaGraphInstantiate(&G.exec, G.graph, cudaGraphInstantiateFlagUseNodePriority) != cudaSuccess) {
     G.release();
     cudaGetLastError();
     return THR_ERR_CUDA;
@@ -386,15 +440,16 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
   MsState* ms = reinterpret_cast<MsState*>(c->dscal);
   MsState* h = reinterpret_cast<MsState*>(c->hscal);
   void* hv_;
-  THR_TRY(c->buffer(thr_ctx::B_HIST, sizeof(MsHist), &hv_));
-  MsHist* hist = (MsHist*)hv_;
+  THR_TRY(c->buffer(thr_ctx::B_HIST, 2 * sizeof(MsHist), &hv_));
+  MsHist* hist = (MsHist*)hv_;  // one history per ring half
   void* cf_;
-  THR_TRY(c->buffer(thr_ctx::B_COEF, sizeof(MsCoef), &cf_));
+  THR_TRY(c->buffer(thr_ctx::B_COEF, 2 * sizeof(MsCoef), &cf_));
   MsCoef* cf = (MsCoef*)cf_;
   THR_TRY(ms_prepare_state(c, h, ndiagq, aden, anum, res, maxcg));
   h->kbase = 0;
   h->batches = 0;
-  h->max_batches = (maxcg > 0 ? maxcg : 0) / kBatch + 3;
+  // flushes (one per batch, plus the final one; the graph runs batches in pairs)
+  h->max_batches = (maxcg > 0 ? maxcg : 0) / kBatch + 5;
   THR_CUDA(cudaMemcpyAsync(ms, h, sizeof(MsState), cudaMemcpyHostToDevice, c->st));
   THR_CUDA(cudaMemcpyAsync(ring, in, n * sizeof(V), cudaMemcpyDeviceToDevice, c->st));  // r = input (slot 0)
   THR_CUDA(cudaMemcpyAsync(p, in, n * sizeof(V), cudaMemcpyDeviceToDevice, c->st));     // p = r
@@ -415,17 +470,28 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
     const size_t prof_first = c->prof_kind.size();
     double flushed = 0.0;
     long long flushes = 0;
-    for (long long k = 0;; k += kBatch) {
-      int pf = -1;
-      THR_TRY(enqueue_batch<V>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, k, c->prof_on, &pf));
-      THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
-      THR_CUDA(cudaStreamSynchronize(c->st));
-      // flush traffic: each recorded step's residual read once, each shift field of the
-      // batch's window read and written once (out and sf)
+    // flush traffic: each recorded step's residual read once, each shift field of the
+    // batch's window read and written once (out and sf)
+    auto account = [&](int pf) {
       c->prof_set_bytes(pf, (h->flush_fields - flushed) * n * sizeof(V));
       if (h->flush_fields > flushed) flushes++;
       flushed = h->flush_fields;
-      if (h->done) break;
+    };
+    int half = 0;
+    for (long long k = 0;; k += kBatch, half ^= 1) {
+      int pf = -1;
+      THR_TRY(enqueue_batch<V>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, half, k, c->prof_on, &pf));
+      THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
+      THR_CUDA(cudaStreamSynchronize(c->st));
+      account(pf);
+      if (h->done) {
+        // the last batch's own flush
+        enqueue_flush<V>(c, c->st, ms, hist + half, cf + half, out, sf, ring, half, c->prof_on, k, &pf);
+        THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
+        THR_CUDA(cudaStreamSynchronize(c->st));
+        account(pf);
+        break;
+      }
       if (h->batches >= h->max_batches) return THR_ERR_CUDA;  // the device state stopped advancing
     }
     if (c->prof_on) {

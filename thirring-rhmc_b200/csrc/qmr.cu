@@ -54,7 +54,7 @@ int multishift_into(thr_ctx* c, const double2* Phi, double2* x1, int nq, const d
     THR_TRY(c->buffer(thr_ctx::B_SF64, (size_t)nq * n * sizeof(double2), &sf));
     THR_TRY(c->ensure_w64(8));
     if (batched) {
-      THR_TRY(c->buffer(thr_ctx::B_RING, (size_t)(kBatch + 1) * n * sizeof(double2), &ring));
+      THR_TRY(c->buffer(thr_ctx::B_RING, (size_t)(2 * kBatch) * n * sizeof(double2), &ring));
       return multishift_batched_dev<double2>(c, Phi, x1, (double2*)sf, (double2*)ring, c->w64[5], c->w64[6],
                                              c->w64[7], nq, aden, anum, res, am, imass, maxcg, itercg, cg_returns);
     }
@@ -70,7 +70,7 @@ int multishift_into(thr_ctx* c, const double2* Phi, double2* x1, int nq, const d
   int rc;
   if (batched) {
     void* ring;
-    THR_TRY(c->buffer(thr_ctx::B_RING, (size_t)(kBatch + 1) * n * sizeof(double2), &ring));
+    THR_TRY(c->buffer(thr_ctx::B_RING, (size_t)(2 * kBatch) * n * sizeof(double2), &ring));
     rc = multishift_batched_dev<float2>(c, w + 4 * n, (float2*)out32, (float2*)sf32, (float2*)ring, w, w + n,
                                         w + 2 * n, nq, aden, anum, res, am, imass, maxcg, itercg, cg_returns);
   } else {

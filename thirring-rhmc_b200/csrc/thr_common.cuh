@@ -78,7 +78,40 @@ struct Geom {
   long long v5;  // ls*v3
   int layout;
   int hv3;       // v3/2 (even-odd)
+  // division by a lattice extent d as a high multiply: q = umulhi(n, m) with
+  // m = ceil(2^32 / d) equals n / d whenever n * d < 2^32 (the rounding excess
+  // n * (m d - 2^32) / 2^32 < n d / 2^32 never reaches the next multiple);
+  // 0 where a quotient range breaks that bound (plain division then)
+  unsigned mdx = 0;  // for site / lx (natural) and k / (lx/2) (even-odd)
+  unsigned mdy = 0;  // for row / ly
 };
+
+__host__ __device__ __forceinline__ unsigned geom_magic(long long nmax, int d) {
+  if (d < 2 || (unsigned long long)nmax * (unsigned long long)d >= (1ULL << 32)) return 0u;
+  return (unsigned)(((1ULL << 32) + (unsigned long long)d - 1) / (unsigned long long)d);
+}
+
+__host__ __device__ __forceinline__ Geom geom_make(int lx, int ly, int lt, int ls, int layout) {
+  Geom g;
+  g.lx = lx; g.ly = ly; g.lt = lt; g.ls = ls;
+  g.v3 = lx * ly * lt;
+  g.v5 = (long long)g.v3 * ls;
+  g.layout = layout;
+  g.hv3 = g.v3 / 2;
+  g.mdx = layout == LAYOUT_EO ? geom_magic(g.hv3, lx >> 1) : geom_magic(g.v3, lx);
+  g.mdy = geom_magic((long long)ly * lt, ly);
+  return g;
+}
+
+// n / d for 0 <= n, with the magic multiplier m of d (0: divide)
+__host__ __device__ __forceinline__ int geom_div(int n, int d, unsigned m) {
+#ifdef __CUDA_ARCH__
+  if (m) return (int)__umulhi((unsigned)n, m);
+#else
+  if (m) return (int)(((unsigned long long)(unsigned)n * m) >> 32);
+#endif
+  return n / d;
+}
 
 // 0-based coordinates of storage site `site`
 __host__ __device__ __forceinline__ void site_coords(const Geom& g, int site, int& x, int& y, int& t) {
@@ -86,15 +119,15 @@ __host__ __device__ __forceinline__ void site_coords(const Geom& g, int site, in
     int p = site >= g.hv3;
     int k = site - p * g.hv3;
     int hx = g.lx >> 1;
-    int row = k / hx;
+    int row = geom_div(k, hx, g.mdx);
     int xh = k - row * hx;
-    t = row / g.ly;
+    t = geom_div(row, g.ly, g.mdy);
     y = row - t * g.ly;
     x = 2 * xh + ((p + y + t + 1) & 1);
   } else {
-    int row = site / g.lx;
+    int row = geom_div(site, g.lx, g.mdx);
     x = site - row * g.lx;
-    t = row / g.ly;
+    t = geom_div(row, g.ly, g.mdy);
     y = row - t * g.ly;
   }
 }
@@ -113,8 +146,20 @@ __host__ __device__ __forceinline__ int site_index(const Geom& g, int x, int y, 
 struct Nbr {
   int f[3], b[3];
 };
-__host__ __device__ __forceinline__ Nbr neighbours(const Geom& g, int x, int y, int t) {
+// `site` is the storage site of (x, y, t); in the natural order the neighbours
+// are that index plus a stride, minus the extent at a periodic wrap
+__host__ __device__ __forceinline__ Nbr neighbours(const Geom& g, int site, int x, int y, int t) {
   Nbr n;
+  if (g.layout != LAYOUT_EO) {
+    const int sy = g.lx, st = g.lx * g.ly;
+    n.f[0] = site + (x + 1 == g.lx ? 1 - g.lx : 1);
+    n.b[0] = site + (x == 0 ? g.lx - 1 : -1);
+    n.f[1] = site + (y + 1 == g.ly ? sy - st : sy);
+    n.b[1] = site + (y == 0 ? st - sy : -sy);
+    n.f[2] = site + (t + 1 == g.lt ? st - g.v3 : st);
+    n.b[2] = site + (t == 0 ? g.v3 - st : -st);
+    return n;
+  }
   int xp = x + 1 == g.lx ? 0 : x + 1, xm = x == 0 ? g.lx - 1 : x - 1;
   int yp = y + 1 == g.ly ? 0 : y + 1, ym = y == 0 ? g.ly - 1 : y - 1;
   int tp = t + 1 == g.lt ? 0 : t + 1, tm = t == 0 ? g.lt - 1 : t - 1;

@@ -25,7 +25,8 @@ int launch_dslash_axpy(const Geom& g, int kernel, bool dag, S* rnew, const S* in
 // same, with one FP64 partial per block of sum |out|^2
 template <class S>
 int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
-                       float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials);
+                       float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials,
+                       int rev = 0);
 
 // layout.cu: Fortran halo'd host layout <-> device fields
 // spinor (0:Ls+1,0:Lx+1,0:Ly+1,0:Lt+1,4) complex(dp)  <-> S[4][V3][Ls]
