@@ -115,6 +115,37 @@ def test_autotuner_keeps_results_bit_identical(tmp_path):
     assert np.array_equal(a, np.load(tmp_path / "out.npy"))
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("force", ["7", "6"])
+def test_register_budgets_bit_identical(tmp_path, force):
+    """Every register budget the stencil tuner may pick gives the same bits for
+    M, M^dagger and congrad (whose stencils carry the |Mp|^2 and the fused
+    residual-update epilogues): THR_TUNE=<n> forces budget n, THR_TUNE=0 the
+    default."""
+    import os
+    import subprocess
+    import sys
+    rng = np.random.default_rng(7)
+    L = O.lat(8, 6, 4, 16)
+    u = rand_links(L, rng)
+    R = rand_spinor(L, rng)
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "thirring-rhmc_b200")
+    np.save(tmp_path / "R.npy", R)
+    np.save(tmp_path / "u.npy", u)
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import thirring; d = %r; t = sys.argv[1];"
+            "R = np.asfortranarray(np.load(d + '/R.npy')); u = np.asfortranarray(np.load(d + '/u.npy'));"
+            "G = thirring.Lattice(8, 6, 4, 16); G.set_links(u);"
+            "a = G.dslash(R, None, 0.05, 3); b = G.dslashd(R, None, 0.05, 1);"
+            "X = np.zeros_like(R); it, _ = G.congrad(R, X, 1e-6, 0.05, 1);"
+            "np.savez(d + '/out_' + t + '.npz', a=a, b=b, x=X, it=it); G.close()"
+            % (pkg, str(tmp_path)))
+    for t in ("0", force):
+        subprocess.run([sys.executable, "-c", code, t], check=True, env=dict(os.environ, THR_TUNE=t))
+    ref, got = np.load(tmp_path / "out_0.npz"), np.load(tmp_path / ("out_%s.npz" % force))
+    for k in ("a", "b", "x", "it"):
+        assert np.array_equal(ref[k], got[k]), k
+
+
 def _dev_dslash(G, R, precision, am, imass, dag):
     import ctypes as C
     L = thirring.lib()

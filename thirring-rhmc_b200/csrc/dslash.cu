@@ -346,25 +346,38 @@ __global__ void __launch_bounds__(NT, MINB)
   }
 }
 
-// FP32 storage, Shamir kernel, even Ls: one thread owns two consecutive s of a
+// Shamir kernel, even Ls, FP32 storage: one thread owns two consecutive s of a
 // site (s0 = 2 threadIdx.x and s0 + 1), so every spinor access is one 16-byte
 // load or store (float4) instead of two 8-byte ones; the arithmetic per element
 // is that of shamir_site.  blockDim = (Ls / 2, sites per block) with the sites
 // per block of the one-s kernel, so the grid -- and the partials of the
-// epilogues -- are the same; blocks have about 64 threads, 16 per SM.
+// epilogues -- are the same; blocks have about 64 threads, 16 per SM.  (Written
+// for either complex type; for FP64 storage it ran at 45-49 us against the
+// one-s kernel's 38 us on the 32^2x32, Ls 32 lattice, so FP64 keeps one s per
+// thread.)
 __device__ __forceinline__ void ld_pair(const float2* p, unsigned i, float2& a, float2& b) {
   const float4 v = __ldg(reinterpret_cast<const float4*>(p + i));
   a = make_float2(v.x, v.y);
   b = make_float2(v.z, v.w);
 }
-template <bool DAG, int EPI, int MINB>
+__device__ __forceinline__ void ld_pair(const double2* p, unsigned i, double2& a, double2& b) {
+  a = __ldg(p + i);
+  b = __ldg(p + i + 1);
+}
+__device__ __forceinline__ void st_pair(float2* p, unsigned i, float2 a, float2 b) {
+  *reinterpret_cast<float4*>(p + i) = make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void st_pair(double2* p, unsigned i, double2 a, double2 b) {
+  p[i] = a;
+  p[i + 1] = b;
+}
+template <class C, bool DAG, int EPI, int MINB>
 __global__ void __launch_bounds__(64, MINB)
-    k_dslash_pair(float2* __restrict__ out, const float2* __restrict__ in, const float2* __restrict__ u, Geom g, float am,
-                  int imass, float am3, const int* skip, const float2* __restrict__ aux, const double* __restrict__ coef,
+    k_dslash_pair(C* __restrict__ out, const C* __restrict__ in, const C* __restrict__ u, Geom g, float am,
+                  int imass, float am3, const int* skip, const C* __restrict__ aux, const double* __restrict__ coef,
                   double* __restrict__ partials, int rev) {
   if (skip && *skip) return;
-  using C = float2;
-  using R = float;
+  using R = typename Sto<C>::R;
   const R om = EPI == 1 ? (R)(*coef) : R(0);
   const int s0 = 2 * threadIdx.x;
   const int bid = rev ? (int)gridDim.x - 1 - (int)blockIdx.x : (int)blockIdx.x;
@@ -376,7 +389,7 @@ __global__ void __launch_bounds__(64, MINB)
     int x, y, t;
     site_coords(g, site, x, y, t);
     const Nbr nb = neighbours(g, site, x, y, t);
-    SpinorView<float2> Rv{in, g};
+    SpinorView<C> Rv{in, g};
     const int Ls = g.ls;
     const R diag = (R)((3.0f - am3) + 1.0f);
     C c0[4], c1[4], a0c[4], a1c[4];
@@ -426,8 +439,8 @@ __global__ void __launch_bounds__(64, MINB)
         v0 = q0 + om * v0;  // r = r + omega*s (multishift_module.F90:137)
         v1 = q1 + om * v1;
       }
-      *reinterpret_cast<float4*>(out + i) = make_float4(v0.x, v0.y, v1.x, v1.y);
-      if (EPI != 0) racc += epi_norm<float2>(v0) + epi_norm<float2>(v1);
+      st_pair(out, i, v0, v1);
+      if (EPI != 0) racc += epi_norm<C>(v0) + epi_norm<C>(v1);
     }
   }
   if (EPI != 0) {
@@ -513,12 +526,14 @@ unsigned stencil_grid(const Geom& g, int kernel) {
 // each candidate runs 1 + 3 times on the call's own fields (the launches are
 // idempotent: out and partials are overwritten), the fastest is kept for the
 // process.  Block shape and reduction order do not change, so neither do the
-// results.  THR_TUNE=0 in the environment keeps the defaults (8, 2).  Launches
-// made while the stream is being captured into a graph use the default until
-// a tuned value exists.
+// results.  THR_TUNE=0 in the environment keeps the defaults (8, 2);
+// THR_TUNE=<n> runs the budget n wherever it is a candidate.  Launches made
+// while the stream is being captured into a graph use the default until a
+// tuned value exists.
 namespace {
 constexpr int kTuneShamir[3] = {8, 7, 6};
 constexpr int kTuneWilson[2] = {2, 1};
+constexpr int kMaxCand = 3;
 struct TuneKey {
   int dev, sid, ker, dag, epi, lx, ly, lt, ls, layout;
   bool operator<(const TuneKey& o) const {
@@ -531,15 +546,17 @@ struct TuneKey {
 };
 struct TuneVal {
   int pick, ncand;
-  float us[3];
+  float us[kMaxCand];
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneVal> g_tune;
 int g_tune_mode = -1;  // -1: not read yet, 0 off, 1 on
+int g_tune_force = 0;  // THR_TUNE=<candidate code>: that candidate wherever it is one
 bool tune_on() {
   if (g_tune_mode < 0) {
     const char* e = std::getenv("THR_TUNE");
     g_tune_mode = (e && e[0] == '0') ? 0 : 1;
+    if (e && std::atoi(e) >= 2) g_tune_force = std::atoi(e);
   }
   return g_tune_mode == 1;
 }
@@ -578,6 +595,7 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   } while (0)
   // FP32 Shamir with even Ls: two s per thread (k_dslash_pair), same grid
   const bool pair = storage_id<S>() == 1 && kernel == 0 && nt == 128 && g.ls % 2 == 0;
+
   // the register budget (resident blocks per SM) of the common configurations is
   // tuned: Shamir 128-thread blocks {8, 7, 6} (pair kernel: 64-thread blocks {16, 14, 12}),
   // Wilson 256-thread blocks {2, 1}
@@ -589,7 +607,7 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
       const float2* aux2 = reinterpret_cast<const float2*>(aux);
       const float2* u2 = reinterpret_cast<const float2*>(u);
 #define THR_P(D, E, MB) \
-  k_dslash_pair<D, E, MB><<<grd, pblk, 0, st>>>(out2, in2, u2, g, am, imass, am3, skip, aux2, coef, partials, rev)
+  k_dslash_pair<float2, D, E, MB><<<grd, pblk, 0, st>>>(out2, in2, u2, g, am, imass, am3, skip, aux2, coef, partials, rev)
 #define THR_PE(D, MB)                    \
   do {                                   \
     if (e == 1) THR_P(D, 1, MB);         \
@@ -643,8 +661,11 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
         found = true;
       }
     }
-    if (!found && tune_on() && !capturing(st)) {
-      TuneVal tv{cand[0], ncand, {0.f, 0.f, 0.f}};
+    if (!found && tune_on() && g_tune_force) {
+      for (int c = 0; c < ncand; c++)
+        if (cand[c] == g_tune_force) minb = g_tune_force;
+    } else if (!found && tune_on() && !capturing(st)) {
+      TuneVal tv{cand[0], ncand, {}};
       cudaEvent_t e0, e1;
       if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
         float best = 1e30f;

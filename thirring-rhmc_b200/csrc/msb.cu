@@ -289,8 +289,10 @@ int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* 
   const typename Sto<V>::C* u =
       sp ? (const typename Sto<V>::C*)(const void*)c->u32 : (const typename Sto<V>::C*)(const void*)c->u64;
   const double lb = sp ? sizeof(float2) : sizeof(double2);
-  // the previous batch's flush, forked onto the side stream (c->overlap_flush 0: in line)
-  const bool fork = c->overlap_flush != 0;
+  // the previous batch's flush, forked onto the side stream (c->overlap_flush 0: in line;
+  // also in line while kernel timings are sampled, so that each sampled duration is
+  // that kernel's alone and not one shared with a concurrent flush)
+  const bool fork = c->overlap_flush != 0 && !prof;
   if (fork) {
     THR_CUDA(cudaEventRecord(c->ev_fork[half], c->st));
     THR_CUDA(cudaStreamWaitEvent(c->st2, c->ev_fork[half], 0));
