@@ -136,6 +136,10 @@ for name, res, args in [
                                       C.POINTER(Counts)]),
     ("orc_trajectory", C.c_int, [_L, _v, _v, C.POINTER(Rational), C.c_int, C.c_float, C.c_float, C.c_int, C.c_float,
                                  C.c_float, C.c_int, C.c_int, C.c_int, C.POINTER(TrajResult), C.POINTER(Counts)]),
+    ("orc_zolo_coeffs", None, [C.c_int, C.c_double, C.c_double, _v]),
+    ("orc_odslash", None, [_L, _v, _v, _v, C.c_float, C.c_int, _v]),
+    ("orc_odslashd", None, [_L, _v, _v, _v, C.c_float, C.c_int, _v]),
+    ("orc_congrad_o", C.c_int, [_L, _v, _v, _v, C.c_float, C.c_float, C.c_int, _v, C.c_int, C.POINTER(C.c_int)]),
     ("orc_num_threads", C.c_int, []),
     ("orc_set_num_threads", None, [C.c_int]),
 ]:
@@ -177,6 +181,43 @@ def dirac_operator(L, X, u, am, imass):
     out = spinor(L)
     lib.orc_dirac_operator(C.byref(L), P(out), P(X), P(u), am, imass)
     return out
+
+
+def zolo_coeffs(n, lmin=0.1, lmax=5.0):
+    """coeffs(1..n) of prepZolo (measure_OWilson.F90:169-188; defaults as there)."""
+    c = np.zeros(n)
+    lib.orc_zolo_coeffs(n, lmin, lmax, P(c))
+    return c
+
+
+def zolo_sign(coeffs, lmin, x):
+    """The sign function from the roots 1/coeffs (zsgnrts, ZOLO/zolomodule.f:253-270)."""
+    t = np.ones_like(np.asarray(x, dtype=float))
+    for r in 1.0 / np.asarray(coeffs):
+        t = t * (r - x) / (r + x)
+    return (1 - t) / (1 + t)
+
+
+def odslash(L, R, u, am, imass, coeffs):
+    Phi = spinor(L)
+    lib.orc_odslash(C.byref(L), P(Phi), P(R), P(u), am, imass, P(np.ascontiguousarray(coeffs, np.float64)))
+    return Phi
+
+
+def odslashd(L, R, u, am, imass, coeffs):
+    Phi = spinor(L)
+    lib.orc_odslashd(C.byref(L), P(Phi), P(R), P(u), am, imass, P(np.ascontiguousarray(coeffs, np.float64)))
+    return Phi
+
+
+def congrad_o(L, Phi, u, res, am, imass, coeffs, niterc=None):
+    """congradO (measure_OWilson.F90:190-268): returns (X, itercg, iterations)."""
+    X = spinor(L)
+    it = C.c_int(0)
+    niterc = niterc if niterc is not None else L.ls * L.lx * L.ly * L.lt
+    itercg = lib.orc_congrad_o(C.byref(L), P(Phi), P(X), P(u), res, am, imass,
+                               P(np.ascontiguousarray(coeffs, np.float64)), niterc, C.byref(it))
+    return X, itercg, it.value
 
 
 def update_halo_5(L, a):

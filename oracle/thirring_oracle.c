@@ -1392,3 +1392,250 @@ int orc_trajectory(const orc_lat *L, orc_rng *g, float *theta, const orc_rationa
   free(u); free(Phi); free(thetat); free(pp); free(dSdpi);
   return rc;
 }
+
+/* ------------------------------------------------------------------------ */
+/* overlap (Zolotarev domain-wall) operator: measure_OWilson.F90             */
+/* ------------------------------------------------------------------------ */
+/* The coefficients coeffs(1..Ls) of prepZolo (measure_OWilson.F90:169-188):
+ * setZolo + getRoots of ZOLO/zolomodule.f:26-65, :253-300 with lmin 0.1, lmax 5
+ * by default.  The reference evaluates the elliptic functions by published
+ * approximations, restated here so that the coefficients agree:
+ *   K(k)       Hastings' polynomial approximation (Abramowitz & Stegun 17.3.34),
+ *              as COMELP (ZOLO/ellipticmodule.f:114-197);
+ *   sn(u|k)    descending Landen / arithmetic-geometric mean (A&S 16.4), stopped
+ *              when c < 1e-7, as JELP (:19-112);
+ *   arcsn(x|k) its integral by 3-point Gauss-Legendre quadrature over N panels,
+ *              as arcsn (:417-438). */
+static double zolo_K(double k) {
+  const double m1 = 1.0 - k * k;
+  if (k == 1.0) return 1.0e300;
+  const double a = (((0.01451196212 * m1 + 0.03742563713) * m1 + 0.03590092383) * m1 + 0.09666344259) * m1 +
+                   1.38629436112;
+  const double b = (((0.00441787012 * m1 + 0.03328355346) * m1 + 0.06880248576) * m1 + 0.12498593597) * m1 + 0.5;
+  return a - b * log(m1);
+}
+/* sn, dn of (u | modulus k) */
+static void zolo_sn(double u, double k, double *sn, double *dn) {
+  double r[41];
+  double a0 = 1.0, b0 = sqrt(1.0 - k * k), a = 1.0;
+  int n;
+  for (n = 1; n <= 40; n++) {
+    a = 0.5 * (a0 + b0);
+    const double b = sqrt(a0 * b0), c = 0.5 * (a0 - b0);
+    r[n] = c / a;
+    if (c < 1.0e-7) break;
+    a0 = a;
+    b0 = b;
+  }
+  if (n > 40) n = 40;
+  double ph = pow(2.0, n) * a * u, d = ph;
+  for (int j = n; j >= 1; j--) {
+    const double t = r[j] * sin(ph);
+    d = 0.5 * (ph + atan(t / sqrt(fabs(1.0 - t * t))));
+    ph = d;
+  }
+  *sn = sin(d);
+  if (dn) *dn = sqrt(1.0 - k * k * (*sn) * (*sn));
+}
+static double zolo_arcsn_integrand(double x, double k) {
+  return pow((1.0 + x) * (1.0 - x), -0.5) * pow((1.0 + k * x) * (1.0 - k * x), -0.5);
+}
+static double zolo_arcsn(double xmax, double k, int N) {
+  const double dx = xmax / N, h = sqrt(3.0 / 5.0) * dx / 2.0;
+  double x = dx / 2.0, acc = 0.0;
+  for (int i = 0; i < N; i++) {
+    const double vm = zolo_arcsn_integrand(x - h, k), v0 = zolo_arcsn_integrand(x, k),
+                 vp = zolo_arcsn_integrand(x + h, k);
+    acc += (5.0 / 9.0 * vm + 8.0 / 9.0 * v0 + 5.0 / 9.0 * vp) * dx / 2.0;
+    x += dx;
+  }
+  return acc;
+}
+/* the product R(x) of zolomodule.f:114-123 over the N/2 factor pairs */
+static double zolo_R(double x, const double *cnum, const double *cden, int nh) {
+  double v = 1.0;
+  for (int l = 0; l < nh; l++) v = v * (1.0 - x / cnum[l]) / (1.0 - x / cden[l]);
+  return v;
+}
+void orc_zolo_coeffs(int N, double lmin, double lmax, double *coeffs) {
+  const double beta = lmax / lmin, k = 1.0 / beta, kd = sqrt(1.0 - k) * sqrt(1.0 + k);
+  const double K = zolo_K(k), Kd = zolo_K(kd);
+  const int nh = N / 2;
+  double *cnum = (double *)malloc((nh + 1) * sizeof(double)), *cden = (double *)malloc((nh + 1) * sizeof(double));
+  for (int l = 0; l < nh; l++) { /* setInnerCoeffs, zolomodule.f:67-94 */
+    double s;
+    zolo_sn((2 * l + 2) * Kd / N, kd, &s, NULL);
+    cnum[l] = -s / (1.0 - s) * s / (1.0 + s);
+    zolo_sn((2 * l + 1) * Kd / N, kd, &s, NULL);
+    cden[l] = -s / (1.0 - s) * s / (1.0 + s);
+  }
+  const double M = zolo_R(1.0, cnum, cden, nh); /* calcM */
+  double esn, edn, dsn, ddn;                     /* calcC, :135-154 */
+  zolo_sn(K, k, &esn, &edn);
+  zolo_sn(Kd / N, kd, &dsn, &ddn);
+  const double C = esn * ddn / (1.0 - edn * edn * dsn * dsn);
+  const double lam = M / (C * zolo_R(C * C, cnum, cden, nh)); /* calcLambda */
+  /* getRoots (Chiu's formula with this lambda), :196-251 */
+  const double arg = sqrt((1.0 + 3.0 * lam) / ((1.0 + lam) * (1.0 + lam) * (1.0 + lam)));
+  const double lk = sqrt((1.0 + lam) * (1.0 - lam));
+  const double c1 = M * zolo_arcsn(arg, lk, 10000), c2 = 2.0 * Kd / N;
+  for (int s = 0; s < N; s++) {
+    const double v = ((s % 2) ? -c1 : c1) + ((s + 1) / 2) * c2;
+    double sn;
+    zolo_sn(v, kd, &sn, NULL);
+    const double omega = sqrt(1.0 - kd * kd * sn * sn) / lmin;
+    const double root = 1.0 / omega;
+    coeffs[s] = 1.0 / root; /* coeffs = 1d0/zolo%roots (measure_OWilson.F90:182) */
+  }
+  free(cnum);
+  free(cden);
+}
+
+/* Phi(il, spins d0..d1, interior) += c * (a[q] if a) + cb * (b[q] if b) with complex c, cb */
+static void acc_slice_z(const orc_lat *L, orc_zd *Phi, int il, int d0, int d1, orc_zd c, const orc_zd *a, orc_zd cb,
+                        const orc_zd *b) {
+  for (int d = d0; d <= d1; d++)
+    for (int t = 1; t <= L->lt; t++)
+      for (int y = 1; y <= L->ly; y++)
+        for (int x = 1; x <= L->lx; x++) {
+          size_t q = I4(x, y, t, d), o = I5(il, x, y, t, d);
+          orc_zd v = Phi[o];
+          if (a) v = zadd(v, zmul(c, a[q]));
+          if (b) v = zadd(v, zmul(cb, b[q]));
+          Phi[o] = v;
+        }
+}
+
+/* odslash, measure_OWilson.F90:14-89: DWilson(-am3) per slice with the
+ * coefficients coeffs (0-based here) */
+void orc_odslash(const orc_lat *L, orc_zd *Phi, const orc_zd *R, const orc_zd *u, float am, int imass,
+                 const double *coeffs) {
+  size_t n4 = orc_n4(L) * 4, n5 = orc_n5(L);
+  int Ls = L->ls;
+  double dgw = (double)(3.0f + (-L->am3));
+  orc_zd *Rs = (orc_zd *)malloc(n4 * sizeof(orc_zd));
+  orc_zd *Ps = (orc_zd *)malloc(n4 * sizeof(orc_zd));
+  for (size_t i = 0; i < n5; i++) Phi[i] = zd(0, 0);
+  const orc_zd one = zd(1.0, 0.0), mone = zd(-1.0, 0.0);
+  for (int il = 1; il <= Ls; il++) { /* diagonal, :31-36 */
+    get_slice(L, Rs, R, il, 0, 3);
+    dwilson(L, Ps, Rs, u, dgw, +1.0);
+    acc_slice_z(L, Phi, il, 0, 3, zd(coeffs[il - 1], 0.0), Ps, one, Rs);
+  }
+  for (int il = 1; il < Ls; il++) { /* upper diagonal, :38-47: P- R(il+1) */
+    memset(Rs, 0, n4 * sizeof(orc_zd));
+    get_slice(L, Rs, R, il + 1, 2, 3);
+    dwilson(L, Ps, Rs, u, dgw, +1.0);
+    acc_slice_z(L, Phi, il, 0, 3, zd(coeffs[il - 1], 0.0), Ps, mone, Rs);
+  }
+  for (int il = 2; il <= Ls; il++) { /* lower diagonal, :49-58: P+ R(il-1) */
+    memset(Rs, 0, n4 * sizeof(orc_zd));
+    get_slice(L, Rs, R, il - 1, 0, 1);
+    dwilson(L, Ps, Rs, u, dgw, +1.0);
+    acc_slice_z(L, Phi, il, 0, 3, zd(coeffs[il - 1], 0.0), Ps, mone, Rs);
+  }
+  /* mass terms, :60-85: -am | i am times (coeffs(1) DWilson(P+ R(Ls)) - P+ R(Ls)) into slice 1,
+   * -am | -i am times (coeffs(Ls) DWilson(P- R(1)) - P- R(1)) into slice Ls */
+  for (int wall = 0; wall < 2; wall++) {
+    memset(Rs, 0, n4 * sizeof(orc_zd));
+    if (wall == 0) get_slice(L, Rs, R, Ls, 0, 1);
+    else get_slice(L, Rs, R, 1, 2, 3);
+    dwilson(L, Ps, Rs, u, dgw, +1.0);
+    const int tgt = wall == 0 ? 1 : Ls;
+    const double cf = coeffs[tgt - 1];
+    const orc_zd m = imass == 1 ? zd(-(double)am, 0.0) : (wall == 0 ? zd(0.0, (double)am) : zd(0.0, -(double)am));
+    acc_slice_z(L, Phi, tgt, 0, 3, zmul(m, zd(cf, 0.0)), Ps, zmul(m, mone), Rs);
+  }
+  free(Rs);
+  free(Ps);
+}
+
+/* odslashd, measure_OWilson.F90:91-167 */
+void orc_odslashd(const orc_lat *L, orc_zd *Phi, const orc_zd *R, const orc_zd *u, float am, int imass,
+                  const double *coeffs) {
+  size_t n4 = orc_n4(L) * 4, n5 = orc_n5(L);
+  int Ls = L->ls;
+  double dgw = (double)(float)(3.0f + (-L->am3));
+  orc_zd *Rs = (orc_zd *)malloc(n4 * sizeof(orc_zd));
+  orc_zd *Ps = (orc_zd *)malloc(n4 * sizeof(orc_zd));
+  for (size_t i = 0; i < n5; i++) Phi[i] = zd(0, 0);
+  const orc_zd one = zd(1.0, 0.0), mone = zd(-1.0, 0.0);
+  for (int il = 1; il <= Ls; il++) {
+    get_slice(L, Rs, R, il, 0, 3);
+    dwilson(L, Ps, Rs, u, dgw, -1.0);
+    const orc_zd c = zd(coeffs[il - 1], 0.0);
+    acc_slice_z(L, Phi, il, 0, 3, c, Ps, one, Rs);                 /* diagonal, :110-114 */
+    if (il > 1) acc_slice_z(L, Phi, il - 1, 0, 1, c, Ps, mone, Rs); /* upper diagonal, :117-124 */
+    if (il < Ls) acc_slice_z(L, Phi, il + 1, 2, 3, c, Ps, mone, Rs); /* lower diagonal, :127-134 */
+  }
+  /* mass terms, :137-160 */
+  for (int wall = 0; wall < 2; wall++) {
+    const int src = wall == 0 ? Ls : 1, tgt = wall == 0 ? 1 : Ls, d0 = wall == 0 ? 2 : 0;
+    get_slice(L, Rs, R, src, 0, 3);
+    dwilson(L, Ps, Rs, u, dgw, -1.0);
+    const orc_zd zk = imass == 1 ? zd(-(double)am, 0.0) : (wall == 0 ? zd(0.0, (double)am) : zd(0.0, -(double)am));
+    acc_slice_z(L, Phi, tgt, d0, d0 + 1, zmul(zk, zd(coeffs[src - 1], 0.0)), Ps, zmul(zk, mone), Rs);
+  }
+  free(Rs);
+  free(Ps);
+}
+
+static double redot_int(const orc_lat *L, const orc_zd *a, const orc_zd *b) {
+  double acc = 0.0;
+  FOR_INTERIOR({ acc += a[i].re * b[i].re + a[i].im * b[i].im; })
+  return acc;
+}
+
+/* congradO, measure_OWilson.F90:190-268: CG on odslash^dagger odslash starting
+ * from X = Phi; returns itercg, *iterations = the loop index at exit */
+int orc_congrad_o(const orc_lat *L, const orc_zd *Phi, orc_zd *X, const orc_zd *u, float res, float am, int imass,
+                  const double *coeffs, int niterc, int *iterations) {
+  size_t n = orc_n5(L);
+  orc_zd *x1 = (orc_zd *)calloc(n, sizeof(orc_zd));
+  orc_zd *x2 = (orc_zd *)calloc(n, sizeof(orc_zd));
+  orc_zd *p = (orc_zd *)malloc(n * sizeof(orc_zd));
+  orc_zd *r = (orc_zd *)malloc(n * sizeof(orc_zd));
+  int ivol = 4 * L->lx * L->ly * L->lt * L->ls;
+  float resid = ((float)ivol * res) * res; /* :214 */
+  int itercg = 0, i = 0;
+  memcpy(r, Phi, n * sizeof(orc_zd));
+  memcpy(X, r, n * sizeof(orc_zd));
+  orc_update_halo_5(L, X);
+  orc_odslash(L, x1, X, u, am, imass, coeffs);
+  orc_update_halo_5(L, x1);
+  orc_odslashd(L, x2, x1, u, am, imass, coeffs);
+#pragma omp parallel for schedule(static)
+  for (size_t q = 0; q < n; q++) r[q] = zsub(Phi[q], x2[q]);
+  orc_update_halo_5(L, r);
+  memcpy(p, r, n * sizeof(orc_zd));
+  double betacgn = norm2_int(L, r), alphan, alphad, alpha, betacg;
+  if (!(betacgn < (double)resid)) {
+    for (i = 1; i <= niterc; i++) {
+      itercg++;
+      orc_odslash(L, x1, p, u, am, imass, coeffs);
+      orc_update_halo_5(L, x1);
+      orc_odslashd(L, x2, x1, u, am, imass, coeffs);
+      alphan = norm2_int(L, r);
+      alphad = redot_int(L, p, x2);
+      alpha = alphan / alphad;
+#pragma omp parallel for schedule(static)
+      for (size_t q = 0; q < n; q++) {
+        X[q] = zadd(X[q], zscal(alpha, p[q]));
+        r[q] = zsub(r[q], zscal(alpha, x2[q]));
+      }
+      orc_update_halo_5(L, r);
+      betacgn = norm2_int(L, r);
+      if (betacgn < (double)resid) break;
+      betacg = betacgn / alphan;
+#pragma omp parallel for schedule(static)
+      for (size_t q = 0; q < n; q++) p[q] = zadd(r[q], zscal(betacg, p[q]));
+      orc_update_halo_5(L, p);
+    }
+  }
+  if (iterations) *iterations = i;
+  free(x1);
+  free(x2);
+  free(p);
+  free(r);
+  return itercg;
+}

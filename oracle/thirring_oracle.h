@@ -170,6 +170,17 @@ int orc_trajectory(const orc_lat *L, orc_rng *g, float *theta, const orc_rationa
                    int iterl, float dt, float am, int imass, float rescga, float rescgg, int use_sp,
                    int max_qmr_iters, int fixed_steps, orc_traj_result *out, orc_md_counts *cnt);
 
+/* overlap operator, measure_OWilson.F90: the Zolotarev coefficients of prepZolo
+ * (:169-188, ZOLO/zolomodule.f) for N = Ls slices on [lmin, lmax]; odslash (:14-89),
+ * odslashd (:91-167) and congradO (:190-268) with coefficients coeffs[0..Ls-1] */
+void orc_zolo_coeffs(int N, double lmin, double lmax, double *coeffs);
+void orc_odslash(const orc_lat *L, orc_zd *Phi, const orc_zd *R, const orc_zd *u, float am, int imass,
+                 const double *coeffs);
+void orc_odslashd(const orc_lat *L, orc_zd *Phi, const orc_zd *R, const orc_zd *u, float am, int imass,
+                  const double *coeffs);
+int orc_congrad_o(const orc_lat *L, const orc_zd *Phi, orc_zd *X, const orc_zd *u, float res, float am, int imass,
+                  const double *coeffs, int niterc, int *iterations);
+
 /* threads used by the OpenMP loops */
 int orc_num_threads(void);
 void orc_set_num_threads(int n);

@@ -246,3 +246,36 @@ def test_congrad_graph_equals_host_launched():
             outs.append((it, nx, X))
     for it, nx, X in outs[1:]:
         assert (it, nx) == outs[0][:2] and np.array_equal(X, outs[0][2])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("env", [{"THR_OVERLAP": "0"}, {"THR_REVERSE": "1"}, {"THR_REVERSE": "0"},
+                                 {"THR_GRAPHS": "0"}])
+def test_solver_schedules_bit_identical(tmp_path, env):
+    """Where the batched multishift's flush runs (side stream or in line), which
+    way the solver kernels sweep the sites, and whether the loops are graphs or
+    host-launched change the schedule only: the multishift (FP64 and FP32
+    vectors) and congrad give the same bits and iteration counts."""
+    import os
+    import subprocess
+    import sys
+    rng = np.random.default_rng(31)
+    L = O.lat(4, 4, 6, 8)
+    u = rand_links(L, rng)
+    inp = rand_spinor(L, rng)
+    an, ad, _, _ = remez("remez4g", 12)
+    np.savez(tmp_path / "in.npz", u=u, inp=inp, an=an, ad=ad)
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "thirring-rhmc_b200")
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import thirring; d = %r; t = sys.argv[1];"
+            "z = np.load(d + '/in.npz'); u = np.asfortranarray(z['u']); inp = np.asfortranarray(z['inp']);"
+            "G = thirring.Lattice(4, 4, 6, 8); r = {};"
+            "r['x64'], r['i64'], r['c64'] = G.multishift_solver(u, 0.05, 3, z['ad'], z['an'][1:], inp, 1e-9, 5000);"
+            "r['x32'], r['i32'], r['c32'] = G.multishift_solver(u, 0.05, 3, z['ad'], z['an'][1:], inp, 1e-6, 5000,"
+            " sp=True);"
+            "G.set_links(u); X = np.zeros_like(inp); r['icg'], _ = G.congrad(inp, X, 1e-9, 0.05, 3); r['xcg'] = X;"
+            "np.savez(d + '/out_' + t + '.npz', **r); G.close()" % (pkg, str(tmp_path)))
+    subprocess.run([sys.executable, "-c", code, "ref"], check=True)
+    subprocess.run([sys.executable, "-c", code, "alt"], check=True, env=dict(os.environ, **env))
+    ref, got = np.load(tmp_path / "out_ref.npz"), np.load(tmp_path / "out_alt.npz")
+    for k in ref.files:
+        assert np.array_equal(ref[k], got[k]), k

@@ -79,21 +79,54 @@ __global__ void k_alpha(MsState* ms, MsHist* hist, const double* partials, int n
   }
 }
 
-// :143, :148-150, recording gammas; closes the step's record
+// :143, :148-150, recording gammas; closes the step's record.  Then the step's
+// end (:178-180, :230-275: cg_returns, convergence test, window, zeta shift,
+// delta) with one thread per shift: ms_converge_step's statements, the window's
+// new bounds from a shared-memory min / max (blockDim.x >= kMaxShift)
 __global__ void k_lambda(MsState* ms, MsHist* hist, const double* partials, int np) {
   if (ms->done) return;
+  __shared__ int s_lo, s_hi;
   const double lambda = block_sum_partials(partials, np);
   if (threadIdx.x == 0) ms_lambda_scalar(ms, lambda);
   __syncthreads();
-  const int k = ms->lo + threadIdx.x;
-  if (k <= ms->hi) {
+  const int lo0 = ms->lo, hi0 = ms->hi;
+  const int k = lo0 + threadIdx.x;
+  if (k <= hi0) {
     ms_lambda_shift(ms, k);
     hist->ga[hist->nsteps][k] = ms->gammas[k];
   }
+  const int nq = ms->ndiagq, it = ms->it;
+  const double delta = ms->delta, res = (double)ms->res;  // delta of this step (replaced below)
+  if (threadIdx.x == 0) {
+    s_lo = nq;
+    s_hi = -1;
+  }
   __syncthreads();
+  const int q = threadIdx.x;
+  if (q < nq) {
+    if (q >= lo0 && q <= hi0) ms->cg_returns[q] = it;
+    if (ms->flags[q]) {
+      if (sqrt(delta * ms->zeta_ii[q] * ms->zeta_ii[q]) * ms->correction[q] < res) {
+        ms->flags[q] = 0;
+      } else {
+        atomicMin(&s_lo, q);
+        atomicMax(&s_hi, q);
+      }
+    }
+  }
+  __syncthreads();
+  const int mini = s_lo, maxi = s_hi;
+  if (q >= mini && q <= maxi) {
+    ms->zeta_i[q] = ms->zeta_ii[q];
+    ms->zeta_ii[q] = ms->zeta_iii[q];
+  }
   if (threadIdx.x == 0) {
     hist->nsteps += 1;
-    ms_converge_step(ms);  // :240-258, after the step's gammas are recorded
+    ms->lo = mini;
+    ms->hi = maxi;
+    ms->delta = ms->lambda;
+    if (!(ms->lambda == ms->lambda)) ms->status = THR_ERR_NAN;
+    if (maxi < mini || ms->it >= ms->maxcg || ms->status) ms->done = 1;
   }
 }
 
