@@ -319,6 +319,63 @@ def run_ours(args, rank, world, local_rank):
     return res
 
 
+def run_overlap(args):
+    """The overlap operator of measure_OWilson.F90: odslash / odslashd at 48^2x48,
+    Ls = 16 (algorithmic GB/s: one read of the input spinor, one write of the
+    output, three link fields; 0.23 GB per launch, above L2) and congradO on
+    16^2x16, Ls = 8 with the reference's prepZolo coefficients (0.1, 5)."""
+    import torch
+    import thirring
+    from thirring import _lib
+    L = _lib.lib()
+    out = {}
+    lx, ls = 48, 16
+    G = thirring.Lattice(lx, lx, lx, ls, kernel=1)
+    rng = np.random.default_rng(7)
+    G.coef(np.asfortranarray(rng.standard_normal((lx, lx, lx, 3)) / np.sqrt(BETA), np.float32))
+    a, b = C.c_void_p(), C.c_void_p()
+    L.thr_field_create(G.h, 0, C.byref(a))
+    L.thr_field_create(G.h, 0, C.byref(b))
+    R = thirring.spinor(G)
+    R[1:-1, 1:-1, 1:-1, 1:-1, :] = rng.standard_normal(R[1:-1, 1:-1, 1:-1, 1:-1, :].shape)
+    L.thr_field_upload(G.h, a, 0, R.ctypes.data_as(C.c_void_p))
+    s = C.c_void_p()
+    L.thr_get_stream(G.h, C.byref(s))
+    st = torch.cuda.ExternalStream(s.value)
+    v3 = lx ** 3
+    byts = 2 * 4 * ls * v3 * 16 + 3 * v3 * 16
+    for dag in (0, 1):
+        for _ in range(max(args.warmup, 3)):
+            L.thr_odslash_dev(G.h, b, a, AM, 1, dag)
+        L.thr_sync(G.h)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            L.thr_odslash_dev(G.h, b, a, AM, 1, dag)
+        e1.record(st)
+        e1.synchronize()
+        us = e0.elapsed_time(e1) / args.steps * 1e3
+        out["odslashd" if dag else "odslash"] = {"us": round(us, 2), "gbs": round(byts / us / 1e3, 1)}
+    L.thr_field_destroy(G.h, a)
+    L.thr_field_destroy(G.h, b)
+    G.close()
+    lx, ls = 16, 8
+    G = thirring.Lattice(lx, lx, lx, ls, kernel=1)
+    G.coef(np.asfortranarray(rng.standard_normal((lx, lx, lx, 3)) / np.sqrt(BETA), np.float32))
+    Phi = thirring.spinor(G)
+    Phi[1:-1, 1:-1, 1:-1, 1:-1, :] = rng.standard_normal(Phi[1:-1, 1:-1, 1:-1, 1:-1, :].shape)
+    G.congrad_o(Phi, 1e-6, AM, 1)  # warm-up
+    t0 = time.perf_counter()
+    X, it, nx = G.congrad_o(Phi, 1e-6, AM, 1)
+    dt = time.perf_counter() - t0
+    out["congrad_o_16x16x16_ls8"] = {"s": round(dt, 4), "itercg": it, "us_per_iteration": round(dt / max(it, 1) * 1e6, 2),
+                                     "res": 1e-6, "am": AM, "zolo": [0.1, 5.0]}
+    G.close()
+    return {"workload": "overlap operator (measure_OWilson.F90): odslash/odslashd 48^2x48 Ls16, congradO 16^3 Ls8",
+            "results": out}
+
+
 def dslash_bandwidth(args, dev, lx=48, ls=48, iters=20, warmup=3):
     """FP64 Shamir M at lx^2 x lx, Ls = ls: algorithmic GB/s over `iters` launches
     (one read of the input spinor, one write of the output, three link fields)."""
@@ -581,7 +638,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="fp64", choices=["fp64", "sp", "mixed", "bf16"])
     ap.add_argument("--workload", default="multishift",
-                    choices=["multishift", "measurement", "packed", "trajectory", "trajectory48", "dslash"],
+                    choices=["multishift", "measurement", "packed", "trajectory", "trajectory48", "dslash",
+                             "overlap"],
                     help="secondary workloads print their own JSON line (not the headline contract)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-iters", type=int, default=6, help="multishift iterations in the CPU sample")
@@ -615,7 +673,7 @@ def main():
         return
     if args.workload != "multishift":
         fn = {"measurement": run_measurement, "packed": run_packed, "trajectory": run_trajectory,
-              "trajectory48": run_trajectory48}[args.workload]
+              "trajectory48": run_trajectory48, "overlap": run_overlap}[args.workload]
         print(json.dumps(fn(args)), flush=True)
         return
 

@@ -186,6 +186,32 @@ int thr_meson(thr_ctx *ctx, float res, float am, int imass, int nsource, int pre
 int thr_fermion(thr_ctx *ctx, float res, float am, int imass, int nsource, int precision, double *cferm1,
                 double *cferm2, int *itercg, float *aviter);
 
+/* ---- measure_OWilson.F90: the overlap (Zolotarev domain-wall) operator ---- */
+/* The coefficients coeffs(1:Ls) of prepZolo (measure_OWilson.F90:169-188,
+ * ZOLO/zolomodule.f setZolo + getRoots): the Zolotarev approximation of sign(x)
+ * on [lmin, lmax] with Ls roots (the reference uses lmin 0.1, lmax 5).  Host
+ * only; coeffs[0..ls-1]. */
+int thr_zolo_coeffs(int ls, double lmin, double lmax, double *coeffs);
+/* prepZolo for this context's Ls on [lmin, lmax]; without a call the context
+ * uses the reference's 0.1, 5 on first use.  thr_zolo_get copies them out. */
+int thr_prep_zolo(thr_ctx *ctx, double lmin, double lmax);
+int thr_zolo_get(thr_ctx *ctx, double *coeffs);
+/* odslash(Phi, R, u, am, imass), measure_OWilson.F90:14-89, and
+ * odslashd(Phi, R, u, am, imass[, reqs_R]), :91-167: the Wilson-kernel
+ * domain-wall operator with slice il's DWilson term scaled by coeffs(il) (the
+ * imass 3 walls with the module's sign).  Fortran halo'd spinors as thr_dslash;
+ * u may be NULL for the current links; imass 1 or 3. */
+int thr_odslash(thr_ctx *ctx, double *Phi, const double *R, const double *u, float am, int imass);
+int thr_odslashd(thr_ctx *ctx, double *Phi, const double *R, const double *u, float am, int imass);
+/* congradO(Phi, res, itercg, am, imass[, iterations]), measure_OWilson.F90:190-268:
+ * CG on odslash^dagger odslash with the current links, starting from X = Phi
+ * (X is output only, the module variable vector::x).  Stops when |r|^2 <
+ * 4*Lx*Ly*Lt*Ls*res^2 or after Ls*Lx*Ly*Lt iterations (THR_ERR_MAXITER, where
+ * the reference prints a warning).  *iterations gets the loop index at exit
+ * (0 when the start already meets the stopping rule). */
+int thr_congrad_o(thr_ctx *ctx, const double *Phi, double *X, float res, int *itercg, float am, int imass,
+                  int *iterations);
+
 /* ---- multishift_module.F90 ----------------------------------------------- */
 /* multishift_solver(u, am, imass, ndiagq, aden, anum, output, input, res,
  * maxcg, cg_return[, cg_returns]), multishift_module.F90:13-284: solves
@@ -340,6 +366,8 @@ int thr_field_upload(thr_ctx *ctx, void *field, int precision, const double *hos
 int thr_field_download(thr_ctx *ctx, double *host_spinor, const void *field, int precision);
 /* out = M in (dag = 0) or M^dagger in (dag = 1) with the current links */
 int thr_dslash_dev(thr_ctx *ctx, void *out, const void *in, int precision, float am, int imass, int dag);
+/* out = odslash in (dag = 0) or odslashd in (dag = 1), FP64 fields, current links */
+int thr_odslash_dev(thr_ctx *ctx, void *out, const void *in, float am, int imass, int dag);
 /* qmrherm on FP64 device fields (the device layout of thr_field_create with
  * THR_FP64): same semantics as thr_qmrherm; dSdpi and Phi0 stay in the
  * context.  Returns when the solve has converged (its scalars are polled). */

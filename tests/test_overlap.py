@@ -1,0 +1,162 @@
+"""The overlap (Zolotarev domain-wall) operator of measure_OWilson.F90.
+
+The reference ships no golden values for it, so the oracle is pinned by
+properties: its Zolotarev coefficients give the optimal rational approximation
+of sign(x) (the error of an N-root approximation on [lmin, lmax] falls off as
+exp(-N pi^2 / (2 ln(4 lmax/lmin)))); with every coefficient 1 odslash and
+odslashd reduce to the Wilson-kernel dslash / dslashd (dirac.F90:226-626, whose
+oracle the reference's own fixtures pin) -- equal for imass 1, with am -> -am
+for imass 3, whose walls the module flips; odslashd is the adjoint of odslash;
+congradO's solution solves M^dagger M X = Phi.  The GPU is then held to the
+oracle: 1e-13 (max norm) for the operators, the iteration count within 2 and
+1e-5 on the solution for congradO (rounding order differs in the reductions),
+whose true residual meets the stopping rule.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import thirring
+from helpers import interior, rand_links, rand_spinor, rel_err
+
+TOL = 1e-13
+
+
+def _vdot(a, b):
+    return np.vdot(interior(a).ravel(), interior(b).ravel())
+
+
+# ---------------------------------------------------------------- CPU
+@pytest.mark.parametrize("n", [4, 8, 12, 16, 32])
+def test_zolo_coefficients_match_oracle_and_approximate_sign(n):
+    got = thirring.zolo_coeffs(n)
+    ref = O.zolo_coeffs(n)
+    assert np.array_equal(got, ref)
+    x = np.logspace(-1, np.log10(5.0), 4001)
+    err = np.max(np.abs(O.zolo_sign(ref, 0.1, x) - 1.0))
+    bound = 8.0 * np.exp(-n * np.pi ** 2 / (2.0 * np.log(4.0 * 5.0 / 0.1)))
+    assert err <= bound, (err, bound)
+    assert np.allclose(O.zolo_sign(ref, 0.1, -x), -O.zolo_sign(ref, 0.1, x), rtol=0, atol=1e-14)
+
+
+def test_zolo_coefficients_arguments():
+    c = np.zeros(8)
+    L = thirring.lib()
+    assert L.thr_zolo_coeffs(8, 0.0, 5.0, c.ctypes.data) == 1
+    assert L.thr_zolo_coeffs(8, 5.0, 0.1, c.ctypes.data) == 1
+    assert L.thr_zolo_coeffs(0, 0.1, 5.0, c.ctypes.data) == 1
+    assert L.thr_zolo_coeffs(8, 0.05, 8.0, c.ctypes.data) == 0
+    assert np.array_equal(c, O.zolo_coeffs(8, 0.05, 8.0))
+
+
+@pytest.mark.parametrize("imass", [1, 3])
+def test_oracle_unit_coefficients_are_the_wilson_kernel(imass):
+    rng = np.random.default_rng(5 + imass)
+    L = O.lat(4, 4, 4, 6, kernel=1)
+    u, R = rand_links(L, rng), rand_spinor(L, rng)
+    one = np.ones(6)
+    amw = 0.07 if imass == 1 else -0.07
+    a = O.odslash(L, R, u, 0.07, imass, one)
+    b = O.dslash(L, R, u, amw, imass)
+    assert rel_err(interior(a), interior(b)) <= 1e-14
+    a = O.odslashd(L, R, u, 0.07, imass, one)
+    b = O.dslashd(L, R, u, amw, imass)
+    assert rel_err(interior(a), interior(b)) <= 1e-14
+
+
+# congradO converges slowly with the reference's [0.1, 5] coefficients (they span
+# 9.5 .. 0.2 at Ls 8, and the 5D system is ill-conditioned: ~900 iterations on a
+# 4^3 x 8 lattice, beyond the Ls*V3 cap); the solver tests use [0.5, 5].
+SOLVE = dict(beta=2.0, am=0.5, res=1e-6, lmin=0.5, lmax=5.0)
+
+
+@pytest.mark.parametrize("imass", [1, 3])
+def test_oracle_adjoint_and_congrad_o(imass):
+    rng = np.random.default_rng(11 + imass)
+    L = O.lat(4, 4, 4, 8, kernel=1)
+    u, a, b = rand_links(L, rng), rand_spinor(L, rng), rand_spinor(L, rng)
+    c = O.zolo_coeffs(8)
+    lhs = _vdot(a, O.odslash(L, b, u, 0.05, imass, c))
+    rhs = _vdot(O.odslashd(L, a, u, 0.05, imass, c), b)
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+    L = O.lat(6, 6, 4, 4, kernel=1)
+    u, a = rand_links(L, rng, beta=SOLVE["beta"]), rand_spinor(L, rng)
+    c = O.zolo_coeffs(4, SOLVE["lmin"], SOLVE["lmax"])
+    am = SOLVE["am"]
+    X, itercg, iters = O.congrad_o(L, a, u, SOLVE["res"], am, imass, c)
+    assert 0 < itercg == iters < 6 * 6 * 4 * 4
+    X = O.update_halo_5(L, X)
+    y = O.update_halo_5(L, O.odslash(L, X, u, am, imass, c))
+    y = O.odslashd(L, y, u, am, imass, c)
+    assert rel_err(interior(y), interior(a)) <= 1e-5
+
+
+# ---------------------------------------------------------------- GPU
+@pytest.mark.gpu
+@pytest.mark.parametrize("imass", [1, 3])
+@pytest.mark.parametrize("dims", [(4, 6, 8, 8), (6, 4, 4, 12), (4, 4, 6, 5)])
+def test_odslash_vs_oracle(imass, dims):
+    lx, ly, lt, ls = dims
+    rng = np.random.default_rng(hash((imass,) + dims) % 2**32)
+    L = O.lat(lx, ly, lt, ls, kernel=1)
+    u, R = rand_links(L, rng), rand_spinor(L, rng)
+    c = O.zolo_coeffs(ls)
+    with thirring.Lattice(lx, ly, lt, ls, kernel=1) as G:
+        assert np.array_equal(G.zolo(), c)
+        for dag in (False, True):
+            ref = (O.odslashd if dag else O.odslash)(L, R, u, 0.03, imass, c)
+            got = (G.odslashd if dag else G.odslash)(R, u, 0.03, imass)
+            e = rel_err(interior(got), interior(ref))
+            assert e <= TOL, (dag, e)
+
+
+@pytest.mark.gpu
+def test_odslash_prep_zolo_and_adjoint():
+    rng = np.random.default_rng(17)
+    L = O.lat(4, 4, 6, 8, kernel=1)
+    u, a, b = rand_links(L, rng), rand_spinor(L, rng), rand_spinor(L, rng)
+    c = O.zolo_coeffs(8, 0.05, 8.0)
+    with thirring.Lattice(4, 4, 6, 8, kernel=1) as G:
+        G.prep_zolo(0.05, 8.0)
+        assert np.array_equal(G.zolo(), c)
+        Ma = G.odslash(b, u, 0.05, 3)
+        assert rel_err(interior(Ma), interior(O.odslash(L, b, u, 0.05, 3, c))) <= TOL
+        Mda = G.odslashd(a, u, 0.05, 3)
+        lhs, rhs = _vdot(a, Ma), _vdot(Mda, b)
+        assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("imass", [1, 3])
+@pytest.mark.parametrize("dims", [(6, 6, 4, 4), (4, 4, 6, 6)])
+def test_congrad_o_vs_oracle(imass, dims):
+    lx, ly, lt, ls = dims
+    rng = np.random.default_rng(23 + imass)
+    L = O.lat(lx, ly, lt, ls, kernel=1)
+    u, Phi = rand_links(L, rng, beta=SOLVE["beta"]), rand_spinor(L, rng)
+    c = O.zolo_coeffs(ls, SOLVE["lmin"], SOLVE["lmax"])
+    am, res = SOLVE["am"], SOLVE["res"]
+    Xr, itr, nxr = O.congrad_o(L, Phi, u, res, am, imass, c)
+    with thirring.Lattice(lx, ly, lt, ls, kernel=1) as G:
+        G.prep_zolo(SOLVE["lmin"], SOLVE["lmax"])
+        G.set_links(u)
+        X, it, nx = G.congrad_o(Phi, res, am, imass)
+    assert abs(it - itr) <= 2 and nx == it, (it, itr, nx)
+    assert rel_err(interior(X), interior(Xr)) <= 1e-5
+    # the true residual meets the stopping rule (|r|^2 < 4 V Ls res^2), with room for rounding
+    Xh = O.update_halo_5(L, X.copy(order="F"))
+    y = O.odslashd(L, O.update_halo_5(L, O.odslash(L, Xh, u, am, imass, c)), u, am, imass, c)
+    r2 = float(np.sum(np.abs(interior(y) - interior(Phi)) ** 2))
+    assert r2 <= 4.0 * 4 * lx * ly * lt * ls * res * res
+
+
+@pytest.mark.gpu
+def test_congrad_o_start_already_converged():
+    L = O.lat(4, 4, 4, 4, kernel=1)
+    rng = np.random.default_rng(3)
+    u = rand_links(L, rng)
+    Phi = O.spinor(L)
+    with thirring.Lattice(4, 4, 4, 4, kernel=1) as G:
+        G.set_links(u)
+        X, it, nx = G.congrad_o(Phi, 1e-6, 0.05, 1)
+    assert it == 0 and nx == 0 and not np.any(interior(X))

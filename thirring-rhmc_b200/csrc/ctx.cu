@@ -206,6 +206,7 @@ int thr_destroy(thr_ctx* c) {
   cudaFree(c->stage);
   cudaFree(c->stage2);
   cudaFree(c->partials);
+  cudaFree(c->zolo_dev);
   cudaFree(c->dscal);
   cudaFree(c->iscal);
   if (c->hscal) cudaFreeHost(c->hscal);

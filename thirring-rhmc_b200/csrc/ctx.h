@@ -87,6 +87,10 @@ struct thr_ctx {
   // so each kernel starts on the sites its predecessor wrote last
   int rev_sweep = 2;
   int overlap_flush = 1;     // batched multishift flushes on the side stream (THR_OVERLAP=0: in line)
+  // measure_OWilson's coeffs(1:Ls) (prepZolo) and their device copy
+  std::vector<double> zolo;
+  double* zolo_dev = nullptr;
+  bool zolo_dirty = false;
   double md_counts[8] = {};  // ancg, ancgpv, ancgf, ancgfpv, ancgh, ancghpv, ancgpf, ancgpfpv
   void* bufs[B_COUNT] = {};
   size_t buf_bytes[B_COUNT] = {};

@@ -274,6 +274,112 @@ __device__ __forceinline__ void wilson_site(const S* __restrict__ in, const type
   }
 }
 
+// ---------------------------------------------------------------- overlap
+// The Zolotarev domain-wall operator of measure_OWilson.F90 (odslash :14-89,
+// odslashd :91-167): the Wilson-kernel operator with slice s's 3D Wilson term
+// D_W = DWilson(-am3) scaled by its coefficient c[s] (prepZolo, :169-188) and
+// the imass 3 walls of the opposite sign.  By linearity
+//   M:      Phi(s) = c[s] D_W Q(s) + 2 R(s) - Q(s),
+//           Q(s) = R(s) + P- R(s+1) + P+ R(s-1)   (walls: m1 P+ R(Ls) into s = 1,
+//           m2 P- R(1) into s = Ls; m1 = -am | +i am, m2 = -am | -i am)
+//   M^dag:  Phi(s)[P+] = D_W^dag(c[s] R(s) + c[s+1] R(s+1)) + R(s) - R(s+1)
+//           (s = Ls: c[Ls] R(Ls) + z2 c[1] R(1), non-D part R(Ls) - z2 R(1), z2 = -am | -i am)
+//           Phi(s)[P-] = D_W^dag(c[s] R(s) + c[s-1] R(s-1)) + R(s) - R(s-1)
+//           (s = 1: c[1] R(1) + z1 c[Ls] R(Ls), non-D part R(1) - z1 R(Ls), z1 = -am | +i am)
+// (1-based slices as in the reference).  One thread per 5D site, FP64.
+__device__ __forceinline__ void overlap_qd(const SpinorView<double2>& Rv, int s, int site, int sn, bool inner, int swall,
+                                           double a, double b, double2 zb, double2* q) {
+#pragma unroll
+  for (int d = 0; d < 4; d++)
+    q[d] = inner ? a * Rv(s, site, d) + b * Rv(sn, site, d) : a * Rv(s, site, d) + cmul(zb, Rv(swall, site, d));
+}
+
+template <bool DAG>
+__device__ __forceinline__ void overlap_site(const double2* __restrict__ in, const double2* __restrict__ u,
+                                             const Geom& g, int s, int site, float am, int imass, float am3,
+                                             const double* __restrict__ zc, double2* res) {
+  using C = double2;
+  using R = double;
+  int x, y, t;
+  site_coords(g, site, x, y, t);
+  const Nbr nb = neighbours(g, site, x, y, t);
+  SpinorView<double2> Rv{in, g};
+  const int Ls = g.ls;
+  const R a = (R)am;
+  const R dgw = (R)(3.0f + (-am3));  // DWilson(..., -am3) diagonal: dirac.F90:191, :505
+  const R cs = __ldg(zc + s);
+  if (!DAG) {
+    const C m1 = imass == 1 ? mk(-a, R(0)) : mk(R(0), a);   // measure_OWilson.F90:66-71
+    const C m2 = imass == 1 ? mk(-a, R(0)) : mk(R(0), -a);  // :78-83
+    C q[4];
+    wilson_q<double2>(Rv, s, site, Ls, m1, m2, q);
+#pragma unroll
+    for (int d = 0; d < 4; d++) res[d] = (cs * dgw - R(1)) * q[d] + R(2) * Rv(s, site, d);
+#pragma unroll
+    for (int mu = 0; mu < 3; mu++) {
+      const C U = cs * __ldg(u + (size_t)mu * g.v3 + site);
+      const C Ub = cs * cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
+      wilson_q<double2>(Rv, s, nb.f[mu], Ls, m1, m2, q);
+      hop_projected<C, R>(mu, true, U, q, res);
+      wilson_q<double2>(Rv, s, nb.b[mu], Ls, m1, m2, q);
+      hop_projected<C, R>(mu, false, Ub, q, res);
+    }
+  } else {
+    const C z1 = imass == 1 ? mk(-a, R(0)) : mk(R(0), a);   // upper right, measure_OWilson.F90:139-144
+    const C z2 = imass == 1 ? mk(-a, R(0)) : mk(R(0), -a);  // lower left, :152-157
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      // half 0: output spins 0,1 from slice s+1 (wall: slice 0 with z2); half 1: spins 2,3 from s-1 (wall: Ls-1, z1)
+      const bool inner = half == 0 ? (s < Ls - 1) : (s > 0);
+      const int sn = half == 0 ? s + 1 : s - 1;
+      const int sw = half == 0 ? 0 : Ls - 1;
+      const C zz = half == 0 ? z2 : z1;
+      const R cn = __ldg(zc + (inner ? sn : sw));
+      const C zb = cn * zz;
+      C q[4];
+      overlap_qd(Rv, s, site, sn, inner, sw, cs, cn, zb, q);
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        const int d = 2 * half + k;
+        const C xo = inner ? Rv(sn, site, d) : cmul(zz, Rv(sw, site, d));
+        res[d] = dgw * q[d] + Rv(s, site, d) - xo;
+      }
+#pragma unroll
+      for (int mu = 0; mu < 3; mu++) {
+        const C U = __ldg(u + (size_t)mu * g.v3 + site);
+        const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
+#pragma unroll
+        for (int dir = 0; dir < 2; dir++) {
+          overlap_qd(Rv, s, dir == 0 ? nb.f[mu] : nb.b[mu], sn, inner, sw, cs, cn, zb, q);
+          const C W = dir == 0 ? U : Ub;
+#pragma unroll
+          for (int k = 0; k < 2; k++) {
+            const int d = 2 * half + k;
+            const GammaEntry ge = gamma_entry(mu, d);
+            const C gq = gp(ge, q[ge.gin]);
+            res[d] = res[d] - R(0.5) * cmul(W, dir == 0 ? q[d] + gq : q[d] - gq);
+          }
+        }
+      }
+    }
+  }
+}
+
+// odslash / odslashd on one lattice: blockDim = (Ls, sites per block) as the Wilson kernel's
+template <bool DAG>
+__global__ void __launch_bounds__(256, 1)
+    k_odslash(double2* __restrict__ out, const double2* __restrict__ in, const double2* __restrict__ u, Geom g,
+              float am, int imass, float am3, const double* __restrict__ zc, const int* skip) {
+  if (skip && *skip) return;
+  const int s = threadIdx.x;
+  const int site = blockIdx.x * blockDim.y + threadIdx.y;
+  if (site >= g.v3) return;
+  double2 acc[4];
+  overlap_site<DAG>(in, u, g, s, site, am, imass, am3, zc, acc);
+#pragma unroll
+  for (int d = 0; d < 4; d++) Sto<double2>::st(out, sidx32(g, s, site, d), acc[d]);
+}
+
 template <class S, int KER, bool DAG, bool SHFL = false>
 __device__ __forceinline__ void apply_site(const S* in, const typename Sto<S>::C* u, const Geom& g, int s, int site,
                                            float am, int imass, float am3, typename Sto<S>::C* acc) {
@@ -717,6 +823,18 @@ int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, cons
                   int imass, float am3, cudaStream_t st, const int* skip) {
   return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr, nullptr, 0,
                                0);
+}
+
+int launch_odslash(const Geom& g, bool dag, double2* out, const double2* in, const double2* u, float am, int imass,
+                   float am3, const double* zc, cudaStream_t st, const int* skip) {
+  if (g.ls > 1024) return THR_ERR_BADSHAPE;
+  if (4ULL * (unsigned long long)g.v5 >= (1ULL << 32)) return THR_ERR_BADSHAPE;  // 32-bit element offsets
+  if (imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // measure_OWilson.F90:66-83
+  const dim3 blk = stencil_block(g, 1);
+  const dim3 grd(stencil_grid(g, 1));
+  if (dag) k_odslash<true><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, zc, skip);
+  else k_odslash<false><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, zc, skip);
+  return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
 
 template <class S>

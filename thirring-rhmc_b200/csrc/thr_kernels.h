@@ -28,6 +28,10 @@ int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in,
                        float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials,
                        int rev = 0);
 
+// odslash / odslashd (measure_OWilson.F90:14-167), FP64, with the slice coefficients zc[0..Ls-1] on the device
+int launch_odslash(const Geom& g, bool dag, double2* out, const double2* in, const double2* u, float am, int imass,
+                   float am3, const double* zc, cudaStream_t st, const int* skip = nullptr);
+
 // layout.cu: Fortran halo'd host layout <-> device fields
 // spinor (0:Ls+1,0:Lx+1,0:Ly+1,0:Lt+1,4) complex(dp)  <-> S[4][V3][Ls]
 template <class S>

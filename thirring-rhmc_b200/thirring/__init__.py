@@ -9,4 +9,5 @@ GPU; errors are raised as ThirringError with the library's status code.
 """
 from ._lib import LibraryMissing, header_functions, lib  # noqa: F401
 from .api import (CON_MPIIO, CON_SERIAL, Lattice, Pack, ThirringError, TrajResult, field3, links,  # noqa: F401
-                  ps_field, read_con, read_remez_file, readseed, remez_set, saveseed, shift_out, spinor, write_con)
+                  ps_field, read_con, read_remez_file, readseed, remez_set, saveseed, shift_out, spinor, write_con,
+                  zolo_coeffs)

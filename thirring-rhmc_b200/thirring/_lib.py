@@ -55,6 +55,13 @@ SIGNATURES = {
     "thr_fermion": (_i, [_v, _f, _f, _i, _i, _i, _v, _v, _pi, C.POINTER(C.c_float)]),
     "thr_measure": (_i, [_v, _i, _f, _f, _i, _i, _i, C.POINTER(C.c_float), C.POINTER(C.c_float),
                          C.POINTER(C.c_float), _v, _v]),
+    "thr_zolo_coeffs": (_i, [_i, _d, _d, _v]),
+    "thr_prep_zolo": (_i, [_v, _d, _d]),
+    "thr_zolo_get": (_i, [_v, _v]),
+    "thr_odslash": (_i, [_v, _v, _v, _v, _f, _i]),
+    "thr_odslashd": (_i, [_v, _v, _v, _v, _f, _i]),
+    "thr_congrad_o": (_i, [_v, _v, _v, _f, _pi, _f, _i, _pi]),
+    "thr_odslash_dev": (_i, [_v, _v, _v, _f, _i, _i]),
     "thr_multishift_solver": (_i, [_v, _v, _f, _i, _i, _v, _v, _v, _v, _f, _i, _pi, _v]),
     "thr_multishift_solver_sp": (_i, [_v, _v, _f, _i, _i, _v, _v, _v, _v, _f, _i, _pi, _v]),
     "thr_qmrherm": (_i, [_v, _v, _v, _f, _pi, _f, _i, _v, _v, _i, _i, _i, _v, _v, _v, _i]),

@@ -176,6 +176,13 @@ def _need(a, shape, dtype, name):
                          f"{a.dtype} {a.shape}")
 
 
+def zolo_coeffs(ls, lmin=0.1, lmax=5.0):
+    """coeffs(1:ls) of prepZolo (measure_OWilson.F90:169-188); host only."""
+    c = np.zeros(ls)
+    _check(_lib.lib().thr_zolo_coeffs(ls, lmin, lmax, _p(c)), "zolo_coeffs")
+    return c
+
+
 class Lattice:
     """One lattice (sizes, kernel, layout) bound to one GPU context."""
 
@@ -255,6 +262,47 @@ class Lattice:
         Phi = out if out is not None else spinor(self)
         _check(self._L.thr_dslashd(self.h, _p(Phi), _p(R), _p(u), am, imass), "dslashd")
         return Phi
+
+    # ---- measure_OWilson.F90
+    def prep_zolo(self, lmin=0.1, lmax=5.0):
+        """prepZolo (measure_OWilson.F90:169-188) on [lmin, lmax] for this Ls."""
+        _check(self._L.thr_prep_zolo(self.h, lmin, lmax), "prep_zolo")
+
+    def zolo(self):
+        """The context's coeffs(1:Ls)."""
+        c = np.zeros(self.ls)
+        _check(self._L.thr_zolo_get(self.h, _p(c)), "zolo_get")
+        return c
+
+    def odslash(self, R, u, am, imass, out=None):
+        """Phi = M_ov R  (odslash, measure_OWilson.F90:14-89).  u=None: current links."""
+        _need(R, self.sshape, np.complex128, "R")
+        if u is not None:
+            _need(u, self.ushape, np.complex128, "u")
+        Phi = out if out is not None else spinor(self)
+        _check(self._L.thr_odslash(self.h, _p(Phi), _p(R), _p(u), am, imass), "odslash")
+        return Phi
+
+    def odslashd(self, R, u, am, imass, out=None):
+        """Phi = M_ov^dagger R  (odslashd, measure_OWilson.F90:91-167)."""
+        _need(R, self.sshape, np.complex128, "R")
+        if u is not None:
+            _need(u, self.ushape, np.complex128, "u")
+        Phi = out if out is not None else spinor(self)
+        _check(self._L.thr_odslashd(self.h, _p(Phi), _p(R), _p(u), am, imass), "odslashd")
+        return Phi
+
+    def congrad_o(self, Phi, res, am, imass):
+        """congradO (measure_OWilson.F90:190-268) on the current links: returns
+        (X, itercg, iterations); X starts from Phi."""
+        _need(Phi, self.sshape, np.complex128, "Phi")
+        X = spinor(self)
+        it = C.c_int(0)
+        nx = C.c_int(0)
+        rc = self._L.thr_congrad_o(self.h, _p(Phi), _p(X), res, C.byref(it), am, imass, C.byref(nx))
+        if rc not in (0, 3):
+            _check(rc, "congrad_o")
+        return X, it.value, nx.value
 
     # ---- random.f90 / site_random.f90 / gaussian.F90
     def init_random(self, seed, site=True):
