@@ -159,7 +159,10 @@ int thr_pack_get_stream(thr_pack *pack, void **stream);
  * links with the context's random numbers.  kernel_meas selects the
  * measurement routine the reference picks at compile time: 0 = measure_shamir
  * (:170-423, MEASURE_SHAMIR), 1 = measure_wilson (:431-670, MEASURE_WILSON;
- * imass 1 or 3).  congrad runs on the context's (generation) kernel, as in the
+ * imass 1 or 3), 2 = measure_wilsonKDDW (measure_OWilson.F90:646-673,
+ * MEASURE_OWILSON; imass 1 or 3, THR_FP64 only): per noise four gauss0 draws,
+ * each through IKDDW4 with congradO at res (the reference passes params.F90
+ * respbp = 1e-6 there); parts[4n..4n+1] = Re/Im of the noise's pbp, aviter 0.  congrad runs on the context's (generation) kernel, as in the
  * reference.  knoise = params.F90 knoise (10 in the reference).  All
  * 4*knoise (Shamir) or 8*knoise (Wilson) solves run as one batched congrad
  * (precision: thr_precision; THR_FP64 is the reference's arithmetic).

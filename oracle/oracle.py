@@ -476,6 +476,83 @@ def measure(L, g, u, res, am, imass, kernel_meas=0, knoise=10):
                 pbp=pbp, itercg=its)
 
 
+def permm(L, R, dagger):
+    """PermM (measure_OWilson.F90:546-576) on halo'd 5D arrays, slices 1..Ls:
+    PR(l) = P- R(l) + P+ R(l+1) with R(Ls+1) -> R(1); dagger: P+ R(l-1) with
+    R(0) -> R(Ls).  P+ = spins 1,2 (Pplus :524-533), P- = spins 3,4 (:535-544)."""
+    Ls = L.ls
+    PR = spinor(L)
+    PR[1:Ls + 1, :, :, :, 2:4] = R[1:Ls + 1, :, :, :, 2:4]
+    for l in range(1, Ls + 1):
+        if not dagger:
+            tgt = Ls if l == 1 else l - 1
+        else:
+            tgt = 1 if l == Ls else l + 1
+        PR[tgt, :, :, :, 0:2] += R[l, :, :, :, 0:2]
+    return PR
+
+
+def iddw(L, u, R, mass, imass, coeffs, respbp):
+    """IDDW (measure_OWilson.F90:270-289): congradO(odslashd R) = DDW^-1 R; (X, itercg)."""
+    IDR = update_halo_5(L, odslashd(L, R, u, mass, imass, coeffs))
+    X, itc, _ = congrad_o(L, IDR, u, respbp, mass, imass, coeffs)
+    return X, itc
+
+
+def kddw(L, u, R, bmass, imass, coeffs, respbp):
+    """KDDW (:342-367): PermM^dag . DDW(1)^-1 . DDW(bmass) . PermM R."""
+    DR = update_halo_5(L, odslash(L, permm(L, R, False), u, bmass, imass, coeffs))
+    X, _ = iddw(L, u, DR, 1.0, 1, coeffs, respbp)
+    return permm(L, X, True)
+
+
+def ikddw(L, u, R, bmass, imass, coeffs, respbp):
+    """IKDDW (:369-393): PermM^dag . DDW(bmass)^-1 . DDW(1) . PermM R; (result, itercg)."""
+    DR = update_halo_5(L, odslash(L, permm(L, R, False), u, 1.0, 1, coeffs))
+    X, itc = iddw(L, u, DR, bmass, imass, coeffs, respbp)
+    return permm(L, X, True), itc
+
+
+def measure_ow(L, g, u, respbp, bmass, imass, coeffs, knoise=10):
+    """measure_wilsonKDDW (measure_OWilson.F90:646-673, the MEASURE_OWILSON branch
+    of measure, measure_module.F90:158-160): per noise evalSingleCondNoise_KDDW4
+    (:704-757) -- for idx = 1..4 gauss0(ps), eta = cmplx(ps) on spin idx, IKDDW4
+    (:462-478: eta on the slice s = 1 of a 5D field, IKDDW :369-393 = PermM^dag .
+    IDDW(bmass) . odslash(mass 1, imass 1) . PermM, with IDDW :270-289 = congradO
+    (respbp) of odslashd(bmass)), trace conj(eta) (IKDDW4 eta - eta) over spin idx
+    divided by 1 - bmass (imass 1) or (-bmass, +-1) (imass 3), / kvol.
+    psibarpsi = sum Re(pbp) / knoise, susclsing as output_OW (:674-702), aviter 0."""
+    kvol = L.lx * L.ly * L.lt
+    vpbp, cpbp, its = [], [], []
+    for n in range(knoise):
+        pbp = 0j
+        for idx in range(4):
+            ps = g.gauss0()
+            eta = np.zeros((L.lx + 2, L.ly + 2, L.lt + 2, 4), np.complex128, order="F")
+            eta[:, :, :, idx] = ps[:, :, :, 0].astype(np.float64) + 1j * ps[:, :, :, 1].astype(np.float64)
+            R5 = spinor(L)
+            R5[1] = eta  # IKDDW4 (:462-478)
+            DR5, itc = ikddw(L, u, R5, bmass, imass, coeffs, respbp)
+            its.append(itc)
+            DR4 = DR5[1]
+            tr = np.sum((np.conj(eta) * (DR4 - eta))[1:-1, 1:-1, 1:-1, idx])
+            if imass == 1:
+                denom = complex(float(np.float32(1.0) - np.float32(bmass)), 0.0)
+            else:
+                denom = complex(-float(np.float32(bmass)), 1.0 if idx < 2 else -1.0)
+            pbp += tr / denom
+        pbp = pbp / kvol
+        cpbp.append(pbp)
+        vpbp.append(pbp.real)
+    vp = np.array(vpbp)
+    psibarpsi = np.float32(np.sum(vp) / knoise)
+    sus = np.float32(0.0)
+    for n in range(knoise):
+        sus = np.float32(sus + np.float32(np.sum(vp[n] * vp[n + 1:])))
+    sus = np.float32(np.float32(2 * kvol) * sus / np.float32(knoise * (knoise - 1)))
+    return dict(psibarpsi=float(psibarpsi), susclsing=float(sus), aviter=0.0, cpbp=cpbp, itercg=its)
+
+
 def _wall_props(L, u, xi_src, res, am, imass):
     """measure_module.F90:811-826 (and :1162-1177): Phi = M^dagger xi, the initial
     guess M^dagger Phi, congrad; returns (itercg, solution)."""

@@ -160,3 +160,46 @@ def test_congrad_o_start_already_converged():
         G.set_links(u)
         X, it, nx = G.congrad_o(Phi, 1e-6, 0.05, 1)
     assert it == 0 and nx == 0 and not np.any(interior(X))
+
+
+# ---------------------------------------------------------------- overlap measurement
+def test_oracle_permm_and_ikddw_identities():
+    """The reference's own checks TEST_PermM (measure_OWilson.F90:578-602) and
+    TEST_IKDDW (:395-421): PermM^dag PermM = 1 exactly, IKDDW KDDW = 1 to the
+    solver's tolerance (bmass 0.01, imass 3 as there; coefficients on [0.5, 5]
+    so that congradO converges on a small lattice)."""
+    rng = np.random.default_rng(29)
+    L = O.lat(6, 6, 4, 4, kernel=1)
+    u, R = rand_links(L, rng, beta=SOLVE["beta"]), rand_spinor(L, rng)
+    assert np.array_equal(interior(O.permm(L, O.permm(L, R, False), True)), interior(R))
+    c = O.zolo_coeffs(4, SOLVE["lmin"], SOLVE["lmax"])
+    K = O.update_halo_5(L, O.kddw(L, u, R, 0.01, 3, c, 1e-9))
+    F, _ = O.ikddw(L, u, K, 0.01, 3, c, 1e-9)
+    assert rel_err(interior(F), interior(R)) <= 1e-7
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("imass", [1, 3])
+def test_measure_ow_vs_oracle(imass):
+    """measure with kernel_meas = 2 (measure_wilsonKDDW) against the oracle on the
+    same links and site random streams: each congradO within 2 iterations, each
+    noise's pbp to 1e-6 relative (both solutions meet the stopping rule)."""
+    dims = (6, 6, 4, 4)
+    L = O.lat(*dims, kernel=1)
+    u = rand_links(L, np.random.default_rng(50 + imass), beta=SOLVE["beta"])
+    seed, knoise, respbp = 4139764973254.0, 3, 1e-6
+    c = O.zolo_coeffs(4, SOLVE["lmin"], SOLVE["lmax"])
+    g = O.RNG(L, True).init(seed)
+    ref = O.measure_ow(L, g, u, respbp, SOLVE["am"], imass, c, knoise=knoise)
+    with thirring.Lattice(*dims, kernel=1) as G:
+        G.prep_zolo(SOLVE["lmin"], SOLVE["lmax"])
+        G.set_links(u)
+        G.init_random(seed)
+        got = G.measure(respbp, SOLVE["am"], imass, kernel_meas=2, knoise=knoise)
+    assert np.all(np.abs(np.array(got["itercg"]) - np.array(ref["itercg"])) <= 2)
+    want = np.array([[p.real, p.imag] for p in ref["cpbp"]])
+    scale = np.max(np.abs(want[:, 0]))
+    assert np.max(np.abs(got["parts"][:, :2] - want)) <= 1e-6 * scale
+    assert not np.any(got["parts"][:, 2:])
+    assert abs(got["psibarpsi"] - ref["psibarpsi"]) <= 1e-5 * abs(ref["psibarpsi"])
+    assert got["aviter"] == 0.0

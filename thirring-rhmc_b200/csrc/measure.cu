@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "ctx.h"
+#include "overlap.h"
 #include "rng.h"
 
 namespace thr {
@@ -199,6 +200,12 @@ extern "C" {
 int thr_measure(thr_ctx* c, int kernel_meas, float res, float am, int imass, int knoise, int precision,
                 float* psibarpsi, float* susclsing, float* aviter, double* parts, int* itercg) {
   if (!c || !psibarpsi || !susclsing || !aviter || knoise < 1) return THR_ERR_BADARG;
+  if (kernel_meas == 2) {  // measure_wilsonKDDW, FP64 only
+    if (precision != THR_FP64) return THR_ERR_UNSUPPORTED;
+    if (!c->links_ok || !c->rng.ready) return THR_ERR_BADARG;
+    cudaSetDevice(c->dev);
+    return measure_ow(c, res, am, imass, knoise, psibarpsi, susclsing, aviter, parts, itercg);
+  }
   if (kernel_meas != 0 && kernel_meas != 1) return THR_ERR_BADARG;
   if (imass != 1 && imass != 3 && imass != 5) return THR_ERR_BADARG;
   if (kernel_meas == 1 && imass == 5) return THR_ERR_UNSUPPORTED;  // measure_wilson has no imass 5 branch

@@ -17,7 +17,11 @@
 #include <cmath>
 #include <vector>
 
+#include <algorithm>
+
 #include "ctx.h"
+#include "overlap.h"
+#include "rng.h"
 #include "thr_reduce.cuh"
 
 namespace thr {
@@ -262,6 +266,144 @@ int congrad_o_dev(thr_ctx* c, const double2* phi, double2* X, float res, float a
   if (itercg) *itercg = h.itercg;
   if (iterations) *iterations = h.iters;
   return h.status ? h.status : THR_OK;
+}
+
+// ---------------------------------------------------------------- overlap measurement
+// measure_wilsonKDDW (measure_OWilson.F90:646-673), the MEASURE_OWILSON branch of
+// measure (measure_module.F90:158-160).  Per noise, evalSingleCondNoise_KDDW4
+// (:704-757) draws gauss0 four times; the draw idx becomes eta on spin idx of the
+// slice s = 1 of a 5D field (IKDDW4, :462-478) and
+//   IKDDW = PermM^dag . IDDW(bmass) . odslash(mass 1, imass 1) . PermM   (:369-393)
+//   IDDW(m) R = congradO(odslashd(m) R) at respbp                       (:270-289)
+// is applied; the trace of conj(eta) (result - eta) over spin idx of the slice,
+// divided by 1 - bmass (imass 1) or (-bmass, +-1) (imass 3), summed over idx and
+// divided by kvol is the noise's psibarpsi.
+namespace {
+constexpr int kOwThreads = 256;
+
+// R5 = 0 except slice 0, spin d: cmplx(ps(:,:,:,1), ps(:,:,:,2)) (:722-724)
+__global__ void k_ow_source(double2* R5, const float* __restrict__ ps, Geom g, int d) {
+  const int site = blockIdx.x * blockDim.x + threadIdx.x;
+  if (site >= g.v3) return;
+  R5[sidx(g, 0, site, d)] = make_double2((double)ps[site], (double)ps[g.v3 + site]);
+}
+// PermM (:546-576): out(s) = P- in(s) + P+ in(s+1) (s+1 past the last slice -> the
+// first); dag: P+ in(s-1) (before the first -> the last).  P+ = spins 0,1.
+__global__ void k_permm(double2* __restrict__ out, const double2* __restrict__ in, Geom g, int dag) {
+  const size_t n = (size_t)g.ls * g.v3;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int s = (int)(e % g.ls);
+    const int site = (int)(e / g.ls);
+    const int sp = dag ? (s == 0 ? g.ls - 1 : s - 1) : (s == g.ls - 1 ? 0 : s + 1);
+#pragma unroll
+    for (int d = 0; d < 4; d++) out[sidx(g, s, site, d)] = in[sidx(g, d < 2 ? sp : s, site, d)];
+  }
+}
+// partials per block of conj(eta) (DR(slice 0, spin d) - eta) (:725-747)
+__global__ void __launch_bounds__(kOwThreads) k_ow_contract(const double2* __restrict__ DR, const float* __restrict__ ps,
+                                                            Geom g, int d, double2* __restrict__ partials) {
+  const int site = blockIdx.x * blockDim.x + threadIdx.x;
+  double2 acc = make_double2(0.0, 0.0);
+  if (site < g.v3) {
+    const double2 eta = make_double2((double)ps[site], (double)ps[g.v3 + site]);
+    acc = cjmul(eta, DR[sidx(g, 0, site, d)] - eta);
+  }
+  __shared__ double2 sh[kOwThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
+    acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
+  }
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double2 v = sh[0];
+    for (int w = 1; w < kOwThreads / 32; w++) v = v + sh[w];
+    partials[blockIdx.x] = v;
+  }
+}
+}  // namespace
+
+int measure_ow(thr_ctx* c, float respbp, float bmass, int imass, int knoise, float* psibarpsi, float* susclsing,
+               float* aviter, double* parts, int* itercg) {
+  if (imass != 1 && imass != 3) return THR_ERR_BADARG;  // evalSingleCondNoise_KDDW4 :733-741
+  const Geom& g = c->g;
+  const double* zc = nullptr;
+  THR_TRY(zolo_device(c, &zc));
+  THR_TRY(c->ensure_w64(8));
+  double2 *R5 = c->w64[0], *T = c->w64[1], *DR = c->w64[2], *IDR = c->w64[3];
+  const size_t n4 = c->n4();
+  const int nsolve = 4 * knoise;
+  // every draw first, in the reference's order (the solves draw no random numbers)
+  float* eta = nullptr;
+  THR_CUDA(cudaMalloc(&eta, sizeof(float) * 2 * (size_t)g.v3 * nsolve));
+  const unsigned nblk = (unsigned)((g.v3 + kOwThreads - 1) / kOwThreads);
+  double2* part = nullptr;
+  int rc = cudaMalloc(&part, sizeof(double2) * nblk) == cudaSuccess ? THR_OK : THR_ERR_NOMEM;
+  for (int j = 0; !rc && j < nsolve; j++) rc = rng_gauss_dev(c, -1.0f, eta + (size_t)j * 2 * g.v3);
+  const int niterc = g.ls * g.v3;  // params.F90:57
+  std::vector<double2> hp(nblk);
+  std::vector<double2> cpbp(knoise, make_double2(0.0, 0.0));
+  std::vector<int> its(nsolve, 0);
+  size_t pgrid = ((size_t)g.ls * g.v3 + kOwThreads - 1) / kOwThreads;
+  if (pgrid > 148 * 8) pgrid = 148 * 8;
+  for (int j = 0; !rc && j < nsolve; j++) {
+    const int d = j % 4;
+    const float* e = eta + (size_t)j * 2 * g.v3;
+    if (cudaMemsetAsync(R5, 0, n4 * sizeof(double2), c->st) != cudaSuccess) { rc = THR_ERR_CUDA; break; }
+    k_ow_source<<<nblk, kOwThreads, 0, c->st>>>(R5, e, g, d);
+    k_permm<<<(unsigned)pgrid, kOwThreads, 0, c->st>>>(T, R5, g, 0);
+    rc = launch_odslash(g, false, DR, T, c->u64, 1.0f, 1, c->p.am3, zc, c->st);  // DDW(1), mtype 1
+    if (!rc) rc = launch_odslash(g, true, IDR, DR, c->u64, bmass, imass, c->p.am3, zc, c->st);
+    if (rc) break;
+    int it = 0, nx = 0;
+    rc = congrad_o_dev(c, IDR, T, respbp, bmass, imass, niterc, &it, &nx);
+    if (rc == THR_ERR_MAXITER) rc = THR_OK;  // congradO only prints a warning (:250)
+    if (rc) break;
+    its[j] = it;
+    k_permm<<<(unsigned)pgrid, kOwThreads, 0, c->st>>>(DR, T, g, 1);
+    k_ow_contract<<<nblk, kOwThreads, 0, c->st>>>(DR, e, g, d, part);
+    if (cudaMemcpyAsync(hp.data(), part, sizeof(double2) * nblk, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
+        cudaStreamSynchronize(c->st) != cudaSuccess) {
+      rc = THR_ERR_CUDA;
+      break;
+    }
+    double2 tr = make_double2(0.0, 0.0);
+    for (unsigned b = 0; b < nblk; b++) tr = tr + hp[b];
+    // trcomp = sum / denom: denom = one - bmass in default real (imass 1), cmplx(-bmass, +-1) (imass 3)
+    const double dr = imass == 1 ? (double)(1.0f - bmass) : -(double)bmass;
+    const double di = imass == 1 ? 0.0 : (d < 2 ? 1.0 : -1.0);
+    const double dd = dr * dr + di * di;
+    cpbp[j / 4] = cpbp[j / 4] + make_double2((tr.x * dr + tr.y * di) / dd, (tr.y * dr - tr.x * di) / dd);
+  }
+  cudaFree(eta);
+  cudaFree(part);
+  if (rc) return rc;
+  const double kvol = (double)g.v3;
+  std::vector<double> vpbp(knoise);
+  for (int n = 0; n < knoise; n++) {
+    const double2 p = make_double2(cpbp[n].x / kvol, cpbp[n].y / kvol);
+    vpbp[n] = p.x;
+    if (parts) {
+      parts[4 * n + 0] = p.x;
+      parts[4 * n + 1] = p.y;
+      parts[4 * n + 2] = 0.0;
+      parts[4 * n + 3] = 0.0;
+    }
+  }
+  double sum = 0.0;
+  for (int n = 0; n < knoise; n++) sum += vpbp[n];
+  float sus = 0.0f;  // output_OW (:683-687)
+  for (int n = 0; n < knoise; n++) {
+    double sv = 0.0;
+    for (int m = n + 1; m < knoise; m++) sv += vpbp[n] * vpbp[m];
+    sus = sus + (float)sv;
+  }
+  *psibarpsi = (float)(sum / knoise);  // pbp = sum(vpbp)/knoise (:669)
+  *susclsing = (float)(2 * g.v3) * sus / (float)(knoise * (knoise - 1));
+  *aviter = 0.0f;  // "not currently calculated" (:671)
+  if (itercg) std::copy(its.begin(), its.end(), itercg);
+  return THR_OK;
 }
 
 }  // namespace thr

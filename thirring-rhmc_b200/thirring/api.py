@@ -398,8 +398,12 @@ class Lattice:
         """measure(psibarpsi, res, aviter, am, imass), measure_module.F90:142-162,
         on the current links and random numbers.  Returns a dict with psibarpsi,
         susclsing, aviter (float32 values), parts (knoise x [Re p1, Im p1, Re p2,
-        Im p2], the fort.100 columns) and itercg (one per solve)."""
-        per = 4 if kernel_meas == SHAMIR else 8
+        Im p2], the fort.100 columns) and itercg (one per solve).
+        kernel_meas = 2 is measure_wilsonKDDW (the overlap operator,
+        measure_OWilson.F90:646-673): res is then congradO's residual (the
+        reference's params.F90 respbp = 1e-6), parts[n] = [Re pbp, Im pbp, 0, 0],
+        four solves per noise and aviter 0 as in the reference."""
+        per = 8 if kernel_meas == 1 else 4
         pb, sus, av = C.c_float(0), C.c_float(0), C.c_float(0)
         parts = np.zeros((knoise, 4), np.float64)
         its = np.zeros(per * knoise, np.int32)
