@@ -209,11 +209,13 @@ __global__ void __launch_bounds__(kFlushThreads, kFlushBlocks)
   const int lo = cf->lo, hi = cf->hi;  // lo > hi: no shift active in the batch
   if (lo > hi) return;
   // the maps of the window's shifts (the only rows read below)
-  __shared__ R s_A[kMaxShift], s_P[kMaxShift], s_B[kMaxShift][kBatch], s_Q[kMaxShift][kBatch];
+  // B and Q of a (shift, step) side by side: one 16-byte (FP64) shared load per term of the FMA chains
+  using R2 = typename Sto<V>::C;
+  __shared__ R s_A[kMaxShift], s_P[kMaxShift];
+  __shared__ R2 s_BQ[kMaxShift][kBatch];
   for (int t = threadIdx.x; t < (hi - lo + 1) * kBatch; t += blockDim.x) {
     const int k = lo + t / kBatch, i = t % kBatch;
-    s_B[k][i] = (R)cf->B[k][i];
-    s_Q[k][i] = (R)cf->Q[k][i];
+    s_BQ[k][i] = mk((R)cf->B[k][i], (R)cf->Q[k][i]);
     if (i == 0) {
       s_A[k] = (R)cf->A[k];
       s_P[k] = (R)cf->P[k];
@@ -239,8 +241,9 @@ __global__ void __launch_bounds__(kFlushThreads, kFlushBlocks)
 #pragma unroll
       for (int j = 0; j < kBatch; j++) {
         if (j < ns) {
-          f = f + s_B[k][j] * rj[j];
-          o = o - s_Q[k][j] * rj[j];
+          const R2 bq = s_BQ[k][j];
+          f = f + bq.x * rj[j];
+          o = o - bq.y * rj[j];
         }
       }
       sf[k * stride + i] = f;
