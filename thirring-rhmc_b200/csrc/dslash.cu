@@ -192,14 +192,6 @@ __device__ __forceinline__ void wilson_q(const SpinorView<S>& Rv, int s, int sit
   for (int d = 2; d < 4; d++) q[d] = (s < Ls - 1) ? r[d] + Rv(s + 1, site, d) : r[d] + cmul(c2, Rv(0, site, d));
 }
 
-// Q for the adjoint: all four spins of R(s) + (inner ? R(s+ds) : z * R(wall))
-template <class S>
-__device__ __forceinline__ void wilson_qd(const SpinorView<S>& Rv, int s, int site, int sn, bool inner, int swall,
-                                          typename Sto<S>::C z, typename Sto<S>::C* q) {
-#pragma unroll
-  for (int d = 0; d < 4; d++) q[d] = inner ? Rv(s, site, d) + Rv(sn, site, d) : Rv(s, site, d) + cmul(z, Rv(swall, site, d));
-}
-
 template <class S, bool DAG>
 __device__ __forceinline__ void wilson_site(const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u,
                                             const Geom& g, int s, int site, float am, int imass, float am3,
@@ -236,38 +228,45 @@ __device__ __forceinline__ void wilson_site(const S* __restrict__ in, const type
     // z = -am | -i am (upper right, dirac.F90:602-606); z' = -am | +i am (lower left, :615-619)
     const C z = imass == 1 ? mk(-a, R(0)) : mk(R(0), -a);
     const C zp = imass == 1 ? mk(-a, R(0)) : mk(R(0), a);
-    // half 0: output spins 0,1 use Qp = R(s) + R(s+1) | z' R(1); half 1: spins 2,3 use Qm = R(s) + R(s-1) | z R(Ls)
+    // half 0: output spins 0,1 use Qp = R(s) + R(s+1) | z' R(1); half 1: spins 2,3 use Qm = R(s) + R(s-1) | z R(Ls).
+    // One pass over the neighbours serves both halves: R(s) and the two partner slices are loaded
+    // once per site (each output element gets the same operations in the same order as half by half)
+    const bool in0 = s < Ls - 1, in1 = s > 0;
+    const int sp0 = in0 ? s + 1 : 0, sp1 = in1 ? s - 1 : Ls - 1;
+    auto qpair = [&](int st, C* q0, C* q1) {
 #pragma unroll
-    for (int half = 0; half < 2; half++) {
-      const bool inner = half == 0 ? (s < Ls - 1) : (s > 0);
-      const int sn = half == 0 ? s + 1 : s - 1;
-      const int sw = half == 0 ? 0 : Ls - 1;
-      const C zz = half == 0 ? zp : z;
-      C q[4];
-      wilson_qd<S>(Rv, s, site, sn, inner, sw, zz, q);
+      for (int d = 0; d < 4; d++) {
+        const C r = Rv(s, st, d), a0 = Rv(sp0, st, d), a1 = Rv(sp1, st, d);
+        q0[d] = in0 ? r + a0 : r + cmul(zp, a0);
+        q1[d] = in1 ? r + a1 : r + cmul(z, a1);
+      }
+    };
+    {
+      C q0[4], q1[4];
+      qpair(site, q0, q1);
 #pragma unroll
       for (int k = 0; k < 2; k++) {
-        const int d = 2 * half + k;
-        res[d] = (dgw - R(1)) * q[d] + R(2) * Rv(s, site, d);
+        res[k] = (dgw - R(1)) * q0[k] + R(2) * Rv(s, site, k);
+        res[2 + k] = (dgw - R(1)) * q1[2 + k] + R(2) * Rv(s, site, 2 + k);
       }
-      // D_W^dagger hops (dirac.F90:511-531): -1/2 W [q(d) +- 2gamma(mu,d) q(gin)], only
-      // the output spins of this half (their partners belong to the other half)
+    }
+    // D_W^dagger hops (dirac.F90:511-531): -1/2 W [q(d) +- 2gamma(mu,d) q(gin)], each half's
+    // output spins from its own Q
 #pragma unroll
-      for (int mu = 0; mu < 3; mu++) {
-        const C U = __ldg(u + (size_t)mu * g.v3 + site);
-        const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
+    for (int mu = 0; mu < 3; mu++) {
+      const C U = __ldg(u + (size_t)mu * g.v3 + site);
+      const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
 #pragma unroll
-        for (int dir = 0; dir < 2; dir++) {
-          C q[4];
-          wilson_qd<S>(Rv, s, dir == 0 ? nb.f[mu] : nb.b[mu], sn, inner, sw, zz, q);
-          const C W = dir == 0 ? U : Ub;
+      for (int dir = 0; dir < 2; dir++) {
+        C q0[4], q1[4];
+        qpair(dir == 0 ? nb.f[mu] : nb.b[mu], q0, q1);
+        const C W = dir == 0 ? U : Ub;
 #pragma unroll
-          for (int k = 0; k < 2; k++) {
-            const int d = 2 * half + k;
-            const GammaEntry ge = gamma_entry(mu, d);
-            const C gq = gp(ge, q[ge.gin]);
-            res[d] = res[d] - R(0.5) * cmul(W, dir == 0 ? q[d] + gq : q[d] - gq);
-          }
+        for (int d = 0; d < 4; d++) {
+          const C* q = d < 2 ? q0 : q1;
+          const GammaEntry ge = gamma_entry(mu, d);
+          const C gq = gp(ge, q[ge.gin]);
+          res[d] = res[d] - R(0.5) * cmul(W, dir == 0 ? q[d] + gq : q[d] - gq);
         }
       }
     }
@@ -287,13 +286,6 @@ __device__ __forceinline__ void wilson_site(const S* __restrict__ in, const type
 //           Phi(s)[P-] = D_W^dag(c[s] R(s) + c[s-1] R(s-1)) + R(s) - R(s-1)
 //           (s = 1: c[1] R(1) + z1 c[Ls] R(Ls), non-D part R(1) - z1 R(Ls), z1 = -am | +i am)
 // (1-based slices as in the reference).  One thread per 5D site, FP64.
-__device__ __forceinline__ void overlap_qd(const SpinorView<double2>& Rv, int s, int site, int sn, bool inner, int swall,
-                                           double a, double b, double2 zb, double2* q) {
-#pragma unroll
-  for (int d = 0; d < 4; d++)
-    q[d] = inner ? a * Rv(s, site, d) + b * Rv(sn, site, d) : a * Rv(s, site, d) + cmul(zb, Rv(swall, site, d));
-}
-
 template <bool DAG>
 __device__ __forceinline__ void overlap_site(const double2* __restrict__ in, const double2* __restrict__ u,
                                              const Geom& g, int s, int site, float am, int imass, float am3,
@@ -327,38 +319,46 @@ __device__ __forceinline__ void overlap_site(const double2* __restrict__ in, con
   } else {
     const C z1 = imass == 1 ? mk(-a, R(0)) : mk(R(0), a);   // upper right, measure_OWilson.F90:139-144
     const C z2 = imass == 1 ? mk(-a, R(0)) : mk(R(0), -a);  // lower left, :152-157
+    // output spins 0,1 from slice s+1 (wall: slice 0 with z2), spins 2,3 from s-1 (wall: Ls-1, z1);
+    // one pass over the neighbours loads R(s) and both partner slices once
+    const bool in0 = s < Ls - 1, in1 = s > 0;
+    const int sp0 = in0 ? s + 1 : 0, sp1 = in1 ? s - 1 : Ls - 1;
+    const R cn0 = __ldg(zc + sp0), cn1 = __ldg(zc + sp1);
+    const C zb0 = cn0 * z2, zb1 = cn1 * z1;
+    auto qpair = [&](int st, C* q0, C* q1) {
 #pragma unroll
-    for (int half = 0; half < 2; half++) {
-      // half 0: output spins 0,1 from slice s+1 (wall: slice 0 with z2); half 1: spins 2,3 from s-1 (wall: Ls-1, z1)
-      const bool inner = half == 0 ? (s < Ls - 1) : (s > 0);
-      const int sn = half == 0 ? s + 1 : s - 1;
-      const int sw = half == 0 ? 0 : Ls - 1;
-      const C zz = half == 0 ? z2 : z1;
-      const R cn = __ldg(zc + (inner ? sn : sw));
-      const C zb = cn * zz;
-      C q[4];
-      overlap_qd(Rv, s, site, sn, inner, sw, cs, cn, zb, q);
-#pragma unroll
-      for (int k = 0; k < 2; k++) {
-        const int d = 2 * half + k;
-        const C xo = inner ? Rv(sn, site, d) : cmul(zz, Rv(sw, site, d));
-        res[d] = dgw * q[d] + Rv(s, site, d) - xo;
+      for (int d = 0; d < 4; d++) {
+        const C r = Rv(s, st, d), a0 = Rv(sp0, st, d), a1 = Rv(sp1, st, d);
+        q0[d] = in0 ? cs * r + cn0 * a0 : cs * r + cmul(zb0, a0);
+        q1[d] = in1 ? cs * r + cn1 * a1 : cs * r + cmul(zb1, a1);
       }
+    };
+    {
+      C q0[4], q1[4];
+      qpair(site, q0, q1);
 #pragma unroll
-      for (int mu = 0; mu < 3; mu++) {
-        const C U = __ldg(u + (size_t)mu * g.v3 + site);
-        const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
+      for (int d = 0; d < 4; d++) {
+        const bool lo = d < 2;
+        const C a2 = Rv(lo ? sp0 : sp1, site, d);
+        const C xo = (lo ? in0 : in1) ? a2 : cmul(lo ? z2 : z1, a2);
+        res[d] = dgw * (lo ? q0[d] : q1[d]) + Rv(s, site, d) - xo;
+      }
+    }
 #pragma unroll
-        for (int dir = 0; dir < 2; dir++) {
-          overlap_qd(Rv, s, dir == 0 ? nb.f[mu] : nb.b[mu], sn, inner, sw, cs, cn, zb, q);
-          const C W = dir == 0 ? U : Ub;
+    for (int mu = 0; mu < 3; mu++) {
+      const C U = __ldg(u + (size_t)mu * g.v3 + site);
+      const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
 #pragma unroll
-          for (int k = 0; k < 2; k++) {
-            const int d = 2 * half + k;
-            const GammaEntry ge = gamma_entry(mu, d);
-            const C gq = gp(ge, q[ge.gin]);
-            res[d] = res[d] - R(0.5) * cmul(W, dir == 0 ? q[d] + gq : q[d] - gq);
-          }
+      for (int dir = 0; dir < 2; dir++) {
+        C q0[4], q1[4];
+        qpair(dir == 0 ? nb.f[mu] : nb.b[mu], q0, q1);
+        const C W = dir == 0 ? U : Ub;
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+          const C* q = d < 2 ? q0 : q1;
+          const GammaEntry ge = gamma_entry(mu, d);
+          const C gq = gp(ge, q[ge.gin]);
+          res[d] = res[d] - R(0.5) * cmul(W, dir == 0 ? q[d] + gq : q[d] - gq);
         }
       }
     }
