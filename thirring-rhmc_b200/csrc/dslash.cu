@@ -366,8 +366,8 @@ __device__ __forceinline__ void overlap_site(const double2* __restrict__ in, con
 }
 
 // odslash / odslashd on one lattice: blockDim = (Ls, sites per block) as the Wilson kernel's
-template <bool DAG>
-__global__ void __launch_bounds__(256, 1)
+template <bool DAG, int MINB>
+__global__ void __launch_bounds__(256, MINB)
     k_odslash(double2* __restrict__ out, const double2* __restrict__ in, const double2* __restrict__ u, Geom g,
               float am, int imass, float am3, const double* __restrict__ zc, const int* skip) {
   if (skip && *skip) return;
@@ -627,18 +627,19 @@ unsigned stencil_grid(const Geom& g, int kernel) {
 // ---------------------------------------------------------------- autotuner
 // For the stencils in FP64 and FP32 storage the register budget (blocks per SM
 // the compiler may assume: 8, 7 or 6 for the Shamir kernel's 128-thread blocks,
-// 2 or 1 for the Wilson kernel's 256-thread blocks) is tuned per (storage,
+// 4, 3 or 2 for the Wilson kernel's 256-thread blocks) is tuned per (storage,
 // kernel, M or M^dagger, epilogue, lattice, layout, device) on first use:
 // each candidate runs 1 + 3 times on the call's own fields (the launches are
 // idempotent: out and partials are overwritten), the fastest is kept for the
 // process.  Block shape and reduction order do not change, so neither do the
-// results.  THR_TUNE=0 in the environment keeps the defaults (8, 2);
+// results.  THR_TUNE=0 in the environment keeps the defaults (8, 4);
 // THR_TUNE=<n> runs the budget n wherever it is a candidate.  Launches made
 // while the stream is being captured into a graph use the default until a
 // tuned value exists.
 namespace {
 constexpr int kTuneShamir[3] = {8, 7, 6};
-constexpr int kTuneWilson[2] = {2, 1};
+constexpr int kTuneWilson[3] = {4, 3, 2};
+constexpr int kTuneOverlap[3] = {4, 3, 1};  // k_odslash's 256-thread blocks
 constexpr int kMaxCand = 3;
 struct TuneKey {
   int dev, sid, ker, dag, epi, lx, ly, lt, ls, layout;
@@ -673,6 +674,52 @@ bool capturing(cudaStream_t st) {
 }
 template <class S> constexpr int storage_id() { return sizeof(S) == sizeof(double2) ? 0 : sizeof(S) == sizeof(float2) ? 1 : 2; }
 }  // namespace
+
+// the tuned candidate for `key`: looked up, forced by THR_TUNE=<n>, or timed now
+// (each candidate 1 + 3 launches on the call's own fields) unless the stream is
+// being captured; cand[0] when tuning is off or cannot run
+template <class F>
+int tune_pick(const TuneKey& key, const int* cand, int ncand, cudaStream_t st, F&& launch) {
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second.pick;
+  }
+  if (!tune_on()) return cand[0];
+  if (g_tune_force) {
+    for (int c = 0; c < ncand; c++)
+      if (cand[c] == g_tune_force) return g_tune_force;
+    return cand[0];
+  }
+  if (capturing(st)) return cand[0];
+  TuneVal tv{cand[0], ncand, {}};
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return cand[0];
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return cand[0];
+  }
+  float best = 1e30f;
+  for (int c = 0; c < ncand; c++) {
+    launch(cand[c]);
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < 3; r++) launch(cand[c]);
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    tv.us[c] = ms * 1e3f / 3.f;
+    if (tv.us[c] < best) {
+      best = tv.us[c];
+      tv.pick = cand[c];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tune[key] = tv;
+  return tv.pick;
+}
 
 // epi: 0 none, 1 out = aux + (*coef) M in with |out|^2 per block, 2 |out|^2 per block
 template <class S>
@@ -736,8 +783,9 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
     }
     if (kernel == 1) {
       if (nt != 256) THR_D(1, 1024, false, 1);
-      else if (minb == 2) THR_D(1, 256, false, 2);
-      else THR_D(1, 256, false, 1);
+      else if (minb == 4) THR_D(1, 256, false, 4);
+      else if (minb == 3) THR_D(1, 256, false, 3);
+      else THR_D(1, 256, false, 2);
     } else if (nt != 128) {
       THR_D(0, 1024, false, 1);
     } else if (shfl) {
@@ -752,50 +800,13 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   };
   const bool tunable = storage_id<S>() < 2 && nt == (kernel == 0 ? 128 : 256);
   const int* cand = kernel == 0 ? kTuneShamir : kTuneWilson;
-  const int ncand = kernel == 0 ? 3 : 2;
+  const int ncand = 3;
   int minb = cand[0];
   if (tunable) {
     int dev = 0;
     cudaGetDevice(&dev);
-    const TuneKey key{dev, storage_id<S>(), kernel, dag ? 1 : 0, e, g.lx, g.ly, g.lt, g.ls, g.layout};
-    bool found = false;
-    {
-      std::lock_guard<std::mutex> lock(g_tune_mu);
-      auto it = g_tune.find(key);
-      if (it != g_tune.end()) {
-        minb = it->second.pick;
-        found = true;
-      }
-    }
-    if (!found && tune_on() && g_tune_force) {
-      for (int c = 0; c < ncand; c++)
-        if (cand[c] == g_tune_force) minb = g_tune_force;
-    } else if (!found && tune_on() && !capturing(st)) {
-      TuneVal tv{cand[0], ncand, {}};
-      cudaEvent_t e0, e1;
-      if (cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess) {
-        float best = 1e30f;
-        for (int c = 0; c < ncand; c++) {
-          launch(cand[c]);
-          cudaEventRecord(e0, st);
-          for (int r = 0; r < 3; r++) launch(cand[c]);
-          cudaEventRecord(e1, st);
-          cudaEventSynchronize(e1);
-          float ms = 0.f;
-          cudaEventElapsedTime(&ms, e0, e1);
-          tv.us[c] = ms * 1e3f / 3.f;
-          if (tv.us[c] < best) {
-            best = tv.us[c];
-            tv.pick = cand[c];
-          }
-        }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        std::lock_guard<std::mutex> lock(g_tune_mu);
-        g_tune[key] = tv;
-        minb = tv.pick;
-      }
-    }
+    minb = tune_pick(TuneKey{dev, storage_id<S>(), kernel, dag ? 1 : 0, e, g.lx, g.ly, g.lt, g.ls, g.layout}, cand,
+                     ncand, st, launch);
   }
   launch(minb);
 #undef THR_D
@@ -832,8 +843,26 @@ int launch_odslash(const Geom& g, bool dag, double2* out, const double2* in, con
   if (imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // measure_OWilson.F90:66-83
   const dim3 blk = stencil_block(g, 1);
   const dim3 grd(stencil_grid(g, 1));
-  if (dag) k_odslash<true><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, zc, skip);
-  else k_odslash<false><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, zc, skip);
+  // register budget (resident 256-thread blocks per SM) tuned per lattice and direction like
+  // the other stencils: 4 and 3 win on large lattices, 1 on small ones
+#define THR_O(D, MB) k_odslash<D, MB><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, zc, skip)
+  auto launch = [&](int mb) {
+    if (dag) {
+      if (mb == 4) THR_O(true, 4);
+      else if (mb == 3) THR_O(true, 3);
+      else THR_O(true, 1);
+    } else {
+      if (mb == 4) THR_O(false, 4);
+      else if (mb == 3) THR_O(false, 3);
+      else THR_O(false, 1);
+    }
+  };
+#undef THR_O
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int mb = tune_pick(TuneKey{dev, 0, 2, dag ? 1 : 0, 0, g.lx, g.ly, g.lt, g.ls, g.layout}, kTuneOverlap, 3, st,
+                           launch);
+  launch(mb);
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
 
@@ -876,7 +905,7 @@ THR_INST(__half2, float2)
 }  // namespace thr
 
 // The autotuner's choices so far, one line each:
-//   <storage> <shamir|wilson> <M|Mdag> epi=<e> <lx>x<ly>x<lt> Ls=<ls> layout=<l> dev=<d> minb=<pick> us=<per candidate>
+//   <storage> <shamir|wilson|overlap> <M|Mdag> epi=<e> <lx>x<ly>x<lt> Ls=<ls> layout=<l> dev=<d> minb=<pick> us=<per candidate>
 extern "C" int thr_tune_report(char* buf, int len) {
   using namespace thr;
   if (!buf || len < 1) return THR_ERR_BADARG;
@@ -887,7 +916,8 @@ extern "C" int thr_tune_report(char* buf, int len) {
       const TuneKey& k = kv.first;
       char line[256];
       int w = std::snprintf(line, sizeof(line), "%s %s %s epi=%d %dx%dx%d Ls=%d layout=%d dev=%d minb=%d us=",
-                            k.sid == 0 ? "fp64" : "fp32", k.ker ? "wilson" : "shamir", k.dag ? "Mdag" : "M", k.epi,
+                            k.sid == 0 ? "fp64" : "fp32", k.ker == 2 ? "overlap" : k.ker ? "wilson" : "shamir",
+                            k.dag ? "Mdag" : "M", k.epi,
                             k.lx, k.ly, k.lt, k.ls, k.layout, k.dev, kv.second.pick);
       for (int c = 0; c < kv.second.ncand && w > 0 && w < (int)sizeof(line); c++)
         w += std::snprintf(line + w, sizeof(line) - w, c ? "/%.2f" : "%.2f", kv.second.us[c]);
