@@ -95,13 +95,14 @@ def test_oracle_adjoint_and_congrad_o(imass):
 @pytest.mark.gpu
 @pytest.mark.parametrize("imass", [1, 3])
 @pytest.mark.parametrize("dims", [(4, 6, 8, 8), (6, 4, 4, 12), (4, 4, 6, 5)])
-def test_odslash_vs_oracle(imass, dims):
+@pytest.mark.parametrize("layout", [0, 1])
+def test_odslash_vs_oracle(imass, dims, layout):
     lx, ly, lt, ls = dims
     rng = np.random.default_rng(hash((imass,) + dims) % 2**32)
     L = O.lat(lx, ly, lt, ls, kernel=1)
     u, R = rand_links(L, rng), rand_spinor(L, rng)
     c = O.zolo_coeffs(ls)
-    with thirring.Lattice(lx, ly, lt, ls, kernel=1) as G:
+    with thirring.Lattice(lx, ly, lt, ls, kernel=1, layout=layout) as G:
         assert np.array_equal(G.zolo(), c)
         for dag in (False, True):
             ref = (O.odslashd if dag else O.odslash)(L, R, u, 0.03, imass, c)
