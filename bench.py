@@ -47,7 +47,7 @@ FP64_ITERS_REF = 17118  # measured on B200 for the seeded input below
 METRIC = "multishift solve throughput (qmrherm, 25 poles, FP64 residual 1e-9)"
 # kernel timing inside the timed region: every PROF_STRIDE-th launch of each kind
 PROF_STRIDE = 8
-PROF_KINDS = ((0, "k_dslash_M_norm"), (2, "k_dslash_Mdag"), (1, "k_flush"))
+PROF_KINDS = ((0, "k_dslash_M_hrec"), (2, "k_dslash_Mdag"), (1, "k_flush"))
 UNIT = "solves/s"
 HBM_FALLBACK = 6650.0
 
@@ -248,13 +248,14 @@ def run_ours(args, rank, world, local_rank):
         tot = C.c_double(0)
         L.thr_profile_read(h, kind, C.byref(n), C.byref(t), C.byref(b), C.byref(tot))
         prof[name] = dict(sampled=n.value, ms=t.value, bytes=b.value, launches=tot.value)
-    # the batched solver's graph runs batches in pairs: a batch is 32 iterations of 5
-    # kernels (M with |Mp|^2, alpha, M^dagger with the residual update, lambda, p update)
-    # plus the previous batch's flush (coefficients, flush, history reset), a pair ends in
-    # the loop control; per solve 3 set-up kernels, the last batch's flush and the pole sum
+    # the batched solver's graph runs batches in pairs: a batch is 32 iterations of 4
+    # kernels (M with the h recurrence and |h|^2, alpha, M^dagger with the residual
+    # update, lambda) plus the previous batch's flush (coefficients, flush, history
+    # reset), a pair ends in the loop control; per solve 3 set-up kernels, the last
+    # batch's flush and the pole sum
     def batch_launches(i):
         pairs = (i + 63) // 64
-        return 3 + pairs * (2 * (32 * 5 + 3) + 1) + 3 + 1
+        return 3 + pairs * (2 * (32 * 4 + 3) + 1) + 3 + 1
     launches = int(sum(batch_launches(i) for i in its))
 
     # ---- plain FP64 GPU path for comparison: FP64 everywhere and the reference's

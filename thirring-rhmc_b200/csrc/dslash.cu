@@ -397,7 +397,9 @@ __device__ __forceinline__ void apply_site(const S* in, const typename Sto<S>::C
 //
 // Epilogues (EPI): 0 store out = M in; 2 also one FP64 partial per block of
 // |out|^2; 1 the residual update of the multishift solver fused in -- out =
-// aux + (*coef) * (M in), with M in never stored, and a partial of |out|^2.
+// aux + (*coef) * (M in), with M in never stored, and a partial of |out|^2;
+// 3 out = M in + (*coef) * aux with a partial of |out|^2 (the batched
+// multishift keeps h = M p by this recurrence instead of storing p).
 template <class S, int KER, bool DAG, int EPI, int NT, bool SHFL, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     k_dslash(S* __restrict__ out, const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u, Geom g, float am,
@@ -406,7 +408,7 @@ __global__ void __launch_bounds__(NT, MINB)
   if (skip && *skip) return;
   using C = typename Sto<S>::C;
   using R = typename Sto<S>::R;
-  const R om = EPI == 1 ? (R)(*coef) : R(0);
+  const R om = (EPI == 1 || EPI == 3) ? (R)(*coef) : R(0);
   const int s = threadIdx.x;
   double racc = 0.0;
   // rev: blocks walk the sites from the top, so that the first blocks find the
@@ -426,6 +428,10 @@ __global__ void __launch_bounds__(NT, MINB)
           const C rn = Sto<S>::ld(aux, i) + om * acc[d];  // r = r + omega*s (multishift_module.F90:137)
           Sto<S>::st(out, i, rn);
           racc += epi_norm<S>(rn);
+        } else if (EPI == 3) {
+          const C hn = acc[d] + om * Sto<S>::ld(aux, i);  // h = M r + gamma h (= M p by linearity)
+          Sto<S>::st(out, i, hn);
+          racc += epi_norm<S>(hn);
         } else {
           Sto<S>::st(out, i, acc[d]);
           if (EPI == 2) racc += epi_norm<S>(acc[d]);
@@ -484,7 +490,7 @@ __global__ void __launch_bounds__(64, MINB)
                   double* __restrict__ partials, int rev) {
   if (skip && *skip) return;
   using R = typename Sto<C>::R;
-  const R om = EPI == 1 ? (R)(*coef) : R(0);
+  const R om = (EPI == 1 || EPI == 3) ? (R)(*coef) : R(0);
   const int s0 = 2 * threadIdx.x;
   const int bid = rev ? (int)gridDim.x - 1 - (int)blockIdx.x : (int)blockIdx.x;
   const int site0 = bid * blockDim.y + threadIdx.y;
@@ -544,6 +550,11 @@ __global__ void __launch_bounds__(64, MINB)
         ld_pair(aux, i, q0, q1);
         v0 = q0 + om * v0;  // r = r + omega*s (multishift_module.F90:137)
         v1 = q1 + om * v1;
+      } else if (EPI == 3) {
+        C q0, q1;
+        ld_pair(aux, i, q0, q1);
+        v0 = v0 + om * q0;  // h = M r + gamma h
+        v1 = v1 + om * q1;
       }
       st_pair(out, i, v0, v1);
       if (EPI != 0) racc += epi_norm<C>(v0) + epi_norm<C>(v1);
@@ -739,6 +750,7 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   do {                                         \
     if (e == 1) THR_L(K, D, 1, N, SH, MB);     \
     else if (e == 2) THR_L(K, D, 2, N, SH, MB); \
+    else if (e == 3) THR_L(K, D, 3, N, SH, MB); \
     else THR_L(K, D, 0, N, SH, MB);            \
   } while (0)
 #define THR_D(K, N, SH, MB)                        \
@@ -765,6 +777,7 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   do {                                   \
     if (e == 1) THR_P(D, 1, MB);         \
     else if (e == 2) THR_P(D, 2, MB);    \
+    else if (e == 3) THR_P(D, 3, MB);    \
     else THR_P(D, 0, MB);                \
   } while (0)
       const int mb = minb == 8 ? 16 : minb == 7 ? 14 : 12;
@@ -820,6 +833,13 @@ int launch_dslash_axpy(const Geom& g, int kernel, bool dag, S* rnew, const S* in
                        float am, int imass, float am3, cudaStream_t st, const int* skip, const S* rold,
                        const double* coef, double* partials, int rev) {
   return launch_dslash_mode<S>(g, kernel, dag, rnew, in, u, am, imass, am3, st, skip, rold, coef, partials, 1, rev);
+}
+
+template <class S>
+int launch_dslash_accum(const Geom& g, int kernel, bool dag, S* hnew, const S* in, const typename Sto<S>::C* u,
+                        float am, int imass, float am3, cudaStream_t st, const int* skip, const S* hold,
+                        const double* coef, double* partials, int rev) {
+  return launch_dslash_mode<S>(g, kernel, dag, hnew, in, u, am, imass, am3, st, skip, hold, coef, partials, 3, rev);
 }
 
 template <class S>
@@ -894,6 +914,8 @@ int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const
                                      cudaStream_t, const int*, const S*, const double*, double*, int);            \
   template int launch_dslash_norm<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
                                      cudaStream_t, const int*, double*, int);                                     \
+  template int launch_dslash_accum<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,          \
+                                      cudaStream_t, const int*, const S*, const double*, double*, int);           \
   template int launch_dslash_batch<S>(const BatchTable&, int, bool, S*, const S*, const L*, float, int, float,    \
                                       cudaStream_t, const int*, const S*, double*, int);
 THR_INST(double2, double2)

@@ -16,9 +16,11 @@
 // low-priority side stream while the next batch iterates on the main stream
 // (it reads the other half of the ring and the other of two histories), so
 // the bandwidth-bound flush fills the time the latency-bound stencils and the
-// one-block scalar kernels leave unused.  In addition alpha =
-// Re<p, M^dagger M p> (= |M p|^2) is accumulated in the epilogue of the M
-// stencil from the values it writes, so neither p nor s is re-read for it.
+// one-block scalar kernels leave unused.  The search direction p enters the
+// base recurrence only through h = M p, which is kept by h_new = M r + gammag h
+// (p = r + gammag p and linearity), so p is never formed and the p update pass
+// is gone; alpha = Re<p, M^dagger M p> (= |h|^2) is accumulated in the epilogue
+// of the M stencil from the values it writes, so neither h nor s is re-read for it.
 #include <cmath>
 #include <cstring>
 
@@ -127,21 +129,6 @@ __global__ void k_lambda(MsState* ms, MsHist* hist, const double* partials, int 
     ms->delta = ms->lambda;
     if (!(ms->lambda == ms->lambda)) ms->status = THR_ERR_NAN;
     if (maxi < mini || ms->it >= ms->maxcg || ms->status) ms->done = 1;
-  }
-}
-
-// p = r + gammag*p (:145), in site order: a thread takes the four spin planes of
-// one (s, site) element of the plane (np = n / 4 elements), so the sweep moves
-// through the sites like the stencils do; rev: from the top site down
-template <class V>
-__global__ void k_pupdate(const MsState* ms, V* p, const V* r, size_t np, int rev) {
-  if (ms->done) return;
-  using R = typename W<V>::R;
-  const R gg = W<V>::cast(ms->gammag);
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < np; e += (size_t)gridDim.x * blockDim.x) {
-    const size_t i = rev ? np - 1 - e : e;
-#pragma unroll
-    for (int d = 0; d < 4; d++) p[i + d * np] = r[i + d * np] + gg * p[i + d * np];
   }
 }
 
@@ -336,33 +323,34 @@ int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* 
   enqueue_flush<V>(c, fork ? c->st2 : c->st, ms, hist + (1 - half), cf + (1 - half), out, sf, ring, 1 - half, prof,
                    k0 - kBatch, prof_flush);
   if (fork) THR_CUDA(cudaEventRecord(c->ev_join[half], c->st2));
-  // algorithmic bytes: M reads p, writes h, reads the links (|M p|^2 comes from
-  // registers); the M^dagger launch reads h, the links and r_old and writes r_new
-  const double b_m = 2.0 * n * sizeof(V) + 3.0 * c->g.v3 * lb, b_md = b_m + (double)n * sizeof(V);
+  // h = M p is kept by the recurrence h_new = M r + gammag h_old (p = r + gammag p
+  // and linearity), so p is never formed: the M launch reads the newest residual,
+  // the previous h and the links and writes h (|h|^2 from registers); the
+  // M^dagger launch reads h, the links and r_old and writes r_new.  The two h
+  // fields alternate (hv on even iterations, p's field on odd ones; kBatch is even).
+  // M sweeps up and M^dagger down, so each starts on the sites the other wrote last.
+  const double b_md = 3.0 * n * sizeof(V) + 3.0 * c->g.v3 * lb;
   MsHist* rec = hist + half;
-  // sweep directions alternate with the iteration's parity (kBatch is even) so that
-  // every kernel starts on the sites its predecessor wrote last, still in L2:
-  //   even: M forward, M^dagger top down, p update forward; odd: the reverse
-  // (partials are indexed by site block, so the direction does not change results)
+  const int rev_md = c->rev_sweep ? 1 : 0;
+  (void)gb;
   for (int j = 0; j < kBatch; j++) {
-    const int odd = c->rev_sweep == 2 ? (j & 1) : 0;
-    const int rev_m = odd, rev_md = c->rev_sweep ? 1 - odd : 0, rev_p = odd;
     const int so = half * kBatch + j, sn = so + 1 == 2 * kBatch ? 0 : so + 1;
     V* rold = ring + (size_t)so * n;
     V* rnew = ring + (size_t)sn * n;
-    // alpha = Re<p, M^dagger M p> (:104) evaluated as |M p|^2 in the M epilogue
-    int pe = prof ? c->prof_begin(thr_ctx::P_DSLASH, b_m, k0 + j) : -1;
-    THR_TRY(launch_dslash_norm<V>(c->g, c->p.kernel, false, hv, p, u, am, imass, c->p.am3, c->st, &ms->done,
-                                  c->partials, rev_m));
+    V* hcur = (j & 1) ? p : hv;
+    const V* hprev = (j & 1) ? hv : p;
+    // alpha = Re<p, M^dagger M p> (:104) evaluated as |h|^2 = |M p|^2 in the M epilogue
+    int pe = prof ? c->prof_begin(thr_ctx::P_DSLASH, b_md, k0 + j) : -1;
+    THR_TRY(launch_dslash_accum<V>(c->g, c->p.kernel, false, hcur, rold, u, am, imass, c->p.am3, c->st, &ms->done,
+                                   hprev, &ms->gammag, c->partials, 0));
     c->prof_end(pe);
     k_alpha<<<1, 1024, 0, c->st>>>(ms, rec, c->partials, gs);
     // s = M^dagger h is never stored: the epilogue forms r = r + omega*s (:137) and |r|^2 (:138)
     pe = prof ? c->prof_begin(thr_ctx::P_DSLASH_DAG, b_md, k0 + j) : -1;
-    THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, rnew, hv, u, am, imass, c->p.am3, c->st, &ms->done, rold,
-                                  &ms->omega, c->partials, rev_md));
+    THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, rnew, hcur, u, am, imass, c->p.am3, c->st, &ms->done,
+                                  rold, &ms->omega, c->partials, rev_md));
     c->prof_end(pe);
     k_lambda<<<1, 1024, 0, c->st>>>(ms, rec, c->partials, gs);
-    k_pupdate<V><<<gb, kThreads, 0, c->st>>>(ms, p, rnew, n / 4, rev_p);
   }
   (void)s;
   if (fork) THR_CUDA(cudaStreamWaitEvent(c->st, c->ev_join[half], 0));
@@ -407,11 +395,11 @@ int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V
   G.release();
   // run the two stencils of an iteration once outside the capture, so that the
   // autotuner settles their configuration before it is baked into the graph
-  // (hv, s and the partials are scratch at this point; p holds the source)
+  // (hv, p, s and the partials are scratch at this point; the solve clears hv and p after)
   {
     const typename Sto<V>::C* uu = (const typename Sto<V>::C*)u;
-    THR_TRY(launch_dslash_norm<V>(c->g, c->p.kernel, false, hv, p, uu, am, imass, c->p.am3, c->st, &ms->done,
-                                  c->partials));
+    THR_TRY(launch_dslash_accum<V>(c->g, c->p.kernel, false, hv, ring, uu, am, imass, c->p.am3, c->st, &ms->done, p,
+                                   &ms->gammag, c->partials, 0));
     THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, s, hv, uu, am, imass, c->p.am3, c->st, &ms->done, ring,
                                   &ms->omega, c->partials, c->rev_sweep ? 1 : 0));
   }
@@ -490,7 +478,6 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
   h->max_batches = (maxcg > 0 ? maxcg : 0) / kBatch + 5;
   THR_CUDA(cudaMemcpyAsync(ms, h, sizeof(MsState), cudaMemcpyHostToDevice, c->st));
   THR_CUDA(cudaMemcpyAsync(ring, in, n * sizeof(V), cudaMemcpyDeviceToDevice, c->st));  // r = input (slot 0)
-  THR_CUDA(cudaMemcpyAsync(p, in, n * sizeof(V), cudaMemcpyDeviceToDevice, c->st));     // p = r
   const unsigned gb = vec_grid(n);
   k_norm2<V><<<gb, kThreads, 0, c->st>>>(ring, n, c->partials);
   k_init<<<1, kThreads, 0, c->st>>>(ms, hist, c->partials, gb);
@@ -500,11 +487,16 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
     // one graph launch runs every batch until convergence; one synchronisation
     cudaGraphExec_t exec = nullptr;
     THR_TRY(ms_graph<V>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, &exec));
+    // h = M p starts as M r (p = r, gammag = 0): the previous h of the first iteration is zero
+    THR_CUDA(cudaMemsetAsync(hv, 0, n * sizeof(V), c->st));
+    THR_CUDA(cudaMemsetAsync(p, 0, n * sizeof(V), c->st));
     THR_CUDA(cudaGraphLaunch(exec, c->st));
     THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
     THR_CUDA(cudaStreamSynchronize(c->st));
   } else {
     // stream-launched batches, one synchronisation per batch (and kernel timing)
+    THR_CUDA(cudaMemsetAsync(hv, 0, n * sizeof(V), c->st));
+    THR_CUDA(cudaMemsetAsync(p, 0, n * sizeof(V), c->st));
     const size_t prof_first = c->prof_kind.size();
     double flushed = 0.0;
     long long flushes = 0;

@@ -32,6 +32,13 @@ int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in,
 int launch_odslash(const Geom& g, bool dag, double2* out, const double2* in, const double2* u, float am, int imass,
                    float am3, const double* zc, cudaStream_t st, const int* skip = nullptr);
 
+// hnew = (M or M^dagger) in + (*coef) * hold and one FP64 partial per block of |hnew|^2
+// (hnew and hold distinct fields)
+template <class S>
+int launch_dslash_accum(const Geom& g, int kernel, bool dag, S* hnew, const S* in, const typename Sto<S>::C* u,
+                        float am, int imass, float am3, cudaStream_t st, const int* skip, const S* hold,
+                        const double* coef, double* partials, int rev = 0);
+
 // layout.cu: Fortran halo'd host layout <-> device fields
 // spinor (0:Ls+1,0:Lx+1,0:Ly+1,0:Lt+1,4) complex(dp)  <-> S[4][V3][Ls]
 template <class S>
