@@ -18,8 +18,11 @@ CASES = [(k, im, lay) for k in (0, 1) for im in ((1, 3, 5) if k == 0 else (1, 3)
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("kernel,imass,layout", CASES)
-@pytest.mark.parametrize("dims", [(4, 6, 8, 8), (6, 4, 4, 12)])
+@pytest.mark.parametrize("dims", [(4, 6, 8, 8), (6, 4, 4, 12), (4, 4, 6, 8), (8, 4, 2, 16)])
 def test_dslash_random(kernel, imass, layout, dims):
+    """The last two shapes are ones the staged-tile FP64 Shamir kernel (THR_TILE=1)
+    takes in the natural site order (Lx, Ly multiples of 4, Lt of 2, Ls of 8);
+    by default they run on k_dslash like the first two."""
     rng = np.random.default_rng(hash((kernel, imass, layout) + dims) % 2**32)
     lx, ly, lt, ls = dims
     L = O.lat(lx, ly, lt, ls, kernel=kernel, am3=1.0)
@@ -144,6 +147,40 @@ def test_register_budgets_bit_identical(tmp_path, kernel, force):
     ref, got = np.load(tmp_path / "out_0.npz"), np.load(tmp_path / ("out_%s.npz" % force))
     for k in ("a", "b", "x", "it"):
         assert np.array_equal(ref[k], got[k]), k
+
+
+@pytest.mark.gpu
+def test_tiled_stencil_matches_k_dslash(tmp_path):
+    """The staged-tile FP64 Shamir kernel (THR_TILE=1) against k_dslash (the
+    default, oracle-checked above) in two processes on a lattice both take: M and M^dagger to rounding (the same
+    arithmetic, operation for operation), and congrad -- whose stencils carry the
+    |Mp|^2 and residual-update epilogues, with partial sums over other blocks --
+    to its own tolerance with the iteration count within 1."""
+    import os
+    import subprocess
+    import sys
+    rng = np.random.default_rng(71)
+    dims = (8, 8, 4, 16)
+    L = O.lat(*dims)
+    u = rand_links(L, rng)
+    R = rand_spinor(L, rng)
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "thirring-rhmc_b200")
+    np.save(tmp_path / "R.npy", R)
+    np.save(tmp_path / "u.npy", u)
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import thirring; d = %r; t = sys.argv[1];"
+            "R = np.asfortranarray(np.load(d + '/R.npy')); u = np.asfortranarray(np.load(d + '/u.npy'));"
+            "G = thirring.Lattice(*%r); G.set_links(u);"
+            "a = G.dslash(R, None, 0.05, 3); b = G.dslashd(R, None, 0.05, 1); c = G.dslash(R, None, 0.05, 5);"
+            "X = np.zeros_like(R); it, _ = G.congrad(R, X, 1e-8, 0.05, 1);"
+            "np.savez(d + '/out_' + t + '.npz', a=a, b=b, c=c, x=X, it=it); G.close()"
+            % (pkg, str(tmp_path), dims))
+    for t in ("0", "1"):
+        subprocess.run([sys.executable, "-c", code, t], check=True, env=dict(os.environ, THR_TILE=t))
+    ref, got = np.load(tmp_path / "out_0.npz"), np.load(tmp_path / "out_1.npz")
+    for k in ("a", "b", "c"):
+        assert rel_err(interior(got[k]), interior(ref[k])) <= 1e-15, k
+    assert abs(int(got["it"]) - int(ref["it"])) <= 1
+    assert rel_err(interior(got["x"]), interior(ref["x"])) <= 1e-7
 
 
 def _dev_dslash(G, R, precision, am, imass, dag):

@@ -133,7 +133,7 @@ int cg_enqueue_chunk(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r
                      int imass) {
   const size_t n = c->n4();
   const unsigned gb = vec_grid(n / 4);
-  const unsigned gs = stencil_grid(c->g, c->p.kernel);
+  const unsigned gs = stencil_parts(c->g, c->p.kernel, true);
   for (int k = 0; k < kCgChunk; k++) {
     // sweep directions alternate with the iteration's parity (kCgChunk is even): each
     // kernel starts on the sites its predecessor wrote last (results do not depend on it)

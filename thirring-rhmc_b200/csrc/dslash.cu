@@ -20,6 +20,9 @@
 // The per-site arithmetic lives in shamir_site / wilson_site; the single-
 // lattice kernels and the batched kernel (many right-hand sides or many
 // lattices of different shapes in one persistent launch) share it.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cstdio>
 #include <cstdlib>
 #include <map>
@@ -576,6 +579,273 @@ __global__ void __launch_bounds__(64, MINB)
   }
 }
 
+// ---------------------------------------------------------------- Shamir, staged tiles
+// FP64 Shamir kernel for the natural site order with Lx, Ly divisible by 4, Lt
+// by 2 and Ls by 8.  A block owns a 4x4x2 tile of sites and 8 consecutive s
+// (256 threads: s fastest, then x, y, t).  One thread first stages everything
+// the block's sites read into shared memory with 14 TMA tensor copies (no
+// multicast) completing on one mbarrier: the tile's spinors with one s on
+// either side (the s-neighbours), the six one-site faces around the tile, and
+// the links of the tile and of its three lower faces.  The spinor field is a
+// 5D tensor (2 Ls doubles, Lx, Ly, Lt, 4 spins), the links one of (2 doubles,
+// Lx, Ly, Lt, 3); a box of the tile or of a face lands in shared memory in
+// that dimension order.  At the ends of the fifth dimension the s-neighbour
+// slots lie outside the tensor (filled with zeros) and take the wall values
+// R(Ls-1) and R(0) instead, loaded by the block's threads while the copies are
+// in flight.  The arithmetic is then shamir_site's, operation for operation,
+// with every operand from shared memory: a 5D site costs 3.4 spinor reads from
+// L2 (tile plus faces) instead of 7, and neither load latency nor address
+// arithmetic sits inside it.  54 KB of shared memory per block, 4 blocks
+// (1024 threads) per SM.
+namespace tile {
+constexpr int TX = 4, TY = 4, TT = 2, SC = 8;
+constexpr int NT = TX * TY * TT * SC;  // 256 threads
+constexpr int NS = TX * TY * TT;       // 32 sites
+constexpr int CW = SC + 2;             // centre row: s0 - 1 .. s0 + SC
+// regions of the shared tile (offsets in double2, each a multiple of 8 = 128 bytes)
+constexpr int CEN = 0;                        // [d][t][y][x][CW]
+constexpr int XFD = TT * TY * SC;             // x faces [dir][d][t][y][SC]: spin stride
+constexpr int YFD = TT * TX * SC;             // y faces [dir][d][t][x][SC]
+constexpr int TFD = TY * TX * SC;             // t faces [dir][d][y][x][SC]
+constexpr int XF = CEN + 4 * NS * CW;
+constexpr int YF = XF + 2 * 4 * XFD;
+constexpr int TF = YF + 2 * 4 * YFD;
+constexpr int UT = TF + 2 * 4 * TFD;          // [mu][t][y][x]  links of the tile
+constexpr int UX = UT + 3 * NS;               // [t][y]  u(0) on the x - 1 face
+constexpr int UY = UX + TT * TY;              // [t][x]  u(1) on the y - 1 face
+constexpr int UTM = UY + TT * TX;             // [y][x]  u(2) on the t - 1 face
+constexpr int END = UTM + TY * TX;            // 3456 double2 = 54 KB
+constexpr int SMEM = END * (int)sizeof(double2) + 128;  // + alignment slack
+static_assert(XF % 8 == 0 && YF % 8 == 0 && TF % 8 == 0 && UT % 8 == 0 && UX % 8 == 0 && UY % 8 == 0 &&
+                  UTM % 8 == 0 && (4 * XFD) % 8 == 0 && (4 * TFD) % 8 == 0,
+              "TMA destinations must be 128-byte aligned");
+// the tensor maps of one launch: spinor boxes (centre, x, y, t faces) and link boxes
+struct alignas(64) Maps {
+  CUtensorMap cen, xf, yf, tf, ut, ux, uy, utm;
+};
+constexpr unsigned kWaitPolls = 1u << 22;  // bound on the mbarrier wait (seconds at most)
+}  // namespace tile
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void tma_load5(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
+                                          unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
+      "[%7];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <bool DAG, int EPI>
+__global__ void __launch_bounds__(tile::NT, 4)
+    k_dslash_tile(double2* __restrict__ out, const double2* __restrict__ in, const __grid_constant__ tile::Maps maps,
+                  Geom g, float am, int imass, float am3, const int* skip, const double2* __restrict__ aux,
+                  const double* __restrict__ coef, double* __restrict__ partials, int rev) {
+  using namespace tile;
+  if (skip && *skip) return;
+  // the dynamic region is allocated 128 bytes long and rounded up to a 128-byte
+  // boundary of the shared window, where TMA destinations must start
+  extern __shared__ __align__(16) double2 smraw[];
+  double2* const sm = smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u) / 16u;
+  __shared__ __align__(8) unsigned long long bar;
+  const int Lx = g.lx, Ly = g.ly, Lt = g.lt, Ls = g.ls;
+  const unsigned v3 = (unsigned)g.v3;
+  const int nch = Ls / SC;
+  // rev: blocks walk the tiles from the top (see k_dslash)
+  const int bid = rev ? (int)gridDim.x - 1 - (int)blockIdx.x : (int)blockIdx.x;
+  const int ch = bid % nch, ti = bid / nch;
+  const int ntx = Lx / TX, nty = Ly / TY;
+  const int x0 = (ti % ntx) * TX, y0 = ((ti / ntx) % nty) * TY, t0 = (ti / (ntx * nty)) * TT, s0 = ch * SC;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const int xm = x0 == 0 ? Lx - 1 : x0 - 1, xp = x0 + TX == Lx ? 0 : x0 + TX;
+    const int ym = y0 == 0 ? Ly - 1 : y0 - 1, yp = y0 + TY == Ly ? 0 : y0 + TY;
+    const int tm = t0 == 0 ? Lt - 1 : t0 - 1, tp = t0 + TT == Lt ? 0 : t0 + TT;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(&bar)),
+                 "r"(END * (int)sizeof(double2))
+                 : "memory");
+    const int c0 = 2 * s0;  // fifth-dimension coordinate in doubles: 16-byte multiples
+    tma_load5(sm + CEN, &maps.cen, c0 - 2, x0, y0, t0, 0, &bar);
+    tma_load5(sm + XF, &maps.xf, c0, xm, y0, t0, 0, &bar);
+    tma_load5(sm + XF + 4 * XFD, &maps.xf, c0, xp, y0, t0, 0, &bar);
+    tma_load5(sm + YF, &maps.yf, c0, x0, ym, t0, 0, &bar);
+    tma_load5(sm + YF + 4 * YFD, &maps.yf, c0, x0, yp, t0, 0, &bar);
+    tma_load5(sm + TF, &maps.tf, c0, x0, y0, tm, 0, &bar);
+    tma_load5(sm + TF + 4 * TFD, &maps.tf, c0, x0, y0, tp, 0, &bar);
+    tma_load5(sm + UT, &maps.ut, 0, x0, y0, t0, 0, &bar);
+    tma_load5(sm + UX, &maps.ux, 0, xm, y0, t0, 0, &bar);
+    tma_load5(sm + UY, &maps.uy, 0, x0, ym, t0, 1, &bar);
+    tma_load5(sm + UTM, &maps.utm, 0, x0, y0, tm, 2, &bar);
+  }
+  // wall values for the s-neighbour slots outside the tensor: R(Ls-1) before s = 0
+  // (threads 0-127, one centre row each) and R(0) after s = Ls-1 (threads 128-255)
+  const int row = tid & 127;
+  const bool wall = tid < 128 ? ch == 0 : ch == nch - 1;
+  double2 wv = mk(0.0, 0.0);
+  if (wall) {
+    const unsigned wsite = (unsigned)(x0 + (row & 3) + Lx * (y0 + ((row >> 2) & 3) + Ly * (t0 + ((row >> 4) & 1))));
+    wv = in[(unsigned)(tid < 128 ? Ls - 1 : 0) + (unsigned)Ls * (wsite + v3 * (unsigned)(row >> 5))];
+  }
+  unsigned done = 0;
+  for (unsigned k = 0; k < kWaitPolls && !done; k++) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(&bar))
+        : "memory");
+  }
+  if (wall) sm[CEN + row * CW + (tid < 128 ? 0 : CW - 1)] = wv;
+  if (!__syncthreads_and(done)) {
+    // the copies did not complete: the block's outputs and partial become NaN
+    if (EPI != 0 && tid == 0) partials[bid] = __longlong_as_double(0x7ff8000000000000LL);
+    return;
+  }
+
+  const int sl = tid & 7, xs = (tid >> 3) & 3, ys = (tid >> 5) & 3, ts = tid >> 7;
+  const int s = s0 + sl;
+  const unsigned site = (unsigned)(x0 + xs + Lx * (y0 + ys + Ly * (t0 + ts)));
+  const int q = (ts * TY + ys) * TX + xs;  // tile site
+  constexpr int CD = NS * CW;              // centre: stride of the spin index
+  const double2* cen = sm + CEN + q * CW + sl + 1;  // R(s) of spin 0 at this site
+  const double om = (EPI == 1 || EPI == 3) ? *coef : 0.0;
+  const double diag = (double)((3.0f - am3) + 1.0f);  // dirac.F90:45, default real
+  double2 rc[4], acc[4];
+#pragma unroll
+  for (int d = 0; d < 4; d++) {
+    rc[d] = cen[d * CD];
+    acc[d] = diag * rc[d];
+  }
+  // fifth dimension and walls as in shamir_site: the slot after s holds R(s+1),
+  // or R(0) at s = Ls-1; the slot before s holds R(s-1), or R(Ls-1) at s = 0
+  const int a0 = DAG ? 0 : 2, b0 = DAG ? 2 : 0;
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    if (s < Ls - 1) acc[a0 + k] = acc[a0 + k] - cen[(a0 + k) * CD + 1];
+    if (s > 0) acc[b0 + k] = acc[b0 + k] - cen[(b0 + k) * CD - 1];
+  }
+  const double a = (double)am;
+  const bool five = imass == 5;
+  const double2 cA = imass == 1 ? mk(a, 0.0) : mk(0.0, (five && DAG) ? -a : a);
+  const double2 cB = imass == 1 ? mk(a, 0.0) : mk(0.0, five ? (DAG ? -a : a) : -a);
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    if (s == Ls - 1) acc[a0 + k] = acc[a0 + k] + cmul(cA, five ? rc[b0 + k] : cen[(a0 + k) * CD + 1]);
+    if (s == 0) acc[b0 + k] = acc[b0 + k] + cmul(cB, five ? rc[a0 + k] : cen[(b0 + k) * CD - 1]);
+  }
+  // hops in shamir_site's order: per direction forward then backward
+#pragma unroll
+  for (int mu = 0; mu < 3; mu++) {
+#pragma unroll
+    for (int dir = 0; dir < 2; dir++) {
+      const double2* p;
+      int dstr;
+      double2 W;
+      if (mu == 0) {
+        const bool in_tile = dir == 0 ? xs < TX - 1 : xs > 0;
+        p = in_tile ? cen + (dir == 0 ? CW : -CW) : sm + XF + (dir == 0 ? 4 * XFD : 0) + (ts * TY + ys) * SC + sl;
+        dstr = in_tile ? CD : XFD;
+        W = dir == 0 ? sm[UT + q] : cconj(xs > 0 ? sm[UT + q - 1] : sm[UX + ts * TY + ys]);
+      } else if (mu == 1) {
+        const bool in_tile = dir == 0 ? ys < TY - 1 : ys > 0;
+        p = in_tile ? cen + (dir == 0 ? TX * CW : -TX * CW)
+                    : sm + YF + (dir == 0 ? 4 * YFD : 0) + (ts * TX + xs) * SC + sl;
+        dstr = in_tile ? CD : YFD;
+        W = dir == 0 ? sm[UT + NS + q] : cconj(ys > 0 ? sm[UT + NS + q - TX] : sm[UY + ts * TX + xs]);
+      } else {
+        const bool in_tile = dir == 0 ? ts < TT - 1 : ts > 0;
+        p = in_tile ? cen + (dir == 0 ? TY * TX * CW : -TY * TX * CW)
+                    : sm + TF + (dir == 0 ? 4 * TFD : 0) + (ys * TX + xs) * SC + sl;
+        dstr = in_tile ? CD : TFD;
+        W = dir == 0 ? sm[UT + 2 * NS + q] : cconj(ts > 0 ? sm[UT + 2 * NS + q - TY * TX] : sm[UTM + ys * TX + xs]);
+      }
+      double2 r[4];
+#pragma unroll
+      for (int d = 0; d < 4; d++) r[d] = p[d * dstr];
+      hop_projected<double2, double>(mu, (dir == 0) != DAG, W, r, acc);
+    }
+  }
+  double racc = 0.0;
+#pragma unroll
+  for (int d = 0; d < 4; d++) {
+    const unsigned i = (unsigned)s + (unsigned)Ls * (site + v3 * (unsigned)d);
+    if (EPI == 1) {
+      const double2 rn = aux[i] + om * acc[d];  // r = r + omega*s (multishift_module.F90:137)
+      out[i] = rn;
+      racc += epi_norm<double2>(rn);
+    } else if (EPI == 3) {
+      const double2 hn = acc[d] + om * aux[i];  // h = M r + gamma h (= M p by linearity)
+      out[i] = hn;
+      racc += epi_norm<double2>(hn);
+    } else {
+      out[i] = acc[d];
+      if (EPI == 2) racc += epi_norm<double2>(acc[d]);
+    }
+  }
+  if (EPI != 0) {
+    // one FP64 partial per block, fixed order: warp sums, then the 8 warps in turn
+    __shared__ double red[NT / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) racc += __shfl_down_sync(0xffffffffu, racc, o);
+    if ((tid & 31) == 0) red[tid >> 5] = racc;
+    __syncthreads();
+    if (tid == 0) {
+      double v = 0.0;
+#pragma unroll
+      for (int w = 0; w < NT / 32; w++) v += red[w];
+      partials[bid] = v;
+    }
+  }
+}
+
+// Tensor maps of the staged-tile kernel for the spinor field `in` and the links u
+// (cuTensorMapEncodeTiled through the runtime's driver entry point; the maps are
+// plain host structures passed by value, so graphs capture them with the launch)
+namespace {
+using EncodeFn = PFN_cuTensorMapEncodeTiled_v12000;
+EncodeFn tile_encoder() {
+  static EncodeFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<EncodeFn>(p);
+  }();
+  return fn;
+}
+bool tile_map(EncodeFn enc, CUtensorMap* m, const void* base, const cuuint64_t* dim, const cuuint64_t* stride,
+              const cuuint32_t* box) {
+  const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<void*>(base), dim, stride, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+bool tile_maps(const Geom& g, const double2* in, const double2* u, tile::Maps* m) {
+  using namespace tile;
+  const EncodeFn enc = tile_encoder();
+  if (!enc) return false;
+  const cuuint64_t row = 16ull * g.ls;  // bytes of one (site, spin) run of the fifth dimension
+  const cuuint64_t sd[5] = {2ull * g.ls, (cuuint64_t)g.lx, (cuuint64_t)g.ly, (cuuint64_t)g.lt, 4};
+  const cuuint64_t ss[4] = {row, row * g.lx, row * g.lx * g.ly, row * g.v3};
+  const cuuint64_t ud[5] = {2, (cuuint64_t)g.lx, (cuuint64_t)g.ly, (cuuint64_t)g.lt, 3};
+  const cuuint64_t us[4] = {16, 16ull * g.lx, 16ull * g.lx * g.ly, 16ull * g.v3};
+  const cuuint32_t bc[5] = {2 * CW, TX, TY, TT, 4}, bx[5] = {2 * SC, 1, TY, TT, 4}, by[5] = {2 * SC, TX, 1, TT, 4},
+                   bt[5] = {2 * SC, TX, TY, 1, 4};
+  const cuuint32_t ut[5] = {2, TX, TY, TT, 3}, ux[5] = {2, 1, TY, TT, 1}, uy[5] = {2, TX, 1, TT, 1},
+                   utm[5] = {2, TX, TY, 1, 1};
+  return tile_map(enc, &m->cen, in, sd, ss, bc) && tile_map(enc, &m->xf, in, sd, ss, bx) &&
+         tile_map(enc, &m->yf, in, sd, ss, by) && tile_map(enc, &m->tf, in, sd, ss, bt) &&
+         tile_map(enc, &m->ut, u, ud, us, ut) && tile_map(enc, &m->ux, u, ud, us, ux) &&
+         tile_map(enc, &m->uy, u, ud, us, uy) && tile_map(enc, &m->utm, u, ud, us, utm);
+}
+}  // namespace
+
 // Batched stencil: a persistent grid walks the work blocks of all entries
 // (right-hand sides or lattices).  Work block wb belongs to the entry e with
 // blk0[e] <= wb < blk0[e+1]; inside it, thread tid handles s = tid % Ls of
@@ -620,7 +890,27 @@ int stencil_threads(const Geom& g, int kernel) {
   return g.ls <= nt ? nt : 1024;
 }
 bool stencil_shfl(const Geom& g, int kernel) { return kernel == 0 && g.ls <= 32 && (g.ls & (g.ls - 1)) == 0; }
+// THR_TILE=1 in the environment puts the FP64 Shamir stencil on the staged-tile
+// kernel where the lattice allows it.  It is off by default: on B200 it measured
+// 51-54 us per launch in the 32^2x32, Ls 32 multishift solve against k_dslash's
+// 48-50 us, and 162 us against 156-159 us at 48^2x48, Ls 48.
+bool tile_on() {
+  static const bool on = [] {
+    const char* e = std::getenv("THR_TILE");
+    return e && e[0] == '1' && e[1] == 0;
+  }();
+  return on;
+}
+bool tile_ok(const Geom& g, int kernel) {
+  return kernel == 0 && g.layout != LAYOUT_EO && g.lx % tile::TX == 0 && g.ly % tile::TY == 0 &&
+         g.lt % tile::TT == 0 && g.ls % tile::SC == 0 && tile_on();
+}
+unsigned tile_grid(const Geom& g) { return (unsigned)(g.v3 / tile::NS) * (unsigned)(g.ls / tile::SC); }
 }  // namespace
+
+unsigned stencil_parts(const Geom& g, int kernel, bool fp64) {
+  return fp64 && tile_ok(g, kernel) ? tile_grid(g) : stencil_grid(g, kernel);
+}
 
 dim3 stencil_block(const Geom& g, int kernel) {
   int spb = stencil_threads(g, kernel) / g.ls;
@@ -740,6 +1030,37 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   if (g.ls > 1024) return THR_ERR_BADSHAPE;
   if (4ULL * (unsigned long long)g.v5 >= (1ULL << 32)) return THR_ERR_BADSHAPE;  // 32-bit element offsets
   if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
+  if (storage_id<S>() == 0 && tile_ok(g, kernel)) {
+    double2* o = reinterpret_cast<double2*>(out);
+    const double2* i = reinterpret_cast<const double2*>(in);
+    const double2* ax = reinterpret_cast<const double2*>(aux);
+    const unsigned grd = tile_grid(g);
+    tile::Maps maps;
+    if (!tile_maps(g, i, reinterpret_cast<const double2*>(u), &maps)) return THR_ERR_CUDA;
+#define THR_T(D, E)                                                                                          \
+  do {                                                                                                       \
+    static bool attr = false;                                                                                \
+    if (!attr) {                                                                                             \
+      cudaFuncSetAttribute(k_dslash_tile<D, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile::SMEM);    \
+      cudaFuncSetAttribute(k_dslash_tile<D, E>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);        \
+      attr = true;                                                                                           \
+    }                                                                                                        \
+    k_dslash_tile<D, E><<<grd, tile::NT, tile::SMEM, st>>>(o, i, maps, g, am, imass, am3, skip, ax, coef, partials, \
+                                                           rev);                                             \
+  } while (0)
+#define THR_TE(D)                 \
+  do {                            \
+    if (e == 1) THR_T(D, 1);      \
+    else if (e == 2) THR_T(D, 2); \
+    else if (e == 3) THR_T(D, 3); \
+    else THR_T(D, 0);             \
+  } while (0)
+    if (dag) THR_TE(true);
+    else THR_TE(false);
+#undef THR_TE
+#undef THR_T
+    return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+  }
   const dim3 blk = stencil_block(g, kernel);
   const dim3 grd(stencil_grid(g, kernel));
   const int nt = stencil_threads(g, kernel);

@@ -307,7 +307,7 @@ int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* 
                   float am, int imass, int half, long long k0, bool prof, int* prof_flush) {
   const size_t n = c->n4();
   const unsigned gb = vec_grid(n / 4);
-  const unsigned gs = stencil_grid(c->g, c->p.kernel);
+  const unsigned gs = stencil_parts(c->g, c->p.kernel, sizeof(V) == sizeof(double2));
   const bool sp = sizeof(V) == sizeof(float2);
   const typename Sto<V>::C* u =
       sp ? (const typename Sto<V>::C*)(const void*)c->u32 : (const typename Sto<V>::C*)(const void*)c->u64;

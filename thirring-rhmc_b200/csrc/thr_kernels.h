@@ -10,6 +10,8 @@ constexpr int kMaxPartials = 4096;
 
 dim3 stencil_block(const Geom& g, int kernel);
 unsigned stencil_grid(const Geom& g, int kernel);  // blocks of one stencil launch (= partials it writes)
+// partials an epilogue launch writes (the FP64 Shamir kernel on staged tiles has its own grid)
+unsigned stencil_parts(const Geom& g, int kernel, bool fp64);
 
 // dslash.cu
 template <class S>
