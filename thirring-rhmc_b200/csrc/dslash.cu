@@ -1037,13 +1037,15 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
     const unsigned grd = tile_grid(g);
     tile::Maps maps;
     if (!tile_maps(g, i, reinterpret_cast<const double2*>(u), &maps)) return THR_ERR_CUDA;
+    int dev = 0;
+    cudaGetDevice(&dev);
 #define THR_T(D, E)                                                                                          \
   do {                                                                                                       \
-    static bool attr = false;                                                                                \
-    if (!attr) {                                                                                             \
+    static unsigned long long attr = 0; /* devices whose attributes are set */                               \
+    if (dev >= 64 || !(attr >> dev & 1ull)) {                                                                \
       cudaFuncSetAttribute(k_dslash_tile<D, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile::SMEM);    \
       cudaFuncSetAttribute(k_dslash_tile<D, E>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);        \
-      attr = true;                                                                                           \
+      if (dev < 64) attr |= 1ull << dev;                                                                     \
     }                                                                                                        \
     k_dslash_tile<D, E><<<grd, tile::NT, tile::SMEM, st>>>(o, i, maps, g, am, imass, am3, skip, ax, coef, partials, \
                                                            rev);                                             \
