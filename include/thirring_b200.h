@@ -124,7 +124,11 @@ int thr_congrad(thr_ctx *ctx, const double *Phi, double *X, float res, int *iter
  * capture.  All calls share the array: calls that overlap on the GPU (other
  * threads, other streams) race and must be serialised by the caller.
  * `stream` is a cudaStream_t (NULL = the legacy default stream); the call
- * returns when the solve has finished.  Semantics otherwise as thr_congrad. */
+ * returns when the solve has finished.  It runs no autotuning: the stencils
+ * use a register budget tuned earlier in the process or the default (same
+ * results either way), so nothing but the solve itself is launched on the
+ * caller's stream and no CUDA event is created.  Semantics otherwise as
+ * thr_congrad. */
 int thr_congrad_static(const thr_params *p, const void *u, const void *Phi, void *X, float res, int *itercg,
                        float am, int imass, int *iterations, void *stream);
 

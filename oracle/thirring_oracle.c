@@ -550,18 +550,29 @@ void orc_dirac_operator(const orc_lat *L, orc_zd *xout, const orc_zd *xin, const
 /* ------------------------------------------------------------------------ */
 /* interior reductions and updates                                           */
 /* ------------------------------------------------------------------------ */
+/* `body` adds into `acc`.  Each time slice is summed into its own partial and the
+ * partials are added in slice order, so the result does not depend on the number
+ * of threads (an OpenMP reduction clause would make it depend on the machine). */
 #define FOR_INTERIOR(body)                                                            \
-  _Pragma("omp parallel for schedule(static) reduction(+:acc)")                       \
-  for (int t = 1; t <= L->lt; t++)                                                    \
-    for (int d = 0; d < 4; d++)                                                       \
-      for (int y = 1; y <= L->ly; y++)                                                \
-        for (int x = 1; x <= L->lx; x++)                                              \
-          for (int s_ = 1; s_ <= L->ls; s_++) { size_t i = I5(s_, x, y, t, d); body; }
+  do {                                                                                \
+    double *part_ = (double *)calloc((size_t)L->lt, sizeof(double));                  \
+    _Pragma("omp parallel for schedule(static)")                                      \
+    for (int t = 1; t <= L->lt; t++) {                                                \
+      double acc = 0.0;                                                               \
+      for (int d = 0; d < 4; d++)                                                     \
+        for (int y = 1; y <= L->ly; y++)                                              \
+          for (int x = 1; x <= L->lx; x++)                                            \
+            for (int s_ = 1; s_ <= L->ls; s_++) { size_t i = I5(s_, x, y, t, d); body; } \
+      part_[t - 1] = acc;                                                             \
+    }                                                                                 \
+    for (int t = 0; t < L->lt; t++) acc += part_[t];                                  \
+    free(part_);                                                                      \
+  } while (0)
 
 /* sum(abs(z)**2) over the interior, abs = hypot as Fortran's intrinsic */
 static double norm2_int(const orc_lat *L, const orc_zd *a) {
   double acc = 0.0;
-  FOR_INTERIOR({ double m = hypot(a[i].re, a[i].im); acc += m * m; })
+  FOR_INTERIOR({ double m = hypot(a[i].re, a[i].im); acc += m * m; });
   return acc;
 }
 
@@ -727,7 +738,7 @@ void orc_multishift_solver(const orc_lat *L, const orc_zd *u, float am, int imas
     double alpha = 0.0;
     {
       double acc = 0.0;
-      FOR_INTERIOR({ acc += p[i].re * s[i].re - (-p[i].im) * s[i].im; })
+      FOR_INTERIOR({ acc += p[i].re * s[i].re - (-p[i].im) * s[i].im; });
       alpha = acc;
     }
     ms_after_alpha(&c, alpha, aden);
@@ -1323,7 +1334,7 @@ int orc_hamilton(const orc_lat *L, const orc_zd *u, const float *theta, const fl
   double hf = 0.0;
   {
     double acc = 0.0;
-    FOR_INTERIOR({ acc += R[i].re * Xr[i].re - (-R[i].im) * Xr[i].im; })
+    FOR_INTERIOR({ acc += R[i].re * Xr[i].re - (-R[i].im) * Xr[i].im; });
     hf = acc;
   }
   *h = *hg + *hp + hf;
@@ -1582,7 +1593,7 @@ void orc_odslashd(const orc_lat *L, orc_zd *Phi, const orc_zd *R, const orc_zd *
 
 static double redot_int(const orc_lat *L, const orc_zd *a, const orc_zd *b) {
   double acc = 0.0;
-  FOR_INTERIOR({ acc += a[i].re * b[i].re + a[i].im * b[i].im; })
+  FOR_INTERIOR({ acc += a[i].re * b[i].re + a[i].im * b[i].im; });
   return acc;
 }
 

@@ -130,3 +130,34 @@ def test_meson_and_fermion_converged(kernel, imass):
         got = G.fermion(1e-8, 0.1, imass, nsource=3)
         for k in ("cferm1", "cferm2"):
             np.testing.assert_allclose(got[k], ref[k], rtol=1e-5, atol=1e-6 * np.max(np.abs(ref[k])))
+
+
+def _measure_bits():
+    """One Wilson-kernel measurement (the set-up of test_measure_wilson_wilson[1]) as exact bits."""
+    dims = (6, 6, 8, 8)
+    L = O.lat(*dims, kernel=1)
+    u = rand_links(L, np.random.default_rng(51), beta=2.0)
+    with thirring.Lattice(*dims, kernel=1) as G:
+        G.set_links(u)
+        G.init_random(987654321.0)
+        got = G.measure(1e-8, 0.1, 1, kernel_meas=1, knoise=3)
+    return (np.asarray(got["parts"], dtype=np.float64).tobytes().hex(),
+            [int(v) for v in got["itercg"]], float(got["psibarpsi"]))
+
+
+@pytest.mark.gpu
+def test_measure_same_bits_in_fresh_processes():
+    # the batched FP64 measurement solves have no run-dependent choice: two fresh
+    # processes (each tuning its stencils anew) give identical bits
+    import os
+    import subprocess
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    code = ("import sys, json; sys.path.insert(0, %r); import conftest; import test_measure_gpu as t; "
+            "print(json.dumps(t._measure_bits()))" % here)
+    outs = []
+    for _ in range(2):
+        r = subprocess.run([sys.executable, "-c", code], cwd=here, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout + r.stderr
+        outs.append(r.stdout.strip().splitlines()[-1])
+    assert outs[0] == outs[1]

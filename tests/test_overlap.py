@@ -183,8 +183,10 @@ def test_oracle_permm_and_ikddw_identities():
 @pytest.mark.parametrize("imass", [1, 3])
 def test_measure_ow_vs_oracle(imass):
     """measure with kernel_meas = 2 (measure_wilsonKDDW) against the oracle on the
-    same links and site random streams: each congradO within 2 iterations, each
-    noise's pbp to 1e-6 relative (both solutions meet the stopping rule)."""
+    same links and site random streams: each congradO within 2 iterations or 2 %
+    of its count (about 180 here: on this operator, whose slice coefficients span
+    0.5 to 5, sums taken in another order move the exit by a few iterations),
+    each noise's pbp to 1e-6 relative (both solutions meet the stopping rule)."""
     dims = (6, 6, 4, 4)
     L = O.lat(*dims, kernel=1)
     u = rand_links(L, np.random.default_rng(50 + imass), beta=SOLVE["beta"])
@@ -197,7 +199,8 @@ def test_measure_ow_vs_oracle(imass):
         G.set_links(u)
         G.init_random(seed)
         got = G.measure(respbp, SOLVE["am"], imass, kernel_meas=2, knoise=knoise)
-    assert np.all(np.abs(np.array(got["itercg"]) - np.array(ref["itercg"])) <= 2)
+    its, its_ref = np.array(got["itercg"]), np.array(ref["itercg"])
+    assert np.all(np.abs(its - its_ref) <= np.maximum(2, 0.02 * its_ref))
     want = np.array([[p.real, p.imag] for p in ref["cpbp"]])
     scale = np.max(np.abs(want[:, 0]))
     assert np.max(np.abs(got["parts"][:, :2] - want)) <= 1e-6 * scale

@@ -8,6 +8,9 @@ at the first failure, every other test has already run.  It passes both run
 alone in a fresh process and after the rest of the suite.
 """
 import ctypes as C
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -30,8 +33,8 @@ def _dev_links(torch, u):
     return torch.from_numpy(np.ascontiguousarray(i.transpose(3, 2, 1, 0))).cuda()
 
 
-@pytest.mark.gpu
-def test_congrad_static_matches_congrad_twice():
+def _check_static_twice():
+    """thr_congrad_static twice in a row against thr_congrad on the congrad fixture."""
     import torch
     # tests/test_congrad.F90 fixture: 12^3 x 24, res 0.1, am 0.05, imass 3
     L = O.lat(12, 12, 12, 24)
@@ -56,6 +59,24 @@ def test_congrad_static_matches_congrad_twice():
         got = x.cpu().numpy()
         err = np.max(np.abs(got - ref)) / np.max(np.abs(ref))
         assert err <= TOL, (call, err)
+
+
+@pytest.mark.gpu
+def test_congrad_static_matches_congrad_twice():
+    _check_static_twice()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tune", ["0", "1"])
+def test_congrad_static_fresh_process(tune):
+    # alone in a fresh process, with the stencil autotuner off (THR_TUNE=0) and on: the
+    # allocation-free call never tunes, so it gives the same answer either way
+    here = os.path.dirname(os.path.abspath(__file__))
+    code = ("import sys; sys.path.insert(0, %r); import conftest; import test_zz_no_alloc as t; "
+            "t._check_static_twice(); print('ok')" % here)
+    env = dict(os.environ, THR_TUNE=tune)
+    r = subprocess.run([sys.executable, "-c", code], cwd=here, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
 
 
 @pytest.mark.gpu

@@ -7,12 +7,15 @@
 // vector kernels take the entry from blockIdx.y, and each entry keeps its
 // own CG scalars in device memory (converged entries are skipped).
 //
-// Precision: FP64 runs CG on the correction e of A e = b - A x0 in FP64
-// (congrad's stopping rule |r|^2 < 4*V*Ls*res^2 on every entry).  The mixed
-// modes keep x and the true residual in FP64 and solve each correction in
-// low precision (FP32 vectors, or BF16 storage of the stencil operands with
-// FP32 arithmetic) to a relative 1e-5 / 1e-2, then recompute the FP64 true
-// residual (defect correction) until every entry meets the rule.
+// Precision: FP64 is congrad itself (measure_module.F90:56-121) on every
+// entry: one CG from r = b - A x0, stopped by the recursive residual on
+// congrad's rule |r|^2 < 4*V*Ls*res^2 and never restarted, so the iteration
+// counts are the reference's (the solution is accumulated as x0 + e, which
+// differs from x += alpha p by rounding only).  The mixed modes keep x and
+// the true residual in FP64 and solve each correction in low precision (FP32
+// vectors, or BF16 storage of the stencil operands with FP32 arithmetic) to a
+// relative 1e-5 / 1e-2, then recompute the FP64 true residual (defect
+// correction) until every entry meets the rule on it.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -263,6 +266,15 @@ __global__ void k_reopen(BcgState* stt, int* skip, int nent) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e < nent) skip[e] = stt[e].done_outer;
 }
+
+// FP64 (congrad): the entry is finished when its CG met the rule on the
+// recursive residual; one that ran into the iteration cap stays open (MAXITER)
+__global__ void k_close_fp64(BcgState* stt, int nent) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nent) return;
+  BcgState& s = stt[e];
+  if (!s.done_outer && !s.status && s.rr < s.resid) s.done_outer = 1;
+}
 }  // namespace
 
 // FP64 operator T = M^dagger M X on the batch
@@ -341,6 +353,9 @@ int bcg_solve(BcgRun& br, int precision, float res, int max_outer, int* iters, i
       THR_TRY(bcg_inner<double2, double2>(br, (double2*)br.r, (double2*)br.p, (double2*)br.h, (double2*)br.q,
                                           (double2*)br.e, tol, inner_cap));
       k_accumulate<double2><<<vg, kT, 0, br.st>>>(tab.dev, br.state, br.X, (const double2*)br.e);
+      k_close_fp64<<<(ne + 127) / 128, 128, 0, br.st>>>(br.state, ne);
+      br.launches += 2;
+      break;  // congrad never restarts
     } else if (precision == THR_MIXED_BF16) {
       THR_TRY(bcg_inner<__nv_bfloat162, float2>(br, (float2*)br.r, (__nv_bfloat162*)br.p, (__nv_bfloat162*)br.h,
                                                 (__nv_bfloat162*)br.q, (float2*)br.e, tol, inner_cap));
@@ -357,8 +372,9 @@ int bcg_solve(BcgRun& br, int precision, float res, int max_outer, int* iters, i
   int rc = THR_OK;
   for (int e = 0; e < ne; e++) {
     // CG steps plus one per FP64 residual that started a correction (the
-    // reference counts its initial-residual pass as an iteration too)
-    if (iters) iters[e] = h[e].iters + h[e].rounds;
+    // reference counts its initial-residual pass as an iteration too: in FP64
+    // that pass is always one, itercg = 1 when the guess already meets the rule)
+    if (iters) iters[e] = h[e].iters + (precision == THR_FP64 ? 1 : h[e].rounds);
     if (h[e].status) rc = h[e].status;
     else if (!h[e].done_outer && rc == THR_OK) rc = THR_ERR_MAXITER;
   }

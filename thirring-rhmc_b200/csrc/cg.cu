@@ -344,10 +344,11 @@ extern "C" int thr_congrad_static(const thr_params* prm, const void* u, const vo
   const int chunk = 8;
   for (int base_it = 0; base_it < h.niterc + chunk; base_it += chunk) {
     for (int k = 0; k < chunk; k++) {
-      THR_TRY(launch_dslash<double2>(g, prm->kernel, false, x1, p, ud, am, imass, prm->am3, st, &cs->done));
+      // fixed-footprint stencils: no autotuner timing runs on the caller's stream
+      THR_TRY(launch_dslash_untuned<double2>(g, prm->kernel, false, x1, p, ud, am, imass, prm->am3, st, &cs->done));
       k_cg_norm2<<<gb, kThreads, 0, st>>>(cs, x1, n, partials);
       k_cg_alpha<<<1, 1024, 0, st>>>(cs, partials, gb);
-      THR_TRY(launch_dslash<double2>(g, prm->kernel, true, x2, x1, ud, am, imass, prm->am3, st, &cs->done));
+      THR_TRY(launch_dslash_untuned<double2>(g, prm->kernel, true, x2, x1, ud, am, imass, prm->am3, st, &cs->done));
       k_cg_rupdate<<<gb, kThreads, 0, st>>>(cs, r, x2, n, partials);
       k_cg_beta<<<1, 1024, 0, st>>>(cs, partials, gb);
       k_cg_xp<<<vec_grid(n / 4), kThreads, 0, st>>>(cs, Xd, p, r, n / 4, 0);

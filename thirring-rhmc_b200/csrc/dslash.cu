@@ -23,6 +23,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <map>
@@ -583,7 +584,7 @@ __global__ void __launch_bounds__(64, MINB)
 // FP64 Shamir kernel for the natural site order with Lx, Ly divisible by 4, Lt
 // by 2 and Ls by 8.  A block owns a 4x4x2 tile of sites and 8 consecutive s
 // (256 threads: s fastest, then x, y, t).  One thread first stages everything
-// the block's sites read into shared memory with 14 TMA tensor copies (no
+// the block's sites read into shared memory with 11 TMA tensor copies (no
 // multicast) completing on one mbarrier: the tile's spinors with one s on
 // either side (the s-neighbours), the six one-site faces around the tile, and
 // the links of the tile and of its three lower faces.  The spinor field is a
@@ -1022,11 +1023,19 @@ int tune_pick(const TuneKey& key, const int* cand, int ncand, cudaStream_t st, F
   return tv.pick;
 }
 
+// the candidate already tuned for `key`, else cand[0]; never times anything
+int tune_lookup(const TuneKey& key, const int* cand) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto it = g_tune.find(key);
+  return it != g_tune.end() ? it->second.pick : cand[0];
+}
+
 // epi: 0 none, 1 out = aux + (*coef) M in with |out|^2 per block, 2 |out|^2 per block
+// may_tune false: no timing launches and no events (a budget tuned earlier is still used)
 template <class S>
 int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
                        int imass, float am3, cudaStream_t st, const int* skip, const S* aux, const double* coef,
-                       double* partials, int e, int rev) {
+                       double* partials, int e, int rev, bool may_tune = true) {
   if (g.ls > 1024) return THR_ERR_BADSHAPE;
   if (4ULL * (unsigned long long)g.v5 >= (1ULL << 32)) return THR_ERR_BADSHAPE;  // 32-bit element offsets
   if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
@@ -1041,11 +1050,11 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
     cudaGetDevice(&dev);
 #define THR_T(D, E)                                                                                          \
   do {                                                                                                       \
-    static unsigned long long attr = 0; /* devices whose attributes are set */                               \
-    if (dev >= 64 || !(attr >> dev & 1ull)) {                                                                \
+    static std::atomic<unsigned long long> attr{0}; /* devices whose attributes are set */                 \
+    if (dev >= 64 || !(attr.load() >> dev & 1ull)) {                                                         \
       cudaFuncSetAttribute(k_dslash_tile<D, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile::SMEM);    \
       cudaFuncSetAttribute(k_dslash_tile<D, E>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);        \
-      if (dev < 64) attr |= 1ull << dev;                                                                     \
+      if (dev < 64) attr.fetch_or(1ull << dev);                                                              \
     }                                                                                                        \
     k_dslash_tile<D, E><<<grd, tile::NT, tile::SMEM, st>>>(o, i, maps, g, am, imass, am3, skip, ax, coef, partials, \
                                                            rev);                                             \
@@ -1141,8 +1150,8 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   if (tunable) {
     int dev = 0;
     cudaGetDevice(&dev);
-    minb = tune_pick(TuneKey{dev, storage_id<S>(), kernel, dag ? 1 : 0, e, g.lx, g.ly, g.lt, g.ls, g.layout}, cand,
-                     ncand, st, launch);
+    const TuneKey key{dev, storage_id<S>(), kernel, dag ? 1 : 0, e, g.lx, g.ly, g.lt, g.ls, g.layout};
+    minb = may_tune ? tune_pick(key, cand, ncand, st, launch) : tune_lookup(key, cand);
   }
   launch(minb);
 #undef THR_D
@@ -1177,6 +1186,13 @@ int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, cons
                   int imass, float am3, cudaStream_t st, const int* skip) {
   return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr, nullptr, 0,
                                0);
+}
+
+template <class S>
+int launch_dslash_untuned(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
+                          float am, int imass, float am3, cudaStream_t st, const int* skip) {
+  return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr, nullptr, 0, 0,
+                               false);
 }
 
 int launch_odslash(const Geom& g, bool dag, double2* out, const double2* in, const double2* u, float am, int imass,
@@ -1233,6 +1249,8 @@ int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const
 #define THR_INST(S, L)                                                                                            \
   template int launch_dslash<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float, cudaStream_t,   \
                                 const int*);                                                                      \
+  template int launch_dslash_untuned<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,        \
+                                        cudaStream_t, const int*);                                                \
   template int launch_dslash_axpy<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
                                      cudaStream_t, const int*, const S*, const double*, double*, int);            \
   template int launch_dslash_norm<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \

@@ -17,6 +17,12 @@ unsigned stencil_parts(const Geom& g, int kernel, bool fp64);
 template <class S>
 int launch_dslash(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
                   int imass, float am3, cudaStream_t st, const int* skip = nullptr);
+// as launch_dslash, but never runs the autotuner's timing launches (no events, no
+// synchronisation): the register budget is one tuned earlier in the process or the
+// default, which gives the same results
+template <class S>
+int launch_dslash_untuned(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
+                          float am, int imass, float am3, cudaStream_t st, const int* skip = nullptr);
 // rnew = rold + (*coef) * (M or M^dagger) in, without storing the stencil's output,
 // and one FP64 partial per block of |rnew|^2.  rev != 0: blocks take the sites from
 // the top down (same results; better L2 reuse of a field written just before)
