@@ -1,6 +1,6 @@
 """Regenerate the fixtures in this folder from the reference checkout.
 
-    python tests/golden/make_golden.py [/path/to/thirring-rhmc]
+    python tests/golden/make_golden.py /path/to/thirring-rhmc
 
 Copies the reference's rational-approximation coefficient files (data read
 by dwf3d_lib.F90:205-209 through remez_common_subroutines.F90:20-35) and the
@@ -46,4 +46,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py /path/to/thirring-rhmc")
+    main(sys.argv[1])

@@ -1,5 +1,5 @@
-"""bench.py's reference arm on CPU: the JSON line the round-end driver reads
-(one line, the contract's keys, the oracle timed on the host cores)."""
+"""bench.py's reference arm on CPU: it prints one JSON line with the
+benchmark contract's keys, the oracle timed on the host cores."""
 import json
 import os
 import subprocess
