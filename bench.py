@@ -50,6 +50,9 @@ PROF_STRIDE = 8
 PROF_KINDS = ((0, "k_dslash_M_hrec"), (2, "k_dslash_Mdag"), (1, "k_flush"))
 UNIT = "solves/s"
 HBM_FALLBACK = 6650.0
+# arithmetic of each mode: the mixed modes run FP64 first and FP32 (BF16 storage,
+# FP32 arithmetic) once the residual is small, with FP64 shift fields throughout
+DTYPES = {"fp64": "f64", "sp": "f32", "mixed": "f64+f32", "bf16": "f64+bf16"}
 
 
 def rational():
@@ -248,6 +251,24 @@ def run_ours(args, rank, world, local_rank):
         tot = C.c_double(0)
         L.thr_profile_read(h, kind, C.byref(n), C.byref(t), C.byref(b), C.byref(tot))
         prof[name] = dict(sampled=n.value, ms=t.value, bytes=b.value, launches=tot.value)
+    # ---- accuracy of the timed solves: the true residual of every shifted system of
+    # the last one (FP64, on the device), against the stopping rule of
+    # multishift_module.F90:244 (|r_k| * correction_k < res)
+    acc = shift_accuracy(L, h, pd, ad, an)
+    acc["left_fp64_at_iteration"] = G.mixed_switched_at() if mode in (2, 3) else None
+    # the batched FP64 solve (the arm mode would replace) timed once for the ratio, and
+    # for a low-precision mode the per-shift error of its solutions against it
+    fp64b_s = None
+    if mode != 0:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        it64 = solve(0)
+        e1.record(stream)
+        e1.synchronize()
+        fp64b_s = e0.elapsed_time(e1) / 1e3
+        acc["fp64_iterations"] = it64
+        acc["fp64_shift_true_residual"] = shift_accuracy(L, h, pd, ad, an)
+        acc["per_shift_rel_error_vs_fp64"] = shift_errors_vs_fp64(G, phi, anum, aden, mode)
     # the batched solver's graph runs batches in pairs: a batch is 32 iterations of 4
     # kernels (M with the h recurrence and |h|^2, alpha, M^dagger with the residual
     # update, lambda) plus the previous batch's flush (coefficients, flush, history
@@ -312,12 +333,49 @@ def run_ours(args, rank, world, local_rank):
     L.thr_tune_report(buf, len(buf))
     tune = [ln for ln in buf.value.decode().splitlines() if ln]
     res = dict(ms=ms, its=its, prof=prof, launches=launches, fp64_s=fp64_s, fp64_iters=fp64_iters, stream_s=stream_s,
-               tune=tune,
+               tune=tune, accuracy=acc, fp64_batched_s=fp64b_s,
                e2e_ms=e2e_ms, clocks=clk.summary(), dslash=dslash, phi_bytes=phi.nbytes)
     L.thr_field_destroy(h, pd)
     L.thr_field_destroy(h, px)
     G.close()
     return res
+
+
+def correction(anum, aden):
+    """multishift_module.F90:87-88: |anum/aden| over its geometric mean"""
+    c = np.abs(np.asarray(anum[1:]) / np.asarray(aden))
+    return c / np.exp(np.mean(np.log(c)))
+
+
+def shift_accuracy(L, h, pd, ad, an):
+    """True residual |Phi - (M^dagger M + aden_k) x_k| of every shifted solution of the
+    context's last solve (thr_shift_residuals_dev), times correction_k, over res."""
+    r2 = np.zeros(len(ad))
+    rc = L.thr_shift_residuals_dev(h, pd, None, len(ad), ad.ctypes.data_as(C.c_void_p), AM, IMASS,
+                                   r2.ctypes.data_as(C.c_void_p))
+    if rc != 0:
+        return {"error": rc}
+    t = np.sqrt(r2) * correction(an, ad) / RES
+    return {"max_true_residual_over_res": float(t.max()), "shift_of_max": int(t.argmax()),
+            "per_shift_true_residual_over_res": [float("%.3g" % v) for v in t],
+            "rule": "|Phi - (M^dagger M + aden_k) x_k| * correction_k / res (multishift_module.F90:244 tests the "
+                    "recursive residual against 1)"}
+
+
+def shift_errors_vs_fp64(G, phi, anum, aden, mode):
+    """|x_k - x_k(FP64)| / |x_k(FP64)| per shift, both solves through the C ABI (iflag 1
+    returns the shifted solutions in Phi0)."""
+    outs = []
+    for m in (0, mode):
+        Phi0 = np.zeros(G.sshape + (G.ndiag,), np.complex128, order="F")
+        G.qmrherm(phi, RES, AM, IMASS, anum, aden, 1, use_sp=m, Phi0=Phi0)
+        outs.append(Phi0)
+    err = []
+    for k in range(len(aden)):
+        a = outs[1][1:-1, 1:-1, 1:-1, 1:-1, :, k]
+        b = outs[0][1:-1, 1:-1, 1:-1, 1:-1, :, k]
+        err.append(float("%.3g" % (np.linalg.norm(a - b) / np.linalg.norm(b))))
+    return err
 
 
 def run_overlap(args):
@@ -431,10 +489,10 @@ def cpu_sample(iters_sample, threads=None):
     theta, phi = inputs(0)
     Lo = O.lat(LX, LY, LT, LS, beta=BETA, am3=AM3)
     u = O.coef(Lo, theta)
-    t0 = time.perf_counter()
+    # the oracle times its own iteration loop: the allocation and filling of the 25
+    # shift fields before it are not part of the sample
     O.multishift(Lo, u, AM, IMASS, anum[1:], aden, phi, RES, iters_sample)
-    dt = time.perf_counter() - t0
-    return dt / iters_sample, nthreads
+    return O.lib.orc_last_loop_seconds() / iters_sample, nthreads
 
 
 def cpu_model():
@@ -643,7 +701,7 @@ def main():
                              "overlap"],
                     help="secondary workloads print their own JSON line (not the headline contract)")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--cpu-iters", type=int, default=6, help="multishift iterations in the CPU sample")
+    ap.add_argument("--cpu-iters", type=int, default=50, help="multishift iterations in the CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--lx", type=int, default=0, help="profiling case: lattice extent (all three directions)")
     ap.add_argument("--ls", type=int, default=0, help="profiling case: fifth-dimension extent")
@@ -685,7 +743,7 @@ def main():
         per_iter = []
         nthreads = 0
         for _ in range(args.warmup + args.steps):
-            s, nthreads = cpu_sample(max(1, args.cpu_iters // 2))
+            s, nthreads = cpu_sample(max(1, args.cpu_iters // 2))  # loop time only, set-up excluded
             per_iter.append(s)
         timed = per_iter[args.warmup:]
         s_iter = float(np.mean(timed))
@@ -698,8 +756,9 @@ def main():
                 "config": workload_config(),
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port",
                                  "sample": f"{max(1, args.cpu_iters // 2)} multishift iterations per step of the "
-                                           f"same solve, scaled by the {iters} iterations a full solve takes; "
-                                           f"{cpu_model()}"},
+                                           f"same solve (the iteration loop timed, its set-up excluded), the solve "
+                                           f"time projected to the {iters} iterations a full FP64 solve takes "
+                                           f"({s_iter:.3f} s per iteration); {cpu_model()}"},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "wall_s": round(time.perf_counter() - t0, 1)}
         print(json.dumps(line), flush=True)
@@ -749,8 +808,9 @@ def main():
         s_iter, nthreads = cpu_sample(args.cpu_iters)
         cpu_val = 1.0 / (s_iter * iters)
         cpu = {"value": cpu_val, "unit": UNIT, "cores": nthreads, "kind": "port",
-               "sample": f"{args.cpu_iters} FP64 multishift iterations of the same solve ({s_iter:.3f} s/iter), "
-                         f"scaled to the {iters} iterations the solve takes; {cpu_model()}"}
+               "sample": f"{args.cpu_iters} FP64 multishift iterations of the same solve (the iteration loop "
+                         f"timed, set-up excluded: {s_iter:.3f} s per iteration), projected to the {iters} "
+                         f"iterations the solve takes; {cpu_model()}"}
     e2e = None
     if r["e2e_ms"]:
         e2e = {"value": job_throughput(world, args.e2e_steps, r["e2e_ms"]), "unit": UNIT,
@@ -758,7 +818,7 @@ def main():
                "path": "thr_qmrherm (C ABI) with page-locked Fortran-layout host arrays"}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.mode == "fp64" else args.mode,
+            "vs_baseline": None, "dtype": DTYPES[args.mode],
             "data": "synthetic (seeded Gaussian theta, complex Gaussian source)",
             "config": workload_config(), "iterations": iters, "e2e": e2e, "roofline": roofline,
             "kernels": other, "cpu_baseline": cpu, "gpu_launches": r["launches"], "clocks": r["clocks"],
@@ -766,6 +826,9 @@ def main():
             "plain_fp64_gpu_solve_s": r["fp64_s"], "plain_fp64_gpu_iterations": r["fp64_iters"],
             "speedup_vs_plain_fp64_gpu": (r["fp64_s"] / (ms_step / 1e3)) if r["fp64_s"] else None,
             "batched_host_launched_solve_s": r["stream_s"],
+            "batched_fp64_solve_s": r["fp64_batched_s"] if r["fp64_batched_s"] else ms_step / 1e3,
+            "speedup_vs_batched_fp64": (r["fp64_batched_s"] / (ms_step / 1e3)) if r["fp64_batched_s"] else None,
+            "accuracy": r["accuracy"],
             "autotune": r["tune"],
             "dslash_48x48x48_ls48_fp64": r["dslash"]}
     print(json.dumps(line), flush=True)

@@ -254,8 +254,14 @@ int thr_set_solver(thr_ctx *ctx, int multishift_algo);
  *   iflag 2: x = anum(0) Phi; dSdpi += sum_i derivs(x_i, M x_i, anum(i), 0)
  *   iflag 3: x = anum(0) Phi; dSdpi += sum_i [derivs(Phi0_i, M x_i, -anum(i), 0)
  *                                            + derivs(M Phi0_i, x_i, -anum(i), 1)]
- * anum has ndiagq+1 entries (anum(0:ndiagq)).  use_sp != 0 selects the
- * single-precision multishift (Shamir only, as in the reference).
+ * anum has ndiagq+1 entries (anum(0:ndiagq)).  use_sp selects the multishift
+ * precision: 0 FP64; 1 the reference's single-precision multishift (FP32
+ * vectors, FP64 scalars; Shamir only, as in the reference, else FP64);
+ * THR_MIXED_FP32 (2) / THR_MIXED_BF16 (3) the mixed solver -- FP64 until the
+ * base residual falls below a fraction of |Phi| (thr_set_mixed), then the
+ * stencils, residuals and search direction in FP32 (BF16 storage with FP32
+ * arithmetic) while the shifted solutions stay FP64; with the batched
+ * organisation only (thr_set_solver 0 runs these modes in FP64).
  * dSdpi (gforce::dSdpi, accumulated) and Phi0 (qmrherm_module::Phi0,
  * (0:Ls+1,…,4,ndiag)) may be NULL to keep them in the context only; the
  * context always keeps the last Phi0 written by iflag 1.
@@ -264,6 +270,16 @@ int thr_set_solver(thr_ctx *ctx, int multishift_algo);
 int thr_qmrherm(thr_ctx *ctx, const double *Phi, double *x, float res, int *itercg, float am, int imass,
                 const double *anum, const double *aden, int ndiagq, int iflag, int use_sp, int *cg_returns,
                 double *dSdpi, double *Phi0, int max_qmr_iters);
+
+/* The mixed multishift's precision switch -- no counterpart in the reference.
+ * The base iteration leaves FP64 for FP32 (BF16 storage) once |r| < switch *
+ * |input|; defaults 1e-8 and 1e-13.  Rounding made while |r| is still large
+ * stays in every shifted solution (the shifted systems have no residual of
+ * their own to correct it), so a switch made too early costs accuracy, not
+ * iterations; 0 never switches.  thr_mixed_switched_at returns the iteration
+ * at which the last mixed solve switched (0: it finished in FP64). */
+int thr_set_mixed(thr_ctx *ctx, double switch_fp32, double switch_bf16);
+int thr_mixed_switched_at(thr_ctx *ctx, int *iteration);
 
 /* ---- derivs_module.F90 --------------------------------------------------- */
 /* derivs(R, X2, anum, iflag, am, imass), derivs_module.F90:8-26: adds the
@@ -380,6 +396,23 @@ int thr_odslash_dev(thr_ctx *ctx, void *out, const void *in, float am, int imass
  * context.  Returns when the solve has converged (its scalars are polled). */
 int thr_qmrherm_dev(thr_ctx *ctx, const void *Phi, void *x, float res, int *itercg, float am, int imass,
                     const double *anum, const double *aden, int ndiagq, int iflag, int use_sp, int *cg_returns);
+/* The solvers' fused stencil epilogues on device fields of one precision, so a
+ * caller can build its own iteration from them -- no counterpart in the
+ * reference.  With Op = M (dag = 0) or M^dagger (dag = 1) and the current links:
+ *   mode 0: out = Op in                  (*norm2 = |out|^2 when norm2 != NULL)
+ *   mode 1: out = aux + coef * Op in     (*norm2 = |out|^2; Op in is never stored)
+ *   mode 3: out = Op in + coef * aux     (*norm2 = |out|^2)
+ * aux must differ from in and out.  |out|^2 is summed in FP64 in a fixed order.
+ * Returns after the sum is on the host (mode 0 without norm2: enqueued only). */
+int thr_dslash_fused_dev(thr_ctx *ctx, void *out, const void *in, const void *aux, double coef, int precision,
+                         float am, int imass, int dag, int mode, double *norm2);
+/* The true residual of every shifted system, r2[k] = |Phi - (M^dagger M + aden[k]) x_k|^2
+ * in FP64 for k < nq, with the current links -- no counterpart in the reference,
+ * whose stopping rule (multishift_module.F90:244) tests the recursive residual.
+ * Phi and x are FP64 device fields (x: nq consecutive fields); x = NULL takes the
+ * context's last multishift solutions (those of the last qmrherm call). */
+int thr_shift_residuals_dev(thr_ctx *ctx, const void *Phi, const void *x, int nq, const double *aden, float am,
+                            int imass, double *r2);
 int thr_sync(thr_ctx *ctx);
 /* the context's cudaStream_t, for event timing by the caller */
 int thr_get_stream(thr_ctx *ctx, void **stream);

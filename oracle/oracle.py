@@ -141,6 +141,7 @@ for name, res, args in [
     ("orc_odslashd", None, [_L, _v, _v, _v, C.c_float, C.c_int, _v]),
     ("orc_congrad_o", C.c_int, [_L, _v, _v, _v, C.c_float, C.c_float, C.c_int, _v, C.c_int, C.POINTER(C.c_int)]),
     ("orc_num_threads", C.c_int, []),
+    ("orc_last_loop_seconds", C.c_double, []),
     ("orc_set_num_threads", None, [C.c_int]),
 ]:
     f = getattr(lib, name)

@@ -708,6 +708,8 @@ static void ms_converge(ms_scalars *c, double lambda, float res) {
   c->delta = lambda;
 }
 
+static double g_last_loop_seconds = 0.0;
+
 void orc_multishift_solver(const orc_lat *L, const orc_zd *u, float am, int imass, int ndiagq, const double *aden,
                            const double *anum, orc_zd *output, const orc_zd *input, float res, int maxcg,
                            int *cg_return, int *cg_returns) {
@@ -730,6 +732,7 @@ void orc_multishift_solver(const orc_lat *L, const orc_zd *u, float am, int imas
           for (int x = 1; x <= L->lx; x++)
             for (int ss = 1; ss <= L->ls; ss++) sf[IO(ss, x, y, t, d, k)] = input[I5(ss, x, y, t, d)];
   int it = 0;
+  const double t_loop = omp_get_wtime();
   while (c.maxishift > c.minishift - 1 && it < maxcg) {
     it++;
     orc_dslash(L, h, p, u, am, imass);
@@ -767,9 +770,13 @@ void orc_multishift_solver(const orc_lat *L, const orc_zd *u, float am, int imas
     orc_update_halo_5(L, p);
   }
   *cg_return = it;
+  g_last_loop_seconds = omp_get_wtime() - t_loop;
   ms_free(&c);
   free(r); free(h); free(s); free(p); free(sf);
 }
+
+/* seconds the last orc_multishift_solver spent in its iteration loop (set-up excluded) */
+double orc_last_loop_seconds(void) { return g_last_loop_seconds; }
 
 /* reduce_real_dp5d (reductions.F90:6-32): FP32 terms summed into FP64 with
  * the FIRST index outermost and the fifth innermost. */

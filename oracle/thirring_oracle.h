@@ -183,6 +183,8 @@ int orc_congrad_o(const orc_lat *L, const orc_zd *Phi, orc_zd *X, const orc_zd *
 
 /* threads used by the OpenMP loops */
 int orc_num_threads(void);
+/* seconds the last orc_multishift_solver spent in its iteration loop (set-up excluded) */
+double orc_last_loop_seconds(void);
 void orc_set_num_threads(int n);
 
 #ifdef __cplusplus

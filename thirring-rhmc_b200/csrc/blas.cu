@@ -12,7 +12,7 @@ constexpr int kRedThreads = 256;
 
 inline int red_blocks(size_t n) {
   size_t b = (n + kRedThreads * 4 - 1) / (kRedThreads * 4);
-  if (b > 148 * 8) b = 148 * 8;
+  if (b > device_sms() * 8) b = device_sms() * 8;
   if (b < 1) b = 1;
   return (int)b;
 }
@@ -83,7 +83,7 @@ __global__ void k_scale_copy(double2* y, const double2* x, double a, size_t n) {
 
 inline unsigned ew_grid(size_t n) {
   size_t b = (n + 255) / 256;
-  if (b > 148 * 16) b = 148 * 16;
+  if (b > device_sms() * 16) b = device_sms() * 16;
   return (unsigned)(b ? b : 1);
 }
 }  // namespace

@@ -122,7 +122,7 @@ __global__ void k_cg_loop(CgState* cs, cudaGraphConditionalHandle h) {
 
 inline unsigned vec_grid(size_t n) {
   size_t b = (n + kThreads - 1) / kThreads;
-  if (b > 148 * 8) b = 148 * 8;
+  if (b > device_sms() * 8) b = device_sms() * 8;
   return (unsigned)(b ? b : 1);
 }
 

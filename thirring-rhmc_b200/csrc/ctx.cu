@@ -3,6 +3,7 @@
 #include <cstdlib>
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 #include "ctx.h"
 #include "ms.h"
@@ -365,6 +366,59 @@ int thr_dslash_dev(thr_ctx* c, void* out, const void* in, int precision, float a
                                            (const __nv_bfloat162*)in, c->u32, am, imass, c->p.am3, c->st);
     default: return THR_ERR_BADARG;
   }
+}
+
+// the solvers' fused stencil epilogues on device fields; the coefficient goes
+// through a device scalar (the kernels read it from memory, as in the solvers)
+int thr_dslash_fused_dev(thr_ctx* c, void* out, const void* in, const void* aux, double coef, int precision,
+                         float am, int imass, int dag, int mode, double* norm2) {
+  if (!c || !out || !in) return THR_ERR_BADARG;
+  if (imass != 1 && imass != 3 && imass != 5) return THR_ERR_BADARG;
+  if (mode != 0 && mode != 1 && mode != 3) return THR_ERR_BADARG;
+  if (mode != 0 && (!aux || aux == out || aux == in)) return THR_ERR_BADARG;
+  if (mode == 3 && !norm2) return THR_ERR_BADARG;
+  if (mode == 1 && !norm2) return THR_ERR_BADARG;
+  if (!c->links_ok) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  double* dcoef = c->dscal + kScalFusedCoef;
+  double* dsum = c->dscal + kScalFusedSum;
+  THR_CUDA(cudaMemcpyAsync(dcoef, &coef, sizeof(double), cudaMemcpyHostToDevice, c->st));
+  const bool fp64 = precision == THR_FP64;
+  const int epi = mode == 0 ? (norm2 ? 2 : 0) : mode;
+  auto run = [&](auto* o, const auto* i, const auto* a, const auto* u) -> int {
+    using S = std::remove_cv_t<std::remove_pointer_t<decltype(o)>>;
+    if (epi == 0) return launch_dslash<S>(c->g, c->p.kernel, dag != 0, o, i, u, am, imass, c->p.am3, c->st);
+    if (epi == 2)
+      return launch_dslash_norm<S>(c->g, c->p.kernel, dag != 0, o, i, u, am, imass, c->p.am3, c->st, nullptr,
+                                   c->partials);
+    if (epi == 1)
+      return launch_dslash_axpy<S>(c->g, c->p.kernel, dag != 0, o, i, u, am, imass, c->p.am3, c->st, nullptr, a,
+                                   dcoef, c->partials);
+    return launch_dslash_accum<S>(c->g, c->p.kernel, dag != 0, o, i, u, am, imass, c->p.am3, c->st, nullptr, a,
+                                  dcoef, c->partials);
+  };
+  int rc;
+  switch (precision) {
+    case THR_FP64:
+      rc = run((double2*)out, (const double2*)in, (const double2*)aux, (const double2*)c->u64);
+      break;
+    case THR_FP32_REF:
+    case THR_MIXED_FP32:
+      rc = run((float2*)out, (const float2*)in, (const float2*)aux, (const float2*)c->u32);
+      break;
+    case THR_MIXED_BF16:
+      rc = run((__nv_bfloat162*)out, (const __nv_bfloat162*)in, (const __nv_bfloat162*)aux, (const float2*)c->u32);
+      break;
+    default: return THR_ERR_BADARG;
+  }
+  if (rc) return rc;
+  if (epi != 0) {
+    finish_sum(c->partials, (int)stencil_parts(c->g, c->p.kernel, fp64), dsum, c->st);
+    THR_CUDA(cudaMemcpyAsync(c->hscal + kScalFusedSum, dsum, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    THR_TRY(c->sync());
+    *norm2 = c->hscal[kScalFusedSum];
+  }
+  return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
 
 int thr_sync(thr_ctx* c) {

@@ -20,6 +20,12 @@
     if (rc_ != THR_OK) return rc_;    \
   } while (0)
 
+// slots of the context's device scalar block (dscal, 4096 doubles) outside the
+// solver states that start at its base
+constexpr int kScalHamSum = 4000;      // hamilton's fermion sum
+constexpr int kScalFusedCoef = 4090;   // thr_dslash_fused_dev: the epilogue coefficient
+constexpr int kScalFusedSum = 4091;    // thr_dslash_fused_dev / thr_shift_residuals_dev: a reduced sum
+
 struct thr_ctx {
   thr_params p;
   thr::Geom g;
@@ -80,7 +86,13 @@ struct thr_ctx {
   int max_qmr_iters = 50000;
   int ms_algo = 1;          // multishift: 0 = per-iteration shift updates, 1 = batched
   bool use_graphs = true;   // batched solver loops as one CUDA graph (WHILE node) per solve
-  void* ms_graphs[2] = {};  // cached batched-multishift graphs (FP64, FP32 vectors)
+  // cached batched-multishift graphs: FP64; FP32 vectors; FP32 and BF16 base
+  // iteration with FP64 shift fields (the low-precision phase of the mixed solver)
+  void* ms_graphs[4] = {};
+  // mixed-precision multishift: relative base residual |r|/|input| below which the
+  // base iteration leaves FP64 (FP32, BF16 storage); thr_set_mixed
+  double mixed_switch[2] = {1e-8, 1e-13};
+  int mixed_switched_at = 0;  // iteration the last mixed solve left FP64 at (0: never)
   void* cg_graph = nullptr;  // cached congrad graph
   // sweep directions of the solver kernels (THR_REVERSE=0|1|2): 0 all bottom up; 1 the
   // M^dagger-with-update stencil top down; 2 (default) directions alternate per iteration

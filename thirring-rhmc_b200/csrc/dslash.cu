@@ -885,6 +885,21 @@ __global__ void __launch_bounds__(256, KER == 0 ? 4 : 1)
 }
 
 // ---------------------------------------------------------------- launch
+int device_sms() {
+  constexpr int kDevs = 64;
+  static std::atomic<int> cache[kDevs];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return 148;
+  if (dev < kDevs) {
+    const int v = cache[dev].load(std::memory_order_relaxed);
+    if (v > 0) return v;
+  }
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
+  if (dev < kDevs) cache[dev].store(sms, std::memory_order_relaxed);
+  return sms;
+}
+
 namespace {
 int stencil_threads(const Geom& g, int kernel) {
   const int nt = kernel == 0 ? 128 : 256;
@@ -1231,7 +1246,7 @@ int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const
                         double* partials, int grid) {
   if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;
   const bool epi = aux != nullptr;
-  const int g = grid > 0 ? grid : (b.total_blocks < 148 * 8 ? b.total_blocks : 148 * 8);
+  const int g = grid > 0 ? grid : (b.total_blocks < device_sms() * 8 ? b.total_blocks : device_sms() * 8);
 #define THR_L(K, D, E)                                                                                          \
   k_dslash_batch<S, K, D, E><<<g, 256, 0, st>>>(out, in, u, b.dev, b.nent, b.total_blocks, am, imass, am3, skip, \
                                                 aux, partials)

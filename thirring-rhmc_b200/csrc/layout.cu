@@ -139,7 +139,7 @@ __global__ void k_to_fortran_ps(float* fout, const float* in, Geom g) {
 
 inline unsigned grid_for(size_t n, int threads = 256) {
   size_t b = (n + threads - 1) / threads;
-  if (b > 148 * 32) b = 148 * 32;
+  if (b > device_sms() * 32) b = device_sms() * 32;
   if (b < 1) b = 1;
   return (unsigned)b;
 }

@@ -88,7 +88,7 @@ __global__ void k_finish(const double* partials, int np, double* out) {
 
 inline unsigned grid(size_t n) {
   size_t b = (n + kThreads - 1) / kThreads;
-  if (b > 148 * 4) b = 148 * 4;
+  if (b > device_sms() * 4) b = device_sms() * 4;
   return (unsigned)(b ? b : 1);
 }
 }  // namespace
@@ -111,10 +111,10 @@ int md_fields(thr_ctx* c, MdFields* f) {
 }
 
 static int reduce_to_host(thr_ctx* c, int np, double* out) {
-  k_finish<<<1, 1024, 0, c->st>>>(c->partials, np, c->dscal + 4000);
-  THR_CUDA(cudaMemcpyAsync(c->hscal + 4000, c->dscal + 4000, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  k_finish<<<1, 1024, 0, c->st>>>(c->partials, np, c->dscal + kScalHamSum);
+  THR_CUDA(cudaMemcpyAsync(c->hscal + kScalHamSum, c->dscal + kScalHamSum, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   THR_CUDA(cudaStreamSynchronize(c->st));
-  *out = c->hscal[4000];
+  *out = c->hscal[kScalHamSum];
   return THR_OK;
 }
 

@@ -150,7 +150,7 @@ __global__ void k_fill_shifts(V* sf, const V* in, size_t n, size_t stride, int n
 
 inline unsigned vec_grid(size_t n) {
   size_t b = (n + kThreads - 1) / kThreads;
-  if (b > 148 * 8) b = 148 * 8;
+  if (b > device_sms() * 8) b = device_sms() * 8;
   return (unsigned)(b ? b : 1);
 }
 }  // namespace

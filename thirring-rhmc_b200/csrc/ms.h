@@ -14,6 +14,9 @@ struct MsState {
   double flush_fields;  // fields moved by the batched shift updates (for traffic accounting)
   long long kbase;      // batched solver: first iteration of the current batch (ring slot base)
   int batches, max_batches;  // batched solver: batches run, and the bound on them
+  // mixed precision (batched solver): the FP64 phase ends once delta = |r|^2 falls
+  // below switch_delta = switch_rel2 * |input|^2 (0: never)
+  double switch_rel2, switch_delta;
   double zeta_i[kMaxShift], zeta_ii[kMaxShift], zeta_iii[kMaxShift];
   double omegas[kMaxShift], gammas[kMaxShift], correction[kMaxShift], aden[kMaxShift];
   int flags[kMaxShift], cg_returns[kMaxShift];
@@ -95,6 +98,18 @@ template <class V>
 int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p, V* hv, V* s, int ndiagq,
                            const double* aden, const double* anum, float res, float am, int imass, int maxcg,
                            int* cg_return, int* cg_returns);
+
+// Mixed precision: the batched FP64 solve until |r| < switch_rel |input|, then
+// the base iteration (stencils, residual ring, h) in the storage type VL
+// (float2: FP32; __nv_bfloat162: BF16 storage with FP32 arithmetic) while the
+// shift fields out/sf stay FP64.  ring64 holds 2 kBatch FP64 fields; the VL
+// ring is placed in its upper half.  low: 3 VL work fields.  *switched_at
+// gets the iteration the precision changed at (0: the solve ended in FP64).
+template <class VL>
+int multishift_mixed_dev(thr_ctx* c, const double2* in, double2* out, double2* sf, double2* ring64, double2* p,
+                         double2* hv, double2* s, VL* low, int ndiagq, const double* aden, const double* anum,
+                         float res, float am, int imass, int maxcg, double switch_rel, int* cg_return,
+                         int* cg_returns, int* switched_at);
 
 template <class V>
 int multishift_dev(thr_ctx* c, const V* u_dummy, const V* in, V* out, V* sf, V* r, V* p, V* hv, V* s, int ndiagq,

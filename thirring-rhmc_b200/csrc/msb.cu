@@ -58,6 +58,7 @@ __global__ void k_init(MsState* ms, MsHist* hist, const double* partials, int np
   const double d = block_sum_partials(partials, np);
   if (threadIdx.x == 0) {
     ms->delta = d;
+    ms->switch_delta = ms->switch_rel2 * d;
     hist[0].nsteps = 0;
     hist[1].nsteps = 0;
   }
@@ -186,9 +187,18 @@ __global__ void k_flush_coef(MsState* ms, const MsHist* hist, MsCoef* cf) {
 // current one is combined.
 constexpr int kFlushThreads = 128;
 constexpr int kFlushBlocks = 3;  // resident per SM at the register budget of kBatch residuals
-template <class V>
+// a ring value in the shift fields' complex type (exact widening)
+__device__ __forceinline__ double2 widen(double2 v, double2) { return v; }
+__device__ __forceinline__ double2 widen(float2 v, double2) { return make_double2((double)v.x, (double)v.y); }
+__device__ __forceinline__ double2 widen(__nv_bfloat162 v, double2) {
+  const float2 f = __bfloat1622float2(v);
+  return make_double2((double)f.x, (double)f.y);
+}
+__device__ __forceinline__ float2 widen(float2 v, float2) { return v; }
+
+template <class V, class VR = V>
 __global__ void __launch_bounds__(kFlushThreads, kFlushBlocks)
-    k_flush(const MsCoef* cf, V* __restrict__ out, V* __restrict__ sf, const V* __restrict__ ring, size_t n,
+    k_flush(const MsCoef* cf, V* __restrict__ out, V* __restrict__ sf, const VR* __restrict__ ring, size_t n,
             size_t stride, int first) {
   using R = typename W<V>::R;
   const int ns = cf->ns;
@@ -210,7 +220,7 @@ __global__ void __launch_bounds__(kFlushThreads, kFlushBlocks)
   }
   __syncthreads();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    V rj[kBatch];
+    VR rj[kBatch];  // held in the ring's own type, widened where used
 #pragma unroll
     for (int j = 0; j < kBatch; j++) {
       const int slot = first + j < 2 * kBatch ? first + j : first + j - 2 * kBatch;
@@ -229,8 +239,9 @@ __global__ void __launch_bounds__(kFlushThreads, kFlushBlocks)
       for (int j = 0; j < kBatch; j++) {
         if (j < ns) {
           const R2 bq = s_BQ[k][j];
-          f = f + bq.x * rj[j];
-          o = o - bq.y * rj[j];
+          const V r = widen(rj[j], V{});
+          f = f + bq.x * r;
+          o = o - bq.y * r;
         }
       }
       sf[k * stride + i] = f;
@@ -259,6 +270,8 @@ __global__ void k_loop_ctl(MsState* ms, cudaGraphConditionalHandle h) {
   unsigned more = 1u;
   if (ms->done) {
     more = 0u;
+  } else if (ms->switch_delta > 0.0 && ms->delta < ms->switch_delta) {
+    more = 0u;  // the FP64 phase of a mixed solve ends here (after this pair of batches)
   } else if (ms->batches >= ms->max_batches) {
     ms->status = THR_ERR_MAXITER;
     ms->done = 1;
@@ -277,20 +290,21 @@ __global__ void k_fill(V* sf, const V* in, size_t n, size_t stride, int nq) {
 
 inline unsigned vec_grid(size_t n) {
   size_t b = (n + kThreads - 1) / kThreads;
-  if (b > 148 * 8) b = 148 * 8;
+  if (b > device_sms() * 8) b = device_sms() * 8;
   return (unsigned)(b ? b : 1);
 }
 }  // namespace
 
 namespace {
-// flush of the batch recorded in hist (ring half `half`) on stream `on`
-template <class V>
-void enqueue_flush(thr_ctx* c, cudaStream_t on, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, const V* ring,
+// flush of the batch recorded in hist (ring half `half`) on stream `on`; the
+// shift fields are VO, the ring V
+template <class V, class VO = V>
+void enqueue_flush(thr_ctx* c, cudaStream_t on, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO* sf, const V* ring,
                    int half, bool prof, long long tag, int* prof_flush) {
   const size_t n = c->n4();
   const int pe = prof ? c->prof_begin(thr_ctx::P_SHIFTUPD, 0.0, tag, on) : -1;
   k_flush_coef<<<1, kMaxShift, 0, on>>>(ms, hist, cf);
-  k_flush<V><<<flush_grid(n), kFlushThreads, 0, on>>>(cf, out, sf, ring, n, n, half * kBatch + 1);
+  k_flush<VO, V><<<flush_grid(n), kFlushThreads, 0, on>>>(cf, out, sf, ring, n, n, half * kBatch + 1);
   c->prof_end(pe, on);
   if (prof_flush) *prof_flush = pe;
   k_reset<<<1, 1, 0, on>>>(hist, ms);
@@ -302,16 +316,16 @@ void enqueue_flush(thr_ctx* c, cudaStream_t on, MsState* ms, MsHist* hist, MsCoe
 // reads r from slot half*kBatch + j and writes the new r to the next slot (mod
 // 2 kBatch), so each half's batch starts from the other half's last residual.
 // prof: sample kernel timings with events (stream-launched solves only).
-template <class V>
-int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V* ring, V* p, V* hv, V* s,
+template <class V, class VO = V>
+int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO* sf, V* ring, V* p, V* hv, V* s,
                   float am, int imass, int half, long long k0, bool prof, int* prof_flush) {
   const size_t n = c->n4();
   const unsigned gb = vec_grid(n / 4);
-  const unsigned gs = stencil_parts(c->g, c->p.kernel, sizeof(V) == sizeof(double2));
-  const bool sp = sizeof(V) == sizeof(float2);
+  const bool fp64 = sizeof(V) == sizeof(double2);
+  const unsigned gs = stencil_parts(c->g, c->p.kernel, fp64);
   const typename Sto<V>::C* u =
-      sp ? (const typename Sto<V>::C*)(const void*)c->u32 : (const typename Sto<V>::C*)(const void*)c->u64;
-  const double lb = sp ? sizeof(float2) : sizeof(double2);
+      fp64 ? (const typename Sto<V>::C*)(const void*)c->u64 : (const typename Sto<V>::C*)(const void*)c->u32;
+  const double lb = fp64 ? sizeof(double2) : sizeof(float2);
   // the previous batch's flush, forked onto the side stream (c->overlap_flush 0: in line;
   // also in line while kernel timings are sampled, so that each sampled duration is
   // that kernel's alone and not one shared with a concurrent flush)
@@ -320,8 +334,8 @@ int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* 
     THR_CUDA(cudaEventRecord(c->ev_fork[half], c->st));
     THR_CUDA(cudaStreamWaitEvent(c->st2, c->ev_fork[half], 0));
   }
-  enqueue_flush<V>(c, fork ? c->st2 : c->st, ms, hist + (1 - half), cf + (1 - half), out, sf, ring, 1 - half, prof,
-                   k0 - kBatch, prof_flush);
+  enqueue_flush<V, VO>(c, fork ? c->st2 : c->st, ms, hist + (1 - half), cf + (1 - half), out, sf, ring, 1 - half,
+                       prof, k0 - kBatch, prof_flush);
   if (fork) THR_CUDA(cudaEventRecord(c->ev_join[half], c->st2));
   // h = M p is kept by the recurrence h_new = M r + gammag h_old (p = r + gammag p
   // and linearity), so p is never formed: the M launch reads the newest residual,
@@ -379,13 +393,18 @@ struct MsGraph {
   }
 };
 
-template <class V>
-int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V* ring, V* p, V* hv, V* s, float am,
+// graph cache slot of a (base storage, shift field) pair
+template <class V, class VO> constexpr int graph_slot() {
+  return sizeof(VO) == sizeof(float2) ? 1 : sizeof(V) == sizeof(double2) ? 0 : sizeof(V) == sizeof(float2) ? 2 : 3;
+}
+
+template <class V, class VO = V>
+int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO* sf, V* ring, V* p, V* hv, V* s, float am,
              int imass, cudaGraphExec_t* exec_out) {
-  const int slot = sizeof(V) == sizeof(float2) ? 1 : 0;
+  const int slot = graph_slot<V, VO>();
   if (!c->ms_graphs[slot]) c->ms_graphs[slot] = new MsGraph();
   MsGraph& G = *static_cast<MsGraph*>(c->ms_graphs[slot]);
-  const void* u = sizeof(V) == sizeof(float2) ? (const void*)c->u32 : (const void*)c->u64;
+  const void* u = sizeof(V) == sizeof(double2) ? (const void*)c->u64 : (const void*)c->u32;
   if (G.exec && G.out == out && G.sf == sf && G.ring == ring && G.p == p && G.hv == hv && G.s == s && G.u == u &&
       G.partials == c->partials && G.ms == ms && G.hist == hist && G.cf == cf && G.am == am && G.am3 == c->p.am3 && G.imass == imass &&
       G.kernel == c->p.kernel && G.n == c->n4()) {
@@ -415,8 +434,9 @@ int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V
   THR_CUDA(cudaGraphAddNode(&node, G.graph, nullptr, 0, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   THR_CUDA(cudaStreamBeginCaptureToGraph(c->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  int rc = enqueue_batch<V>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 0, 0, false, nullptr);
-  if (rc == THR_OK) rc = enqueue_batch<V>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 1, 0, false, nullptr);
+  int rc = enqueue_batch<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 0, 0, false, nullptr);
+  if (rc == THR_OK)
+    rc = enqueue_batch<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 1, 0, false, nullptr);
   if (rc == THR_OK) k_loop_ctl<<<1, 1, 0, c->st>>>(ms, handle);
   cudaGraph_t captured = nullptr;
   cudaError_t ce = cudaStreamEndCapture(c->st, &captured);
@@ -424,7 +444,7 @@ int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, V* out, V* sf, V
     // after the loop: the flush of the last batch (ring half 1)
     ce = cudaStreamBeginCaptureToGraph(c->st, G.graph, &node, nullptr, 1, cudaStreamCaptureModeThreadLocal);
     if (ce == cudaSuccess) {
-      enqueue_flush<V>(c, c->st, ms, hist + 1, cf + 1, out, sf, ring, 1, false, 0, nullptr);
+      enqueue_flush<V, VO>(c, c->st, ms, hist + 1, cf + 1, out, sf, ring, 1, false, 0, nullptr);
       ce = cudaStreamEndCapture(c->st, &captured);
     }
   }
@@ -457,85 +477,191 @@ void ms_graphs_release(thr_ctx* c) {
   }
 }
 
-template <class V>
-int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p, V* hv, V* s, int ndiagq,
-                           const double* aden, const double* anum, float res, float am, int imass, int maxcg,
-                           int* cg_return, int* cg_returns) {
+namespace {
+// double2 -> the low-precision storage of the mixed solver's second phase (round to nearest)
+__device__ __forceinline__ void narrow(float2* d, double2 v) { *d = make_float2((float)v.x, (float)v.y); }
+__device__ __forceinline__ void narrow(__nv_bfloat162* d, double2 v) {
+  *d = __float22bfloat162_rn(make_float2((float)v.x, (float)v.y));
+}
+template <class VL>
+__global__ void k_narrow(VL* d, const double2* s, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    narrow(d + i, s[i]);
+}
+__global__ void k_end_phase(MsState* ms) { ms->switch_delta = 0.0; }
+
+// Runs batches (base storage V, shift fields VO) from the device state until the solve
+// is done or -- when the state's switch_delta is set -- the base residual falls below
+// it (tested after each pair of batches, in the graph and on the host alike); ends
+// with the last batch's flush.  `prime` runs after the graph is built and before the
+// first batch (it sets up the h fields).  The state after the run is left in *h.
+template <class V, class VO, class Prime>
+int run_batches(thr_ctx* c, MsState* ms, MsState* h, MsHist* hist, MsCoef* cf, VO* out, VO* sf, V* ring, V* p, V* hv,
+                V* s, float am, int imass, Prime&& prime) {
   const size_t n = c->n4();
-  const size_t stride = n;
+  if (c->use_graphs && !c->prof_on) {
+    // one graph launch runs every batch until convergence (or the switch); one synchronisation
+    cudaGraphExec_t exec = nullptr;
+    THR_TRY(ms_graph<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, &exec));
+    THR_TRY(prime());
+    THR_CUDA(cudaGraphLaunch(exec, c->st));
+    THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
+    THR_CUDA(cudaStreamSynchronize(c->st));
+    return THR_OK;
+  }
+  // stream-launched batches, one synchronisation per batch (and kernel timing)
+  THR_TRY(prime());
+  const size_t prof_first = c->prof_kind.size();
+  THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
+  THR_CUDA(cudaStreamSynchronize(c->st));
+  const long long it0 = h->it;
+  double flushed = h->flush_fields;
+  long long flushes = 0;
+  // flush traffic: each recorded step's residual read once, each shift field of the
+  // batch's window read and written once (out and sf), counted at the shift fields' width
+  auto account = [&](int pf) {
+    c->prof_set_bytes(pf, (h->flush_fields - flushed) * n * sizeof(VO));
+    if (h->flush_fields > flushed) flushes++;
+    flushed = h->flush_fields;
+  };
+  int half = 0;
+  for (long long k = it0;; k += kBatch, half ^= 1) {
+    int pf = -1;
+    THR_TRY(enqueue_batch<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, half, k, c->prof_on, &pf));
+    THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
+    THR_CUDA(cudaStreamSynchronize(c->st));
+    account(pf);
+    const bool sw = half == 1 && h->switch_delta > 0.0 && h->delta < h->switch_delta;
+    if (h->done || sw) {
+      // the last batch's own flush
+      enqueue_flush<V, VO>(c, c->st, ms, hist + half, cf + half, out, sf, ring, half, c->prof_on, k, &pf);
+      THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
+      THR_CUDA(cudaStreamSynchronize(c->st));
+      account(pf);
+      break;
+    }
+    if (h->batches >= h->max_batches) return THR_ERR_CUDA;  // the device state stopped advancing
+  }
+  if (c->prof_on) {
+    c->prof_trim(prof_first, h->it);  // launches after convergence skipped their work
+    c->prof_work[thr_ctx::P_DSLASH] += h->it - it0;
+    c->prof_work[thr_ctx::P_DSLASH_DAG] += h->it - it0;
+    c->prof_work[thr_ctx::P_SHIFTUPD] += flushes;
+  }
+  return THR_OK;
+}
+
+// state, histories and coefficient tables of a batched solve; r = input in ring slot 0,
+// delta = |input|^2, out = 0, sf = input
+template <class V>
+int batched_setup(thr_ctx* c, const V* in, V* out, V* sf, V* ring, int ndiagq, const double* aden, const double* anum,
+                  float res, int maxcg, double switch_rel, MsState** ms_out, MsState** h_out, MsHist** hist_out,
+                  MsCoef** cf_out) {
+  const size_t n = c->n4();
   MsState* ms = reinterpret_cast<MsState*>(c->dscal);
   MsState* h = reinterpret_cast<MsState*>(c->hscal);
   void* hv_;
   THR_TRY(c->buffer(thr_ctx::B_HIST, 2 * sizeof(MsHist), &hv_));
-  MsHist* hist = (MsHist*)hv_;  // one history per ring half
   void* cf_;
   THR_TRY(c->buffer(thr_ctx::B_COEF, 2 * sizeof(MsCoef), &cf_));
-  MsCoef* cf = (MsCoef*)cf_;
+  MsHist* hist = (MsHist*)hv_;  // one history per ring half
   THR_TRY(ms_prepare_state(c, h, ndiagq, aden, anum, res, maxcg));
   h->kbase = 0;
   h->batches = 0;
   // flushes (one per batch, plus the final one; the graph runs batches in pairs)
   h->max_batches = (maxcg > 0 ? maxcg : 0) / kBatch + 5;
+  h->switch_rel2 = switch_rel * switch_rel;
   THR_CUDA(cudaMemcpyAsync(ms, h, sizeof(MsState), cudaMemcpyHostToDevice, c->st));
   THR_CUDA(cudaMemcpyAsync(ring, in, n * sizeof(V), cudaMemcpyDeviceToDevice, c->st));  // r = input (slot 0)
   const unsigned gb = vec_grid(n);
   k_norm2<V><<<gb, kThreads, 0, c->st>>>(ring, n, c->partials);
   k_init<<<1, kThreads, 0, c->st>>>(ms, hist, c->partials, gb);
-  THR_CUDA(cudaMemsetAsync(out, 0, (size_t)ndiagq * stride * sizeof(V), c->st));
-  k_fill<V><<<gb, kThreads, 0, c->st>>>(sf, in, n, stride, ndiagq);
-  if (c->use_graphs && !c->prof_on) {
-    // one graph launch runs every batch until convergence; one synchronisation
-    cudaGraphExec_t exec = nullptr;
-    THR_TRY(ms_graph<V>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, &exec));
-    // h = M p starts as M r (p = r, gammag = 0): the previous h of the first iteration is zero
+  THR_CUDA(cudaMemsetAsync(out, 0, (size_t)ndiagq * n * sizeof(V), c->st));
+  k_fill<V><<<gb, kThreads, 0, c->st>>>(sf, in, n, n, ndiagq);
+  *ms_out = ms;
+  *h_out = h;
+  *hist_out = hist;
+  *cf_out = (MsCoef*)cf_;
+  return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+}  // namespace
+
+template <class V>
+int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p, V* hv, V* s, int ndiagq,
+                           const double* aden, const double* anum, float res, float am, int imass, int maxcg,
+                           int* cg_return, int* cg_returns) {
+  const size_t n = c->n4();
+  MsState *ms, *h;
+  MsHist* hist;
+  MsCoef* cf;
+  THR_TRY(batched_setup<V>(c, in, out, sf, ring, ndiagq, aden, anum, res, maxcg, 0.0, &ms, &h, &hist, &cf));
+  // h = M p starts as M r (p = r, gammag = 0): the previous h of the first iteration is zero
+  auto prime = [&]() -> int {
     THR_CUDA(cudaMemsetAsync(hv, 0, n * sizeof(V), c->st));
     THR_CUDA(cudaMemsetAsync(p, 0, n * sizeof(V), c->st));
-    THR_CUDA(cudaGraphLaunch(exec, c->st));
-    THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
-    THR_CUDA(cudaStreamSynchronize(c->st));
-  } else {
-    // stream-launched batches, one synchronisation per batch (and kernel timing)
-    THR_CUDA(cudaMemsetAsync(hv, 0, n * sizeof(V), c->st));
-    THR_CUDA(cudaMemsetAsync(p, 0, n * sizeof(V), c->st));
-    const size_t prof_first = c->prof_kind.size();
-    double flushed = 0.0;
-    long long flushes = 0;
-    // flush traffic: each recorded step's residual read once, each shift field of the
-    // batch's window read and written once (out and sf)
-    auto account = [&](int pf) {
-      c->prof_set_bytes(pf, (h->flush_fields - flushed) * n * sizeof(V));
-      if (h->flush_fields > flushed) flushes++;
-      flushed = h->flush_fields;
+    return THR_OK;
+  };
+  THR_TRY(run_batches<V, V>(c, ms, h, hist, cf, out, sf, ring, p, hv, s, am, imass, prime));
+  if (cg_return) *cg_return = h->it;
+  if (cg_returns)
+    for (int q = 0; q < ndiagq; q++) cg_returns[q] = h->cg_returns[q];
+  return h->status ? h->status : THR_OK;
+}
+
+// Mixed precision.  FP32 (or BF16) rounding of the base iteration enters every shifted
+// solution with the size of the base residual at the time it is made, and the shifted
+// systems have no residual of their own that could correct it later; so the solve runs
+// in FP64 while |r| is large and moves the base iteration to low precision only once
+// |r| < switch_rel |input|, where that rounding stays below FP64's own.  The shift
+// fields out and sf stay FP64 throughout: the flush widens the low-precision residuals.
+// The precision changes between two pairs of batches: the FP64 ring's last residual
+// (slot 0) and h (in p) are rounded into the low-precision ring's slot 0 and h field,
+// and the recurrences continue.
+template <class VL>
+int multishift_mixed_dev(thr_ctx* c, const double2* in, double2* out, double2* sf, double2* ring64, double2* p,
+                         double2* hv, double2* s, VL* low, int ndiagq, const double* aden, const double* anum,
+                         float res, float am, int imass, int maxcg, double switch_rel, int* cg_return,
+                         int* cg_returns, int* switched_at) {
+  const size_t n = c->n4();
+  MsState *ms, *h;
+  MsHist* hist;
+  MsCoef* cf;
+  THR_TRY(batched_setup<double2>(c, in, out, sf, ring64, ndiagq, aden, anum, res, maxcg, switch_rel, &ms, &h, &hist,
+                                 &cf));
+  auto prime64 = [&]() -> int {
+    THR_CUDA(cudaMemsetAsync(hv, 0, n * sizeof(double2), c->st));
+    THR_CUDA(cudaMemsetAsync(p, 0, n * sizeof(double2), c->st));
+    return THR_OK;
+  };
+  THR_TRY(run_batches<double2, double2>(c, ms, h, hist, cf, out, sf, ring64, p, hv, s, am, imass, prime64));
+  if (switched_at) *switched_at = 0;
+  if (!h->done && !h->status) {
+    // the low-precision ring occupies the upper half of the FP64 ring's memory
+    // (2 kBatch fields of n VL are at most kBatch FP64 fields), clear of slot 0
+    VL* ring = reinterpret_cast<VL*>(ring64 + (size_t)kBatch * n);
+    VL *pl = low, *hl = low + n, *sl = low + 2 * n;
+    if (switched_at) *switched_at = h->it;
+    auto prime = [&]() -> int {
+      const unsigned gb = vec_grid(n);
+      k_narrow<VL><<<gb, kThreads, 0, c->st>>>(ring, ring64, n);  // latest residual, slot 0
+      k_narrow<VL><<<gb, kThreads, 0, c->st>>>(pl, p, n);         // latest h (odd iterations write p)
+      k_end_phase<<<1, 1, 0, c->st>>>(ms);
+      return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
     };
-    int half = 0;
-    for (long long k = 0;; k += kBatch, half ^= 1) {
-      int pf = -1;
-      THR_TRY(enqueue_batch<V>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, half, k, c->prof_on, &pf));
-      THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
-      THR_CUDA(cudaStreamSynchronize(c->st));
-      account(pf);
-      if (h->done) {
-        // the last batch's own flush
-        enqueue_flush<V>(c, c->st, ms, hist + half, cf + half, out, sf, ring, half, c->prof_on, k, &pf);
-        THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
-        THR_CUDA(cudaStreamSynchronize(c->st));
-        account(pf);
-        break;
-      }
-      if (h->batches >= h->max_batches) return THR_ERR_CUDA;  // the device state stopped advancing
-    }
-    if (c->prof_on) {
-      c->prof_trim(prof_first, h->it);  // launches after convergence skipped their work
-      c->prof_work[thr_ctx::P_DSLASH] += h->it;
-      c->prof_work[thr_ctx::P_DSLASH_DAG] += h->it;
-      c->prof_work[thr_ctx::P_SHIFTUPD] += flushes;
-    }
+    THR_TRY(run_batches<VL, double2>(c, ms, h, hist, cf, out, sf, ring, pl, hl, sl, am, imass, prime));
   }
   if (cg_return) *cg_return = h->it;
   if (cg_returns)
     for (int q = 0; q < ndiagq; q++) cg_returns[q] = h->cg_returns[q];
   return h->status ? h->status : THR_OK;
 }
+
+template int multishift_mixed_dev<float2>(thr_ctx*, const double2*, double2*, double2*, double2*, double2*, double2*,
+                                          double2*, float2*, int, const double*, const double*, float, float, int,
+                                          int, double, int*, int*, int*);
+template int multishift_mixed_dev<__nv_bfloat162>(thr_ctx*, const double2*, double2*, double2*, double2*, double2*,
+                                                  double2*, double2*, __nv_bfloat162*, int, const double*,
+                                                  const double*, float, float, int, int, double, int*, int*, int*);
 
 template int multishift_batched_dev<double2>(thr_ctx*, const double2*, double2*, double2*, double2*, double2*,
                                              double2*, double2*, int, const double*, const double*, float, float, int,

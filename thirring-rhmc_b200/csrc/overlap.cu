@@ -151,7 +151,7 @@ struct CgoState {
 
 inline unsigned vgrid(size_t n) {
   size_t b = (n + kThreads - 1) / kThreads;
-  if (b > 148 * 8) b = 148 * 8;
+  if (b > device_sms() * 8) b = device_sms() * 8;
   return (unsigned)(b ? b : 1);
 }
 
@@ -346,7 +346,7 @@ int measure_ow(thr_ctx* c, float respbp, float bmass, int imass, int knoise, flo
   std::vector<double2> cpbp(knoise, make_double2(0.0, 0.0));
   std::vector<int> its(nsolve, 0);
   size_t pgrid = ((size_t)g.ls * g.v3 + kOwThreads - 1) / kOwThreads;
-  if (pgrid > 148 * 8) pgrid = 148 * 8;
+  if (pgrid > device_sms() * 8) pgrid = device_sms() * 8;
   for (int j = 0; !rc && j < nsolve; j++) {
     const int d = j % 4;
     const float* e = eta + (size_t)j * 2 * g.v3;

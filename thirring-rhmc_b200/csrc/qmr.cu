@@ -16,7 +16,7 @@ namespace {
 constexpr int kThreads = 256;
 inline unsigned vec_grid(size_t n) {
   size_t b = (n + kThreads - 1) / kThreads;
-  if (b > 148 * 16) b = 148 * 16;
+  if (b > device_sms() * 16) b = device_sms() * 16;
   return (unsigned)(b ? b : 1);
 }
 
@@ -34,6 +34,11 @@ __global__ void k_qmr_combine(double2* x, const double2* Phi, const double2* x1,
     x[i] = v;
   }
 }
+// a = Phi - sigma * x (the shifted part of the true residual)
+__global__ void k_shift_part(double2* a, const double2* Phi, const double2* x, double sigma, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    a[i] = Phi[i] - sigma * x[i];
+}
 __global__ void k_f2d(double2* d, const float2* s, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     d[i] = make_double2((double)s[i].x, (double)s[i].y);
@@ -44,12 +49,30 @@ __global__ void k_d2f(float2* d, const double2* s, size_t n) {
 }
 }  // namespace
 
-// Multishift into x1 (FP64, nq fields of n).  sp selects multishift_solver_sp.
+// Multishift into x1 (FP64, nq fields of n).  sp: 0 FP64; 1 multishift_solver_sp
+// (FP32 vectors throughout, the reference's single-precision solver); 2, 3 the
+// mixed solver (FP64, then an FP32 / BF16-storage base iteration once the residual
+// is small, FP64 shift fields; batched organisation only, else FP64)
 int multishift_into(thr_ctx* c, const double2* Phi, double2* x1, int nq, const double* aden, const double* anum,
                     float res, float am, int imass, int maxcg, int sp, int* itercg, int* cg_returns) {
   const size_t n = c->n4();
   const bool batched = c->ms_algo == 1;
-  if (!sp) {
+  c->mixed_switched_at = 0;
+  if ((sp == 2 || sp == 3) && batched) {
+    void *sf, *ring, *w32;
+    THR_TRY(c->buffer(thr_ctx::B_SF64, (size_t)nq * n * sizeof(double2), &sf));
+    THR_TRY(c->ensure_w64(8));
+    THR_TRY(c->buffer(thr_ctx::B_RING, (size_t)(2 * kBatch) * n * sizeof(double2), &ring));
+    THR_TRY(c->buffer(thr_ctx::B_WORK32, 5 * n * sizeof(float2), &w32));
+    if (sp == 2)
+      return multishift_mixed_dev<float2>(c, Phi, x1, (double2*)sf, (double2*)ring, c->w64[5], c->w64[6], c->w64[7],
+                                          (float2*)w32, nq, aden, anum, res, am, imass, maxcg, c->mixed_switch[0],
+                                          itercg, cg_returns, &c->mixed_switched_at);
+    return multishift_mixed_dev<__nv_bfloat162>(c, Phi, x1, (double2*)sf, (double2*)ring, c->w64[5], c->w64[6],
+                                                c->w64[7], (__nv_bfloat162*)w32, nq, aden, anum, res, am, imass,
+                                                maxcg, c->mixed_switch[1], itercg, cg_returns, &c->mixed_switched_at);
+  }
+  if (sp != 1) {
     void *sf, *ring;
     THR_TRY(c->buffer(thr_ctx::B_SF64, (size_t)nq * n * sizeof(double2), &sf));
     THR_TRY(c->ensure_w64(8));
@@ -81,6 +104,32 @@ int multishift_into(thr_ctx* c, const double2* Phi, double2* x1, int nq, const d
   return rc;
 }
 
+// r2[k] = |Phi - (M^dagger M + aden[k]) x_k|^2 in FP64 for the nq fields x_k
+int shift_residuals(thr_ctx* c, const double2* Phi, const double2* x1, int nq, const double* aden, float am, int imass,
+                    double* r2) {
+  const size_t n = c->n4();
+  THR_TRY(c->ensure_w64(10));
+  double2 *t = c->w64[8], *a = c->w64[9];
+  double* dcoef = c->dscal + kScalFusedCoef;
+  double* dsum = c->dscal + kScalFusedSum;
+  const double minus_one = -1.0;
+  THR_CUDA(cudaMemcpyAsync(dcoef, &minus_one, sizeof(double), cudaMemcpyHostToDevice, c->st));
+  const int np = (int)stencil_parts(c->g, c->p.kernel, true);
+  for (int k = 0; k < nq; k++) {
+    const double2* xk = x1 + (size_t)k * n;
+    k_shift_part<<<vec_grid(n), kThreads, 0, c->st>>>(a, Phi, xk, aden[k], n);
+    THR_TRY(launch_dslash<double2>(c->g, c->p.kernel, false, t, xk, c->u64, am, imass, c->p.am3, c->st));
+    // a = a - M^dagger t, with |a|^2 per block
+    THR_TRY(launch_dslash_axpy<double2>(c->g, c->p.kernel, true, a, t, c->u64, am, imass, c->p.am3, c->st, nullptr, a,
+                                        dcoef, c->partials));
+    finish_sum(c->partials, np, dsum, c->st);
+    THR_CUDA(cudaMemcpyAsync(c->hscal + kScalFusedSum, dsum, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    THR_TRY(c->sync());
+    r2[k] = c->hscal[kScalFusedSum];
+  }
+  return THR_OK;
+}
+
 int qmrherm_dev(thr_ctx* c, const double2* Phi, double2* x, float res, int* itercg, float am, int imass,
                 const double* anum, const double* aden, int nq, int iflag, int use_sp, int* cg_returns, double* dS,
                 int max_iters) {
@@ -88,7 +137,8 @@ int qmrherm_dev(thr_ctx* c, const double2* Phi, double2* x, float res, int* iter
   if (c->g.ls % 4 != 0) return THR_ERR_BADSHAPE;                             // :75-81
   if (iflag < 0 || iflag > 3) return THR_ERR_BADARG;
   const size_t n = c->n4();
-  const bool sp = use_sp && c->p.kernel == 0;  // SP is Shamir-only: :53-63
+  // the reference's SP solver is Shamir-only (:53-63); the mixed modes take either kernel
+  const int sp = use_sp == 1 ? (c->p.kernel == 0 ? 1 : 0) : (use_sp == 2 || use_sp == 3) ? use_sp : 0;
   void *x1v, *phi0v;
   THR_TRY(c->buffer(thr_ctx::B_X1, (size_t)nq * n * sizeof(double2), &x1v));
   double2* x1 = (double2*)x1v;
@@ -250,12 +300,40 @@ int thr_qmrherm(thr_ctx* c, const double* Phi, double* x, float res, int* itercg
   return c->sync();
 }
 
+int thr_set_mixed(thr_ctx* c, double switch_fp32, double switch_bf16) {
+  if (!c || !(switch_fp32 >= 0.0) || !(switch_bf16 >= 0.0)) return THR_ERR_BADARG;
+  c->mixed_switch[0] = switch_fp32;
+  c->mixed_switch[1] = switch_bf16;
+  return THR_OK;
+}
+
+int thr_mixed_switched_at(thr_ctx* c, int* iteration) {
+  if (!c || !iteration) return THR_ERR_BADARG;
+  *iteration = c->mixed_switched_at;
+  return THR_OK;
+}
+
 int thr_set_solver(thr_ctx* c, int multishift_algo) {
   if (!c || multishift_algo < 0 || multishift_algo > 2) return THR_ERR_BADARG;
   c->ms_algo = multishift_algo == 0 ? 0 : 1;
   const char* e = std::getenv("THR_GRAPHS");
   c->use_graphs = multishift_algo == 1 && !(e && e[0] == '0');
   return THR_OK;
+}
+
+int thr_shift_residuals_dev(thr_ctx* c, const void* Phi, const void* x, int nq, const double* aden, float am,
+                            int imass, double* r2) {
+  if (!c || !Phi || !aden || !r2 || nq < 1) return THR_ERR_BADARG;
+  if (imass != 1 && imass != 3 && imass != 5) return THR_ERR_BADARG;
+  if (!c->links_ok) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  const size_t n = c->n4();
+  const double2* x1 = (const double2*)x;
+  if (!x1) {  // the context's last multishift solutions (qmrherm's x1)
+    if (c->buf_bytes[thr_ctx::B_X1] < (size_t)nq * n * sizeof(double2)) return THR_ERR_BADARG;
+    x1 = (const double2*)c->bufs[thr_ctx::B_X1];
+  }
+  return shift_residuals(c, (const double2*)Phi, x1, nq, aden, am, imass, r2);
 }
 
 int thr_qmrherm_dev(thr_ctx* c, const void* Phi, void* x, float res, int* itercg, float am, int imass,

@@ -8,6 +8,10 @@ namespace thr {
 // number of per-block partial sums a reduction may write (>= any grid used)
 constexpr int kMaxPartials = 4096;
 
+// streaming multiprocessors of the current device (looked up once per device);
+// grid-stride kernels size their grids as a multiple of it
+int device_sms();
+
 dim3 stencil_block(const Geom& g, int kernel);
 unsigned stencil_grid(const Geom& g, int kernel);  // blocks of one stencil launch (= partials it writes)
 // partials an epilogue launch writes (the FP64 Shamir kernel on staged tiles has its own grid)

@@ -8,6 +8,6 @@ reference's Fortran layout.  All compute runs in libthirring_b200.so on the
 GPU; errors are raised as ThirringError with the library's status code.
 """
 from ._lib import LibraryMissing, header_functions, lib  # noqa: F401
-from .api import (CON_MPIIO, CON_SERIAL, Lattice, Pack, ThirringError, TrajResult, field3, links,  # noqa: F401
-                  ps_field, read_con, read_remez_file, readseed, remez_set, saveseed, shift_out, spinor, write_con,
-                  zolo_coeffs)
+from .api import (CON_MPIIO, CON_SERIAL, EVEN_ODD, FP32_REF, FP64, MIXED_BF16, MIXED_FP32, NATURAL,  # noqa: F401
+                  SHAMIR, WILSON, Lattice, Pack, ThirringError, TrajResult, field3, links, ps_field, read_con,
+                  read_remez_file, readseed, remez_set, saveseed, shift_out, spinor, write_con, zolo_coeffs)

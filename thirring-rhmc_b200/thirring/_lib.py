@@ -93,7 +93,11 @@ SIGNATURES = {
     "thr_field_download": (_i, [_v, _v, _v, _i]),
     "thr_dslash_dev": (_i, [_v, _v, _v, _i, _f, _i, _i]),
     "thr_qmrherm_dev": (_i, [_v, _v, _v, _f, _pi, _f, _i, _v, _v, _i, _i, _i, _v]),
+    "thr_dslash_fused_dev": (_i, [_v, _v, _v, _v, _d, _i, _f, _i, _i, _i, _pd]),
+    "thr_shift_residuals_dev": (_i, [_v, _v, _v, _i, _v, _f, _i, _v]),
     "thr_set_solver": (_i, [_v, _i]),
+    "thr_set_mixed": (_i, [_v, _d, _d]),
+    "thr_mixed_switched_at": (_i, [_v, _pi]),
     "thr_profile": (_i, [_v, _i, _i]),
     "thr_profile_read": (_i, [_v, _i, _pi, _pd, _pd, _pd]),
     "thr_tune_report": (_i, [C.c_char_p, _i]),

@@ -263,6 +263,56 @@ class Lattice:
         _check(self._L.thr_dslashd(self.h, _p(Phi), _p(R), _p(u), am, imass), "dslashd")
         return Phi
 
+    # ---- device fields
+    def _field(self, precision, host=None):
+        f = C.c_void_p()
+        _check(self._L.thr_field_create(self.h, precision, C.byref(f)), "field_create")
+        if host is not None:
+            _need(host, self.sshape, np.complex128, "field")
+            _check(self._L.thr_field_upload(self.h, f, precision, _p(host)), "field_upload")
+        return f
+
+    def dslash_fused(self, R, aux, coef, am, imass, dag, mode, precision=FP64):
+        """The solvers' fused stencil epilogues on device fields (thr_dslash_fused_dev):
+        mode 0 Op R, 1 aux + coef Op R, 3 Op R + coef aux (Op = M, or M^dagger for dag).
+        Returns (out as a halo'd spinor, |out|^2)."""
+        fs = [self._field(precision, R), self._field(precision)]
+        try:
+            if aux is not None:
+                fs.append(self._field(precision, aux))
+            n2 = C.c_double(0)
+            _check(self._L.thr_dslash_fused_dev(self.h, fs[1], fs[0], fs[2] if aux is not None else None, coef,
+                                                 precision, am, imass, int(dag), mode, C.byref(n2)), "dslash_fused")
+            out = spinor(self)
+            _check(self._L.thr_field_download(self.h, _p(out), fs[1], precision), "field_download")
+            return out, n2.value
+        finally:
+            for f in fs:
+                self._L.thr_field_destroy(self.h, f)
+
+    def shift_residuals(self, Phi, shifts, aden, am, imass):
+        """|Phi - (M^dagger M + aden[k]) x_k|^2 in FP64 for the shifted solutions
+        shifts[..., k] ((Ls,Lx,Ly,Lt,4,n) as multishift_solver returns them), on the
+        current links (thr_shift_residuals_dev)."""
+        aden = np.ascontiguousarray(aden, np.float64)
+        phi = self._field(FP64, Phi)
+        try:
+            r2 = np.zeros(len(aden))
+            for k in range(len(aden)):
+                xs = spinor(self)
+                xs[1:-1, 1:-1, 1:-1, 1:-1, :] = shifts[..., k]
+                xf = self._field(FP64, xs)
+                try:
+                    v = np.zeros(1)
+                    _check(self._L.thr_shift_residuals_dev(self.h, phi, xf, 1, _p(aden[k:k + 1]), am, imass, _p(v)),
+                           "shift_residuals")
+                    r2[k] = v[0]
+                finally:
+                    self._L.thr_field_destroy(self.h, xf)
+            return r2
+        finally:
+            self._L.thr_field_destroy(self.h, phi)
+
     # ---- measure_OWilson.F90
     def prep_zolo(self, lmin=0.1, lmax=5.0):
         """prepZolo (measure_OWilson.F90:169-188) on [lmin, lmax] for this Ls."""
@@ -411,6 +461,16 @@ class Lattice:
                                    C.byref(av), _p(parts), _p(its)), "measure")
         return dict(psibarpsi=pb.value, susclsing=sus.value, aviter=av.value, parts=parts, itercg=its)
 
+    def set_mixed(self, switch_fp32=1e-8, switch_bf16=1e-13):
+        """Relative base residual at which the mixed multishift leaves FP64 (thr_set_mixed)."""
+        _check(self._L.thr_set_mixed(self.h, switch_fp32, switch_bf16), "set_mixed")
+
+    def mixed_switched_at(self):
+        """Iteration at which the last mixed multishift left FP64 (0: it did not)."""
+        v = C.c_int(0)
+        _check(self._L.thr_mixed_switched_at(self.h, C.byref(v)), "mixed_switched_at")
+        return v.value
+
     def set_solver(self, multishift_algo):
         """0: per-iteration shift updates (the reference's loop); 1: batched (default)."""
         _check(self._L.thr_set_solver(self.h, int(multishift_algo)), "set_solver")
@@ -433,7 +493,9 @@ class Lattice:
     def qmrherm(self, Phi, res, am, imass, anum, aden, iflag, use_sp=False, dSdpi=None, Phi0=None,
                 max_qmr_iters=0):
         """x = qmrherm(Phi, …): returns (x, itercg, cg_returns).  dSdpi/Phi0 are
-        updated in place when given (gforce::dSdpi, qmrherm_module::Phi0)."""
+        updated in place when given (gforce::dSdpi, qmrherm_module::Phi0).
+        use_sp: 0/False FP64, 1/True the reference's SP multishift, MIXED_FP32 or
+        MIXED_BF16 the mixed multishift."""
         _need(Phi, self.sshape, np.complex128, "Phi")
         nq = len(aden)
         assert len(anum) == nq + 1
