@@ -47,7 +47,8 @@ FP64_ITERS_REF = 17113  # measured on B200 for the seeded input below
 METRIC = "multishift solve throughput (qmrherm, 25 poles, FP64 residual 1e-9)"
 # kernel timing inside the timed region: every PROF_STRIDE-th launch of each kind
 PROF_STRIDE = 8
-PROF_KINDS = ((0, "k_dslash_M_hrec"), (2, "k_dslash_Mdag"), (1, "k_flush"))
+PROF_KINDS = ((0, "k_dslash_M_hrec"), (2, "k_dslash_Mdag"), (1, "k_flush"), (3, "k_dslash_M_hrec_fp32"),
+              (4, "k_dslash_Mdag_fp32"))
 UNIT = "solves/s"
 HBM_FALLBACK = 6650.0
 # arithmetic of each mode: the mixed modes run FP64 first and FP32 (BF16 storage,
@@ -435,6 +436,80 @@ def run_overlap(args):
             "results": out}
 
 
+def run_dslash_sweep(args):
+    """The config-2 sweep: M and M^dagger at L^2 x L for L in {16, 24, 32, 48} and Ls in
+    {16, 32, 48}, FP64 and FP32 storage, Shamir and Wilson kernels, natural and even-odd
+    site order.  Per case: the mean of `steps` launches (after `warmup`) timed with CUDA
+    events on the library's stream, algorithmic GB/s (one read of the input spinor, one
+    write of the output, three link fields) and its fraction of the measured HBM copy
+    rate, and the largest deviation from the oracle's FP64 operator (dirac.F90) relative
+    to its largest element (natural order; the even-odd order gives the same bits)."""
+    import torch
+    import thirring
+    from thirring import _lib
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+    L = _lib.lib()
+    peak, peak_kind = peaks()
+    sizes = [int(v) for v in (args.sweep_l or "16,24,32,48").split(",")]
+    lss = [int(v) for v in (args.sweep_ls or "16,32,48").split(",")]
+    steps, warmup = max(args.steps, 5), max(args.warmup, 3)
+    cases = []
+    for lx in sizes:
+        for ls in lss:
+            rng = np.random.default_rng(1000 * lx + ls)
+            theta = np.asfortranarray(rng.standard_normal((lx, lx, lx, 3)) / np.sqrt(BETA), np.float32)
+            R = np.zeros((ls + 2, lx + 2, lx + 2, lx + 2, 4), np.complex128, order="F")
+            sh = R[1:-1, 1:-1, 1:-1, 1:-1, :].shape
+            R[1:-1, 1:-1, 1:-1, 1:-1, :] = rng.standard_normal(sh) + 1j * rng.standard_normal(sh)
+            v3 = lx ** 3
+            for kernel, kname in ((0, "shamir"), (1, "wilson")):
+                Lo = O.lat(lx, lx, lx, ls, kernel=kernel, beta=BETA, am3=AM3)
+                u = O.coef(Lo, theta)
+                O.update_halo_5(Lo, R)
+                refs = {dag: (O.dslashd if dag else O.dslash)(Lo, R, u, AM, IMASS) for dag in (0, 1)}
+                scale = {dag: float(np.max(np.abs(O.interior(refs[dag])))) for dag in (0, 1)}
+                for layout, lname in ((0, "natural"), (1, "even_odd")):
+                    G = thirring.Lattice(lx, lx, lx, ls, kernel=kernel, layout=layout, beta=BETA, am3=AM3)
+                    G.set_links(u)
+                    sptr = C.c_void_p()
+                    L.thr_get_stream(G.h, C.byref(sptr))
+                    st = torch.cuda.ExternalStream(sptr.value)
+                    for prec, pname, b in ((0, "fp64", 16), (2, "fp32", 8)):
+                        a, o = G._field(prec, R), G._field(prec)
+                        for dag in (0, 1):
+                            for _ in range(warmup):
+                                L.thr_dslash_dev(G.h, o, a, prec, AM, IMASS, dag)
+                            L.thr_sync(G.h)
+                            e0 = torch.cuda.Event(enable_timing=True)
+                            e1 = torch.cuda.Event(enable_timing=True)
+                            e0.record(st)
+                            for _ in range(steps):
+                                L.thr_dslash_dev(G.h, o, a, prec, AM, IMASS, dag)
+                            e1.record(st)
+                            e1.synchronize()
+                            us = e0.elapsed_time(e1) / steps * 1e3
+                            byts = 2 * 4 * ls * v3 * b + 3 * v3 * b
+                            case = {"L": lx, "Ls": ls, "kernel": kname, "layout": lname, "storage": pname,
+                                    "op": "Mdag" if dag else "M", "us": round(us, 2),
+                                    "gbs": round(byts / us / 1e3, 1), "frac": round(byts / us / 1e3 / peak, 3)}
+                            if layout == 0:
+                                out = thirring.spinor(G)
+                                L.thr_field_download(G.h, out.ctypes.data_as(C.c_void_p), o, prec)
+                                dev = np.max(np.abs(O.interior(out) - O.interior(refs[dag])))
+                                case["max_rel_dev_vs_oracle"] = float("%.3g" % (dev / scale[dag]))
+                            cases.append(case)
+                            print(json.dumps(case), flush=True)
+                        L.thr_field_destroy(G.h, a)
+                        L.thr_field_destroy(G.h, o)
+                    G.close()
+    best = max(cases, key=lambda c: c["frac"])
+    return {"workload": "config-2 dslash sweep: M and M^dagger, L^2xL L in %s, Ls in %s, FP64/FP32, Shamir/Wilson, "
+                        "natural/even-odd, am=%g imass=%d beta=%g" % (sizes, lss, AM, IMASS, BETA),
+            "peak_gbs": peak, "peak_source": peak_kind, "launches_per_case": steps, "cases": cases,
+            "best": best}
+
+
 def dslash_bandwidth(args, dev, lx=48, ls=48, iters=20, warmup=3):
     """FP64 Shamir M at lx^2 x lx, Ls = ls: algorithmic GB/s over `iters` launches
     (one read of the input spinor, one write of the output, three link fields)."""
@@ -617,39 +692,90 @@ def run_packed(args):
 
 
 def run_trajectory(args):
-    """RHMC trajectories on 12^2 x 12, Ls = 16 (beta 0.3, am 0.05, imass 3,
-    10 MD steps of dt 0.05) with the reference's remez2/remez4 (25 poles) and
-    remez2g/remez4g (12 poles) files: guidance solves single precision (spmd)
-    or FP64 with the batched, graph-driven multishift, and the plain FP64 GPU
-    path (the reference's multishift loop structure, host-launched, FP64
-    guidance) for comparison."""
+    """Config 1 on the GPU and on the host: 12^2 x 12, Ls = 16, Shamir, beta 0.3, am 0.05,
+    imass 3, antiperiodic t, seeded Gaussian theta and site streams.
+    (a) one congrad of M^dagger M x = Phi to res 1e-9 (measure_module.F90:9-140): the GPU
+        (thr_congrad, FP64) against the oracle on the host cores, end to end;
+    (b) one trajectory of 10 fixed MD steps, dt 0.05, with the reference's remez2/remez4
+        (25 poles) and remez2g/remez4g (12 poles), rescga 1e-8, rescgg 1e-6, in the
+        configurations: the plain FP64 GPU path (the reference's multishift loop
+        structure, host-driven steps); FP64 batched with each MD step one CUDA graph; the
+        mixed multishift for the action solves with FP64 guidance; the reference's
+        single-precision guidance (spmd).  Each starts from the same theta and seed; its
+        Delta H is compared with the oracle's FP64 trajectory (FP64 guidance) of the same
+        start, whose time on the host cores is the CPU baseline of the trajectory."""
     import thirring
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
     gold = os.path.join(REPO, "tests", "golden") + os.sep
     rat = thirring.remez_set(gold + "remez2", gold + "remez4", 25)
     ratg = thirring.remez_set(gold + "remez2g", gold + "remez4g", 12)
+    lx, ls, beta, am, imass, dt, nstep = 12, 16, 0.3, 0.05, 3, 0.05, 10
+    seed = 4139764973254.0
+    rng = np.random.default_rng(1)
+    th0 = np.asfortranarray(rng.standard_normal((lx, lx, lx, 3)) / np.sqrt(beta), np.float32)
     out = {}
-    for name, spmd, algo in (("spmd_fp32_guidance", 1, 1), ("fp64_guidance", 0, 1), ("plain_fp64_gpu", 0, 0)):
-        G = thirring.Lattice(12, 12, 12, 16, beta=BETA)
+    # (a) congrad to 1e-9
+    Lo = O.lat(lx, lx, lx, ls, beta=beta, am3=AM3)
+    u = O.coef(Lo, th0)
+    phi = np.zeros((ls + 2, lx + 2, lx + 2, lx + 2, 4), np.complex128, order="F")
+    sh = phi[1:-1, 1:-1, 1:-1, 1:-1, :].shape
+    phi[1:-1, 1:-1, 1:-1, 1:-1, :] = rng.standard_normal(sh) + 1j * rng.standard_normal(sh)
+    O.update_halo_5(Lo, phi)
+    t0 = time.perf_counter()
+    xr = O.spinor(Lo)
+    it_ref, _ = O.congrad(Lo, phi, xr, u, 1e-9, am, imass)
+    cpu_cg = time.perf_counter() - t0
+    with thirring.Lattice(lx, lx, lx, ls, beta=beta) as G:
+        G.set_links(u)
+        x = np.zeros_like(phi)
+        G.congrad(phi, x, 1e-9, am, imass)  # warm-up (autotuner, graph)
+        x = np.zeros_like(phi)
+        t0 = time.perf_counter()
+        it, _ = G.congrad(phi, x, 1e-9, am, imass)
+        gpu_cg = time.perf_counter() - t0
+    err = float(np.max(np.abs(O.interior(x) - O.interior(xr))) / np.max(np.abs(O.interior(xr))))
+    out["congrad_1e-9"] = {"gpu_s": round(gpu_cg, 4), "gpu_iterations": it, "cpu_s": round(cpu_cg, 3),
+                           "cpu_iterations": it_ref, "cpu_cores": int(O.lib.orc_num_threads()),
+                           "speedup": round(cpu_cg / gpu_cg, 1), "max_rel_diff_vs_oracle": float("%.3g" % err),
+                           "path": "thr_congrad with host Fortran-layout arrays (copies included)"}
+    # (b) trajectories
+    t0 = time.perf_counter()
+    g = O.RNG(Lo, True).init(seed)
+    th_ref = th0.copy(order="F")
+    orat = O.rational(rat, ratg)
+    ref = O.trajectory(Lo, g, th_ref, orat, nstep, dt, am, imass, 1e-8, 1e-6, 0, fixed_steps=nstep)
+    cpu_traj = time.perf_counter() - t0
+    out["oracle_fp64_trajectory"] = {"s": round(cpu_traj, 1), "dH": ref.dh, "accepted": ref.accepted,
+                                     "cores": int(O.lib.orc_num_threads()), "cpu": cpu_model()}
+    modes = (("plain_fp64_gpu", 0, 0, 0, False), ("fp64_batched_md_graph", 1, 0, 0, True),
+             ("mixed_action_fp64_guidance", 1, 0, 2, True), ("spmd_fp32_guidance", 1, 1, 0, True))
+    for name, algo, spmd, action, md_graph in modes:
+        G = thirring.Lattice(lx, lx, lx, ls, beta=beta)
         G.set_solver(algo)
         G.set_remez(rat, ratg)
         G.set_residuals(1e-8, 1e-6, spmd)
-        G.init_random(4139764973254.0)
-        rng = np.random.default_rng(1)
-        th = np.asfortranarray(rng.standard_normal((12, 12, 12, 3)) / np.sqrt(BETA), np.float32)
-        G.trajectory(th, 10, 0.05, 0.05, 3, fixed_steps=10)  # warm-up
-        t0 = time.perf_counter()
-        ntraj = 3
-        dh = []
-        acc = 0
-        for _ in range(ntraj):
-            r = G.trajectory(th, 10, 0.05, 0.05, 3, fixed_steps=10)
-            dh.append(r.dh)
-            acc += r.accepted
-        dt = (time.perf_counter() - t0) / ntraj
-        out[name] = {"s_per_traj": round(dt, 3), "traj_per_hr": round(3600 / dt, 1), "dH": dh, "accepted": acc}
+        G.set_action_precision(action)
+        times, res = [], None
+        for rep in range(2):  # the first run settles buffers, autotuner and graphs
+            G.init_random(seed)
+            th = th0.copy(order="F")
+            G.md_counters(reset=True)
+            t1 = time.perf_counter()
+            res = G.trajectory(th, nstep, dt, am, imass, fixed_steps=nstep)
+            times.append(time.perf_counter() - t1)
+        out[name] = {"s_per_traj": round(times[-1], 4), "traj_per_hr": round(3600 / times[-1], 1), "dH": res.dh,
+                     "dH_minus_oracle": float("%.3g" % (res.dh - ref.dh)), "accepted": res.accepted,
+                     "md_step_graph": md_graph,
+                     "iterations": {k: v for k, v in G.md_counters().items() if v}}
         G.close()
-    out["speedup_vs_plain_fp64_gpu"] = round(out["plain_fp64_gpu"]["s_per_traj"] / out["spmd_fp32_guidance"]["s_per_traj"], 2)
-    return {"workload": "RHMC 12^2x12 Ls16, 10 MD steps dt 0.05, remez2/4 + remez2g/4g", "results": out}
+    base = out["plain_fp64_gpu"]["s_per_traj"]
+    for name, *_ in modes:
+        out[name]["speedup_vs_plain_fp64_gpu"] = round(base / out[name]["s_per_traj"], 2)
+        out[name]["speedup_vs_oracle_cpu"] = round(cpu_traj / out[name]["s_per_traj"], 1)
+    return {"workload": "config 1: 12^2x12 Ls16 Shamir, beta 0.3, am 0.05, imass 3; congrad to 1e-9; RHMC "
+                        "trajectory of 10 MD steps dt 0.05, remez2/4 + remez2g/4g, rescga 1e-8, rescgg 1e-6",
+            "results": out}
 
 
 def run_trajectory48(args):
@@ -695,10 +821,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--mode", default="fp64", choices=["fp64", "sp", "mixed", "bf16"])
+    ap.add_argument("--mode", default="mixed", choices=["fp64", "sp", "mixed", "bf16"],
+                    help="multishift precision: mixed (default) runs FP64 until |r| < 1e-8 |Phi|, then FP32 "
+                         "stencils and residuals with FP64 shift fields")
     ap.add_argument("--workload", default="multishift",
                     choices=["multishift", "measurement", "packed", "trajectory", "trajectory48", "dslash",
-                             "overlap"],
+                             "dslash_sweep", "overlap"],
                     help="secondary workloads print their own JSON line (not the headline contract)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-iters", type=int, default=50, help="multishift iterations in the CPU sample")
@@ -709,6 +837,8 @@ def main():
     ap.add_argument("--max-iters", type=int, default=0,
                     help="profiling case: stop every solve after this many iterations (not a full solve)")
     ap.add_argument("--no-dslash", action="store_true")
+    ap.add_argument("--sweep-l", default="", help="dslash_sweep: comma-separated lattice extents")
+    ap.add_argument("--sweep-ls", default="", help="dslash_sweep: comma-separated fifth-dimension extents")
     ap.add_argument("--no-compare-plain", dest="compare_plain", action="store_false",
                     help="skip timing the plain FP64 path (reference loop structure)")
     args = ap.parse_args()
@@ -732,7 +862,7 @@ def main():
         return
     if args.workload != "multishift":
         fn = {"measurement": run_measurement, "packed": run_packed, "trajectory": run_trajectory,
-              "trajectory48": run_trajectory48, "overlap": run_overlap}[args.workload]
+              "trajectory48": run_trajectory48, "overlap": run_overlap, "dslash_sweep": run_dslash_sweep}[args.workload]
         print(json.dumps(fn(args)), flush=True)
         return
 

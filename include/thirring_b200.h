@@ -341,8 +341,16 @@ int thr_set_remez(thr_ctx *ctx, int ndiag, const double *anum2, const double *ad
                   const double *bnum4g, const double *bden4g);
 /* Inverter residuals rescga (Hamiltonian, pseudofermion), rescgg (guidance)
  * and spmd (single-precision guidance solves), params.F90:60-64; defaults
- * 1e-8, 1e-6, 1.  max_qmr_iters <= 0 keeps 50000. */
+ * 1e-8, 1e-6, 1.  spmd is qmrherm's use_sp for the guidance (force) solves:
+ * 0 FP64, 1 the reference's single-precision multishift, THR_MIXED_FP32 /
+ * THR_MIXED_BF16 the mixed multishift.  max_qmr_iters <= 0 keeps 50000. */
 int thr_set_residuals(thr_ctx *ctx, float rescga, float rescgg, int spmd, int max_qmr_iters);
+/* Precision of the Hamiltonian and pseudofermion solves (dwf3d_lib.F90:584,590,
+ * evolution.F90:64,69), which the reference always runs in FP64: THR_FP64
+ * (default), THR_MIXED_FP32 or THR_MIXED_BF16 (the mixed multishift, whose
+ * precision switch keeps its rounding below FP64's; thr_set_mixed) -- no
+ * counterpart in the reference. */
+int thr_set_action_precision(thr_ctx *ctx, int precision);
 /* force(Phi, res1, am, imass), force_module.F90:9-113, with the current
  * links; theta (trial::theta) feeds the gauge term; dSdpi is overwritten. */
 int thr_force(thr_ctx *ctx, const double *Phi, float res1, float am, int imass, const float *theta, double *dSdpi);
@@ -421,7 +429,8 @@ int thr_get_stream(thr_ctx *ctx, void **stream);
  * with CUDA events on the context's stream -- kind 0 the stencil M (in the
  * batched multishift with its fused |M p|^2), kind 2 the stencil M^dagger
  * (kind 0 in the per-iteration multishift), kind 1 the shift-field update
- * (k_flush, or k_ms_pshift in the per-iteration solver).  thr_profile_read
+ * (k_flush, or k_ms_pshift in the per-iteration solver), kinds 3 and 4 the
+ * stencils M and M^dagger of the mixed multishift's low-precision phase.  thr_profile_read
  * returns, for one kind, the sampled launches that did work, their summed
  * device time in ms and their summed algorithmic bytes, and the number of
  * launches of that kind that did work (sampled or not). */

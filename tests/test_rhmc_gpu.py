@@ -99,3 +99,62 @@ def test_trajectory_delta_h(spmd):
         assert abs(got.dh - ref.dh) <= (1e-6 if spmd == 0 else 1e-4), (got.dh, ref.dh)
         assert got.accepted == ref.accepted
     assert np.max(np.abs(th - th_ref)) <= 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("spmd", [0, 1])
+def test_trajectory_mixed_action_delta_h(spmd):
+    """The Hamiltonian and pseudofermion solves in the mixed multishift (FP64 until the
+    residual is small, then FP32 with FP64 shift fields): Delta H within 1e-6 of the
+    FP64 oracle's with FP64 guidance, as the FP64 path."""
+    L, G, theta, orat, rng = setup(beta=0.4, seed=9)
+    g = O.RNG(L, True).init(4139764973254.0)
+    th_ref = theta.copy(order="F")
+    ref = O.trajectory(L, g, th_ref, orat, 3, 0.05, 0.05, 3, 1e-8, 1e-6, spmd, fixed_steps=3)
+    with G:
+        G.init_random(4139764973254.0, site=True)
+        G.set_residuals(1e-8, 1e-6, spmd)
+        G.set_action_precision(thirring.MIXED_FP32)
+        G.set_mixed(1e-6, 1e-13)  # early enough that this small solve switches
+        th = theta.copy(order="F")
+        got = G.trajectory(th, 3, 0.05, 0.05, 3, fixed_steps=3)
+    assert got.steps == ref.steps == 3
+    assert abs(got.dh - ref.dh) <= (1e-6 if spmd == 0 else 1e-4), (got.dh, ref.dh)
+
+
+def _traj_run(tmp, tag):
+    """Two fixed-length and two random-length trajectories; results saved for comparison."""
+    import sys
+    L, G, theta, orat, rng = setup(beta=0.4, seed=13)
+    out = {}
+    with G:
+        G.init_random(4139764973254.0, site=True)
+        G.set_residuals(1e-8, 1e-6, 1)
+        th = theta.copy(order="F")
+        rs = [G.trajectory(th, 4, 0.05, 0.05, 3, fixed_steps=4) for _ in range(2)]
+        rs += [G.trajectory(th, 3, 0.05, 0.05, 3) for _ in range(2)]
+        out["dh"] = np.array([r.dh for r in rs])
+        out["steps"] = np.array([r.steps for r in rs])
+        out["acc"] = np.array([r.accepted for r in rs])
+        out["theta"] = th
+        out["counts"] = np.array(list(G.md_counters().values()))
+    np.savez(os.path.join(tmp, "traj_%s.npz" % tag), **out)
+
+
+@pytest.mark.gpu
+def test_md_step_graph_bit_identical(tmp_path):
+    """A leapfrog step replayed as one captured CUDA graph (drift, coef, the four force
+    solves with their batch loops as conditional nodes, the exit draw, the kick) runs
+    exactly the kernels of the host-driven step: identical Delta H, steps, theta and
+    iteration counts for fixed and random trajectory lengths (THR_MD_GRAPH=0: host-driven)."""
+    import subprocess
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    code = ("import sys; sys.path.insert(0, %r); import conftest; import test_rhmc_gpu as t; t._traj_run(%r, sys.argv[1])"
+            % (here, str(tmp_path)))
+    for tag, env in (("graph", {}), ("host", {"THR_MD_GRAPH": "0"})):
+        subprocess.run([sys.executable, "-c", code, tag], check=True, cwd=here, env=dict(os.environ, **env))
+    a, b = np.load(tmp_path / "traj_graph.npz"), np.load(tmp_path / "traj_host.npz")
+    assert np.all(a["steps"] >= 2)
+    for k in a.files:
+        assert np.array_equal(a[k], b[k]), k

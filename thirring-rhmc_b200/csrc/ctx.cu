@@ -6,13 +6,16 @@
 #include <type_traits>
 
 #include "ctx.h"
+#include "md.h"
 #include "ms.h"
 #include "solver.h"
 
 using namespace thr;
 
 int thr_ctx::ensure_w64(int count) {
+  if (md_capture && (int)w64.size() < count) return THR_ERR_BADSHAPE;  // no allocation inside a capture
   while ((int)w64.size() < count) {
+    buf_gen++;
     double2* p = nullptr;
     if (cudaMalloc(&p, n4() * sizeof(double2)) != cudaSuccess) return THR_ERR_NOMEM;
     cudaMemsetAsync(p, 0, n4() * sizeof(double2), st);
@@ -24,6 +27,8 @@ int thr_ctx::ensure_w64(int count) {
 int thr_ctx::buffer(int id, size_t bytes, void** out) {
   if (id < 0 || id >= B_COUNT) return THR_ERR_BADARG;
   if (buf_bytes[id] < bytes) {
+    if (md_capture) return THR_ERR_BADSHAPE;  // no allocation inside a capture
+    buf_gen++;
     cudaStreamSynchronize(st);
     cudaFree(bufs[id]);
     bufs[id] = nullptr;
@@ -158,6 +163,8 @@ int thr_create(const thr_params* p, thr_ctx** out) {
     // graphs with conditional nodes)
     e = std::getenv("THR_GRAPHS");
     if (e && e[0] == '0') c->use_graphs = false;
+    e = std::getenv("THR_MD_GRAPH");
+    if (e && e[0] == '0') c->use_md_graph = false;
   }
   int rc = THR_OK;
   if (cudaSetDevice(c->dev) != cudaSuccess) rc = THR_ERR_CUDA;
@@ -165,6 +172,7 @@ int thr_create(const thr_params* p, thr_ctx** out) {
   if (!rc && cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess) rc = THR_ERR_CUDA;
   if (!rc && cudaStreamCreateWithPriority(&c->st, cudaStreamNonBlocking, prio_hi) != cudaSuccess) rc = THR_ERR_CUDA;
   if (!rc && cudaStreamCreateWithPriority(&c->st2, cudaStreamNonBlocking, prio_lo) != cudaSuccess) rc = THR_ERR_CUDA;
+  if (!rc && cudaStreamCreateWithPriority(&c->st3, cudaStreamNonBlocking, prio_hi) != cudaSuccess) rc = THR_ERR_CUDA;
   if (!rc && (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)) rc = THR_ERR_CUDA;
   for (int i = 0; i < 2 && !rc; i++)
     if (cudaEventCreateWithFlags(&c->ev_fork[i], cudaEventDisableTiming) != cudaSuccess ||
@@ -181,6 +189,7 @@ int thr_create(const thr_params* p, thr_ctx** out) {
   if (!rc && cudaMalloc(&c->iscal, 1024 * sizeof(int)) != cudaSuccess) rc = THR_ERR_NOMEM;
   if (!rc && cudaMallocHost(&c->hscal, 4096 * sizeof(double)) != cudaSuccess) rc = THR_ERR_NOMEM;
   if (!rc && cudaMallocHost(&c->hiscal, 1024 * sizeof(int)) != cudaSuccess) rc = THR_ERR_NOMEM;
+  if (!rc && cudaMallocHost(&c->ms_tmpl, kMsTemplates * sizeof(MsState)) != cudaSuccess) rc = THR_ERR_NOMEM;
   if (rc) {
     thr_destroy(c);
     return rc;
@@ -198,6 +207,7 @@ int thr_destroy(thr_ctx* c) {
   if (c->st2) cudaStreamSynchronize(c->st2);
   ms_graphs_release(c);
   cg_graph_release(c);
+  md_graph_release(c);
   for (auto p : c->w64) cudaFree(p);
   for (auto e : c->prof_ev) cudaEventDestroy(e);
   for (int i = 0; i < thr_ctx::B_COUNT; i++) cudaFree(c->bufs[i]);
@@ -212,6 +222,7 @@ int thr_destroy(thr_ctx* c) {
   cudaFree(c->iscal);
   if (c->hscal) cudaFreeHost(c->hscal);
   if (c->hiscal) cudaFreeHost(c->hiscal);
+  if (c->ms_tmpl) cudaFreeHost(c->ms_tmpl);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   for (int i = 0; i < 2; i++) {
@@ -219,6 +230,7 @@ int thr_destroy(thr_ctx* c) {
     if (c->ev_join[i]) cudaEventDestroy(c->ev_join[i]);
   }
   if (c->st2) cudaStreamDestroy(c->st2);
+  if (c->st3) cudaStreamDestroy(c->st3);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
   return THR_OK;

@@ -25,6 +25,8 @@
 constexpr int kScalHamSum = 4000;      // hamilton's fermion sum
 constexpr int kScalFusedCoef = 4090;   // thr_dslash_fused_dev: the epilogue coefficient
 constexpr int kScalFusedSum = 4091;    // thr_dslash_fused_dev / thr_shift_residuals_dev: a reduced sum
+constexpr int kScalMd = 4064;          // MD step graph: 8 iteration counters, then its control block
+constexpr int kMsTemplates = 8;        // multishift state templates of one captured MD step
 
 struct thr_ctx {
   thr_params p;
@@ -82,7 +84,8 @@ struct thr_ctx {
   } rat;
   // inverter residuals and the guidance-precision switch (params.F90:60-64)
   float rescga = 1e-8f, rescgg = 1e-6f;
-  int spmd = 1;             // 0: FP64 guidance solves; 1: single-precision (reference)
+  int spmd = 1;             // guidance solves: 0 FP64; 1 single precision (reference); 2, 3 mixed multishift
+  int action_sp = 0;        // Hamiltonian and pseudofermion solves: 0 FP64; 2, 3 mixed multishift
   int max_qmr_iters = 50000;
   int ms_algo = 1;          // multishift: 0 = per-iteration shift updates, 1 = batched
   bool use_graphs = true;   // batched solver loops as one CUDA graph (WHILE node) per solve
@@ -104,6 +107,21 @@ struct thr_ctx {
   double* zolo_dev = nullptr;
   bool zolo_dirty = false;
   double md_counts[8] = {};  // ancg, ancgpv, ancgf, ancgfpv, ancgh, ancghpv, ancgpf, ancgpfpv
+  // One leapfrog step of evolve_theta_pp as a CUDA graph (md.cu).  While it is
+  // captured (md_capture), the solver code adds its batch loops as WHILE nodes of
+  // the captured graph (their bodies captured on st3), takes each multishift's
+  // initial state from its own pinned template (ms_tmpl, a slot per solve of the
+  // step), counts iterations on the device (md_dev: per-counter sums, the OR of
+  // the solves' status and the step's exit draw) and never synchronises; a
+  // buffer that would have to grow makes the capture fail (the step then runs
+  // host-driven).  THR_MD_GRAPH=0 turns the graph off.
+  bool md_capture = false;
+  bool use_md_graph = true;
+  cudaStream_t st3 = nullptr;
+  void* ms_tmpl = nullptr;  // pinned, kMsTemplates MsState slots
+  int ms_tmpl_next = 0;
+  void* md_graph = nullptr;  // cached step graph (md.cu)
+  unsigned long long buf_gen = 0;  // bumped whenever a device buffer is (re)allocated
   void* bufs[B_COUNT] = {};
   size_t buf_bytes[B_COUNT] = {};
   bool phi0_valid = false;
@@ -112,7 +130,8 @@ struct thr_ctx {
 
   // optional per-kernel timing: CUDA events around selected launches
   // kernel timing: every prof_stride-th launch of each kind is bracketed by events
-  enum ProfKernel { P_DSLASH = 0, P_SHIFTUPD = 1, P_DSLASH_DAG = 2, P_COUNT = 4 };
+  // (P_DSLASH_LOW / P_DSLASH_DAG_LOW: the same stencils in the low-precision phase of the mixed multishift)
+  enum ProfKernel { P_DSLASH = 0, P_SHIFTUPD = 1, P_DSLASH_DAG = 2, P_DSLASH_LOW = 3, P_DSLASH_DAG_LOW = 4, P_COUNT = 6 };
   bool prof_on = false;
   int prof_stride = 1;
   long long prof_seen[P_COUNT] = {};         // launches offered to prof_begin

@@ -12,6 +12,7 @@
 
 #include "ctx.h"
 #include "md.h"
+#include "ms.h"
 #include "qmr.h"
 #include "rng.h"
 
@@ -86,6 +87,31 @@ __global__ void k_finish(const double* partials, int np, double* out) {
   if (threadIdx.x == 0) *out = acc;
 }
 
+// Control block of a captured MD step (at dscal + kScalMd + 8): the exit draw of the step,
+// whether it was the last, the OR of its solves' status and the fixed-length flag the host
+// sets in pinned memory before each launch
+struct MdCtl {
+  float ytest;
+  int last, status, fixed_last;
+};
+static_assert(sizeof(MdCtl) <= 3 * sizeof(double), "MdCtl fits its slots");
+
+// counts[k] += the iterations of the multishift just run; status |= its status
+__global__ void k_md_count(const MsState* ms, double* counts, int k, MdCtl* ctl) {
+  counts[k] += (double)ms->it;
+  if (ms->status) ctl->status = ms->status;
+}
+// the step's closing kick: pp -= c*dSdpi with c = dt/2 on the last step, dt otherwise
+// (evolution.F90:166-175); last = the host's fixed-length flag or ytest < proby
+__global__ void k_pp_kick_last(float* pp, const double* dS, float dt, float hdt, float proby, int fixed_mode,
+                               MdCtl* ctl, int n) {
+  const bool last = fixed_mode ? ctl->fixed_last != 0 : ctl->ytest < proby;
+  const float c = last ? hdt : dt;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    pp[i] = __fsub_rn(pp[i], (float)((double)c * dS[i]));
+  if (blockIdx.x == 0 && threadIdx.x == 0) ctl->last = last ? 1 : 0;
+}
+
 inline unsigned grid(size_t n) {
   size_t b = (n + kThreads - 1) / kThreads;
   if (b > device_sms() * 4) b = device_sms() * 4;
@@ -130,22 +156,30 @@ int force_dev(thr_ctx* c, MdFields* f, const float* theta, float res1, float am,
   const int sp = c->spmd;
   const float One = 1.0f;
   int it = 0;
+  // iteration sums: on the host, or -- inside a captured MD step -- on the device
+  auto count = [&](int k) {
+    if (c->md_capture)
+      k_md_count<<<1, 1, 0, c->st>>>(reinterpret_cast<const MsState*>(c->dscal), c->dscal + kScalMd, k,
+                                     reinterpret_cast<MdCtl*>(c->dscal + kScalMd + 8));
+    else
+      c->md_counts[k] += it;
+  };
   THR_CUDA(cudaMemsetAsync(f->dS, 0, n3 * sizeof(double), c->st));
   THR_CUDA(cudaMemcpyAsync(f->X2, f->Phi, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
   THR_TRY(qmrherm_dev(c, f->X2, f->Xr, res1, &it, One, 1, R.anum4g.data(), R.aden4g.data(), ng, 1, sp, nullptr,
                       f->dS, c->max_qmr_iters));
-  c->md_counts[1] += it;  // ancgpv
+  count(1);  // ancgpv
   THR_CUDA(cudaMemcpyAsync(f->X2, f->Xr, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
   THR_TRY(qmrherm_dev(c, f->X2, f->Xr, res1, &it, am, imass, R.bnum2g.data(), R.bden2g.data(), ng, 0, sp, nullptr,
                       f->dS, c->max_qmr_iters));
-  c->md_counts[0] += it;  // ancg
+  count(0);  // ancg
   THR_CUDA(cudaMemcpyAsync(f->X2, f->Xr, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
   THR_TRY(qmrherm_dev(c, f->X2, f->Xr, res1, &it, am, imass, R.anum2g.data(), R.aden2g.data(), ng, 2, sp, nullptr,
                       f->dS, c->max_qmr_iters));
-  c->md_counts[2] += it;  // ancgf
+  count(2);  // ancgf
   THR_TRY(qmrherm_dev(c, f->X2, f->Xr, res1, &it, One, 1, R.anum4g.data(), R.aden4g.data(), ng, 3, sp, nullptr,
                       f->dS, c->max_qmr_iters));
-  c->md_counts[3] += it;  // ancgfpv
+  count(3);  // ancgfpv
   const float bnf = c->p.beta * 1.0f;  // beta*Nf, Nf = 1 (params.F90:19)
   k_force_finish<<<grid(n3), kThreads, 0, c->st>>>(f->dS, theta, c->g, c->p.ibound, bnf);
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
@@ -167,13 +201,13 @@ int hamilton_dev(thr_ctx* c, MdFields* f, const float* theta, const float* pp, f
   auto& R = c->rat;
   int it = 0;
   THR_CUDA(cudaMemcpyAsync(f->R, f->Phi, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
-  THR_TRY(qmrherm_dev(c, f->R, f->Xr, res2, &it, 1.0f, 1, R.anum4.data(), R.aden4.data(), R.ndiag, 0, 0, nullptr,
-                      nullptr, c->max_qmr_iters));
+  THR_TRY(qmrherm_dev(c, f->R, f->Xr, res2, &it, 1.0f, 1, R.anum4.data(), R.aden4.data(), R.ndiag, 0, c->action_sp,
+                      nullptr, nullptr, c->max_qmr_iters));
   c->md_counts[5] += it;  // ancghpv
   if (it >= c->max_qmr_iters) return THR_ERR_MAXITER;  // check_qmr_iterations: dwf3d_lib.F90:860-881
   THR_CUDA(cudaMemcpyAsync(f->R, f->Xr, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
-  THR_TRY(qmrherm_dev(c, f->R, f->Xr, res2, &it, am, imass, R.bnum2.data(), R.bden2.data(), R.ndiag, 0, 0, nullptr,
-                      nullptr, c->max_qmr_iters));
+  THR_TRY(qmrherm_dev(c, f->R, f->Xr, res2, &it, am, imass, R.bnum2.data(), R.bden2.data(), R.ndiag, 0,
+                      c->action_sp, nullptr, nullptr, c->max_qmr_iters));
   c->md_counts[4] += it;  // ancgh
   if (it >= c->max_qmr_iters) return THR_ERR_MAXITER;
   k_redot<<<grid(n), kThreads, 0, c->st>>>(f->R, f->Xr, n, c->partials);
@@ -191,18 +225,101 @@ int initialise_phi_dev(thr_ctx* c, MdFields* f, float am, int imass) {
   auto& R = c->rat;
   THR_TRY(rng_phi_draw(c, f->R));
   int it = 0;
-  THR_TRY(qmrherm_dev(c, f->R, f->Xr, c->rescga, &it, am, imass, R.anum4.data(), R.aden4.data(), R.ndiag, 0, 0,
-                      nullptr, nullptr, c->max_qmr_iters));
+  THR_TRY(qmrherm_dev(c, f->R, f->Xr, c->rescga, &it, am, imass, R.anum4.data(), R.aden4.data(), R.ndiag, 0,
+                      c->action_sp, nullptr, nullptr, c->max_qmr_iters));
   c->md_counts[6] += it;  // ancgpf
   THR_CUDA(cudaMemcpyAsync(f->R, f->Xr, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
-  THR_TRY(qmrherm_dev(c, f->R, f->Xr, c->rescga, &it, 1.0f, 1, R.bnum4.data(), R.bden4.data(), R.ndiag, 0, 0,
-                      nullptr, nullptr, c->max_qmr_iters));
+  THR_TRY(qmrherm_dev(c, f->R, f->Xr, c->rescga, &it, 1.0f, 1, R.bnum4.data(), R.bden4.data(), R.ndiag, 0,
+                      c->action_sp, nullptr, nullptr, c->max_qmr_iters));
   c->md_counts[7] += it;  // ancgpfpv
   THR_CUDA(cudaMemcpyAsync(f->Phi, f->Xr, n * sizeof(double2), cudaMemcpyDeviceToDevice, c->st));
   return THR_OK;
 }
 
-// evolution.F90:113-179 on f->thetat / f->pp; links follow thetat.
+namespace {
+// One MD step -- drift, coef, force (four multishift solves, each batch loop a WHILE
+// node), the exit draw at site (1,1,1), the closing kick -- captured once and replayed.
+struct MdGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  MdFields f{};
+  float dt = 0.f, res = 0.f, am = 0.f, proby = 0.f, am3 = 0.f, beta = 0.f;
+  int imass = 0, fixed_mode = 0, spmd = -1;
+  unsigned long long gen = ~0ull;
+  bool failed = false;  // a capture failed for this key: run host-driven
+  void release() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
+};
+constexpr int kFixedLastSlot = 1000;  // hiscal slot the step graph copies its fixed-length flag from
+
+bool md_same(const MdGraph& G, const thr_ctx* c, const MdFields* f, float dt, float res, float am, int imass,
+             float proby, int fixed_mode) {
+  return G.f.Phi == f->Phi && G.f.thetat == f->thetat && G.f.pp == f->pp && G.f.dS == f->dS && G.f.X2 == f->X2 &&
+         G.f.Xr == f->Xr && G.dt == dt && G.res == res && G.am == am && G.imass == imass && G.proby == proby &&
+         G.fixed_mode == fixed_mode && G.gen == c->buf_gen && G.am3 == c->p.am3 && G.beta == c->p.beta &&
+         G.spmd == c->spmd;
+}
+
+// captures the step into G (c->st in capture mode); on failure the capture is discarded
+int md_capture_step(thr_ctx* c, MdGraph& G, MdFields* f, float dt, float res, float am, int imass, float proby,
+                    int fixed_mode) {
+  const int n3 = c->g.v3 * 3;
+  const float hdt = 0.5f * dt;
+  MdCtl* ctl = reinterpret_cast<MdCtl*>(c->dscal + kScalMd + 8);
+  G.release();
+  THR_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+  c->md_capture = true;
+  c->ms_tmpl_next = 0;
+  int rc = THR_OK;
+  if (cudaMemsetAsync(c->dscal + kScalMd, 0, 8 * sizeof(double) + sizeof(MdCtl), c->st) != cudaSuccess ||
+      cudaMemcpyAsync(&ctl->fixed_last, c->hiscal + kFixedLastSlot, sizeof(int), cudaMemcpyHostToDevice, c->st) !=
+          cudaSuccess)
+    rc = THR_ERR_CUDA;
+  if (!rc) {
+    k_theta_drift<<<grid(n3), kThreads, 0, c->st>>>(f->thetat, f->pp, dt, n3);
+    rc = c->coef_dev(f->thetat);
+  }
+  if (!rc) rc = force_dev(c, f, f->thetat, res, am, imass);
+  if (!rc) rc = rng_rano_site(c, 1, 1, 1, &ctl->ytest, nullptr);  // evolution.F90:146
+  if (!rc) k_pp_kick_last<<<grid(n3), kThreads, 0, c->st>>>(f->pp, f->dS, dt, hdt, proby, fixed_mode, ctl, n3);
+  c->md_capture = false;
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(c->st, &g);
+  if (!rc && ce == cudaSuccess && g) {
+    G.graph = g;
+    if (cudaGraphInstantiate(&G.exec, G.graph, cudaGraphInstantiateFlagUseNodePriority) != cudaSuccess)
+      rc = THR_ERR_CUDA;
+  } else {
+    if (g) cudaGraphDestroy(g);
+    if (!rc) rc = THR_ERR_CUDA;
+  }
+  if (rc) {
+    G.release();
+    cudaGetLastError();
+    return rc;
+  }
+  G.f = *f;
+  G.dt = dt; G.res = res; G.am = am; G.imass = imass; G.proby = proby; G.fixed_mode = fixed_mode;
+  G.gen = c->buf_gen; G.am3 = c->p.am3; G.beta = c->p.beta; G.spmd = c->spmd;
+  return THR_OK;
+}
+}  // namespace
+
+void md_graph_release(thr_ctx* c) {
+  if (c->md_graph) {
+    static_cast<MdGraph*>(c->md_graph)->release();
+    delete static_cast<MdGraph*>(c->md_graph);
+    c->md_graph = nullptr;
+  }
+}
+
+// evolution.F90:113-179 on f->thetat / f->pp; links follow thetat.  The first MD step
+// runs host-driven (it sizes every buffer and settles the autotuner); the others replay
+// one captured graph of the step: one launch and one synchronisation per step.
 int evolve_dev(thr_ctx* c, MdFields* f, int iterl, float dt, float res, float am, int imass, int fixed_steps,
                int* itot) {
   const int n3 = c->g.v3 * 3;
@@ -211,13 +328,36 @@ int evolve_dev(thr_ctx* c, MdFields* f, int iterl, float dt, float res, float am
   k_pp_kick<<<grid(n3), kThreads, 0, c->st>>>(f->pp, f->dS, hdt, n3);
   const float proby = 1.0f / (float)iterl;
   const int nmax = fixed_steps > 0 ? fixed_steps : 4 * iterl;
+  const int fixed_mode = fixed_steps > 0 ? 1 : 0;
+  // the step graph needs the site streams (the exit draw on the device), the batched
+  // solver and no kernel sampling
+  bool graph = c->use_md_graph && c->use_graphs && c->ms_algo == 1 && c->rng.site && !c->prof_on;
   int iter;
   for (iter = 1; iter <= nmax; iter++) {
+    if (graph && iter > 1) {
+      if (!c->md_graph) c->md_graph = new MdGraph();
+      MdGraph& G = *static_cast<MdGraph*>(c->md_graph);
+      if (!G.exec || !md_same(G, c, f, dt, res, am, imass, proby, fixed_mode)) {
+        if (md_capture_step(c, G, f, dt, res, am, imass, proby, fixed_mode) != THR_OK) graph = false;
+      }
+      if (graph) {
+        c->hiscal[kFixedLastSlot] = (fixed_mode && iter == fixed_steps) ? 1 : 0;
+        THR_CUDA(cudaGraphLaunch(G.exec, c->st));
+        THR_CUDA(cudaMemcpyAsync(c->hscal + kScalMd, c->dscal + kScalMd, 8 * sizeof(double) + sizeof(MdCtl),
+                                 cudaMemcpyDeviceToHost, c->st));
+        THR_CUDA(cudaStreamSynchronize(c->st));
+        for (int k = 0; k < 8; k++) c->md_counts[k] += c->hscal[kScalMd + k];
+        const MdCtl* hc = reinterpret_cast<const MdCtl*>(c->hscal + kScalMd + 8);
+        if (hc->status) return hc->status;
+        if (hc->last) break;
+        continue;
+      }
+    }
     k_theta_drift<<<grid(n3), kThreads, 0, c->st>>>(f->thetat, f->pp, dt, n3);
     THR_TRY(c->coef_dev(f->thetat));
     THR_TRY(force_dev(c, f, f->thetat, res, am, imass));
     float ytest = 0.0f;
-    THR_TRY(rng_rano_site(c, 1, 1, 1, nullptr, &ytest));  // evolution.F90:441
+    THR_TRY(rng_rano_site(c, 1, 1, 1, nullptr, &ytest));  // evolution.F90:146
     const bool last = fixed_steps > 0 ? (iter == fixed_steps) : (ytest < proby);
     if (last) {
       k_pp_kick<<<grid(n3), kThreads, 0, c->st>>>(f->pp, f->dS, hdt, n3);
@@ -314,11 +454,18 @@ int thr_set_remez(thr_ctx* c, int ndiag, const double* anum2, const double* aden
 }
 
 int thr_set_residuals(thr_ctx* c, float rescga, float rescgg, int spmd, int max_qmr_iters) {
-  if (!c) return THR_ERR_BADARG;
+  if (!c || spmd < 0 || spmd > 3) return THR_ERR_BADARG;
   c->rescga = rescga;
   c->rescgg = rescgg;
   c->spmd = spmd;
   if (max_qmr_iters > 0) c->max_qmr_iters = max_qmr_iters;
+  return THR_OK;
+}
+
+int thr_set_action_precision(thr_ctx* c, int precision) {
+  if (!c || (precision != THR_FP64 && precision != THR_MIXED_FP32 && precision != THR_MIXED_BF16))
+    return THR_ERR_BADARG;
+  c->action_sp = precision;
   return THR_OK;
 }
 

@@ -19,5 +19,7 @@ int evolve_dev(thr_ctx* c, MdFields* f, int iterl, float dt, float res, float am
                int* itot);
 int trajectory_dev(thr_ctx* c, MdFields* f, int iterl, float dt, float am, int imass, int fixed_steps,
                    thr_traj_result* out);
+// destroys the cached MD step graph (context teardown)
+void md_graph_release(thr_ctx* c);
 
 }  // namespace thr

@@ -310,7 +310,7 @@ void enqueue_flush(thr_ctx* c, cudaStream_t on, MsState* ms, MsHist* hist, MsCoe
   k_reset<<<1, 1, 0, on>>>(hist, ms);
 }
 
-// One batch of kBatch iterations on ring half `half` (stream order on c->st),
+// One batch of kBatch iterations on ring half `half` (stream order on `main`),
 // recording into hist[half]; alongside it, on c->st2, the flush of the batch
 // before (hist[1 - half], the other half).  Ring slots: iteration j of the batch
 // reads r from slot half*kBatch + j and writes the new r to the next slot (mod
@@ -318,7 +318,7 @@ void enqueue_flush(thr_ctx* c, cudaStream_t on, MsState* ms, MsHist* hist, MsCoe
 // prof: sample kernel timings with events (stream-launched solves only).
 template <class V, class VO = V>
 int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO* sf, V* ring, V* p, V* hv, V* s,
-                  float am, int imass, int half, long long k0, bool prof, int* prof_flush) {
+                  float am, int imass, int half, long long k0, bool prof, int* prof_flush, cudaStream_t main) {
   const size_t n = c->n4();
   const unsigned gb = vec_grid(n / 4);
   const bool fp64 = sizeof(V) == sizeof(double2);
@@ -331,10 +331,10 @@ int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO
   // that kernel's alone and not one shared with a concurrent flush)
   const bool fork = c->overlap_flush != 0 && !prof;
   if (fork) {
-    THR_CUDA(cudaEventRecord(c->ev_fork[half], c->st));
+    THR_CUDA(cudaEventRecord(c->ev_fork[half], main));
     THR_CUDA(cudaStreamWaitEvent(c->st2, c->ev_fork[half], 0));
   }
-  enqueue_flush<V, VO>(c, fork ? c->st2 : c->st, ms, hist + (1 - half), cf + (1 - half), out, sf, ring, 1 - half,
+  enqueue_flush<V, VO>(c, fork ? c->st2 : main, ms, hist + (1 - half), cf + (1 - half), out, sf, ring, 1 - half,
                        prof, k0 - kBatch, prof_flush);
   if (fork) THR_CUDA(cudaEventRecord(c->ev_join[half], c->st2));
   // h = M p is kept by the recurrence h_new = M r + gammag h_old (p = r + gammag p
@@ -354,20 +354,20 @@ int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO
     V* hcur = (j & 1) ? p : hv;
     const V* hprev = (j & 1) ? hv : p;
     // alpha = Re<p, M^dagger M p> (:104) evaluated as |h|^2 = |M p|^2 in the M epilogue
-    int pe = prof ? c->prof_begin(thr_ctx::P_DSLASH, b_md, k0 + j) : -1;
-    THR_TRY(launch_dslash_accum<V>(c->g, c->p.kernel, false, hcur, rold, u, am, imass, c->p.am3, c->st, &ms->done,
+    int pe = prof ? c->prof_begin(fp64 ? thr_ctx::P_DSLASH : thr_ctx::P_DSLASH_LOW, b_md, k0 + j) : -1;
+    THR_TRY(launch_dslash_accum<V>(c->g, c->p.kernel, false, hcur, rold, u, am, imass, c->p.am3, main, &ms->done,
                                    hprev, &ms->gammag, c->partials, 0));
     c->prof_end(pe);
-    k_alpha<<<1, 1024, 0, c->st>>>(ms, rec, c->partials, gs);
+    k_alpha<<<1, 1024, 0, main>>>(ms, rec, c->partials, gs);
     // s = M^dagger h is never stored: the epilogue forms r = r + omega*s (:137) and |r|^2 (:138)
-    pe = prof ? c->prof_begin(thr_ctx::P_DSLASH_DAG, b_md, k0 + j) : -1;
-    THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, rnew, hcur, u, am, imass, c->p.am3, c->st, &ms->done,
+    pe = prof ? c->prof_begin(fp64 ? thr_ctx::P_DSLASH_DAG : thr_ctx::P_DSLASH_DAG_LOW, b_md, k0 + j) : -1;
+    THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, rnew, hcur, u, am, imass, c->p.am3, main, &ms->done,
                                   rold, &ms->omega, c->partials, rev_md));
     c->prof_end(pe);
-    k_lambda<<<1, 1024, 0, c->st>>>(ms, rec, c->partials, gs);
+    k_lambda<<<1, 1024, 0, main>>>(ms, rec, c->partials, gs);
   }
   (void)s;
-  if (fork) THR_CUDA(cudaStreamWaitEvent(c->st, c->ev_join[half], 0));
+  if (fork) THR_CUDA(cudaStreamWaitEvent(main, c->ev_join[half], 0));
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
 
@@ -434,9 +434,9 @@ int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO* sf,
   THR_CUDA(cudaGraphAddNode(&node, G.graph, nullptr, 0, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   THR_CUDA(cudaStreamBeginCaptureToGraph(c->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  int rc = enqueue_batch<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 0, 0, false, nullptr);
+  int rc = enqueue_batch<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 0, 0, false, nullptr, c->st);
   if (rc == THR_OK)
-    rc = enqueue_batch<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 1, 0, false, nullptr);
+    rc = enqueue_batch<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 1, 0, false, nullptr, c->st);
   if (rc == THR_OK) k_loop_ctl<<<1, 1, 0, c->st>>>(ms, handle);
   cudaGraph_t captured = nullptr;
   cudaError_t ce = cudaStreamEndCapture(c->st, &captured);
@@ -499,6 +499,40 @@ template <class V, class VO, class Prime>
 int run_batches(thr_ctx* c, MsState* ms, MsState* h, MsHist* hist, MsCoef* cf, VO* out, VO* sf, V* ring, V* p, V* hv,
                 V* s, float am, int imass, Prime&& prime) {
   const size_t n = c->n4();
+  if (c->md_capture) {
+    // inside a captured MD step: the batch loop becomes a WHILE node of the graph
+    // being captured on c->st, its body captured on c->st3; nothing is read back
+    THR_TRY(prime());
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    THR_CUDA(cudaStreamGetCaptureInfo(c->st, &cst, nullptr, &g, &deps, &nd));
+    if (cst != cudaStreamCaptureStatusActive) return THR_ERR_CUDA;
+    cudaGraphConditionalHandle handle;
+    THR_CUDA(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    THR_CUDA(cudaGraphAddNode(&node, g, deps, nd, &cp));
+    THR_CUDA(cudaStreamUpdateCaptureDependencies(c->st, &node, 1, cudaStreamSetCaptureDependencies));
+    THR_CUDA(cudaStreamBeginCaptureToGraph(c->st3, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_batch<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 0, 0, false, nullptr, c->st3);
+    if (rc == THR_OK)
+      rc = enqueue_batch<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, 1, 0, false, nullptr, c->st3);
+    if (rc == THR_OK) k_loop_ctl<<<1, 1, 0, c->st3>>>(ms, handle);
+    cudaGraph_t body = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(c->st3, &body);
+    if (rc != THR_OK) return rc;
+    if (ce != cudaSuccess) return THR_ERR_CUDA;
+    // the last batch's flush (ring half 1), after the loop, on the captured stream
+    enqueue_flush<V, VO>(c, c->st, ms, hist + 1, cf + 1, out, sf, ring, 1, false, 0, nullptr);
+    return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+  }
   if (c->use_graphs && !c->prof_on) {
     // one graph launch runs every batch until convergence (or the switch); one synchronisation
     cudaGraphExec_t exec = nullptr;
@@ -527,7 +561,8 @@ int run_batches(thr_ctx* c, MsState* ms, MsState* h, MsHist* hist, MsCoef* cf, V
   int half = 0;
   for (long long k = it0;; k += kBatch, half ^= 1) {
     int pf = -1;
-    THR_TRY(enqueue_batch<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, half, k, c->prof_on, &pf));
+    THR_TRY(
+        enqueue_batch<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, half, k, c->prof_on, &pf, c->st));
     THR_CUDA(cudaMemcpyAsync(h, ms, sizeof(MsState), cudaMemcpyDeviceToHost, c->st));
     THR_CUDA(cudaStreamSynchronize(c->st));
     account(pf);
@@ -543,9 +578,10 @@ int run_batches(thr_ctx* c, MsState* ms, MsState* h, MsHist* hist, MsCoef* cf, V
     if (h->batches >= h->max_batches) return THR_ERR_CUDA;  // the device state stopped advancing
   }
   if (c->prof_on) {
+    const bool fp64 = sizeof(V) == sizeof(double2);
     c->prof_trim(prof_first, h->it);  // launches after convergence skipped their work
-    c->prof_work[thr_ctx::P_DSLASH] += h->it - it0;
-    c->prof_work[thr_ctx::P_DSLASH_DAG] += h->it - it0;
+    c->prof_work[fp64 ? thr_ctx::P_DSLASH : thr_ctx::P_DSLASH_LOW] += h->it - it0;
+    c->prof_work[fp64 ? thr_ctx::P_DSLASH_DAG : thr_ctx::P_DSLASH_DAG_LOW] += h->it - it0;
     c->prof_work[thr_ctx::P_SHIFTUPD] += flushes;
   }
   return THR_OK;
@@ -559,7 +595,13 @@ int batched_setup(thr_ctx* c, const V* in, V* out, V* sf, V* ring, int ndiagq, c
                   MsCoef** cf_out) {
   const size_t n = c->n4();
   MsState* ms = reinterpret_cast<MsState*>(c->dscal);
+  // the initial state is copied from host memory when the copy runs: inside a captured MD
+  // step every solve gets its own pinned template, which stays valid for the graph's life
   MsState* h = reinterpret_cast<MsState*>(c->hscal);
+  if (c->md_capture) {
+    if (c->ms_tmpl_next >= kMsTemplates) return THR_ERR_BADSHAPE;
+    h = reinterpret_cast<MsState*>(c->ms_tmpl) + c->ms_tmpl_next++;
+  }
   void* hv_;
   THR_TRY(c->buffer(thr_ctx::B_HIST, 2 * sizeof(MsHist), &hv_));
   void* cf_;
@@ -602,6 +644,7 @@ int multishift_batched_dev(thr_ctx* c, const V* in, V* out, V* sf, V* ring, V* p
     return THR_OK;
   };
   THR_TRY(run_batches<V, V>(c, ms, h, hist, cf, out, sf, ring, p, hv, s, am, imass, prime));
+  if (c->md_capture) return THR_OK;  // the results stay on the device
   if (cg_return) *cg_return = h->it;
   if (cg_returns)
     for (int q = 0; q < ndiagq; q++) cg_returns[q] = h->cg_returns[q];
@@ -633,6 +676,7 @@ int multishift_mixed_dev(thr_ctx* c, const double2* in, double2* out, double2* s
     THR_CUDA(cudaMemsetAsync(p, 0, n * sizeof(double2), c->st));
     return THR_OK;
   };
+  if (c->md_capture) return THR_ERR_UNSUPPORTED;  // the precision switch is decided on the host
   THR_TRY(run_batches<double2, double2>(c, ms, h, hist, cf, out, sf, ring64, p, hv, s, am, imass, prime64));
   if (switched_at) *switched_at = 0;
   if (!h->done && !h->status) {

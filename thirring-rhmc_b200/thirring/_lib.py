@@ -80,6 +80,7 @@ SIGNATURES = {
     "thr_saveseed": (_i, [C.c_char_p, _d]),
     "thr_set_remez": (_i, [_v, _i] + [_v] * 8 + [_i] + [_v] * 8),
     "thr_set_residuals": (_i, [_v, _f, _f, _i, _i]),
+    "thr_set_action_precision": (_i, [_v, _i]),
     "thr_force": (_i, [_v, _v, _f, _f, _i, _v, _v]),
     "thr_hamilton": (_i, [_v, _v, _pd, _pd, _pd, _pd, _f, _f, _i, _v, _v]),
     "thr_initialise_phi": (_i, [_v, _v, _f, _i]),

@@ -523,7 +523,13 @@ class Lattice:
         _check(self._L.thr_set_remez(*args), "set_remez")
 
     def set_residuals(self, rescga=1e-8, rescgg=1e-6, spmd=1, max_qmr_iters=0):
+        """params.F90:60-64; spmd is the guidance solves' qmrherm use_sp (0 FP64, 1 the
+        reference's SP multishift, MIXED_FP32 / MIXED_BF16 the mixed multishift)."""
         _check(self._L.thr_set_residuals(self.h, rescga, rescgg, int(spmd), max_qmr_iters), "set_residuals")
+
+    def set_action_precision(self, precision=FP64):
+        """Precision of the Hamiltonian and pseudofermion solves (FP64, MIXED_FP32, MIXED_BF16)."""
+        _check(self._L.thr_set_action_precision(self.h, int(precision)), "set_action_precision")
 
     def force(self, Phi, res1, am, imass, theta):
         """dSdpi = force(Phi, res1, am, imass): force_module.F90:9-113 (current links)."""
