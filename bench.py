@@ -510,6 +510,61 @@ def run_dslash_sweep(args):
             "best": best}
 
 
+def run_aux_kernels(args):
+    """The other bandwidth-bound kernels of the path on the headline lattice (or --lx/--ls):
+    derivs (derivs_module.F90:99-196; reads R and X2 once, reads and writes dSdpi) for
+    iflag 0 and 1, and the pseudofermion draw of initialise_phi_1flavour (evolution.F90:
+    40-51; 4 Ls Gaussian pairs per site: reads and writes each site's generator state, 97
+    table entries and 16 bytes, writes the FP64 field).  Per kernel: the mean of `steps`
+    launches after `warmup`, CUDA events on the library's stream, algorithmic GB/s and the
+    fraction of the measured HBM copy rate."""
+    import torch
+    import thirring
+    from thirring import _lib
+    L = _lib.lib()
+    peak, peak_kind = peaks()
+    lx, ls = LX, LS
+    G = thirring.Lattice(lx, lx, lx, ls, beta=BETA)
+    rng = np.random.default_rng(11)
+    G.coef(np.asfortranarray(rng.standard_normal((lx, lx, lx, 3)) / np.sqrt(BETA), np.float32))
+    G.init_random(4139764973254.0)
+    R = thirring.spinor(G)
+    sh = R[1:-1, 1:-1, 1:-1, 1:-1, :].shape
+    R[1:-1, 1:-1, 1:-1, 1:-1, :] = rng.standard_normal(sh) + 1j * rng.standard_normal(sh)
+    a, b = G._field(0, R), G._field(0, R)
+    sptr = C.c_void_p()
+    L.thr_get_stream(G.h, C.byref(sptr))
+    st = torch.cuda.ExternalStream(sptr.value)
+    v3, n = lx ** 3, 4 * ls * lx ** 3
+    steps, warmup = max(args.steps, 10), max(args.warmup, 3)
+    out = {}
+
+    def timed(name, fn, byts):
+        for _ in range(warmup):
+            fn()
+        L.thr_sync(G.h)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(steps):
+            fn()
+        e1.record(st)
+        e1.synchronize()
+        us = e0.elapsed_time(e1) / steps * 1e3
+        out[name] = {"us": round(us, 2), "algorithmic_bytes": int(byts), "gbs": round(byts / us / 1e3, 1),
+                     "frac": round(byts / us / 1e3 / peak, 3)}
+
+    for iflag in (0, 1):
+        timed("k_derivs_iflag%d" % iflag, lambda: L.thr_derivs_dev(G.h, a, b, 0.37, iflag, AM, IMASS),
+              2 * n * 16 + 2 * 3 * v3 * 8)
+    timed("k_phi_draw", lambda: L.thr_phi_draw_dev(G.h, a), n * 16 + 2 * v3 * (97 * 4 + 16))
+    L.thr_field_destroy(G.h, a)
+    L.thr_field_destroy(G.h, b)
+    G.close()
+    return {"workload": "auxiliary kernels at %d^2x%d, Ls=%d: derivs (iflag 0, 1), pseudofermion draw" % (lx, lx, ls),
+            "peak_gbs": peak, "peak_source": peak_kind, "launches": steps, "results": out}
+
+
 def dslash_bandwidth(args, dev, lx=48, ls=48, iters=20, warmup=3):
     """FP64 Shamir M at lx^2 x lx, Ls = ls: algorithmic GB/s over `iters` launches
     (one read of the input spinor, one write of the output, three link fields)."""
@@ -826,7 +881,7 @@ def main():
                          "stencils and residuals with FP64 shift fields")
     ap.add_argument("--workload", default="multishift",
                     choices=["multishift", "measurement", "packed", "trajectory", "trajectory48", "dslash",
-                             "dslash_sweep", "overlap"],
+                             "dslash_sweep", "aux_kernels", "overlap"],
                     help="secondary workloads print their own JSON line (not the headline contract)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-iters", type=int, default=50, help="multishift iterations in the CPU sample")
@@ -862,7 +917,8 @@ def main():
         return
     if args.workload != "multishift":
         fn = {"measurement": run_measurement, "packed": run_packed, "trajectory": run_trajectory,
-              "trajectory48": run_trajectory48, "overlap": run_overlap, "dslash_sweep": run_dslash_sweep}[args.workload]
+              "trajectory48": run_trajectory48, "overlap": run_overlap, "dslash_sweep": run_dslash_sweep,
+              "aux_kernels": run_aux_kernels}[args.workload]
         print(json.dumps(fn(args)), flush=True)
         return
 

@@ -288,6 +288,11 @@ int thr_mixed_switched_at(thr_ctx *ctx, int *iteration);
 int thr_derivs(thr_ctx *ctx, const double *R, const double *X2, double anum, int iflag, float am, int imass,
                double *dSdpi);
 
+/* derivs on FP64 device fields (thr_field_create with THR_FP64) and the current
+ * links, accumulating into the context's dSdpi (the one qmrherm_dev uses);
+ * enqueued on the context's stream. */
+int thr_derivs_dev(thr_ctx *ctx, const void *R, const void *X2, double anum, int iflag, float am, int imass);
+
 /* ---- random.f90 / site_random.f90 / gaussian.F90 ------------------------- */
 /* init_random(seed), site_random.f90:133-148 (site_streams = 1, one stream per
  * 3D site, seeded seed + x + Lx*y + Lx*Lx*t, on the device) or
@@ -299,6 +304,10 @@ int thr_init_random(thr_ctx *ctx, double seed, int site_streams);
 int thr_gauss0(thr_ctx *ctx, float *ps);
 /* gaussp(ps), gaussian.F90:14-61: variance 1 per component. */
 int thr_gaussp(thr_ctx *ctx, float *ps);
+/* The pseudofermion draw of initialise_phi_1flavour (evolution.F90:40-51: R(s, ., d) =
+ * cmplx(gauss0) for d = 1..4, s = 1..Ls, 4 Ls gauss0 calls) into an FP64 device
+ * field, site streams only; enqueued on the context's stream. */
+int thr_phi_draw_dev(thr_ctx *ctx, void *R);
 /* rano(yran, idum, ix, iy, it): one uniform draw from the stream of 1-based
  * site (ix,iy,it) (ignored for the global stream), random.f90:28-58. */
 int thr_rano(thr_ctx *ctx, int ix, int iy, int it, float *out);

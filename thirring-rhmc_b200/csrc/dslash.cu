@@ -23,6 +23,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
@@ -1240,24 +1241,40 @@ int launch_odslash(const Geom& g, bool dag, double2* out, const double2* in, con
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
 
+// The persistent batch stencil's grid (resident blocks per SM) is tuned like the register
+// budgets: work blocks, not CTAs, own the partial sums, so every grid gives the same bits.
+constexpr int kTuneBatchGrid[3] = {8, 4, 16};  // CTAs per SM
+
 template <class S>
 int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
                         float am, int imass, float am3, cudaStream_t st, const int* skip, const S* aux,
                         double* partials, int grid) {
   if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;
   const bool epi = aux != nullptr;
-  const int g = grid > 0 ? grid : (b.total_blocks < device_sms() * 8 ? b.total_blocks : device_sms() * 8);
+  auto launch = [&](int per_sm) {
+    const int g = grid > 0 ? grid : std::min(b.total_blocks, device_sms() * per_sm);
 #define THR_L(K, D, E)                                                                                          \
   k_dslash_batch<S, K, D, E><<<g, 256, 0, st>>>(out, in, u, b.dev, b.nent, b.total_blocks, am, imass, am3, skip, \
                                                 aux, partials)
-  if (kernel == 1) {
-    if (dag) { if (epi) THR_L(1, true, 1); else THR_L(1, true, 0); }
-    else { if (epi) THR_L(1, false, 1); else THR_L(1, false, 0); }
-  } else {
-    if (dag) { if (epi) THR_L(0, true, 1); else THR_L(0, true, 0); }
-    else { if (epi) THR_L(0, false, 1); else THR_L(0, false, 0); }
-  }
+    if (kernel == 1) {
+      if (dag) { if (epi) THR_L(1, true, 1); else THR_L(1, true, 0); }
+      else { if (epi) THR_L(1, false, 1); else THR_L(1, false, 0); }
+    } else {
+      if (dag) { if (epi) THR_L(0, true, 1); else THR_L(0, true, 0); }
+      else { if (epi) THR_L(0, false, 1); else THR_L(0, false, 0); }
+    }
 #undef THR_L
+  };
+  int per_sm = kTuneBatchGrid[0];
+  if (grid <= 0 && b.total_blocks > device_sms() * kTuneBatchGrid[1]) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    // key: the batch kernel family (10 + kernel), its size (total work blocks, entries)
+    per_sm = tune_pick(TuneKey{dev, storage_id<S>(), 10 + kernel, dag ? 1 : 0, epi ? 1 : 0, b.total_blocks, b.nent, 0,
+                               0, 0},
+                       kTuneBatchGrid, 3, st, launch);
+  }
+  launch(per_sm);
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
 
@@ -1293,10 +1310,16 @@ extern "C" int thr_tune_report(char* buf, int len) {
     for (const auto& kv : g_tune) {
       const TuneKey& k = kv.first;
       char line[256];
-      int w = std::snprintf(line, sizeof(line), "%s %s %s epi=%d %dx%dx%d Ls=%d layout=%d dev=%d minb=%d us=",
-                            k.sid == 0 ? "fp64" : "fp32", k.ker == 2 ? "overlap" : k.ker ? "wilson" : "shamir",
-                            k.dag ? "Mdag" : "M", k.epi,
-                            k.lx, k.ly, k.lt, k.ls, k.layout, k.dev, kv.second.pick);
+      const char* sto = k.sid == 0 ? "fp64" : k.sid == 1 ? "fp32" : "bf16";
+      int w;
+      if (k.ker >= 10)  // persistent batch stencil: lx = its work blocks, ly = entries
+        w = std::snprintf(line, sizeof(line), "%s batch-%s %s epi=%d blocks=%d entries=%d dev=%d ctas_per_sm=%d us=",
+                          sto, k.ker == 11 ? "wilson" : "shamir", k.dag ? "Mdag" : "M", k.epi, k.lx, k.ly, k.dev,
+                          kv.second.pick);
+      else
+        w = std::snprintf(line, sizeof(line), "%s %s %s epi=%d %dx%dx%d Ls=%d layout=%d dev=%d minb=%d us=", sto,
+                          k.ker == 2 ? "overlap" : k.ker ? "wilson" : "shamir", k.dag ? "Mdag" : "M", k.epi, k.lx,
+                          k.ly, k.lt, k.ls, k.layout, k.dev, kv.second.pick);
       for (int c = 0; c < kv.second.ncand && w > 0 && w < (int)sizeof(line); c++)
         w += std::snprintf(line + w, sizeof(line) - w, c ? "/%.2f" : "%.2f", kv.second.us[c]);
       r += line;

@@ -223,6 +223,15 @@ int thr_derivs(thr_ctx* c, const double* R, const double* X2, double anum, int i
   return c->sync();
 }
 
+int thr_derivs_dev(thr_ctx* c, const void* R, const void* X2, double anum, int iflag, float am, int imass) {
+  if (!c || !R || !X2) return THR_ERR_BADARG;
+  if (!c->links_ok) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  double* dS;
+  THR_TRY(dsdpi_dev(c, &dS));
+  return launch_derivs(c, dS, (const double2*)R, (const double2*)X2, anum, iflag, am, imass);
+}
+
 static int ms_abi(thr_ctx* c, const double* u, float am, int imass, int ndiagq, const double* aden, const double* anum,
                   double* output, const double* input, float res, int maxcg, int* cg_return, int* cg_returns,
                   int sp) {

@@ -325,6 +325,12 @@ static int gauss_abi(thr_ctx* c, float* ps, float scale) {
   return c->sync();
 }
 
+int thr_phi_draw_dev(thr_ctx* c, void* R) {
+  if (!c || !R) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  return rng_phi_draw(c, (double2*)R);
+}
+
 int thr_gauss0(thr_ctx* c, float* ps) { return gauss_abi(c, ps, -1.0f); }
 int thr_gaussp(thr_ctx* c, float* ps) { return gauss_abi(c, ps, -2.0f); }
 

@@ -96,6 +96,8 @@ SIGNATURES = {
     "thr_qmrherm_dev": (_i, [_v, _v, _v, _f, _pi, _f, _i, _v, _v, _i, _i, _i, _v]),
     "thr_dslash_fused_dev": (_i, [_v, _v, _v, _v, _d, _i, _f, _i, _i, _i, _pd]),
     "thr_shift_residuals_dev": (_i, [_v, _v, _v, _i, _v, _f, _i, _v]),
+    "thr_derivs_dev": (_i, [_v, _v, _v, _d, _i, _f, _i]),
+    "thr_phi_draw_dev": (_i, [_v, _v]),
     "thr_set_solver": (_i, [_v, _i]),
     "thr_set_mixed": (_i, [_v, _d, _d]),
     "thr_mixed_switched_at": (_i, [_v, _pi]),
