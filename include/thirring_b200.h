@@ -446,6 +446,11 @@ int thr_get_stream(thr_ctx *ctx, void **stream);
 int thr_profile(thr_ctx *ctx, int stride, int reset);
 int thr_profile_read(thr_ctx *ctx, int kind, int *sampled, double *ms, double *bytes, double *launches);
 
+/* Blocks of the staged-tile FP64 stencil (THR_TILE=1) whose tile copies did not
+ * arrive within the kernel's bounded wait (0.2 s), since the library was loaded,
+ * on the context's device.  Such a block writes NaN to all its outputs and to its
+ * epilogue sum, so solvers stop with THR_ERR_NAN.  No counterpart in the reference. */
+int thr_stencil_timeouts(thr_ctx *ctx, unsigned long long *count);
 /* The stencil autotuner's choices so far (process-wide), as text: one line per
  * tuned case with the candidates' mean launch times.  The tuner picks the
  * register budget (resident blocks per SM) of the Shamir and Wilson stencils

@@ -219,3 +219,35 @@ def test_dslash_fp32_storage(ls, imass):
             got = _dev_dslash(G, R, 1, 0.05, imass, dag)
             ref = (O.dslashd if dag else O.dslash)(L, R, u, 0.05, imass)
             assert rel_err(interior(got), interior(ref)) <= 2e-6, (ls, imass, dag)
+
+
+@pytest.mark.gpu
+def test_tile_wait_bound_reports_timeout(tmp_path):
+    """The staged-tile stencil's bounded wait.  With THR_TILE_WAIT_TEST=1 every block expects
+    16 bytes more than its copies bring, so its wait runs out although every copy has
+    completed (nothing faults); each block then writes NaN to all its outputs and counts the
+    event (thr_stencil_timeouts).  A normal run of the same kernel counts none."""
+    import os
+    import subprocess
+    import sys
+    rng = np.random.default_rng(5)
+    dims = (8, 8, 4, 16)  # staged-tile shape: 8*8*4/32 tiles x 16/8 s-chunks = 16 blocks
+    L = O.lat(*dims)
+    np.save(tmp_path / "R.npy", rand_spinor(L, rng))
+    np.save(tmp_path / "u.npy", rand_links(L, rng))
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "thirring-rhmc_b200")
+    code = ("import sys, ctypes as C, numpy as np; sys.path.insert(0, %r); import thirring; d = %r;"
+            "R = np.asfortranarray(np.load(d + '/R.npy')); u = np.asfortranarray(np.load(d + '/u.npy'));"
+            "G = thirring.Lattice(*%r); G.set_links(u); out = G.dslash(R, None, 0.05, 1);"
+            "n = C.c_ulonglong(0); assert thirring.lib().thr_stencil_timeouts(G.h, C.byref(n)) == 0;"
+            "np.save(d + '/out_' + sys.argv[1] + '.npy', out); print('timeouts', n.value); G.close()"
+            % (pkg, str(tmp_path), dims))
+    res = {}
+    for tag, env in (("ok", {"THR_TILE": "1"}), ("bound", {"THR_TILE": "1", "THR_TILE_WAIT_TEST": "1"})):
+        r = subprocess.run([sys.executable, "-c", code, tag], capture_output=True, text=True, timeout=300,
+                           env=dict(os.environ, **env))
+        assert r.returncode == 0, r.stdout + r.stderr
+        res[tag] = int(r.stdout.split("timeouts")[-1].split()[0])
+    ok, bound = np.load(tmp_path / "out_ok.npy"), np.load(tmp_path / "out_bound.npy")
+    assert res["ok"] == 0 and np.all(np.isfinite(interior(ok)))
+    assert res["bound"] == 16 and np.all(np.isnan(interior(bound)))

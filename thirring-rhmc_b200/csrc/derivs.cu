@@ -30,9 +30,13 @@ __device__ __forceinline__ double im_cjab(double2 c, double2 a, double2 b) {
 }
 __device__ __forceinline__ double2 gmul_d(GammaEntry e, double2 z) { return gmul<double2, double>(e, z); }
 
-__global__ void __launch_bounds__(256) k_derivs(double* __restrict__ dS, const double2* __restrict__ R,
-                                                const double2* __restrict__ X2, Geom g, int kernel, int iflag,
-                                                double tk, double tz, double2 c1, double2 c2) {
+// KER 0 (Shamir) / 1 (Wilson, adds the slice terms); MINB resident 256-thread blocks per SM
+// bound the registers.  The site's own spinors R(x), X2(x) are loaded once and serve all
+// three directions; per direction only the forward neighbour's are loaded.
+template <int KER, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_derivs(double* __restrict__ dS, const double2* __restrict__ R,
+                                                      const double2* __restrict__ X2, Geom g, int iflag, double tk,
+                                                      double tz, double2 c1, double2 c2) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= g.v3) return;
@@ -44,15 +48,19 @@ __global__ void __launch_bounds__(256) k_derivs(double* __restrict__ dS, const d
   double accm[3] = {0.0, 0.0, 0.0};
   const int Ls = g.ls;
   for (int s = lane; s < Ls; s += 32) {
+    double2 Rx[4], Xx[4];
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+      Rx[d] = __ldg(R + sidx(g, s, site, d));
+      Xx[d] = __ldg(X2 + sidx(g, s, site, d));
+    }
 #pragma unroll
     for (int mu = 0; mu < 3; mu++) {
       const int xf = nb.f[mu];
-      double2 Rx[4], Rf[4], Xx[4], Xf[4];
+      double2 Rf[4], Xf[4];
 #pragma unroll
       for (int d = 0; d < 4; d++) {
-        Rx[d] = __ldg(R + sidx(g, s, site, d));
         Rf[d] = __ldg(R + sidx(g, s, xf, d));
-        Xx[d] = __ldg(X2 + sidx(g, s, site, d));
         Xf[d] = __ldg(X2 + sidx(g, s, xf, d));
       }
       double a1 = 0.0, a2 = 0.0;
@@ -66,7 +74,7 @@ __global__ void __launch_bounds__(256) k_derivs(double* __restrict__ dS, const d
         a2 += gmul_d(ge, t3).y;
       }
       double acc = tk * a1 + sg * tz * a2;
-      if (kernel == 1) {
+      if (KER == 1) {
         // slice terms: partner slice in X2 at s+1 (P-, wall c2) and s-1 (P+, wall c1)
 #pragma unroll
         for (int side = 0; side < 2; side++) {
@@ -127,7 +135,10 @@ int launch_derivs(thr_ctx* c, double* dS, const double2* R, const double2* X2, d
   const double2 c2 = imass == 1 ? make_double2(-a, 0.0) : make_double2(0.0, a);
   const int threads = 256;
   const unsigned blocks = (unsigned)(((size_t)c->g.v3 * 32 + threads - 1) / threads);
-  k_derivs<<<blocks, threads, 0, c->st>>>(dS, R, X2, c->g, c->p.kernel, iflag, tk, tz, c1, c2);
+  if (c->p.kernel == 1)
+    k_derivs<1, 1><<<blocks, threads, 0, c->st>>>(dS, R, X2, c->g, iflag, tk, tz, c1, c2);
+  else
+    k_derivs<0, 3><<<blocks, threads, 0, c->st>>>(dS, R, X2, c->g, iflag, tk, tz, c1, c2);
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
 

@@ -32,6 +32,7 @@
 #include <string>
 
 #include "batch.h"
+#include "ctx.h"
 #include "thr_common.cuh"
 #include "thr_kernels.h"
 
@@ -625,8 +626,32 @@ static_assert(XF % 8 == 0 && YF % 8 == 0 && TF % 8 == 0 && UT % 8 == 0 && UX % 8
 struct alignas(64) Maps {
   CUtensorMap cen, xf, yf, tf, ut, ux, uy, utm;
 };
-constexpr unsigned kWaitPolls = 1u << 22;  // bound on the mbarrier wait (seconds at most)
+constexpr unsigned long long kWaitNs = 200000000ull;  // bound on each mbarrier wait: 0.2 s of global time
 }  // namespace tile
+
+// blocks of the staged-tile stencil whose copies did not arrive within the bound (per device);
+// read by thr_stencil_timeouts
+__device__ unsigned long long g_stencil_timeouts = 0;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// polls the mbarrier's phase 0 until it completes or kWaitNs have passed; 1 if it completed
+__device__ __forceinline__ unsigned mbar_wait_bounded(unsigned bar) {
+  unsigned done = 0;
+  const unsigned long long t0 = global_ns();
+  for (unsigned k = 0; !done; k++) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar)
+        : "memory");
+    if (!done && (k & 63) == 63 && global_ns() - t0 > tile::kWaitNs) break;
+  }
+  return done;
+}
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void tma_load5(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
@@ -643,7 +668,7 @@ template <bool DAG, int EPI>
 __global__ void __launch_bounds__(tile::NT, 4)
     k_dslash_tile(double2* __restrict__ out, const double2* __restrict__ in, const __grid_constant__ tile::Maps maps,
                   Geom g, float am, int imass, float am3, const int* skip, const double2* __restrict__ aux,
-                  const double* __restrict__ coef, double* __restrict__ partials, int rev) {
+                  const double* __restrict__ coef, double* __restrict__ partials, int rev, int extra_tx) {
   using namespace tile;
   if (skip && *skip) return;
   // the dynamic region is allocated 128 bytes long and rounded up to a 128-byte
@@ -670,7 +695,7 @@ __global__ void __launch_bounds__(tile::NT, 4)
     const int ym = y0 == 0 ? Ly - 1 : y0 - 1, yp = y0 + TY == Ly ? 0 : y0 + TY;
     const int tm = t0 == 0 ? Lt - 1 : t0 - 1, tp = t0 + TT == Lt ? 0 : t0 + TT;
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(&bar)),
-                 "r"(END * (int)sizeof(double2))
+                 "r"(END * (int)sizeof(double2) + extra_tx)
                  : "memory");
     const int c0 = 2 * s0;  // fifth-dimension coordinate in doubles: 16-byte multiples
     tma_load5(sm + CEN, &maps.cen, c0 - 2, x0, y0, t0, 0, &bar);
@@ -694,24 +719,29 @@ __global__ void __launch_bounds__(tile::NT, 4)
     const unsigned wsite = (unsigned)(x0 + (row & 3) + Lx * (y0 + ((row >> 2) & 3) + Ly * (t0 + ((row >> 4) & 1))));
     wv = in[(unsigned)(tid < 128 ? Ls - 1 : 0) + (unsigned)Ls * (wsite + v3 * (unsigned)(row >> 5))];
   }
-  unsigned done = 0;
-  for (unsigned k = 0; k < kWaitPolls && !done; k++) {
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(smem_u32(&bar))
-        : "memory");
-  }
+  const unsigned done = mbar_wait_bounded(smem_u32(&bar));
   if (wall) sm[CEN + row * CW + (tid < 128 ? 0 : CW - 1)] = wv;
-  if (!__syncthreads_and(done)) {
-    // the copies did not complete: the block's outputs and partial become NaN
-    if (EPI != 0 && tid == 0) partials[bid] = __longlong_as_double(0x7ff8000000000000LL);
-    return;
-  }
-
   const int sl = tid & 7, xs = (tid >> 3) & 3, ys = (tid >> 5) & 3, ts = tid >> 7;
   const int s = s0 + sl;
   const unsigned site = (unsigned)(x0 + xs + Lx * (y0 + ys + Ly * (t0 + ts)));
+  if (!__syncthreads_and(done)) {
+    // The copies did not all arrive within the bound.  One more bounded wait, so that no
+    // copy still writes this block's shared memory when the block exits (if that wait
+    // also runs out, the block exits anyway); the event is counted for the host
+    // (thr_stencil_timeouts) and every output of the block, and its partial, become NaN,
+    // whichever epilogue runs, so that every caller sees the failure.
+    if (tid == 0) {
+      mbar_wait_bounded(smem_u32(&bar));
+      atomicAdd(&g_stencil_timeouts, 1ull);
+    }
+    const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+    for (int d = 0; d < 4; d++) out[(unsigned)s + (unsigned)Ls * (site + v3 * (unsigned)d)] = mk(qnan, qnan);
+    if (EPI != 0 && tid == 0) partials[bid] = qnan;
+    __syncthreads();
+    return;
+  }
+
   const int q = (ts * TY + ys) * TX + xs;  // tile site
   constexpr int CD = NS * CW;              // centre: stride of the spin index
   const double2* cen = sm + CEN + q * CW + sl + 1;  // R(s) of spin 0 at this site
@@ -918,6 +948,16 @@ bool tile_on() {
   }();
   return on;
 }
+// THR_TILE_WAIT_TEST=1 (with THR_TILE=1) makes the staged-tile kernel expect 16 bytes more
+// than its copies bring, so that its bounded wait runs out with every copy already complete:
+// a test of the timeout path (NaN outputs, thr_stencil_timeouts) that faults nothing
+int tile_extra_tx() {
+  static const int extra = [] {
+    const char* e = std::getenv("THR_TILE_WAIT_TEST");
+    return e && e[0] == '1' && e[1] == 0 ? 16 : 0;
+  }();
+  return extra;
+}
 bool tile_ok(const Geom& g, int kernel) {
   return kernel == 0 && g.layout != LAYOUT_EO && g.lx % tile::TX == 0 && g.ly % tile::TY == 0 &&
          g.lt % tile::TT == 0 && g.ls % tile::SC == 0 && tile_on();
@@ -1073,7 +1113,7 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
       if (dev < 64) attr.fetch_or(1ull << dev);                                                              \
     }                                                                                                        \
     k_dslash_tile<D, E><<<grd, tile::NT, tile::SMEM, st>>>(o, i, maps, g, am, imass, am3, skip, ax, coef, partials, \
-                                                           rev);                                             \
+                                                           rev, tile_extra_tx());                            \
   } while (0)
 #define THR_TE(D)                 \
   do {                            \
@@ -1298,6 +1338,15 @@ THR_INST(__half2, float2)
 #undef THR_INST
 
 }  // namespace thr
+
+// Blocks of the staged-tile stencil whose copies did not arrive in time, on the context's device
+extern "C" int thr_stencil_timeouts(thr_ctx* c, unsigned long long* count) {
+  if (!c || !count) return THR_ERR_BADARG;
+  cudaSetDevice(c->dev);
+  return cudaMemcpyFromSymbol(count, thr::g_stencil_timeouts, sizeof(unsigned long long)) == cudaSuccess
+             ? THR_OK
+             : THR_ERR_CUDA;
+}
 
 // The autotuner's choices so far, one line each:
 //   <storage> <shamir|wilson|overlap> <M|Mdag> epi=<e> <lx>x<ly>x<lt> Ls=<ls> layout=<l> dev=<d> minb=<pick> us=<per candidate>

@@ -72,7 +72,17 @@ struct TableView {
   __device__ __forceinline__ float& operator[](int j) const { return base[(size_t)j * v3 + site]; }
 };
 
-__device__ __forceinline__ float rano_dev(Stream& st, TableView v) {
+// a site's table held in shared memory for the length of a draw: entry j of the block's
+// column `col` at base[j * kDrawThreads + col] (one bank per column, conflict-free)
+constexpr int kDrawThreads = 64;
+struct SmemTable {
+  float* base;
+  int col;
+  __device__ __forceinline__ float& operator[](int j) const { return base[j * kDrawThreads + col]; }
+};
+
+template <class View>
+__device__ __forceinline__ float rano_dev(Stream& st, View v) {
   if (st.idum < 0) {
     st.idum = 1;
     for (int j = 0; j < 97; j++) (void)rranf(st.S);
@@ -100,53 +110,86 @@ __global__ void k_rng_init(Stream* streams, float* tables, Geom g, uint64_t seed
   }
 }
 
-// one gauss0/gaussp call: ps[c][site], c = 0 (sin part), 1 (cos part)
-__global__ void k_gauss(Stream* streams, float* tables, Geom g, float scale, float* ps) {
-  for (int site = blockIdx.x * blockDim.x + threadIdx.x; site < g.v3; site += gridDim.x * blockDim.x) {
-    Stream st = streams[site];
-    TableView v{tables, g.v3, site};
-    const float u1 = rano_dev(st, v);
-    const float u2 = rano_dev(st, v);
-    float a, b;
-    box_muller(u1, u2, scale, a, b);
-    ps[site] = a;
-    ps[(size_t)g.v3 + site] = b;
-    streams[site] = st;
+// The draw kernels run a site's generator many steps in a row (4 Ls Gaussian pairs for the
+// pseudofermion): each step reads and writes one entry of the site's 97-entry shuffle table at
+// a random index.  One thread per site copies its table column into shared memory (coalesced:
+// the tables are [97][V3]), runs the chain there and copies it back, so the dependent table
+// accesses of the chain cost shared-memory latency instead of L2 latency; the arithmetic is
+// the same as from global memory, bit for bit.
+struct DrawSite {
+  float* tab;
+  int site;
+  bool live;
+  __device__ __forceinline__ DrawSite(float* shared_tab, const float* tables, int v3) {
+    tab = shared_tab;
+    site = blockIdx.x * kDrawThreads + threadIdx.x;
+    live = site < v3;
+    if (live)
+      for (int j = 0; j < 97; j++) tab[j * kDrawThreads + threadIdx.x] = tables[(size_t)j * v3 + site];
   }
+  __device__ __forceinline__ SmemTable view() const { return SmemTable{tab, (int)threadIdx.x}; }
+  __device__ __forceinline__ void store(float* tables, int v3) const {
+    for (int j = 0; j < 97; j++) tables[(size_t)j * v3 + site] = tab[j * kDrawThreads + threadIdx.x];
+  }
+};
+
+// one gauss0/gaussp call: ps[c][site], c = 0 (sin part), 1 (cos part)
+__global__ void __launch_bounds__(kDrawThreads) k_gauss(Stream* streams, float* tables, Geom g, float scale,
+                                                        float* ps) {
+  __shared__ float tab[97 * kDrawThreads];
+  const DrawSite ds(tab, tables, g.v3);
+  if (!ds.live) return;
+  const int site = ds.site;
+  Stream st = streams[site];
+  const SmemTable v = ds.view();
+  const float u1 = rano_dev(st, v);
+  const float u2 = rano_dev(st, v);
+  float a, b;
+  box_muller(u1, u2, scale, a, b);
+  ps[site] = a;
+  ps[(size_t)g.v3 + site] = b;
+  streams[site] = st;
+  ds.store(tables, g.v3);
 }
 
 // R(ithird,:,:,:,idirac) = cmplx(gauss0) for idirac = 1..4, ithird = 1..Ls
 // in that order (evolution.F90:40-51): 4*Ls gauss0 calls fused per site.
-__global__ void k_phi_draw(Stream* streams, float* tables, Geom g, double2* R) {
-  for (int site = blockIdx.x * blockDim.x + threadIdx.x; site < g.v3; site += gridDim.x * blockDim.x) {
-    Stream st = streams[site];
-    TableView v{tables, g.v3, site};
-    for (int d = 0; d < 4; d++)
-      for (int s = 0; s < g.ls; s++) {
-        const float u1 = rano_dev(st, v);
-        const float u2 = rano_dev(st, v);
-        float a, b;
-        box_muller(u1, u2, -1.0f, a, b);
-        R[sidx(g, s, site, d)] = make_double2((double)a, (double)b);
-      }
-    streams[site] = st;
-  }
-}
-
-// initialise_pp (evolution.F90:77-111): pp(:,:,:,mu) = sin part of gaussp, mu = 1..3
-__global__ void k_pp_draw(Stream* streams, float* tables, Geom g, float* pp) {
-  for (int site = blockIdx.x * blockDim.x + threadIdx.x; site < g.v3; site += gridDim.x * blockDim.x) {
-    Stream st = streams[site];
-    TableView v{tables, g.v3, site};
-    for (int mu = 0; mu < 3; mu++) {
+__global__ void __launch_bounds__(kDrawThreads) k_phi_draw(Stream* streams, float* tables, Geom g, double2* R) {
+  __shared__ float tab[97 * kDrawThreads];
+  const DrawSite ds(tab, tables, g.v3);
+  if (!ds.live) return;
+  const int site = ds.site;
+  Stream st = streams[site];
+  const SmemTable v = ds.view();
+  for (int d = 0; d < 4; d++)
+    for (int s = 0; s < g.ls; s++) {
       const float u1 = rano_dev(st, v);
       const float u2 = rano_dev(st, v);
       float a, b;
-      box_muller(u1, u2, -2.0f, a, b);
-      pp[(size_t)mu * g.v3 + site] = a;
+      box_muller(u1, u2, -1.0f, a, b);
+      R[sidx(g, s, site, d)] = make_double2((double)a, (double)b);
     }
-    streams[site] = st;
+  streams[site] = st;
+  ds.store(tables, g.v3);
+}
+
+// initialise_pp (evolution.F90:77-111): pp(:,:,:,mu) = sin part of gaussp, mu = 1..3
+__global__ void __launch_bounds__(kDrawThreads) k_pp_draw(Stream* streams, float* tables, Geom g, float* pp) {
+  __shared__ float tab[97 * kDrawThreads];
+  const DrawSite ds(tab, tables, g.v3);
+  if (!ds.live) return;
+  const int site = ds.site;
+  Stream st = streams[site];
+  const SmemTable v = ds.view();
+  for (int mu = 0; mu < 3; mu++) {
+    const float u1 = rano_dev(st, v);
+    const float u2 = rano_dev(st, v);
+    float a, b;
+    box_muller(u1, u2, -2.0f, a, b);
+    pp[(size_t)mu * g.v3 + site] = a;
   }
+  streams[site] = st;
+  ds.store(tables, g.v3);
 }
 
 // one rano draw from the stream of `site`, written to *out
@@ -157,6 +200,7 @@ __global__ void k_rano_one(Stream* streams, float* tables, Geom g, int site, flo
 }
 
 inline unsigned site_grid(int v3) { return (unsigned)((v3 + 127) / 128); }
+inline unsigned draw_grid(int v3) { return (unsigned)((v3 + kDrawThreads - 1) / kDrawThreads); }
 }  // namespace
 
 // ---------------------------------------------------------------- host side
@@ -210,7 +254,8 @@ int rng_gauss_dev(thr_ctx* c, float scale, float* ps) {
   Rng& r = c->rng;
   if (!r.ready) return THR_ERR_BADARG;
   if (r.site) {
-    k_gauss<<<site_grid(c->g.v3), 128, 0, c->st>>>((Stream*)r.dev_streams, (float*)r.dev_tables, c->g, scale, ps);
+    k_gauss<<<draw_grid(c->g.v3), kDrawThreads, 0, c->st>>>((Stream*)r.dev_streams, (float*)r.dev_tables, c->g,
+                                                             scale, ps);
     return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
   }
   // global stream: all first draws in Fortran site order, then all second draws (gaussian.F90:190-206)
@@ -239,7 +284,8 @@ int rng_phi_draw(thr_ctx* c, double2* R) {
   Rng& r = c->rng;
   if (!r.ready) return THR_ERR_BADARG;
   if (r.site) {
-    k_phi_draw<<<site_grid(c->g.v3), 128, 0, c->st>>>((Stream*)r.dev_streams, (float*)r.dev_tables, c->g, R);
+    k_phi_draw<<<draw_grid(c->g.v3), kDrawThreads, 0, c->st>>>((Stream*)r.dev_streams, (float*)r.dev_tables, c->g,
+                                                                R);
     return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
   }
   return THR_ERR_UNSUPPORTED;  // the global stream is drawn on the host by the caller
@@ -249,7 +295,8 @@ int rng_pp_draw(thr_ctx* c, float* pp) {
   Rng& r = c->rng;
   if (!r.ready) return THR_ERR_BADARG;
   if (r.site) {
-    k_pp_draw<<<site_grid(c->g.v3), 128, 0, c->st>>>((Stream*)r.dev_streams, (float*)r.dev_tables, c->g, pp);
+    k_pp_draw<<<draw_grid(c->g.v3), kDrawThreads, 0, c->st>>>((Stream*)r.dev_streams, (float*)r.dev_tables, c->g,
+                                                               pp);
     return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
   }
   return THR_ERR_UNSUPPORTED;

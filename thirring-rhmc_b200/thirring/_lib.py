@@ -104,6 +104,7 @@ SIGNATURES = {
     "thr_profile": (_i, [_v, _i, _i]),
     "thr_profile_read": (_i, [_v, _i, _pi, _pd, _pd, _pd]),
     "thr_tune_report": (_i, [C.c_char_p, _i]),
+    "thr_stencil_timeouts": (_i, [_v, C.POINTER(C.c_ulonglong)]),
     "thr_sync": (_i, [_v]),
     "thr_get_stream": (_i, [_v, C.POINTER(_v)]),
 }
