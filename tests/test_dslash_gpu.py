@@ -174,13 +174,17 @@ def test_tiled_stencil_matches_k_dslash(tmp_path):
             "X = np.zeros_like(R); it, _ = G.congrad(R, X, 1e-8, 0.05, 1);"
             "np.savez(d + '/out_' + t + '.npz', a=a, b=b, c=c, x=X, it=it); G.close()"
             % (pkg, str(tmp_path), dims))
-    for t in ("0", "1"):
+    for t in ("0", "1", "2"):
         subprocess.run([sys.executable, "-c", code, t], check=True, env=dict(os.environ, THR_TILE=t))
-    ref, got = np.load(tmp_path / "out_0.npz"), np.load(tmp_path / "out_1.npz")
+    ref, got, got2 = (np.load(tmp_path / ("out_%s.npz" % t)) for t in ("0", "1", "2"))
     for k in ("a", "b", "c"):
         assert rel_err(interior(got[k]), interior(ref[k])) <= 1e-15, k
     assert abs(int(got["it"]) - int(ref["it"])) <= 1
     assert rel_err(interior(got["x"]), interior(ref["x"])) <= 1e-7
+    # THR_TILE=2, the persistent double-buffered form: the same tiles, arithmetic and
+    # partial-sum order as THR_TILE=1, so the same bits
+    for k in ("a", "b", "c", "x", "it"):
+        assert np.array_equal(got2[k], got[k]), k
 
 
 def _dev_dslash(G, R, precision, am, imass, dag):
@@ -222,7 +226,8 @@ def test_dslash_fp32_storage(ls, imass):
 
 
 @pytest.mark.gpu
-def test_tile_wait_bound_reports_timeout(tmp_path):
+@pytest.mark.parametrize("mode", ["1", "2"])
+def test_tile_wait_bound_reports_timeout(tmp_path, mode):
     """The staged-tile stencil's bounded wait.  With THR_TILE_WAIT_TEST=1 every block expects
     16 bytes more than its copies bring, so its wait runs out although every copy has
     completed (nothing faults); each block then writes NaN to all its outputs and counts the
@@ -243,7 +248,7 @@ def test_tile_wait_bound_reports_timeout(tmp_path):
             "np.save(d + '/out_' + sys.argv[1] + '.npy', out); print('timeouts', n.value); G.close()"
             % (pkg, str(tmp_path), dims))
     res = {}
-    for tag, env in (("ok", {"THR_TILE": "1"}), ("bound", {"THR_TILE": "1", "THR_TILE_WAIT_TEST": "1"})):
+    for tag, env in (("ok", {"THR_TILE": mode}), ("bound", {"THR_TILE": mode, "THR_TILE_WAIT_TEST": "1"})):
         r = subprocess.run([sys.executable, "-c", code, tag], capture_output=True, text=True, timeout=300,
                            env=dict(os.environ, **env))
         assert r.returncode == 0, r.stdout + r.stderr

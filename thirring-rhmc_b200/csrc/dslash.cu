@@ -638,15 +638,16 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// polls the mbarrier's phase 0 until it completes or kWaitNs have passed; 1 if it completed
-__device__ __forceinline__ unsigned mbar_wait_bounded(unsigned bar) {
+// polls the mbarrier until the phase of the given parity completes or kWaitNs have passed;
+// 1 if it completed
+__device__ __forceinline__ unsigned mbar_wait_bounded(unsigned bar, unsigned parity = 0) {
   unsigned done = 0;
   const unsigned long long t0 = global_ns();
   for (unsigned k = 0; !done; k++) {
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(done)
-        : "r"(bar)
+        : "r"(bar), "r"(parity)
         : "memory");
     if (!done && (k & 63) == 63 && global_ns() - t0 > tile::kWaitNs) break;
   }
@@ -664,90 +665,42 @@ __device__ __forceinline__ void tma_load5(void* dst, const CUtensorMap* map, int
       : "memory");
 }
 
-template <bool DAG, int EPI>
-__global__ void __launch_bounds__(tile::NT, 4)
-    k_dslash_tile(double2* __restrict__ out, const double2* __restrict__ in, const __grid_constant__ tile::Maps maps,
-                  Geom g, float am, int imass, float am3, const int* skip, const double2* __restrict__ aux,
-                  const double* __restrict__ coef, double* __restrict__ partials, int rev, int extra_tx) {
+// thread 0 of a block: the 11 tensor copies of the tile at (x0, y0, t0, s0) into sm, all
+// completing on `bar` (expecting `bytes`)
+__device__ __forceinline__ void tile_issue(double2* sm, const tile::Maps& maps, unsigned long long* bar,
+                                           const Geom& g, int x0, int y0, int t0, int s0, int bytes) {
   using namespace tile;
-  if (skip && *skip) return;
-  // the dynamic region is allocated 128 bytes long and rounded up to a 128-byte
-  // boundary of the shared window, where TMA destinations must start
-  extern __shared__ __align__(16) double2 smraw[];
-  double2* const sm = smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u) / 16u;
-  __shared__ __align__(8) unsigned long long bar;
-  const int Lx = g.lx, Ly = g.ly, Lt = g.lt, Ls = g.ls;
-  const unsigned v3 = (unsigned)g.v3;
-  const int nch = Ls / SC;
-  // rev: blocks walk the tiles from the top (see k_dslash)
-  const int bid = rev ? (int)gridDim.x - 1 - (int)blockIdx.x : (int)blockIdx.x;
-  const int ch = bid % nch, ti = bid / nch;
-  const int ntx = Lx / TX, nty = Ly / TY;
-  const int x0 = (ti % ntx) * TX, y0 = ((ti / ntx) % nty) * TY, t0 = (ti / (ntx * nty)) * TT, s0 = ch * SC;
-  const int tid = threadIdx.x;
-  if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bar)) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  __syncthreads();
-  if (tid == 0) {
-    const int xm = x0 == 0 ? Lx - 1 : x0 - 1, xp = x0 + TX == Lx ? 0 : x0 + TX;
-    const int ym = y0 == 0 ? Ly - 1 : y0 - 1, yp = y0 + TY == Ly ? 0 : y0 + TY;
-    const int tm = t0 == 0 ? Lt - 1 : t0 - 1, tp = t0 + TT == Lt ? 0 : t0 + TT;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(&bar)),
-                 "r"(END * (int)sizeof(double2) + extra_tx)
-                 : "memory");
-    const int c0 = 2 * s0;  // fifth-dimension coordinate in doubles: 16-byte multiples
-    tma_load5(sm + CEN, &maps.cen, c0 - 2, x0, y0, t0, 0, &bar);
-    tma_load5(sm + XF, &maps.xf, c0, xm, y0, t0, 0, &bar);
-    tma_load5(sm + XF + 4 * XFD, &maps.xf, c0, xp, y0, t0, 0, &bar);
-    tma_load5(sm + YF, &maps.yf, c0, x0, ym, t0, 0, &bar);
-    tma_load5(sm + YF + 4 * YFD, &maps.yf, c0, x0, yp, t0, 0, &bar);
-    tma_load5(sm + TF, &maps.tf, c0, x0, y0, tm, 0, &bar);
-    tma_load5(sm + TF + 4 * TFD, &maps.tf, c0, x0, y0, tp, 0, &bar);
-    tma_load5(sm + UT, &maps.ut, 0, x0, y0, t0, 0, &bar);
-    tma_load5(sm + UX, &maps.ux, 0, xm, y0, t0, 0, &bar);
-    tma_load5(sm + UY, &maps.uy, 0, x0, ym, t0, 1, &bar);
-    tma_load5(sm + UTM, &maps.utm, 0, x0, y0, tm, 2, &bar);
-  }
-  // wall values for the s-neighbour slots outside the tensor: R(Ls-1) before s = 0
-  // (threads 0-127, one centre row each) and R(0) after s = Ls-1 (threads 128-255)
-  const int row = tid & 127;
-  const bool wall = tid < 128 ? ch == 0 : ch == nch - 1;
-  double2 wv = mk(0.0, 0.0);
-  if (wall) {
-    const unsigned wsite = (unsigned)(x0 + (row & 3) + Lx * (y0 + ((row >> 2) & 3) + Ly * (t0 + ((row >> 4) & 1))));
-    wv = in[(unsigned)(tid < 128 ? Ls - 1 : 0) + (unsigned)Ls * (wsite + v3 * (unsigned)(row >> 5))];
-  }
-  const unsigned done = mbar_wait_bounded(smem_u32(&bar));
-  if (wall) sm[CEN + row * CW + (tid < 128 ? 0 : CW - 1)] = wv;
-  const int sl = tid & 7, xs = (tid >> 3) & 3, ys = (tid >> 5) & 3, ts = tid >> 7;
-  const int s = s0 + sl;
-  const unsigned site = (unsigned)(x0 + xs + Lx * (y0 + ys + Ly * (t0 + ts)));
-  if (!__syncthreads_and(done)) {
-    // The copies did not all arrive within the bound.  One more bounded wait, so that no
-    // copy still writes this block's shared memory when the block exits (if that wait
-    // also runs out, the block exits anyway); the event is counted for the host
-    // (thr_stencil_timeouts) and every output of the block, and its partial, become NaN,
-    // whichever epilogue runs, so that every caller sees the failure.
-    if (tid == 0) {
-      mbar_wait_bounded(smem_u32(&bar));
-      atomicAdd(&g_stencil_timeouts, 1ull);
-    }
-    const double qnan = __longlong_as_double(0x7ff8000000000000LL);
-#pragma unroll
-    for (int d = 0; d < 4; d++) out[(unsigned)s + (unsigned)Ls * (site + v3 * (unsigned)d)] = mk(qnan, qnan);
-    if (EPI != 0 && tid == 0) partials[bid] = qnan;
-    __syncthreads();
-    return;
-  }
+  const int Lx = g.lx, Ly = g.ly, Lt = g.lt;
+  const int xm = x0 == 0 ? Lx - 1 : x0 - 1, xp = x0 + TX == Lx ? 0 : x0 + TX;
+  const int ym = y0 == 0 ? Ly - 1 : y0 - 1, yp = y0 + TY == Ly ? 0 : y0 + TY;
+  const int tm = t0 == 0 ? Lt - 1 : t0 - 1, tp = t0 + TT == Lt ? 0 : t0 + TT;
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  const int c0 = 2 * s0;  // fifth-dimension coordinate in doubles: 16-byte multiples
+  tma_load5(sm + CEN, &maps.cen, c0 - 2, x0, y0, t0, 0, bar);
+  tma_load5(sm + XF, &maps.xf, c0, xm, y0, t0, 0, bar);
+  tma_load5(sm + XF + 4 * XFD, &maps.xf, c0, xp, y0, t0, 0, bar);
+  tma_load5(sm + YF, &maps.yf, c0, x0, ym, t0, 0, bar);
+  tma_load5(sm + YF + 4 * YFD, &maps.yf, c0, x0, yp, t0, 0, bar);
+  tma_load5(sm + TF, &maps.tf, c0, x0, y0, tm, 0, bar);
+  tma_load5(sm + TF + 4 * TFD, &maps.tf, c0, x0, y0, tp, 0, bar);
+  tma_load5(sm + UT, &maps.ut, 0, x0, y0, t0, 0, bar);
+  tma_load5(sm + UX, &maps.ux, 0, xm, y0, t0, 0, bar);
+  tma_load5(sm + UY, &maps.uy, 0, x0, ym, t0, 1, bar);
+  tma_load5(sm + UTM, &maps.utm, 0, x0, y0, tm, 2, bar);
+}
 
+// shamir_site's arithmetic, operation for operation, for the thread's 5D site (s = s0 + sl
+// at tile position xs, ys, ts) with every operand from the staged tile sm
+template <bool DAG>
+__device__ __forceinline__ void tile_site(const double2* sm, int Ls, int s, int sl, int xs, int ys, int ts,
+                                          float am, int imass, float am3, double2* acc) {
+  using namespace tile;
   const int q = (ts * TY + ys) * TX + xs;  // tile site
   constexpr int CD = NS * CW;              // centre: stride of the spin index
   const double2* cen = sm + CEN + q * CW + sl + 1;  // R(s) of spin 0 at this site
-  const double om = (EPI == 1 || EPI == 3) ? *coef : 0.0;
   const double diag = (double)((3.0f - am3) + 1.0f);  // dirac.F90:45, default real
-  double2 rc[4], acc[4];
+  double2 rc[4];
 #pragma unroll
   for (int d = 0; d < 4; d++) {
     rc[d] = cen[d * CD];
@@ -802,6 +755,70 @@ __global__ void __launch_bounds__(tile::NT, 4)
       hop_projected<double2, double>(mu, (dir == 0) != DAG, W, r, acc);
     }
   }
+}
+
+template <bool DAG, int EPI>
+__global__ void __launch_bounds__(tile::NT, 4)
+    k_dslash_tile(double2* __restrict__ out, const double2* __restrict__ in, const __grid_constant__ tile::Maps maps,
+                  Geom g, float am, int imass, float am3, const int* skip, const double2* __restrict__ aux,
+                  const double* __restrict__ coef, double* __restrict__ partials, int rev, int extra_tx) {
+  using namespace tile;
+  if (skip && *skip) return;
+  // the dynamic region is allocated 128 bytes long and rounded up to a 128-byte
+  // boundary of the shared window, where TMA destinations must start
+  extern __shared__ __align__(16) double2 smraw[];
+  double2* const sm = smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u) / 16u;
+  __shared__ __align__(8) unsigned long long bar;
+  const int Lx = g.lx, Ly = g.ly, Lt = g.lt, Ls = g.ls;
+  const unsigned v3 = (unsigned)g.v3;
+  const int nch = Ls / SC;
+  // rev: blocks walk the tiles from the top (see k_dslash)
+  const int bid = rev ? (int)gridDim.x - 1 - (int)blockIdx.x : (int)blockIdx.x;
+  const int ch = bid % nch, ti = bid / nch;
+  const int ntx = Lx / TX, nty = Ly / TY;
+  const int x0 = (ti % ntx) * TX, y0 = ((ti / ntx) % nty) * TY, t0 = (ti / (ntx * nty)) * TT, s0 = ch * SC;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) tile_issue(sm, maps, &bar, g, x0, y0, t0, s0, END * (int)sizeof(double2) + extra_tx);
+  // wall values for the s-neighbour slots outside the tensor: R(Ls-1) before s = 0
+  // (threads 0-127, one centre row each) and R(0) after s = Ls-1 (threads 128-255)
+  const int row = tid & 127;
+  const bool wall = tid < 128 ? ch == 0 : ch == nch - 1;
+  double2 wv = mk(0.0, 0.0);
+  if (wall) {
+    const unsigned wsite = (unsigned)(x0 + (row & 3) + Lx * (y0 + ((row >> 2) & 3) + Ly * (t0 + ((row >> 4) & 1))));
+    wv = in[(unsigned)(tid < 128 ? Ls - 1 : 0) + (unsigned)Ls * (wsite + v3 * (unsigned)(row >> 5))];
+  }
+  const unsigned done = mbar_wait_bounded(smem_u32(&bar));
+  if (wall) sm[CEN + row * CW + (tid < 128 ? 0 : CW - 1)] = wv;
+  const int sl = tid & 7, xs = (tid >> 3) & 3, ys = (tid >> 5) & 3, ts = tid >> 7;
+  const int s = s0 + sl;
+  const unsigned site = (unsigned)(x0 + xs + Lx * (y0 + ys + Ly * (t0 + ts)));
+  if (!__syncthreads_and(done)) {
+    // The copies did not all arrive within the bound.  One more bounded wait, so that no
+    // copy still writes this block's shared memory when the block exits (if that wait
+    // also runs out, the block exits anyway); the event is counted for the host
+    // (thr_stencil_timeouts) and every output of the block, and its partial, become NaN,
+    // whichever epilogue runs, so that every caller sees the failure.
+    if (tid == 0) {
+      mbar_wait_bounded(smem_u32(&bar));
+      atomicAdd(&g_stencil_timeouts, 1ull);
+    }
+    const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+    for (int d = 0; d < 4; d++) out[(unsigned)s + (unsigned)Ls * (site + v3 * (unsigned)d)] = mk(qnan, qnan);
+    if (EPI != 0 && tid == 0) partials[bid] = qnan;
+    __syncthreads();
+    return;
+  }
+
+  const double om = (EPI == 1 || EPI == 3) ? *coef : 0.0;
+  double2 acc[4];
+  tile_site<DAG>(sm, Ls, s, sl, xs, ys, ts, am, imass, am3, acc);
   double racc = 0.0;
 #pragma unroll
   for (int d = 0; d < 4; d++) {
@@ -832,6 +849,149 @@ __global__ void __launch_bounds__(tile::NT, 4)
       for (int w = 0; w < NT / 32; w++) v += red[w];
       partials[bid] = v;
     }
+  }
+}
+
+// Persistent double-buffered form of the staged-tile stencil.  A block walks the tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ... with two tile buffers: while it computes tile k
+// from one, the copies of tile k + 1 land in the other, and the wall values and the
+// epilogue's operand are loaded before the wait, so copies, arithmetic and stores of a block
+// overlap (2 blocks of 2 x 54 KB per SM).  Tile numbering, arithmetic (tile_site), the
+// per-tile partial sums and their order are k_dslash_tile's, so the results are its bits.
+constexpr int kTile2PerSm = 2;
+constexpr int kTile2Buf = ((tile::END + 7) / 8) * 8;  // buffer stride in double2 (a 128-byte multiple)
+constexpr int kTile2Smem = 2 * kTile2Buf * (int)sizeof(double2) + 128;
+
+template <bool DAG, int EPI>
+__global__ void __launch_bounds__(tile::NT, kTile2PerSm)
+    k_dslash_tile2(double2* __restrict__ out, const double2* __restrict__ in, const __grid_constant__ tile::Maps maps,
+                   Geom g, float am, int imass, float am3, const int* skip, const double2* __restrict__ aux,
+                   const double* __restrict__ coef, double* __restrict__ partials, int rev, int extra_tx) {
+  using namespace tile;
+  if (skip && *skip) return;
+  extern __shared__ __align__(16) double2 smraw[];
+  double2* const smb = smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u) / 16u;
+  __shared__ __align__(8) unsigned long long bar[2];
+  __shared__ double red[NT / 32];
+  const int Lx = g.lx, Ly = g.ly, Ls = g.ls;
+  const unsigned v3 = (unsigned)g.v3;
+  const int nch = Ls / SC;
+  const int ntiles = (int)(v3 / (unsigned)NS) * nch;
+  const int ntx = Lx / TX, nty = Ly / TY;
+  const int tid = threadIdx.x;
+  const int bytes = END * (int)sizeof(double2) + extra_tx;
+  // tile -> its index in k_dslash_tile's numbering (rev: from the top) and its origin
+  auto origin = [&](int tl, int& bid, int& ch, int& x0, int& y0, int& t0, int& s0) {
+    bid = rev ? ntiles - 1 - tl : tl;
+    ch = bid % nch;
+    const int ti = bid / nch;
+    x0 = (ti % ntx) * TX;
+    y0 = ((ti / ntx) % nty) * TY;
+    t0 = (ti / (ntx * nty)) * TT;
+    s0 = ch * SC;
+  };
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bar[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bar[1])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  int tl = blockIdx.x;
+  if (tid == 0 && tl < ntiles) {
+    int b0_, c_, x_, y_, t_, s_;
+    origin(tl, b0_, c_, x_, y_, t_, s_);
+    tile_issue(smb, maps, &bar[0], g, x_, y_, t_, s_, bytes);
+  }
+  const double om = (EPI == 1 || EPI == 3) ? *coef : 0.0;
+  const int sl = tid & 7, xs = (tid >> 3) & 3, ys = (tid >> 5) & 3, ts = tid >> 7;
+  const int row = tid & 127;
+  for (int k = 0; tl < ntiles; k++, tl += gridDim.x) {
+    const int b = k & 1;
+    double2* const sm = smb + b * kTile2Buf;
+    int bid, ch, x0, y0, t0, s0;
+    origin(tl, bid, ch, x0, y0, t0, s0);
+    const int next = tl + (int)gridDim.x;
+    if (tid == 0 && next < ntiles) {
+      // the other buffer was last read in iteration k - 1, which ended in a barrier: order
+      // those accesses before the copies that overwrite it
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      int nb, nc, nx0, ny0, nt0, ns0;
+      origin(next, nb, nc, nx0, ny0, nt0, ns0);
+      tile_issue(smb + (b ^ 1) * kTile2Buf, maps, &bar[b ^ 1], g, nx0, ny0, nt0, ns0, bytes);
+    }
+    const int s = s0 + sl;
+    const unsigned site = (unsigned)(x0 + xs + Lx * (y0 + ys + Ly * (t0 + ts)));
+    // the wall values (R(Ls-1) before s = 0, R(0) after s = Ls-1) and the epilogue's operand,
+    // loaded while this tile's copies may still be in flight
+    const bool wall = tid < 128 ? ch == 0 : ch == nch - 1;
+    double2 wv = mk(0.0, 0.0);
+    if (wall) {
+      const unsigned wsite =
+          (unsigned)(x0 + (row & 3) + Lx * (y0 + ((row >> 2) & 3) + Ly * (t0 + ((row >> 4) & 1))));
+      wv = in[(unsigned)(tid < 128 ? Ls - 1 : 0) + (unsigned)Ls * (wsite + v3 * (unsigned)(row >> 5))];
+    }
+    double2 av[4];
+#pragma unroll
+    for (int d = 0; d < 4; d++)
+      av[d] = (EPI == 1 || EPI == 3) ? aux[(unsigned)s + (unsigned)Ls * (site + v3 * (unsigned)d)] : mk(0.0, 0.0);
+    const unsigned done = mbar_wait_bounded(smem_u32(&bar[b]), (unsigned)(k >> 1) & 1u);
+    if (wall) sm[CEN + row * CW + (tid < 128 ? 0 : CW - 1)] = wv;
+    if (!__syncthreads_and(done)) {
+      // The copies did not all arrive within the bound.  Bounded waits for this tile's and
+      // the next tile's copies, so that none still lands in shared memory when the block
+      // exits (if they run out too, the block exits anyway); the event is counted for the
+      // host (thr_stencil_timeouts), and this and every later tile of the block get NaN
+      // outputs and partials, whichever epilogue runs.
+      if (tid == 0) {
+        if (next < ntiles) mbar_wait_bounded(smem_u32(&bar[b ^ 1]), (unsigned)((k + 1) >> 1) & 1u);
+        mbar_wait_bounded(smem_u32(&bar[b]), (unsigned)(k >> 1) & 1u);
+        atomicAdd(&g_stencil_timeouts, 1ull);
+      }
+      const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+      for (int t2 = tl; t2 < ntiles; t2 += gridDim.x) {
+        int b2, c2, x2, y2, tt2, s2;
+        origin(t2, b2, c2, x2, y2, tt2, s2);
+        const unsigned st2 = (unsigned)(x2 + xs + Lx * (y2 + ys + Ly * (tt2 + ts)));
+#pragma unroll
+        for (int d = 0; d < 4; d++) out[(unsigned)(s2 + sl) + (unsigned)Ls * (st2 + v3 * (unsigned)d)] = mk(qnan, qnan);
+        if (EPI != 0 && tid == 0) partials[b2] = qnan;
+      }
+      __syncthreads();
+      return;
+    }
+    double2 acc[4];
+    tile_site<DAG>(sm, Ls, s, sl, xs, ys, ts, am, imass, am3, acc);
+    double racc = 0.0;
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+      const unsigned i = (unsigned)s + (unsigned)Ls * (site + v3 * (unsigned)d);
+      if (EPI == 1) {
+        const double2 rn = av[d] + om * acc[d];  // r = r + omega*s (multishift_module.F90:137)
+        out[i] = rn;
+        racc += epi_norm<double2>(rn);
+      } else if (EPI == 3) {
+        const double2 hn = acc[d] + om * av[d];  // h = M r + gamma h (= M p by linearity)
+        out[i] = hn;
+        racc += epi_norm<double2>(hn);
+      } else {
+        out[i] = acc[d];
+        if (EPI == 2) racc += epi_norm<double2>(acc[d]);
+      }
+    }
+    if (EPI != 0) {
+      // one FP64 partial per tile, the order of k_dslash_tile: warp sums, then the 8 warps in turn
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) racc += __shfl_down_sync(0xffffffffu, racc, o);
+      if ((tid & 31) == 0) red[tid >> 5] = racc;
+      __syncthreads();
+      if (tid == 0) {
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < NT / 32; w++) v += red[w];
+        partials[bid] = v;
+      }
+    }
+    __syncthreads();  // this buffer and red[] are free for the next iteration
   }
 }
 
@@ -941,13 +1101,15 @@ bool stencil_shfl(const Geom& g, int kernel) { return kernel == 0 && g.ls <= 32 
 // kernel where the lattice allows it.  It is off by default: on B200 it measured
 // 51-54 us per launch in the 32^2x32, Ls 32 multishift solve against k_dslash's
 // 48-50 us, and 162 us against 156-159 us at 48^2x48, Ls 48.
-bool tile_on() {
-  static const bool on = [] {
+// THR_TILE: 1 the staged-tile kernel, 2 its persistent double-buffered form
+int tile_mode() {
+  static const int mode = [] {
     const char* e = std::getenv("THR_TILE");
-    return e && e[0] == '1' && e[1] == 0;
+    return (e && (e[0] == '1' || e[0] == '2') && e[1] == 0) ? e[0] - '0' : 0;
   }();
-  return on;
+  return mode;
 }
+bool tile_on() { return tile_mode() != 0; }
 // THR_TILE_WAIT_TEST=1 (with THR_TILE=1) makes the staged-tile kernel expect 16 bytes more
 // than its copies bring, so that its bounded wait runs out with every copy already complete:
 // a test of the timeout path (NaN outputs, thr_stencil_timeouts) that faults nothing
@@ -1100,6 +1262,7 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
     const double2* i = reinterpret_cast<const double2*>(in);
     const double2* ax = reinterpret_cast<const double2*>(aux);
     const unsigned grd = tile_grid(g);
+    const unsigned grd2 = std::min(grd, (unsigned)(kTile2PerSm * device_sms()));
     tile::Maps maps;
     if (!tile_maps(g, i, reinterpret_cast<const double2*>(u), &maps)) return THR_ERR_CUDA;
     int dev = 0;
@@ -1110,10 +1273,16 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
     if (dev >= 64 || !(attr.load() >> dev & 1ull)) {                                                         \
       cudaFuncSetAttribute(k_dslash_tile<D, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, tile::SMEM);    \
       cudaFuncSetAttribute(k_dslash_tile<D, E>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);        \
+      cudaFuncSetAttribute(k_dslash_tile2<D, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTile2Smem);   \
+      cudaFuncSetAttribute(k_dslash_tile2<D, E>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);       \
       if (dev < 64) attr.fetch_or(1ull << dev);                                                              \
     }                                                                                                        \
-    k_dslash_tile<D, E><<<grd, tile::NT, tile::SMEM, st>>>(o, i, maps, g, am, imass, am3, skip, ax, coef, partials, \
-                                                           rev, tile_extra_tx());                            \
+    if (tile_mode() == 2)                                                                                    \
+      k_dslash_tile2<D, E><<<grd2, tile::NT, kTile2Smem, st>>>(o, i, maps, g, am, imass, am3, skip, ax, coef, \
+                                                               partials, rev, tile_extra_tx());              \
+    else                                                                                                     \
+      k_dslash_tile<D, E><<<grd, tile::NT, tile::SMEM, st>>>(o, i, maps, g, am, imass, am3, skip, ax, coef,   \
+                                                             partials, rev, tile_extra_tx());                \
   } while (0)
 #define THR_TE(D)                 \
   do {                            \
