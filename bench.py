@@ -834,40 +834,39 @@ def run_trajectory(args):
 
 
 def run_trajectory48(args):
-    """A sample of the config-5 run: 48^2 x 48, Ls = 48, beta 0.28, am 0.005,
-    imass 3, dt 0.02, remez2/remez4 (25 poles) for the action and remez2g/4g
-    (12 poles) for the guidance force, FP32 guidance solves (spmd), acceptance
-    residual 1e-9.  Two trajectories of 1 and 2 fixed MD steps give the cost of
-    one MD step and the fixed cost per trajectory (pseudofermion and momentum
-    refresh, the two Hamiltonians); the 50-step trajectory time is extrapolated
-    from them and labelled so."""
+    """Config 5, one sample trajectory: 48^2 x 48, Ls = 48, beta 0.28, am 0.005, imass 3,
+    50 fixed MD steps of dt 0.02 (--traj-steps), remez2/remez4 (25 poles) for the action
+    and remez2g/remez4g (12 poles) for the guidance force; the reference's single-precision
+    guidance solves (spmd) at rescgg 1e-6, the Hamiltonian and pseudofermion solves at
+    rescga 1e-9 with the mixed multishift; each MD step after the first replayed as one
+    CUDA graph; Gaussian theta, site streams.  One trajectory, not the 20 of the config:
+    a full one takes about a quarter of an hour on one GPU.  Its Delta H cannot be compared
+    with the oracle here (the oracle would take days at this size); config 1 carries that
+    comparison."""
     import thirring
     gold = os.path.join(REPO, "tests", "golden") + os.sep
     rat = thirring.remez_set(gold + "remez2", gold + "remez4", 25)
     ratg = thirring.remez_set(gold + "remez2g", gold + "remez4g", 12)
     lx, ls, beta, am, dt = 48, 48, 0.28, 0.005, 0.02
+    nstep = args.traj_steps
     G = thirring.Lattice(lx, lx, lx, ls, beta=beta)
     G.set_remez(rat, ratg)
     G.set_residuals(1e-9, 1e-6, 1)
+    G.set_action_precision(thirring.MIXED_FP32)
     G.init_random(4139764973254.0)
     rng = np.random.default_rng(5)
     th = np.asfortranarray(rng.standard_normal((lx, lx, lx, 3)) / np.sqrt(beta), np.float32)
-    times, res = [], []
-    for nsteps in (1, 2):
-        G.md_counters(reset=True)
+    G.md_counters(reset=True)
+    with Clocks(0) as clk:
         t0 = time.perf_counter()
-        r = G.trajectory(th, 50, dt, am, 3, fixed_steps=nsteps)
-        times.append(time.perf_counter() - t0)
-        res.append({"md_steps": nsteps, "s": round(times[-1], 2), "dH": r.dh, "accepted": r.accepted,
-                    "iterations": {k: v for k, v in G.md_counters().items() if v}})
-    step = times[1] - times[0]
-    fixed = times[0] - step
-    t50 = fixed + 50 * step
+        r = G.trajectory(th, nstep, dt, am, 3, fixed_steps=nstep)
+        t = time.perf_counter() - t0
+    its = {k: v for k, v in G.md_counters().items() if v}
     G.close()
-    return {"workload": "RHMC 48^2x48 Ls48 (config 5 shape), beta 0.28, am 0.005, dt 0.02; trajectories of 1 and 2 "
-                        "fixed MD steps", "results": res, "s_per_md_step": round(step, 3),
-            "s_fixed_per_traj": round(fixed, 2), "extrapolated_50_step_traj_s": round(t50, 1),
-            "extrapolated_traj_per_hr": round(3600 / t50, 2)}
+    return {"workload": "config 5 sample: one RHMC trajectory, 48^2x48 Ls48, beta 0.28, am 0.005, imass 3, "
+                        "%d MD steps dt %g, spmd guidance, mixed action solves, MD steps as CUDA graphs" % (nstep, dt),
+            "s_per_traj": round(t, 1), "traj_per_hr": round(3600 / t, 2), "dH": r.dh, "accepted": r.accepted,
+            "steps": r.steps, "iterations": its, "clocks": clk.summary(), "sample": "1 trajectory"}
 
 
 def main():
@@ -892,6 +891,7 @@ def main():
     ap.add_argument("--max-iters", type=int, default=0,
                     help="profiling case: stop every solve after this many iterations (not a full solve)")
     ap.add_argument("--no-dslash", action="store_true")
+    ap.add_argument("--traj-steps", type=int, default=50, help="trajectory48: MD steps of the sample trajectory")
     ap.add_argument("--sweep-l", default="", help="dslash_sweep: comma-separated lattice extents")
     ap.add_argument("--sweep-ls", default="", help="dslash_sweep: comma-separated fifth-dimension extents")
     ap.add_argument("--no-compare-plain", dest="compare_plain", action="store_false",
@@ -985,6 +985,9 @@ def main():
     traffic = ncu_traffic(name, k["algorithmic_bytes_per_launch"])
     roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": traffic,
+                "traffic_source": ("not measured in this run: dram__bytes_read.sum + dram__bytes_write.sum per launch "
+                                   "from the ncu capture summarised in profiles/ (profiles/roofline_traffic.txt)"
+                                   if traffic is not None else None),
                 "algorithmic_bytes_per_launch": k["algorithmic_bytes_per_launch"],
                 "us_per_launch": k["us_per_launch"], "launches": k["launches"], "sampled_launches": k["sampled"],
                 "share_of_step": k["share_of_step"]}

@@ -165,6 +165,8 @@ int thr_create(const thr_params* p, thr_ctx** out) {
     if (e && e[0] == '0') c->use_graphs = false;
     e = std::getenv("THR_MD_GRAPH");
     if (e && e[0] == '0') c->use_md_graph = false;
+    e = std::getenv("THR_PDL");
+    if (e && e[0] == '0') c->use_pdl = false;
   }
   int rc = THR_OK;
   if (cudaSetDevice(c->dev) != cudaSuccess) rc = THR_ERR_CUDA;

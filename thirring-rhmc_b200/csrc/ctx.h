@@ -89,6 +89,7 @@ struct thr_ctx {
   int max_qmr_iters = 50000;
   int ms_algo = 1;          // multishift: 0 = per-iteration shift updates, 1 = batched
   bool use_graphs = true;   // batched solver loops as one CUDA graph (WHILE node) per solve
+  bool use_pdl = true;      // the batched multishift's kernel chain as dependent launches (THR_PDL=0: off)
   // cached batched-multishift graphs: FP64; FP32 vectors; FP32 and BF16 base
   // iteration with FP64 shift fields (the low-precision phase of the mixed solver)
   void* ms_graphs[4] = {};

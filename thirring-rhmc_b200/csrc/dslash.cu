@@ -411,6 +411,8 @@ __global__ void __launch_bounds__(NT, MINB)
     k_dslash(S* __restrict__ out, const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u, Geom g, float am,
              int imass, float am3, const int* skip, const S* __restrict__ aux, const double* __restrict__ coef,
              double* __restrict__ partials, int rev) {
+  pdl_wait();
+  pdl_trigger();
   if (skip && *skip) return;
   using C = typename Sto<S>::C;
   using R = typename Sto<S>::R;
@@ -494,6 +496,8 @@ __global__ void __launch_bounds__(64, MINB)
     k_dslash_pair(C* __restrict__ out, const C* __restrict__ in, const C* __restrict__ u, Geom g, float am,
                   int imass, float am3, const int* skip, const C* __restrict__ aux, const double* __restrict__ coef,
                   double* __restrict__ partials, int rev) {
+  pdl_wait();
+  pdl_trigger();
   if (skip && *skip) return;
   using R = typename Sto<C>::R;
   const R om = (EPI == 1 || EPI == 3) ? (R)(*coef) : R(0);
@@ -1253,7 +1257,7 @@ int tune_lookup(const TuneKey& key, const int* cand) {
 template <class S>
 int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u, float am,
                        int imass, float am3, cudaStream_t st, const int* skip, const S* aux, const double* coef,
-                       double* partials, int e, int rev, bool may_tune = true) {
+                       double* partials, int e, int rev, bool may_tune = true, bool pdl = false) {
   if (g.ls > 1024) return THR_ERR_BADSHAPE;
   if (4ULL * (unsigned long long)g.v5 >= (1ULL << 32)) return THR_ERR_BADSHAPE;  // 32-bit element offsets
   if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;  // dwf3d_lib.F90:152-158
@@ -1301,8 +1305,9 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   const dim3 grd(stencil_grid(g, kernel));
   const int nt = stencil_threads(g, kernel);
   const bool shfl = stencil_shfl(g, kernel);
-#define THR_L(K, D, E, N, SH, MB) \
-  k_dslash<S, K, D, E, N, SH, MB><<<grd, blk, 0, st>>>(out, in, u, g, am, imass, am3, skip, aux, coef, partials, rev)
+#define THR_L(K, D, E, N, SH, MB)                                                                           \
+  launch_k(k_dslash<S, K, D, E, N, SH, MB>, grd, blk, 0, st, pdl, out, in, u, g, am, imass, am3, skip, aux, coef, \
+           partials, rev)
 #define THR_E(K, D, N, SH, MB)                 \
   do {                                         \
     if (e == 1) THR_L(K, D, 1, N, SH, MB);     \
@@ -1328,8 +1333,9 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
       float2* out2 = reinterpret_cast<float2*>(out);
       const float2* aux2 = reinterpret_cast<const float2*>(aux);
       const float2* u2 = reinterpret_cast<const float2*>(u);
-#define THR_P(D, E, MB) \
-  k_dslash_pair<float2, D, E, MB><<<grd, pblk, 0, st>>>(out2, in2, u2, g, am, imass, am3, skip, aux2, coef, partials, rev)
+#define THR_P(D, E, MB)                                                                                     \
+  launch_k(k_dslash_pair<float2, D, E, MB>, grd, pblk, 0, st, pdl, out2, in2, u2, g, am, imass, am3, skip, aux2, \
+           coef, partials, rev)
 #define THR_PE(D, MB)                    \
   do {                                   \
     if (e == 1) THR_P(D, 1, MB);         \
@@ -1388,15 +1394,17 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
 template <class S>
 int launch_dslash_axpy(const Geom& g, int kernel, bool dag, S* rnew, const S* in, const typename Sto<S>::C* u,
                        float am, int imass, float am3, cudaStream_t st, const int* skip, const S* rold,
-                       const double* coef, double* partials, int rev) {
-  return launch_dslash_mode<S>(g, kernel, dag, rnew, in, u, am, imass, am3, st, skip, rold, coef, partials, 1, rev);
+                       const double* coef, double* partials, int rev, bool pdl) {
+  return launch_dslash_mode<S>(g, kernel, dag, rnew, in, u, am, imass, am3, st, skip, rold, coef, partials, 1, rev,
+                               true, pdl);
 }
 
 template <class S>
 int launch_dslash_accum(const Geom& g, int kernel, bool dag, S* hnew, const S* in, const typename Sto<S>::C* u,
                         float am, int imass, float am3, cudaStream_t st, const int* skip, const S* hold,
-                        const double* coef, double* partials, int rev) {
-  return launch_dslash_mode<S>(g, kernel, dag, hnew, in, u, am, imass, am3, st, skip, hold, coef, partials, 3, rev);
+                        const double* coef, double* partials, int rev, bool pdl) {
+  return launch_dslash_mode<S>(g, kernel, dag, hnew, in, u, am, imass, am3, st, skip, hold, coef, partials, 3, rev,
+                               true, pdl);
 }
 
 template <class S>
@@ -1493,11 +1501,11 @@ int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const
   template int launch_dslash_untuned<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,        \
                                         cudaStream_t, const int*);                                                \
   template int launch_dslash_axpy<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
-                                     cudaStream_t, const int*, const S*, const double*, double*, int);            \
+                                     cudaStream_t, const int*, const S*, const double*, double*, int, bool);      \
   template int launch_dslash_norm<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
                                      cudaStream_t, const int*, double*, int);                                     \
   template int launch_dslash_accum<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,          \
-                                      cudaStream_t, const int*, const S*, const double*, double*, int);           \
+                                      cudaStream_t, const int*, const S*, const double*, double*, int, bool);     \
   template int launch_dslash_batch<S>(const BatchTable&, int, bool, S*, const S*, const L*, float, int, float,    \
                                       cudaStream_t, const int*, const S*, double*, int);
 THR_INST(double2, double2)

@@ -66,6 +66,8 @@ __global__ void k_init(MsState* ms, MsHist* hist, const double* partials, int np
 
 // :104, :118-135, recording the step's omegas / zeta_iii / window
 __global__ void k_alpha(MsState* ms, MsHist* hist, const double* partials, int np) {
+  pdl_wait();
+  pdl_trigger();
   if (ms->done) return;
   const double alpha = block_sum_partials(partials, np);
   if (threadIdx.x == 0) {
@@ -87,6 +89,8 @@ __global__ void k_alpha(MsState* ms, MsHist* hist, const double* partials, int n
 // delta) with one thread per shift: ms_converge_step's statements, the window's
 // new bounds from a shared-memory min / max (blockDim.x >= kMaxShift)
 __global__ void k_lambda(MsState* ms, MsHist* hist, const double* partials, int np) {
+  pdl_wait();
+  pdl_trigger();
   if (ms->done) return;
   __shared__ int s_lo, s_hi;
   const double lambda = block_sum_partials(partials, np);
@@ -326,6 +330,7 @@ int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO
   const typename Sto<V>::C* u =
       fp64 ? (const typename Sto<V>::C*)(const void*)c->u64 : (const typename Sto<V>::C*)(const void*)c->u32;
   const double lb = fp64 ? sizeof(double2) : sizeof(float2);
+  const bool pdl = c->use_pdl && !prof;  // sampled launches keep their events between kernels
   // the previous batch's flush, forked onto the side stream (c->overlap_flush 0: in line;
   // also in line while kernel timings are sampled, so that each sampled duration is
   // that kernel's alone and not one shared with a concurrent flush)
@@ -354,17 +359,19 @@ int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO
     V* hcur = (j & 1) ? p : hv;
     const V* hprev = (j & 1) ? hv : p;
     // alpha = Re<p, M^dagger M p> (:104) evaluated as |h|^2 = |M p|^2 in the M epilogue
+    // each kernel of the chain is a dependent launch of the one before (not across a sampled
+    // launch's events, nor for the batch's first, which follows the flush fork)
     int pe = prof ? c->prof_begin(fp64 ? thr_ctx::P_DSLASH : thr_ctx::P_DSLASH_LOW, b_md, k0 + j) : -1;
     THR_TRY(launch_dslash_accum<V>(c->g, c->p.kernel, false, hcur, rold, u, am, imass, c->p.am3, main, &ms->done,
-                                   hprev, &ms->gammag, c->partials, 0));
+                                   hprev, &ms->gammag, c->partials, 0, pdl && j > 0));
     c->prof_end(pe);
-    k_alpha<<<1, 1024, 0, main>>>(ms, rec, c->partials, gs);
+    launch_k(k_alpha, dim3(1), dim3(1024), 0, main, pdl, ms, rec, c->partials, (int)gs);
     // s = M^dagger h is never stored: the epilogue forms r = r + omega*s (:137) and |r|^2 (:138)
     pe = prof ? c->prof_begin(fp64 ? thr_ctx::P_DSLASH_DAG : thr_ctx::P_DSLASH_DAG_LOW, b_md, k0 + j) : -1;
     THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, rnew, hcur, u, am, imass, c->p.am3, main, &ms->done,
-                                  rold, &ms->omega, c->partials, rev_md));
+                                  rold, &ms->omega, c->partials, rev_md, pdl));
     c->prof_end(pe);
-    k_lambda<<<1, 1024, 0, main>>>(ms, rec, c->partials, gs);
+    launch_k(k_lambda, dim3(1), dim3(1024), 0, main, pdl, ms, rec, c->partials, (int)gs);
   }
   (void)s;
   if (fork) THR_CUDA(cudaStreamWaitEvent(main, c->ev_join[half], 0));
@@ -399,8 +406,25 @@ template <class V, class VO> constexpr int graph_slot() {
 }
 
 template <class V, class VO = V>
+int ms_graph_build(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO* sf, V* ring, V* p, V* hv, V* s,
+                   float am, int imass, cudaGraphExec_t* exec_out);
+
+// the cached graph, built if needed; a build with dependent launches that the driver
+// rejects is retried without them (they are then off for the context)
+template <class V, class VO = V>
 int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO* sf, V* ring, V* p, V* hv, V* s, float am,
              int imass, cudaGraphExec_t* exec_out) {
+  int rc = ms_graph_build<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, exec_out);
+  if (rc != THR_OK && c->use_pdl) {
+    c->use_pdl = false;
+    rc = ms_graph_build<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, exec_out);
+  }
+  return rc;
+}
+
+template <class V, class VO>
+int ms_graph_build(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO* sf, V* ring, V* p, V* hv, V* s,
+                   float am, int imass, cudaGraphExec_t* exec_out) {
   const int slot = graph_slot<V, VO>();
   if (!c->ms_graphs[slot]) c->ms_graphs[slot] = new MsGraph();
   MsGraph& G = *static_cast<MsGraph*>(c->ms_graphs[slot]);

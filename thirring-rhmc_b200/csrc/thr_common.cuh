@@ -212,4 +212,13 @@ __device__ __forceinline__ C gp(GammaEntry e, C z) {
   return e.im > 0 ? mk(-z.y, z.x) : mk(z.y, -z.x);
 }
 
+// ---------------------------------------------------------------- dependent launch
+// A kernel that the host launched as a programmatic dependent of the previous kernel on its
+// stream may start before that kernel has finished: pdl_wait() blocks until it has finished
+// and its writes are visible (a no-op for an ordinary launch), and pdl_trigger() lets this
+// kernel's own dependent be launched now.  Every such kernel calls pdl_wait() before it
+// touches memory its predecessor writes.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 }  // namespace thr

@@ -1,12 +1,37 @@
 // thr_kernels.h -- launchers shared between the translation units of the
 // CUDA library.  Host-callable, stream-ordered, no allocation.
 #pragma once
+#include <utility>
+
 #include "thr_common.cuh"
 
 namespace thr {
 
 // number of per-block partial sums a reduction may write (>= any grid used)
 constexpr int kMaxPartials = 4096;
+
+// Launches kern<<<grid, block, smem, st>>>(args...); with pdl as a programmatic dependent of
+// the previous kernel on st (the kernel must call pdl_wait() before it reads that kernel's
+// results), so that its launch and scheduling overlap the predecessor's tail.
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, bool pdl,
+                     Args&&... args) {
+  if (!pdl) {
+    kern<<<grid, block, smem, st>>>(std::forward<Args>(args)...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 // streaming multiprocessors of the current device (looked up once per device);
 // grid-stride kernels size their grids as a multiple of it
@@ -33,7 +58,7 @@ int launch_dslash_untuned(const Geom& g, int kernel, bool dag, S* out, const S* 
 template <class S>
 int launch_dslash_axpy(const Geom& g, int kernel, bool dag, S* rnew, const S* in, const typename Sto<S>::C* u,
                        float am, int imass, float am3, cudaStream_t st, const int* skip, const S* rold,
-                       const double* coef, double* partials, int rev = 0);
+                       const double* coef, double* partials, int rev = 0, bool pdl = false);
 // same, with one FP64 partial per block of sum |out|^2
 template <class S>
 int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
@@ -49,7 +74,7 @@ int launch_odslash(const Geom& g, bool dag, double2* out, const double2* in, con
 template <class S>
 int launch_dslash_accum(const Geom& g, int kernel, bool dag, S* hnew, const S* in, const typename Sto<S>::C* u,
                         float am, int imass, float am3, cudaStream_t st, const int* skip, const S* hold,
-                        const double* coef, double* partials, int rev = 0);
+                        const double* coef, double* partials, int rev = 0, bool pdl = false);
 
 // layout.cu: Fortran halo'd host layout <-> device fields
 // spinor (0:Ls+1,0:Lx+1,0:Ly+1,0:Lt+1,4) complex(dp)  <-> S[4][V3][Ls]
