@@ -250,12 +250,13 @@ def test_congrad_graph_equals_host_launched():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("env", [{"THR_OVERLAP": "0"}, {"THR_REVERSE": "1"}, {"THR_REVERSE": "0"},
-                                 {"THR_GRAPHS": "0"}])
+                                 {"THR_GRAPHS": "0"}, {"THR_PDL": "0"}])
 def test_solver_schedules_bit_identical(tmp_path, env):
     """Where the batched multishift's flush runs (side stream or in line), which
-    way the solver kernels sweep the sites, and whether the loops are graphs or
-    host-launched change the schedule only: the multishift (FP64 and FP32
-    vectors) and congrad give the same bits and iteration counts."""
+    way the solver kernels sweep the sites, whether the loops are graphs or
+    host-launched, and whether the kernel chain uses dependent launches change the
+    schedule only: the multishift (FP64 and FP32 vectors) and congrad give the same
+    bits and iteration counts."""
     import os
     import subprocess
     import sys
