@@ -43,7 +43,9 @@ enum thr_status {
   THR_ERR_NAN = 4,         /* non-finite residual                            */
   THR_ERR_CUDA = 5,        /* CUDA runtime error                             */
   THR_ERR_NOMEM = 6,       /* device allocation failed                       */
-  THR_ERR_UNSUPPORTED = 7  /* e.g. imass = 5 with the Wilson kernel          */
+  THR_ERR_UNSUPPORTED = 7, /* e.g. imass = 5 with the Wilson kernel          */
+  THR_ERR_TIMEOUT = 8      /* a device-side wait gave up (a grid barrier of
+                              the persistent multishift kernel)              */
 };
 
 enum thr_kernel { THR_SHAMIR = 0, THR_WILSON = 1 };

@@ -150,6 +150,43 @@ def test_register_budgets_bit_identical(tmp_path, kernel, force):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("dims,layout", [((8, 6, 4, 16), 0), ((6, 6, 4, 12), 1), ((4, 4, 6, 8), 0)])
+def test_split_stencil_bit_identical(tmp_path, dims, layout):
+    """The four-threads-per-site FP64 Shamir kernel (autotuner candidate 40, forced by
+    THR_TUNE=40) against the one-thread kernel (THR_TUNE=8): the same bits for M and
+    M^dagger, every fused epilogue (residual update, h recurrence, with |out|^2), congrad
+    and the batched multishift, with the warp-shuffle fifth dimension (Ls 16, 8) and
+    without (Ls 12, even-odd order)."""
+    import os
+    import subprocess
+    import sys
+    rng = np.random.default_rng(17)
+    L = O.lat(*dims)
+    np.save(tmp_path / "R.npy", rand_spinor(L, rng))
+    np.save(tmp_path / "A.npy", rand_spinor(L, rng))
+    np.save(tmp_path / "u.npy", rand_links(L, rng))
+    an, ad, _, _ = O.read_remez(os.path.join(os.path.dirname(__file__), "golden", "remez4g"), 12)
+    np.save(tmp_path / "an.npy", an)
+    np.save(tmp_path / "ad.npy", ad)
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "thirring-rhmc_b200")
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import thirring; d = %r; t = sys.argv[1];"
+            "ld = lambda k: np.asfortranarray(np.load(d + '/' + k + '.npy'));"
+            "R, A, u, an, ad = ld('R'), ld('A'), ld('u'), np.load(d + '/an.npy'), np.load(d + '/ad.npy');"
+            "G = thirring.Lattice(*%r, layout=%d); G.set_links(u); r = {};"
+            "r['a'] = G.dslash(R, None, 0.05, 3); r['b'] = G.dslashd(R, None, 0.05, 1);"
+            "r['f1'], r['n1'] = G.dslash_fused(R, A, 0.3, 0.05, 3, True, 1);"
+            "r['f3'], r['n3'] = G.dslash_fused(R, A, -0.7, 0.05, 3, False, 3);"
+            "X = np.zeros_like(R); r['it'], _ = G.congrad(R, X, 1e-6, 0.05, 1); r['x'] = X;"
+            "r['ms'], r['msi'], _ = G.multishift_solver(u, 0.05, 3, ad, an[1:], R, 1e-9, 20000);"
+            "np.savez(d + '/out_' + t + '.npz', **r); G.close()" % (pkg, str(tmp_path), dims, layout))
+    for t in ("8", "40"):
+        subprocess.run([sys.executable, "-c", code, t], check=True, env=dict(os.environ, THR_TUNE=t))
+    ref, got = np.load(tmp_path / "out_8.npz"), np.load(tmp_path / "out_40.npz")
+    for k in ref.files:
+        assert np.array_equal(ref[k], got[k]), k
+
+
+@pytest.mark.gpu
 def test_tiled_stencil_matches_k_dslash(tmp_path):
     """The staged-tile FP64 Shamir kernel (THR_TILE=1) against k_dslash (the
     default, oracle-checked above) in two processes on a lattice both take: M and M^dagger to rounding (the same

@@ -4,7 +4,8 @@ evolution.F90), with the reference's own remez coefficient files.
 
 Bounds: FP64 guidance solves give forces within 1e-9 and Delta H within
 1e-6 (absolute) of the FP64 oracle; the single-precision guidance solver
-(spmd, multishift_solver_sp) within 1e-4 on the force.
+(spmd, multishift_solver_sp) within 1e-4 on the force and SPMD_DH_BOUND on
+Delta H against the oracle's own single-precision trajectory.
 """
 import os
 
@@ -16,6 +17,13 @@ import thirring
 from helpers import interior, rand_theta, rel_err
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+# The reference's single-precision guidance solves (spmd = 1) change the trajectory
+# itself: in the oracle alone, Delta H of these 3-step trajectories moves by up to 2.2e-5
+# against FP64 guidance (seeds 9, 11, 13).  GPU and oracle, both in single precision,
+# round their FP32 sums in different orders and differ by up to 1.6e-5 on the same
+# trajectories (measured on B200); FP64 guidance agrees to 6e-8, within the 1e-6 bar.
+SPMD_DH_BOUND = 5e-5
 
 
 def rats():
@@ -96,7 +104,7 @@ def test_trajectory_delta_h(spmd):
         gots = [G.trajectory(th, 3, 0.05, 0.05, 3, fixed_steps=3) for _ in range(2)]
     for got, ref in zip(gots, refs):
         assert got.steps == ref.steps == 3
-        assert abs(got.dh - ref.dh) <= (1e-6 if spmd == 0 else 1e-4), (got.dh, ref.dh)
+        assert abs(got.dh - ref.dh) <= (1e-6 if spmd == 0 else SPMD_DH_BOUND), (got.dh, ref.dh)
         assert got.accepted == ref.accepted
     assert np.max(np.abs(th - th_ref)) <= 1e-5
 
@@ -119,7 +127,7 @@ def test_trajectory_mixed_action_delta_h(spmd):
         th = theta.copy(order="F")
         got = G.trajectory(th, 3, 0.05, 0.05, 3, fixed_steps=3)
     assert got.steps == ref.steps == 3
-    assert abs(got.dh - ref.dh) <= (1e-6 if spmd == 0 else 1e-4), (got.dh, ref.dh)
+    assert abs(got.dh - ref.dh) <= (1e-6 if spmd == 0 else SPMD_DH_BOUND), (got.dh, ref.dh)
 
 
 def _traj_run(tmp, tag):

@@ -250,13 +250,14 @@ def test_congrad_graph_equals_host_launched():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("env", [{"THR_OVERLAP": "0"}, {"THR_REVERSE": "1"}, {"THR_REVERSE": "0"},
-                                 {"THR_GRAPHS": "0"}, {"THR_PDL": "0"}])
+                                 {"THR_GRAPHS": "0"}, {"THR_PDL": "0"}, {"THR_CHAIN": "1"}])
 def test_solver_schedules_bit_identical(tmp_path, env):
     """Where the batched multishift's flush runs (side stream or in line), which
     way the solver kernels sweep the sites, whether the loops are graphs or
-    host-launched, and whether the kernel chain uses dependent launches change the
-    schedule only: the multishift (FP64 and FP32 vectors) and congrad give the same
-    bits and iteration counts."""
+    host-launched, whether the kernel chain uses dependent launches, and whether a
+    batch runs as the kernel chain or as one persistent kernel (THR_CHAIN=1: this
+    lattice is small enough for it) change the schedule only: the multishift (FP64 and
+    FP32 vectors) and congrad give the same bits and iteration counts."""
     import os
     import subprocess
     import sys
@@ -280,3 +281,62 @@ def test_solver_schedules_bit_identical(tmp_path, env):
     ref, got = np.load(tmp_path / "out_ref.npz"), np.load(tmp_path / "out_alt.npz")
     for k in ref.files:
         assert np.array_equal(ref[k], got[k]), k
+
+
+def _chain_run(tmp_path, dims, tag, env, poles=12, res=1e-9):
+    """A batched FP64 multishift (remez4g's poles) in a fresh process; returns its
+    exit status, output and the solve's status code (0 or the ThirringError's)."""
+    import os
+    import subprocess
+    import sys
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "thirring-rhmc_b200")
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import thirring; d = %r; t = sys.argv[1];"
+            "z = np.load(d + '/in.npz'); u = np.asfortranarray(z['u']); inp = np.asfortranarray(z['inp']);"
+            "G = thirring.Lattice(*%r); r = {'status': 0};"
+            "\ntry:\n r['x'], r['i'], r['c'] = G.multishift_solver(u, 0.05, 3, z['ad'], z['an'][1:], inp, %r, 20000)"
+            "\nexcept thirring.ThirringError as e:\n r['status'] = e.status"
+            "\nG.close(); np.savez(d + '/out_' + t + '.npz', **r)" % (pkg, str(tmp_path), dims, res))
+    r = subprocess.run([sys.executable, "-c", code, tag], capture_output=True, text=True, timeout=600,
+                       env=dict(os.environ, **env))
+    assert r.returncode == 0, r.stdout + r.stderr
+    return np.load(tmp_path / ("out_%s.npz" % tag))
+
+
+@pytest.mark.gpu
+def test_chain_several_site_blocks_per_block(tmp_path):
+    """The persistent multishift kernel forced (THR_CHAIN=2) on a lattice with more
+    stencil site blocks than resident blocks (24^3, Ls 16: 1728 site blocks), so each
+    block walks several of them between two barriers: the same bits and iteration
+    counts as the kernel chain (THR_CHAIN=0)."""
+    rng = np.random.default_rng(41)
+    dims = (24, 24, 24, 16)
+    L = O.lat(*dims)
+    an, ad, _, _ = remez("remez4g", 12)
+    np.savez(tmp_path / "in.npz", u=rand_links(L, rng), inp=rand_spinor(L, rng), an=an, ad=ad)
+    a = _chain_run(tmp_path, dims, "chain", {"THR_CHAIN": "2"}, res=1e-7)
+    b = _chain_run(tmp_path, dims, "plain", {"THR_CHAIN": "0"}, res=1e-7)
+    assert int(a["status"]) == 0 and int(b["status"]) == 0
+    for k in ("x", "i", "c"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.gpu
+def test_chain_barrier_timeout(tmp_path):
+    """The persistent multishift kernel's bounded grid barriers (THR_CHAIN=1).  With
+    THR_CHAIN_WAIT_TEST=1 every barrier waits for one arrival more than the grid
+    has, so each wait runs out after 0.2 s (nothing faults and nothing is left
+    waiting on the GPU): the solve ends with THR_ERR_TIMEOUT (8).  The same solve
+    in a fresh process without the test switch converges and matches the oracle."""
+    rng = np.random.default_rng(43)
+    dims = (4, 4, 6, 8)
+    L = O.lat(*dims)
+    u, inp = rand_links(L, rng), rand_spinor(L, rng)
+    an, ad, _, _ = remez("remez4g", 12)
+    np.savez(tmp_path / "in.npz", u=u, inp=inp, an=an, ad=ad)
+    bad = _chain_run(tmp_path, dims, "bound", {"THR_CHAIN": "1", "THR_CHAIN_WAIT_TEST": "1"})
+    assert int(bad["status"]) == 8
+    good = _chain_run(tmp_path, dims, "ok", {"THR_CHAIN": "1"})
+    assert int(good["status"]) == 0
+    ref, it_ref, _ = O.multishift(L, u, 0.05, 3, an[1:], ad, inp, 1e-9, 20000)
+    assert abs(int(good["i"]) - it_ref) <= 2
+    assert rel_err(good["x"][..., :12], ref[..., :12]) <= 1e-5

@@ -139,6 +139,7 @@ const char* thr_status_string(int s) {
     case THR_ERR_CUDA: return "CUDA error";
     case THR_ERR_NOMEM: return "out of device memory";
     case THR_ERR_UNSUPPORTED: return "unsupported option";
+    case THR_ERR_TIMEOUT: return "device-side wait timed out";
     default: return "unknown status";
   }
 }
@@ -167,6 +168,8 @@ int thr_create(const thr_params* p, thr_ctx** out) {
     if (e && e[0] == '0') c->use_md_graph = false;
     e = std::getenv("THR_PDL");
     if (e && e[0] == '0') c->use_pdl = false;
+    e = std::getenv("THR_CHAIN");
+    if (e && (e[0] == '0' || e[0] == '1' || e[0] == '2') && e[1] == 0) c->chain_mode = e[0] - '0';
   }
   int rc = THR_OK;
   if (cudaSetDevice(c->dev) != cudaSuccess) rc = THR_ERR_CUDA;
@@ -187,6 +190,7 @@ int thr_create(const thr_params* p, thr_ctx** out) {
   // per-block partial sums: the stencil epilogue writes one per block of its grid
   const size_t nparts = std::max<size_t>((size_t)kMaxPartials * 8, (size_t)std::max(stencil_grid(c->g, 0), stencil_grid(c->g, 1)) + 1024);
   if (!rc && cudaMalloc(&c->partials, nparts * sizeof(double)) != cudaSuccess) rc = THR_ERR_NOMEM;
+  c->nparts = nparts;
   if (!rc && cudaMalloc(&c->dscal, 4096 * sizeof(double)) != cudaSuccess) rc = THR_ERR_NOMEM;
   if (!rc && cudaMalloc(&c->iscal, 1024 * sizeof(int)) != cudaSuccess) rc = THR_ERR_NOMEM;
   if (!rc && cudaMallocHost(&c->hscal, 4096 * sizeof(double)) != cudaSuccess) rc = THR_ERR_NOMEM;

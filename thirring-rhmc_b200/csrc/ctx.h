@@ -27,6 +27,7 @@ constexpr int kScalFusedCoef = 4090;   // thr_dslash_fused_dev: the epilogue coe
 constexpr int kScalFusedSum = 4091;    // thr_dslash_fused_dev / thr_shift_residuals_dev: a reduced sum
 constexpr int kScalMd = 4064;          // MD step graph: 8 iteration counters, then its control block
 constexpr int kMsTemplates = 8;        // multishift state templates of one captured MD step
+constexpr int kIscalChainBar = 0;      // iscal[0..2]: the persistent multishift kernel's barrier words
 
 struct thr_ctx {
   thr_params p;
@@ -53,6 +54,7 @@ struct thr_ctx {
   std::vector<double2*> w64;
   // reduction scratch and device scalars
   double* partials = nullptr;
+  size_t nparts = 0;         // entries of partials
   double* dscal = nullptr;   // general device scalar block
   int* iscal = nullptr;
   double* hscal = nullptr;   // pinned host mirror
@@ -90,6 +92,11 @@ struct thr_ctx {
   int ms_algo = 1;          // multishift: 0 = per-iteration shift updates, 1 = batched
   bool use_graphs = true;   // batched solver loops as one CUDA graph (WHILE node) per solve
   bool use_pdl = true;      // the batched multishift's kernel chain as dependent launches (THR_PDL=0: off)
+  // a batch of the batched FP64 multishift as one persistent kernel (msp.cu): 0 (default)
+  // never; 1 where every stencil site block gets its own resident block; 2 wherever the
+  // block shape allows (THR_CHAIN=0|1|2).  Off by default: on B200 the kernel chain with
+  // dependent launches was as fast or faster at every lattice measured
+  int chain_mode = 0;
   // cached batched-multishift graphs: FP64; FP32 vectors; FP32 and BF16 base
   // iteration with FP64 shift fields (the low-precision phase of the mixed solver)
   void* ms_graphs[4] = {};

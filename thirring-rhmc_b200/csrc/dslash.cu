@@ -33,37 +33,11 @@
 
 #include "batch.h"
 #include "ctx.h"
+#include "dslash_site.cuh"
 #include "thr_common.cuh"
 #include "thr_kernels.h"
 
 namespace thr {
-
-template <class S>
-struct SpinorView {
-  const S* p;
-  Geom g;
-  __device__ __forceinline__ typename Sto<S>::C operator()(int s, int site, int d) const {
-    return Sto<S>::ld(p, sidx32(g, s, site, d));
-  }
-};
-
-// Re(conj(aux_i) v) in the working precision, accumulated in FP64 (for FP32
-// storage the term is an FP32 value summed in FP64, as reduce_real_dp5d does)
-template <class S>
-__device__ __forceinline__ double epi_redot(const S* aux, size_t i, typename Sto<S>::C v) {
-  using R = typename Sto<S>::R;
-  const typename Sto<S>::C a = Sto<S>::ld(aux, i);
-  const R t = a.x * v.x + a.y * v.y;
-  return (double)t;
-}
-
-// |v|^2 in the working precision, accumulated in FP64
-template <class S>
-__device__ __forceinline__ double epi_norm(typename Sto<S>::C v) {
-  using R = typename Sto<S>::R;
-  const R t = v.x * v.x + v.y * v.y;
-  return (double)t;
-}
 
 // one FP64 partial per block, fixed reduction order
 __device__ __forceinline__ void block_partial(double v, double* out) {
@@ -82,201 +56,6 @@ __device__ __forceinline__ void block_partial(double v, double* out) {
     if (tid == 0) *out = v;
   }
   __syncthreads();
-}
-
-// ---------------------------------------------------------------- Shamir
-// One hop of the 3D Wilson-Dirac term, spin-projected.  The reference adds
-// -1/2 [T(d) -+ 2gamma(mu,d) T(gin)] with T = W R(neighbour) for each d
-// (dirac.F90:49-76, :464-491).  2gamma(mu,.) is a Hermitian unitary permutation
-// (entries +-1, +-i) pairing each upper spin with a lower one, so
-//   h(d) = R(d) -+ 2gamma(mu,d) R(gin)   for the upper spins d = 0, 1
-// carries the whole hop: W h(d) goes to spin d and -+2gamma(mu,gin) W h(d) to
-// spin gin.  Two complex multiplies per neighbour instead of four; the result
-// differs from the unprojected sum by rounding only.
-template <class C, class R>
-__device__ __forceinline__ void hop_projected(int mu, bool plus, C W, const C* r, C* acc) {
-#pragma unroll
-  for (int d = 0; d < 2; d++) {
-    const GammaEntry ge = gamma_entry(mu, d);
-    const int gi = ge.gin;
-    const C gr = gp(ge, r[gi]);
-    const C wh = cmul(W, plus ? r[d] - gr : r[d] + gr);
-    acc[d] = acc[d] - R(0.5) * wh;
-    const C gw = gp(gamma_entry(mu, gi), wh);
-    acc[gi] = plus ? acc[gi] + R(0.5) * gw : acc[gi] - R(0.5) * gw;
-  }
-}
-
-// SHFL: the fifth-dimension neighbours and wall values come from the lanes of
-// the same site (blockDim.x = Ls a power of two <= 32, so a site's Ls threads
-// are one aligned segment of a warp); every lane must call this.
-template <class S, bool DAG, bool SHFL>
-__device__ __forceinline__ void shamir_site(const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u,
-                                            const Geom& g, int s, int site, float am, int imass, float am3,
-                                            typename Sto<S>::C* acc) {
-  using R = typename Sto<S>::R;
-  using C = typename Sto<S>::C;
-  int x, y, t;
-  site_coords(g, site, x, y, t);
-  const Nbr nb = neighbours(g, site, x, y, t);
-  SpinorView<S> Rv{in, g};
-  const int Ls = g.ls;
-  const R diag = (R)((3.0f - am3) + 1.0f);  // dirac.F90:45, default real
-  C rc[4];
-#pragma unroll
-  for (int d = 0; d < 4; d++) {
-    rc[d] = Rv(s, site, d);
-    acc[d] = diag * rc[d];
-  }
-  // fifth-dimension hop (np_third == 1), dirac.F90:80-87 (M), :317-324 (M^dagger):
-  // spins A take R(s+1), spins B take R(s-1); A = (2,3) for M, (0,1) for M^dagger
-  const int a0 = DAG ? 0 : 2, b0 = DAG ? 2 : 0;
-  C nxt[2], prv[2], w0[2], wl[2];
-  if (SHFL) {
-    const unsigned full = 0xffffffffu;
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-      nxt[k] = mk(__shfl_down_sync(full, rc[a0 + k].x, 1, Ls), __shfl_down_sync(full, rc[a0 + k].y, 1, Ls));
-      prv[k] = mk(__shfl_up_sync(full, rc[b0 + k].x, 1, Ls), __shfl_up_sync(full, rc[b0 + k].y, 1, Ls));
-      w0[k] = mk(__shfl_sync(full, rc[a0 + k].x, 0, Ls), __shfl_sync(full, rc[a0 + k].y, 0, Ls));
-      wl[k] = mk(__shfl_sync(full, rc[b0 + k].x, Ls - 1, Ls), __shfl_sync(full, rc[b0 + k].y, Ls - 1, Ls));
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < 2; k++) {
-    if (s < Ls - 1) acc[a0 + k] = acc[a0 + k] - (SHFL ? nxt[k] : Rv(s + 1, site, a0 + k));
-    if (s > 0) acc[b0 + k] = acc[b0 + k] - (SHFL ? prv[k] : Rv(s - 1, site, b0 + k));
-  }
-  // wall mass term: dirac.F90:119-176 (M), :356-402 (M^dagger).  imass 1, 3 couple
-  // R(1) into s = Ls (spins A) and R(Ls) into s = 1 (spins B); imass 5 mixes the
-  // chiralities at the same s.  Written as acc += c * v with one coefficient per
-  // wall: imass 1: am; imass 3: +i am (A), -i am (B); imass 5: +-i am (M / M^dagger).
-  const R a = (R)am;
-  const bool five = imass == 5;
-  const C cA = imass == 1 ? mk(a, R(0)) : mk(R(0), (five && DAG) ? -a : a);
-  const C cB = imass == 1 ? mk(a, R(0)) : mk(R(0), five ? (DAG ? -a : a) : -a);
-#pragma unroll
-  for (int k = 0; k < 2; k++) {
-    if (s == Ls - 1)
-      acc[a0 + k] = acc[a0 + k] + cmul(cA, five ? rc[b0 + k] : (SHFL ? w0[k] : Rv(0, site, a0 + k)));
-    if (s == 0)
-      acc[b0 + k] = acc[b0 + k] + cmul(cB, five ? rc[a0 + k] : (SHFL ? wl[k] : Rv(Ls - 1, site, b0 + k)));
-  }
-  // Wilson and Dirac hopping terms, forward (U R(x+mu)) then backward
-  // (conj U(x-mu) R(x-mu)) per direction; +gamma forward and -gamma backward in
-  // M, the opposite in M^dagger.  The reference adds them before (M) or after
-  // (M^dagger) the fifth-dimension and mass terms; the order only affects rounding.
-#pragma unroll
-  for (int mu = 0; mu < 3; mu++) {
-#pragma unroll
-    for (int dir = 0; dir < 2; dir++) {
-      const int ns = dir == 0 ? nb.f[mu] : nb.b[mu];
-      const C W = dir == 0 ? __ldg(u + (size_t)mu * g.v3 + site) : cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
-      C r[4];
-#pragma unroll
-      for (int d = 0; d < 4; d++) r[d] = Rv(s, ns, d);
-      hop_projected<C, R>(mu, (dir == 0) != DAG, W, r, acc);
-    }
-  }
-}
-
-// ---------------------------------------------------------------- Wilson
-// Q(s) components for the forward operator at (s, site)
-template <class S>
-__device__ __forceinline__ void wilson_q(const SpinorView<S>& Rv, int s, int site, int Ls,
-                                         typename Sto<S>::C c1, typename Sto<S>::C c2,
-                                         typename Sto<S>::C* q) {
-  using C = typename Sto<S>::C;
-  C r[4];
-#pragma unroll
-  for (int d = 0; d < 4; d++) r[d] = Rv(s, site, d);
-  // P+ (spins 0,1) from s-1, wall: c1 * R(Ls)
-#pragma unroll
-  for (int d = 0; d < 2; d++) q[d] = (s > 0) ? r[d] + Rv(s - 1, site, d) : r[d] + cmul(c1, Rv(Ls - 1, site, d));
-  // P- (spins 2,3) from s+1, wall: c2 * R(1)
-#pragma unroll
-  for (int d = 2; d < 4; d++) q[d] = (s < Ls - 1) ? r[d] + Rv(s + 1, site, d) : r[d] + cmul(c2, Rv(0, site, d));
-}
-
-template <class S, bool DAG>
-__device__ __forceinline__ void wilson_site(const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u,
-                                            const Geom& g, int s, int site, float am, int imass, float am3,
-                                            typename Sto<S>::C* res) {
-  using R = typename Sto<S>::R;
-  using C = typename Sto<S>::C;
-  int x, y, t;
-  site_coords(g, site, x, y, t);
-  const Nbr nb = neighbours(g, site, x, y, t);
-  SpinorView<S> Rv{in, g};
-  const int Ls = g.ls;
-  const R a = (R)am;
-  const R dgw = (R)(3.0f + (-am3));  // DWilson(…, -am3) diagonal: dirac.F90:191, :505
-  if (!DAG) {
-    // c1 = -am | -i am  (dirac.F90:274-278),  c2 = -am | +i am  (dirac.F90:287-291)
-    const C c1 = imass == 1 ? mk(-a, R(0)) : mk(R(0), -a);
-    const C c2 = imass == 1 ? mk(-a, R(0)) : mk(R(0), a);
-    C q[4];
-    wilson_q<S>(Rv, s, site, Ls, c1, c2, q);
-#pragma unroll
-    for (int d = 0; d < 4; d++) res[d] = (dgw - R(1)) * q[d] + R(2) * Rv(s, site, d);
-    // D_W hops of Q (dirac.F90:197-217), spin-projected as in the Shamir kernel
-#pragma unroll
-    for (int mu = 0; mu < 3; mu++) {
-      const C U = __ldg(u + (size_t)mu * g.v3 + site);
-      const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
-      C q[4];
-      wilson_q<S>(Rv, s, nb.f[mu], Ls, c1, c2, q);
-      hop_projected<C, R>(mu, true, U, q, res);
-      wilson_q<S>(Rv, s, nb.b[mu], Ls, c1, c2, q);
-      hop_projected<C, R>(mu, false, Ub, q, res);
-    }
-  } else {
-    // z = -am | -i am (upper right, dirac.F90:602-606); z' = -am | +i am (lower left, :615-619)
-    const C z = imass == 1 ? mk(-a, R(0)) : mk(R(0), -a);
-    const C zp = imass == 1 ? mk(-a, R(0)) : mk(R(0), a);
-    // half 0: output spins 0,1 use Qp = R(s) + R(s+1) | z' R(1); half 1: spins 2,3 use Qm = R(s) + R(s-1) | z R(Ls).
-    // One pass over the neighbours serves both halves: R(s) and the two partner slices are loaded
-    // once per site (each output element gets the same operations in the same order as half by half)
-    const bool in0 = s < Ls - 1, in1 = s > 0;
-    const int sp0 = in0 ? s + 1 : 0, sp1 = in1 ? s - 1 : Ls - 1;
-    auto qpair = [&](int st, C* q0, C* q1) {
-#pragma unroll
-      for (int d = 0; d < 4; d++) {
-        const C r = Rv(s, st, d), a0 = Rv(sp0, st, d), a1 = Rv(sp1, st, d);
-        q0[d] = in0 ? r + a0 : r + cmul(zp, a0);
-        q1[d] = in1 ? r + a1 : r + cmul(z, a1);
-      }
-    };
-    {
-      C q0[4], q1[4];
-      qpair(site, q0, q1);
-#pragma unroll
-      for (int k = 0; k < 2; k++) {
-        res[k] = (dgw - R(1)) * q0[k] + R(2) * Rv(s, site, k);
-        res[2 + k] = (dgw - R(1)) * q1[2 + k] + R(2) * Rv(s, site, 2 + k);
-      }
-    }
-    // D_W^dagger hops (dirac.F90:511-531): -1/2 W [q(d) +- 2gamma(mu,d) q(gin)], each half's
-    // output spins from its own Q
-#pragma unroll
-    for (int mu = 0; mu < 3; mu++) {
-      const C U = __ldg(u + (size_t)mu * g.v3 + site);
-      const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
-#pragma unroll
-      for (int dir = 0; dir < 2; dir++) {
-        C q0[4], q1[4];
-        qpair(dir == 0 ? nb.f[mu] : nb.b[mu], q0, q1);
-        const C W = dir == 0 ? U : Ub;
-#pragma unroll
-        for (int d = 0; d < 4; d++) {
-          const C* q = d < 2 ? q0 : q1;
-          const GammaEntry ge = gamma_entry(mu, d);
-          const C gq = gp(ge, q[ge.gin]);
-          res[d] = res[d] - R(0.5) * cmul(W, dir == 0 ? q[d] + gq : q[d] - gq);
-        }
-      }
-    }
-  }
 }
 
 // ---------------------------------------------------------------- overlap
@@ -386,13 +165,6 @@ __global__ void __launch_bounds__(256, MINB)
   for (int d = 0; d < 4; d++) Sto<double2>::st(out, sidx32(g, s, site, d), acc[d]);
 }
 
-template <class S, int KER, bool DAG, bool SHFL = false>
-__device__ __forceinline__ void apply_site(const S* in, const typename Sto<S>::C* u, const Geom& g, int s, int site,
-                                           float am, int imass, float am3, typename Sto<S>::C* acc) {
-  if (KER == 0) shamir_site<S, DAG, SHFL>(in, u, g, s, site, am, imass, am3, acc);
-  else wilson_site<S, DAG>(in, u, g, s, site, am, imass, am3, acc);
-}
-
 // ---------------------------------------------------------------- kernels
 // One thread per 5D site: blockDim = (Ls, sites per block), NT threads at most.
 // Shamir blocks are small (NT = 128, 8 resident per SM at <= 64 registers):
@@ -414,54 +186,104 @@ __global__ void __launch_bounds__(NT, MINB)
   pdl_wait();
   pdl_trigger();
   if (skip && *skip) return;
-  using C = typename Sto<S>::C;
   using R = typename Sto<S>::R;
   const R om = (EPI == 1 || EPI == 3) ? (R)(*coef) : R(0);
-  const int s = threadIdx.x;
-  double racc = 0.0;
   // rev: blocks walk the sites from the top, so that the first blocks find the
   // end of a field the previous kernel has just written still in L2
   const int bid = rev ? (int)gridDim.x - 1 - (int)blockIdx.x : (int)blockIdx.x;
-  const int site = bid * blockDim.y + threadIdx.y;
-  const bool live = site < g.v3;
-  if (SHFL || live) {  // with SHFL every lane takes part (the last block's spare rows on a clamped site)
-    const int st = live ? site : g.v3 - 1;
-    C acc[4];
-    apply_site<S, KER, DAG, SHFL>(in, u, g, s, st, am, imass, am3, acc);
-    if (live) {
+  dslash_block<S, KER, DAG, EPI, NT, SHFL>(out, in, u, g, am, imass, am3, aux, om, bid, partials);
+}
+
+// Shamir kernel with four threads per 5D site, for lattices too small to fill the GPU
+// with one thread per site (at 12^2x12, Ls 16 the one-thread kernel has 1.5 warps per
+// scheduler, and each warp's ~570 dependent instructions set the launch's latency).
+// blockDim = (Ls, sites per block, 4) over the sites of a 128-thread k_dslash block:
+// threadIdx.z = 0 owns the site (the local terms of shamir_local, then the six hops'
+// contributions in shamir_site's order, the epilogue and the block's partial), z = 1..3
+// form the products W h(d) of the forward and backward hop in direction z - 1
+// (hop_products) and hand them over in shared memory.  Each output element gets the
+// same operations in the same order as in k_dslash, and the partials group the same
+// sites, so the results are the same bits; it is one more register-budget candidate of
+// the autotuner (code kSplitCode), which keeps it only where it is faster.
+// the products of one helper thread: direction MU (a compile-time constant, so that the
+// spin permutation indexes registers), forward and backward hop
+template <class S, bool DAG, int MU>
+__device__ __forceinline__ void split_products(const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u,
+                                               const Geom& g, int s, int site, typename Sto<S>::C (*wh_s)[2][2][128],
+                                               int slot) {
+  using C = typename Sto<S>::C;
+  int x, y, t;
+  site_coords(g, site, x, y, t);
+  const Nbr nb = neighbours(g, site, x, y, t);
+  SpinorView<S> Rv{in, g};
 #pragma unroll
-      for (int d = 0; d < 4; d++) {
-        const unsigned i = sidx32(g, s, site, d);
-        if (EPI == 1) {
-          const C rn = Sto<S>::ld(aux, i) + om * acc[d];  // r = r + omega*s (multishift_module.F90:137)
-          Sto<S>::st(out, i, rn);
-          racc += epi_norm<S>(rn);
-        } else if (EPI == 3) {
-          const C hn = acc[d] + om * Sto<S>::ld(aux, i);  // h = M r + gamma h (= M p by linearity)
-          Sto<S>::st(out, i, hn);
-          racc += epi_norm<S>(hn);
-        } else {
-          Sto<S>::st(out, i, acc[d]);
-          if (EPI == 2) racc += epi_norm<S>(acc[d]);
-        }
+  for (int dir = 0; dir < 2; dir++) {
+    const int ns = dir == 0 ? nb.f[MU] : nb.b[MU];
+    const C W = dir == 0 ? __ldg(u + (size_t)MU * g.v3 + site) : cconj(__ldg(u + (size_t)MU * g.v3 + nb.b[MU]));
+    C r[4];
+#pragma unroll
+    for (int d = 0; d < 4; d++) r[d] = Rv(s, ns, d);
+    C wh[2];
+    hop_products<C>(MU, (dir == 0) != DAG, W, r, wh);
+    wh_s[MU][dir][0][slot] = wh[0];
+    wh_s[MU][dir][1][slot] = wh[1];
+  }
+}
+
+template <class S, bool DAG, int EPI, bool SHFL>
+__global__ void __launch_bounds__(512, 2)
+    k_dslash_split(S* __restrict__ out, const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u, Geom g,
+                   float am, int imass, float am3, const int* skip, const S* __restrict__ aux,
+                   const double* __restrict__ coef, double* __restrict__ partials, int rev) {
+  pdl_wait();
+  pdl_trigger();
+  if (skip && *skip) return;
+  using C = typename Sto<S>::C;
+  using R = typename Sto<S>::R;
+  __shared__ C wh_s[3][2][2][128];  // [mu][dir][d][s + Ls * site in block]
+  const int s = threadIdx.x, zi = threadIdx.y, role = threadIdx.z;
+  const int slot = s + (int)blockDim.x * zi;
+  const int bid = rev ? (int)gridDim.x - 1 - (int)blockIdx.x : (int)blockIdx.x;
+  const int site = bid * (int)blockDim.y + zi;
+  const bool live = site < g.v3;
+  C acc[4];
+  if (role > 0) {
+    if (live) {
+      if (role == 1) split_products<S, DAG, 0>(in, u, g, s, site, wh_s, slot);
+      else if (role == 2) split_products<S, DAG, 1>(in, u, g, s, site, wh_s, slot);
+      else split_products<S, DAG, 2>(in, u, g, s, site, wh_s, slot);
+    }
+  } else if (SHFL || live) {  // with SHFL every owner lane takes part (spare rows on a clamped site)
+    shamir_local<S, DAG, SHFL>(in, g, s, live ? site : g.v3 - 1, am, imass, am3, acc);
+  }
+  __syncthreads();
+  double racc = 0.0;
+  if (role == 0 && live) {
+#pragma unroll
+    for (int mu = 0; mu < 3; mu++) {
+#pragma unroll
+      for (int dir = 0; dir < 2; dir++) {
+        const C wh[2] = {wh_s[mu][dir][0][slot], wh_s[mu][dir][1][slot]};
+        hop_accumulate<C, R>(mu, (dir == 0) != DAG, wh, acc);
       }
     }
+    const R om = (EPI == 1 || EPI == 3) ? (R)(*coef) : R(0);
+#pragma unroll
+    for (int d = 0; d < 4; d++) epi_element<S, EPI, false>(out, aux, om, sidx32(g, s, site, d), acc[d], racc);
   }
   if (EPI != 0) {
-    // one FP64 partial per block in a fixed order.  Blocks of Ls x sites need not be
-    // whole warps (Ls = 12: 120 threads), so the values go through shared memory and
-    // the first warp -- always complete: every configuration has >= 32 threads -- sums them.
-    __shared__ double red[NT];
-    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-    const int nthr = blockDim.x * blockDim.y;
-    red[tid] = racc;
+    // the partial of k_dslash's block: the owners' values in slot order, summed by the
+    // first warp (all owners: the owners are the block's first Ls x sites threads)
+    __shared__ double red[128];
+    const int nown = (int)(blockDim.x * blockDim.y);
+    if (role == 0) red[slot] = racc;
     __syncthreads();
-    if (tid < 32) {
+    if (role == 0 && slot < 32) {
       double v = 0.0;
-      for (int i = tid; i < nthr; i += 32) v += red[i];
+      for (int i = slot; i < nown; i += 32) v += red[i];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-      if (tid == 0) partials[bid] = v;
+      if (slot == 0) partials[bid] = v;
     }
   }
 }
@@ -1162,9 +984,12 @@ unsigned stencil_grid(const Geom& g, int kernel) {
 // tuned value exists.
 namespace {
 constexpr int kTuneShamir[3] = {8, 7, 6};
+// FP64 storage adds the four-threads-per-site kernel (k_dslash_split) as a candidate
+constexpr int kSplitCode = 40;
+constexpr int kTuneShamir64[4] = {8, 7, 6, kSplitCode};
 constexpr int kTuneWilson[3] = {4, 3, 2};
 constexpr int kTuneOverlap[3] = {4, 3, 1};  // k_odslash's 256-thread blocks
-constexpr int kMaxCand = 3;
+constexpr int kMaxCand = 4;
 struct TuneKey {
   int dev, sid, ker, dag, epi, lx, ly, lt, ls, layout;
   bool operator<(const TuneKey& o) const {
@@ -1364,6 +1189,29 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
       else THR_D(1, 256, false, 2);
     } else if (nt != 128) {
       THR_D(0, 1024, false, 1);
+    } else if (minb == kSplitCode) {
+      if constexpr (storage_id<S>() == 0) {
+      const dim3 sblk(blk.x, blk.y, 4);
+#define THR_S(D, E, SH)                                                                                  \
+  launch_k(k_dslash_split<S, D, E, SH>, grd, sblk, 0, st, pdl, out, in, u, g, am, imass, am3, skip, aux, coef, \
+           partials, rev)
+#define THR_SE(D, SH)                \
+  do {                               \
+    if (e == 1) THR_S(D, 1, SH);     \
+    else if (e == 2) THR_S(D, 2, SH); \
+    else if (e == 3) THR_S(D, 3, SH); \
+    else THR_S(D, 0, SH);            \
+  } while (0)
+      if (shfl) {
+        if (dag) THR_SE(true, true);
+        else THR_SE(false, true);
+      } else {
+        if (dag) THR_SE(true, false);
+        else THR_SE(false, false);
+      }
+#undef THR_SE
+#undef THR_S
+      }
     } else if (shfl) {
       if (minb == 8) THR_D(0, 128, true, 8);
       else if (minb == 7) THR_D(0, 128, true, 7);
@@ -1375,8 +1223,9 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
     }
   };
   const bool tunable = storage_id<S>() < 2 && nt == (kernel == 0 ? 128 : 256);
-  const int* cand = kernel == 0 ? kTuneShamir : kTuneWilson;
-  const int ncand = 3;
+  const bool split_ok = kernel == 0 && storage_id<S>() == 0;  // FP64 Shamir, 128-thread blocks
+  const int* cand = kernel == 0 ? (split_ok ? kTuneShamir64 : kTuneShamir) : kTuneWilson;
+  const int ncand = split_ok ? 4 : 3;
   int minb = cand[0];
   if (tunable) {
     int dev = 0;

@@ -85,6 +85,77 @@ struct MsHist {
   double om[kBatch][kMaxShift], ga[kBatch][kMaxShift], ze[kBatch][kMaxShift];
 };
 
+// The batched solver's two scalar steps of an iteration, by the threads of one block
+// (tid = 0 .. at least kMaxShift - 1, every thread of the block calls them).  rec (if not
+// null) records the step's window and coefficients as step nstep of the batch.
+// alpha known (:104): it, omega (:126-127), then zeta_iii and omegas per shift (:129-135)
+__device__ __forceinline__ void ms_alpha_block(MsState* ms, MsHist* rec, int nstep, double alpha, int tid) {
+  if (tid == 0) {
+    ms_alpha_scalar(ms, alpha);
+    if (rec) {
+      rec->lo[nstep] = ms->lo;
+      rec->hi[nstep] = ms->hi;
+    }
+  }
+  __syncthreads();
+  const int k = ms->lo + tid;
+  if (k <= ms->hi) {
+    ms_alpha_shift(ms, k);
+    if (rec) {
+      rec->om[nstep][k] = ms->omegas[k];
+      rec->ze[nstep][k] = ms->zeta_iii[k];
+    }
+  }
+}
+// lambda known (:138): gammag (:143) and gammas per shift (:148-150); then the step's end
+// (:178-180, :230-275: cg_returns, convergence test, window, zeta shift, delta) with one
+// thread per shift -- ms_converge_step's statements, the window's new bounds from a
+// min / max over the block in the shared s_lo, s_hi
+__device__ __forceinline__ void ms_lambda_block(MsState* ms, MsHist* rec, int nstep, double lambda, int tid,
+                                                int* s_lo, int* s_hi) {
+  if (tid == 0) ms_lambda_scalar(ms, lambda);
+  __syncthreads();
+  const int lo0 = ms->lo, hi0 = ms->hi;
+  const int k = lo0 + tid;
+  if (k <= hi0) {
+    ms_lambda_shift(ms, k);
+    if (rec) rec->ga[nstep][k] = ms->gammas[k];
+  }
+  const int nq = ms->ndiagq, it = ms->it;
+  const double delta = ms->delta, res = (double)ms->res;  // delta of this step (replaced below)
+  if (tid == 0) {
+    *s_lo = nq;
+    *s_hi = -1;
+  }
+  __syncthreads();
+  const int q = tid;
+  if (q < nq) {
+    if (q >= lo0 && q <= hi0) ms->cg_returns[q] = it;
+    if (ms->flags[q]) {
+      if (sqrt(delta * ms->zeta_ii[q] * ms->zeta_ii[q]) * ms->correction[q] < res) {
+        ms->flags[q] = 0;
+      } else {
+        atomicMin(s_lo, q);
+        atomicMax(s_hi, q);
+      }
+    }
+  }
+  __syncthreads();
+  const int mini = *s_lo, maxi = *s_hi;
+  if (q >= mini && q <= maxi) {
+    ms->zeta_i[q] = ms->zeta_ii[q];
+    ms->zeta_ii[q] = ms->zeta_iii[q];
+  }
+  if (tid == 0) {
+    if (rec) rec->nsteps = nstep + 1;
+    ms->lo = mini;
+    ms->hi = maxi;
+    ms->delta = ms->lambda;
+    if (!(ms->lambda == ms->lambda)) ms->status = THR_ERR_NAN;
+    if (maxi < mini || ms->it >= ms->maxcg || ms->status) ms->done = 1;
+  }
+}
+
 // a batch's recorded steps folded into one affine map per shift (see msb.cu)
 struct MsCoef {
   int ns, lo, hi, pad;
@@ -110,6 +181,13 @@ int multishift_mixed_dev(thr_ctx* c, const double2* in, double2* out, double2* s
                          double2* hv, double2* s, VL* low, int ndiagq, const double* aden, const double* anum,
                          float res, float am, int imass, int maxcg, double switch_rel, int* cg_return,
                          int* cg_returns, int* switched_at);
+
+// One batch (kBatch iterations on ring half `half`, recorded into rec) of the batched
+// FP64 multishift as one persistent kernel on stream st (msp.cu).  THR_ERR_UNSUPPORTED
+// where it does not apply (context mode, block shape, lattice size): the caller then
+// launches the kernel chain.  dry: only say whether it applies.
+int ms_chain_batch(thr_ctx* c, MsState* ms, MsHist* rec, double2* ring, double2* hv, double2* p, float am, int imass,
+                   int half, cudaStream_t st, bool dry);
 
 template <class V>
 int multishift_dev(thr_ctx* c, const V* u_dummy, const V* in, V* out, V* sf, V* r, V* p, V* hv, V* s, int ndiagq,

@@ -70,71 +70,18 @@ __global__ void k_alpha(MsState* ms, MsHist* hist, const double* partials, int n
   pdl_trigger();
   if (ms->done) return;
   const double alpha = block_sum_partials(partials, np);
-  if (threadIdx.x == 0) {
-    ms_alpha_scalar(ms, alpha);
-    hist->lo[hist->nsteps] = ms->lo;
-    hist->hi[hist->nsteps] = ms->hi;
-  }
-  __syncthreads();
-  const int k = ms->lo + threadIdx.x;
-  if (k <= ms->hi) {
-    ms_alpha_shift(ms, k);
-    hist->om[hist->nsteps][k] = ms->omegas[k];
-    hist->ze[hist->nsteps][k] = ms->zeta_iii[k];
-  }
+  ms_alpha_block(ms, hist, hist->nsteps, alpha, threadIdx.x);
 }
 
-// :143, :148-150, recording gammas; closes the step's record.  Then the step's
-// end (:178-180, :230-275: cg_returns, convergence test, window, zeta shift,
-// delta) with one thread per shift: ms_converge_step's statements, the window's
-// new bounds from a shared-memory min / max (blockDim.x >= kMaxShift)
+// :143, :148-150, recording gammas; closes the step's record and ends the step
+// (convergence test, window, delta: ms_lambda_block)
 __global__ void k_lambda(MsState* ms, MsHist* hist, const double* partials, int np) {
   pdl_wait();
   pdl_trigger();
   if (ms->done) return;
   __shared__ int s_lo, s_hi;
   const double lambda = block_sum_partials(partials, np);
-  if (threadIdx.x == 0) ms_lambda_scalar(ms, lambda);
-  __syncthreads();
-  const int lo0 = ms->lo, hi0 = ms->hi;
-  const int k = lo0 + threadIdx.x;
-  if (k <= hi0) {
-    ms_lambda_shift(ms, k);
-    hist->ga[hist->nsteps][k] = ms->gammas[k];
-  }
-  const int nq = ms->ndiagq, it = ms->it;
-  const double delta = ms->delta, res = (double)ms->res;  // delta of this step (replaced below)
-  if (threadIdx.x == 0) {
-    s_lo = nq;
-    s_hi = -1;
-  }
-  __syncthreads();
-  const int q = threadIdx.x;
-  if (q < nq) {
-    if (q >= lo0 && q <= hi0) ms->cg_returns[q] = it;
-    if (ms->flags[q]) {
-      if (sqrt(delta * ms->zeta_ii[q] * ms->zeta_ii[q]) * ms->correction[q] < res) {
-        ms->flags[q] = 0;
-      } else {
-        atomicMin(&s_lo, q);
-        atomicMax(&s_hi, q);
-      }
-    }
-  }
-  __syncthreads();
-  const int mini = s_lo, maxi = s_hi;
-  if (q >= mini && q <= maxi) {
-    ms->zeta_i[q] = ms->zeta_ii[q];
-    ms->zeta_ii[q] = ms->zeta_iii[q];
-  }
-  if (threadIdx.x == 0) {
-    hist->nsteps += 1;
-    ms->lo = mini;
-    ms->hi = maxi;
-    ms->delta = ms->lambda;
-    if (!(ms->lambda == ms->lambda)) ms->status = THR_ERR_NAN;
-    if (maxi < mini || ms->it >= ms->maxcg || ms->status) ms->done = 1;
-  }
+  ms_lambda_block(ms, hist, hist->nsteps, lambda, threadIdx.x, &s_lo, &s_hi);
 }
 
 // Fold each shift's recorded steps (:155-176 once per step) into one affine map
@@ -352,6 +299,15 @@ int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO
   MsHist* rec = hist + half;
   const int rev_md = c->rev_sweep ? 1 : 0;
   (void)gb;
+  // FP64 on a small lattice: the batch as one persistent kernel (msp.cu), same recurrences
+  if constexpr (sizeof(V) == sizeof(double2) && sizeof(VO) == sizeof(double2)) {
+    if (!prof && ms_chain_batch(c, ms, rec, nullptr, nullptr, nullptr, am, imass, half, main, true) == THR_OK) {
+      THR_TRY(ms_chain_batch(c, ms, rec, reinterpret_cast<double2*>(ring), reinterpret_cast<double2*>(hv),
+                             reinterpret_cast<double2*>(p), am, imass, half, main, false));
+      if (fork) THR_CUDA(cudaStreamWaitEvent(main, c->ev_join[half], 0));
+      return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+    }
+  }
   for (int j = 0; j < kBatch; j++) {
     const int so = half * kBatch + j, sn = so + 1 == 2 * kBatch ? 0 : so + 1;
     V* rold = ring + (size_t)so * n;
@@ -415,6 +371,12 @@ template <class V, class VO = V>
 int ms_graph(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO* sf, V* ring, V* p, V* hv, V* s, float am,
              int imass, cudaGraphExec_t* exec_out) {
   int rc = ms_graph_build<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, exec_out);
+  // a graph that cannot be built with the persistent batch kernel's cooperative
+  // launches, or then with dependent launches, is built without them
+  if (rc != THR_OK && c->chain_mode != 0) {
+    c->chain_mode = 0;
+    rc = ms_graph_build<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, exec_out);
+  }
   if (rc != THR_OK && c->use_pdl) {
     c->use_pdl = false;
     rc = ms_graph_build<V, VO>(c, ms, hist, cf, out, sf, ring, p, hv, s, am, imass, exec_out);

@@ -48,12 +48,14 @@ template <> struct Sto<double2> {
   using R = double;
   using C = double2;
   static __device__ __forceinline__ C ld(const double2* p, size_t i) { return __ldg(p + i); }
+  static __device__ __forceinline__ C ldcg(const double2* p, size_t i) { return __ldcg(p + i); }
   static __device__ __forceinline__ void st(double2* p, size_t i, C v) { p[i] = v; }
 };
 template <> struct Sto<float2> {
   using R = float;
   using C = float2;
   static __device__ __forceinline__ C ld(const float2* p, size_t i) { return __ldg(p + i); }
+  static __device__ __forceinline__ C ldcg(const float2* p, size_t i) { return __ldcg(p + i); }
   static __device__ __forceinline__ void st(float2* p, size_t i, C v) { p[i] = v; }
 };
 template <> struct Sto<__nv_bfloat162> {
