@@ -119,12 +119,12 @@ def test_autotuner_keeps_results_bit_identical(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kernel,force", [(0, "7"), (0, "6"), (1, "3"), (1, "2")])
+@pytest.mark.parametrize("kernel,force", [(0, "7"), (0, "6"), (0, "204"), (0, "203"), (1, "3"), (1, "2")])
 def test_register_budgets_bit_identical(tmp_path, kernel, force):
-    """Every register budget the stencil tuner may pick gives the same bits for
-    M, M^dagger and congrad (whose stencils carry the |Mp|^2 and the fused
-    residual-update epilogues): THR_TUNE=<n> forces budget n, THR_TUNE=0 the
-    default."""
+    """Every register budget and block shape the stencil tuner may pick gives the
+    same bits for M, M^dagger and congrad (whose stencils carry the |Mp|^2 and the
+    fused residual-update epilogues): THR_TUNE=<n> forces candidate n (20x: the
+    Shamir blocks of two site groups), THR_TUNE=0 the default."""
     import os
     import subprocess
     import sys

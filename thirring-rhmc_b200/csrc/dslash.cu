@@ -194,6 +194,52 @@ __global__ void __launch_bounds__(NT, MINB)
   dslash_block<S, KER, DAG, EPI, NT, SHFL>(out, in, u, g, am, imass, am3, aux, om, bid, partials);
 }
 
+// Shamir kernel with two site groups per block (sites per CTA): blockDim = (Ls, 2 x the
+// sites of a 128-thread k_dslash block), for Ls x sites = 128.  Each group of 128 threads
+// computes as one k_dslash block and writes that block's partial (partials[2 bid + group],
+// the same grouping, order and index), so the results are the same bits; the autotuner
+// times it as candidates 200 + MINB (kG2Code).
+template <class S, bool DAG, int EPI, bool SHFL, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    k_dslash_g2(S* __restrict__ out, const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u, Geom g,
+                float am, int imass, float am3, const int* skip, const S* __restrict__ aux,
+                const double* __restrict__ coef, double* __restrict__ partials, int rev, int np) {
+  pdl_wait();
+  pdl_trigger();
+  if (skip && *skip) return;
+  using C = typename Sto<S>::C;
+  using R = typename Sto<S>::R;
+  const R om = (EPI == 1 || EPI == 3) ? (R)(*coef) : R(0);
+  const int bid = rev ? (int)gridDim.x - 1 - (int)blockIdx.x : (int)blockIdx.x;
+  const int s = threadIdx.x;
+  double racc = 0.0;
+  const int site = bid * (int)blockDim.y + threadIdx.y;
+  const bool live = site < g.v3;
+  if (SHFL || live) {  // with SHFL every lane takes part (spare rows on a clamped site)
+    const int st = live ? site : g.v3 - 1;
+    C acc[4];
+    apply_site<S, 0, DAG, SHFL>(in, u, g, s, st, am, imass, am3, acc);
+    if (live) {
+#pragma unroll
+      for (int d = 0; d < 4; d++) epi_element<S, EPI, false>(out, aux, om, sidx32(g, s, site, d), acc[d], racc);
+    }
+  }
+  if (EPI != 0) {
+    __shared__ double red[256];
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    red[tid] = racc;
+    __syncthreads();
+    const int grp = tid >> 7, lt = tid & 127;
+    if (lt < 32) {
+      double v = 0.0;
+      for (int i = lt; i < 128; i += 32) v += red[(grp << 7) + i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lt == 0 && 2 * bid + grp < np) partials[2 * bid + grp] = v;
+    }
+  }
+}
+
 // Shamir kernel with four threads per 5D site, for lattices too small to fill the GPU
 // with one thread per site (at 12^2x12, Ls 16 the one-thread kernel has 1.5 warps per
 // scheduler, and each warp's ~570 dependent instructions set the launch's latency).
@@ -977,19 +1023,25 @@ unsigned stencil_grid(const Geom& g, int kernel) {
 // kernel, M or M^dagger, epilogue, lattice, layout, device) on first use:
 // each candidate runs 1 + 3 times on the call's own fields (the launches are
 // idempotent: out and partials are overwritten), the fastest is kept for the
-// process.  Block shape and reduction order do not change, so neither do the
-// results.  THR_TUNE=0 in the environment keeps the defaults (8, 4);
-// THR_TUNE=<n> runs the budget n wherever it is a candidate.  Launches made
+// process.  For the FP64 Shamir stencil the candidates also vary the threads
+// per site (k_dslash_split, 40) and the sites per block (k_dslash_g2, 204 and
+// 203); every candidate computes each output element with the same operations
+// and sums the partials over the same site groups in the same order, so the
+// results do not change.  THR_TUNE=0 in the environment keeps the defaults
+// (8, 4); THR_TUNE=<n> runs candidate n wherever it is one.  Launches made
 // while the stream is being captured into a graph use the default until a
 // tuned value exists.
 namespace {
 constexpr int kTuneShamir[3] = {8, 7, 6};
 // FP64 storage adds the four-threads-per-site kernel (k_dslash_split) as a candidate
 constexpr int kSplitCode = 40;
-constexpr int kTuneShamir64[4] = {8, 7, 6, kSplitCode};
+// and, where Ls x sites per block = 128, 256-thread blocks of two site groups
+// (k_dslash_g2) at 4 or 3 resident blocks per SM: candidates kG2Code + 4, kG2Code + 3
+constexpr int kG2Code = 200;
+constexpr int kTuneShamir64[6] = {8, 7, 6, kSplitCode, kG2Code + 4, kG2Code + 3};
 constexpr int kTuneWilson[3] = {4, 3, 2};
 constexpr int kTuneOverlap[3] = {4, 3, 1};  // k_odslash's 256-thread blocks
-constexpr int kMaxCand = 4;
+constexpr int kMaxCand = 6;
 struct TuneKey {
   int dev, sid, ker, dag, epi, lx, ly, lt, ls, layout;
   bool operator<(const TuneKey& o) const {
@@ -1189,6 +1241,37 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
       else THR_D(1, 256, false, 2);
     } else if (nt != 128) {
       THR_D(0, 1024, false, 1);
+    } else if (minb > kG2Code) {
+      if constexpr (storage_id<S>() == 0) {
+        const dim3 gblk(blk.x, 2 * blk.y, 1);
+        const dim3 ggrd((grd.x + 1) / 2);
+        const int np = (int)grd.x;
+#define THR_G(D, E, SH, MB)                                                                                   \
+  launch_k(k_dslash_g2<S, D, E, SH, MB>, ggrd, gblk, 0, st, pdl, out, in, u, g, am, imass, am3, skip, aux, coef, \
+           partials, rev, np)
+#define THR_GE(D, SH, MB)                \
+  do {                                   \
+    if (e == 1) THR_G(D, 1, SH, MB);     \
+    else if (e == 2) THR_G(D, 2, SH, MB); \
+    else if (e == 3) THR_G(D, 3, SH, MB); \
+    else THR_G(D, 0, SH, MB);            \
+  } while (0)
+#define THR_GM(SH, MB)                    \
+  do {                                    \
+    if (dag) THR_GE(true, SH, MB);        \
+    else THR_GE(false, SH, MB);           \
+  } while (0)
+        if (shfl) {
+          if (minb == kG2Code + 4) THR_GM(true, 4);
+          else THR_GM(true, 3);
+        } else {
+          if (minb == kG2Code + 4) THR_GM(false, 4);
+          else THR_GM(false, 3);
+        }
+#undef THR_GM
+#undef THR_GE
+#undef THR_G
+      }
     } else if (minb == kSplitCode) {
       if constexpr (storage_id<S>() == 0) {
       const dim3 sblk(blk.x, blk.y, 4);
@@ -1223,9 +1306,12 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
     }
   };
   const bool tunable = storage_id<S>() < 2 && nt == (kernel == 0 ? 128 : 256);
-  const bool split_ok = kernel == 0 && storage_id<S>() == 0;  // FP64 Shamir, 128-thread blocks
+  // FP64 Shamir, 128-thread blocks: the four-threads-per-site kernel; with Ls x sites = 128
+  // also the two-group blocks
+  const bool split_ok = kernel == 0 && storage_id<S>() == 0;
+  const bool g2_ok = split_ok && blk.x * blk.y == 128;
   const int* cand = kernel == 0 ? (split_ok ? kTuneShamir64 : kTuneShamir) : kTuneWilson;
-  const int ncand = split_ok ? 4 : 3;
+  const int ncand = g2_ok ? 6 : split_ok ? 4 : 3;
   int minb = cand[0];
   if (tunable) {
     int dev = 0;
