@@ -119,8 +119,9 @@ def test_autotuner_keeps_results_bit_identical(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kernel,force", [(0, "7"), (0, "6"), (0, "204"), (0, "203"), (1, "3"), (1, "2")])
-def test_register_budgets_bit_identical(tmp_path, kernel, force):
+@pytest.mark.parametrize("kernel,force,ls", [(0, "7", 16), (0, "6", 16), (0, "204", 16), (0, "203", 16),
+                                             (0, "204", 48), (1, "3", 16), (1, "2", 16)])
+def test_register_budgets_bit_identical(tmp_path, kernel, force, ls):
     """Every register budget and block shape the stencil tuner may pick gives the
     same bits for M, M^dagger and congrad (whose stencils carry the |Mp|^2 and the
     fused residual-update epilogues): THR_TUNE=<n> forces candidate n (20x: the
@@ -129,7 +130,7 @@ def test_register_budgets_bit_identical(tmp_path, kernel, force):
     import subprocess
     import sys
     rng = np.random.default_rng(7)
-    L = O.lat(8, 6, 4, 16)
+    L = O.lat(8, 6, 4, ls)
     u = rand_links(L, rng)
     R = rand_spinor(L, rng)
     pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "thirring-rhmc_b200")
@@ -137,11 +138,11 @@ def test_register_budgets_bit_identical(tmp_path, kernel, force):
     np.save(tmp_path / "u.npy", u)
     code = ("import sys, numpy as np; sys.path.insert(0, %r); import thirring; d = %r; t = sys.argv[1];"
             "R = np.asfortranarray(np.load(d + '/R.npy')); u = np.asfortranarray(np.load(d + '/u.npy'));"
-            "G = thirring.Lattice(8, 6, 4, 16, kernel=%d); G.set_links(u);"
+            "G = thirring.Lattice(8, 6, 4, %d, kernel=%d); G.set_links(u);"
             "a = G.dslash(R, None, 0.05, 3); b = G.dslashd(R, None, 0.05, 1);"
             "X = np.zeros_like(R); it, _ = G.congrad(R, X, 1e-6, 0.05, 1);"
             "np.savez(d + '/out_' + t + '.npz', a=a, b=b, x=X, it=it); G.close()"
-            % (pkg, str(tmp_path), kernel))
+            % (pkg, str(tmp_path), ls, kernel))
     for t in ("0", force):
         subprocess.run([sys.executable, "-c", code, t], check=True, env=dict(os.environ, THR_TUNE=t))
     ref, got = np.load(tmp_path / "out_0.npz"), np.load(tmp_path / ("out_%s.npz" % force))

@@ -195,10 +195,11 @@ __global__ void __launch_bounds__(NT, MINB)
 }
 
 // Shamir kernel with two site groups per block (sites per CTA): blockDim = (Ls, 2 x the
-// sites of a 128-thread k_dslash block), for Ls x sites = 128.  Each group of 128 threads
-// computes as one k_dslash block and writes that block's partial (partials[2 bid + group],
-// the same grouping, order and index), so the results are the same bits; the autotuner
-// times it as candidates 200 + MINB (kG2Code).
+// sites of a k_dslash block), where a k_dslash block (Ls x sites threads) is whole warps
+// (128 threads for Ls 32, 16, 8; 96 for Ls 48).  Each group computes as one k_dslash
+// block and writes that block's partial (partials[2 bid + group], the same grouping,
+// order and index), so the results are the same bits; the autotuner times it as
+// candidates 200 + MINB (kG2Code).
 template <class S, bool DAG, int EPI, bool SHFL, int MINB>
 __global__ void __launch_bounds__(256, MINB)
     k_dslash_g2(S* __restrict__ out, const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u, Geom g,
@@ -227,12 +228,13 @@ __global__ void __launch_bounds__(256, MINB)
   if (EPI != 0) {
     __shared__ double red[256];
     const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int gsz = (int)(blockDim.x * blockDim.y) >> 1;  // threads of one group (whole warps)
     red[tid] = racc;
     __syncthreads();
-    const int grp = tid >> 7, lt = tid & 127;
+    const int grp = tid >= gsz ? 1 : 0, lt = tid - grp * gsz;
     if (lt < 32) {
       double v = 0.0;
-      for (int i = lt; i < 128; i += 32) v += red[(grp << 7) + i];
+      for (int i = lt; i < gsz; i += 32) v += red[grp * gsz + i];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
       if (lt == 0 && 2 * bid + grp < np) partials[2 * bid + grp] = v;
@@ -1035,8 +1037,9 @@ namespace {
 constexpr int kTuneShamir[3] = {8, 7, 6};
 // FP64 storage adds the four-threads-per-site kernel (k_dslash_split) as a candidate
 constexpr int kSplitCode = 40;
-// and, where Ls x sites per block = 128, 256-thread blocks of two site groups
-// (k_dslash_g2) at 4 or 3 resident blocks per SM: candidates kG2Code + 4, kG2Code + 3
+// and, where a block's Ls x sites threads are whole warps, blocks of two site groups
+// (k_dslash_g2, up to 256 threads) at 4 or 3 resident blocks per SM: candidates
+// kG2Code + 4, kG2Code + 3
 constexpr int kG2Code = 200;
 constexpr int kTuneShamir64[6] = {8, 7, 6, kSplitCode, kG2Code + 4, kG2Code + 3};
 constexpr int kTuneWilson[3] = {4, 3, 2};
@@ -1306,10 +1309,10 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
     }
   };
   const bool tunable = storage_id<S>() < 2 && nt == (kernel == 0 ? 128 : 256);
-  // FP64 Shamir, 128-thread blocks: the four-threads-per-site kernel; with Ls x sites = 128
-  // also the two-group blocks
+  // FP64 Shamir, 128-thread blocks: the four-threads-per-site kernel; where a block is
+  // whole warps also the two-group blocks
   const bool split_ok = kernel == 0 && storage_id<S>() == 0;
-  const bool g2_ok = split_ok && blk.x * blk.y == 128;
+  const bool g2_ok = split_ok && (blk.x * blk.y) % 32 == 0;
   const int* cand = kernel == 0 ? (split_ok ? kTuneShamir64 : kTuneShamir) : kTuneWilson;
   const int ncand = g2_ok ? 6 : split_ok ? 4 : 3;
   int minb = cand[0];
