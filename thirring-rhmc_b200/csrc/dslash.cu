@@ -1026,8 +1026,10 @@ unsigned stencil_grid(const Geom& g, int kernel) {
 // each candidate runs 1 + 3 times on the call's own fields (the launches are
 // idempotent: out and partials are overwritten), the fastest is kept for the
 // process.  For the FP64 Shamir stencil the candidates also vary the threads
-// per site (k_dslash_split, 40) and the sites per block (k_dslash_g2, 204 and
-// 203); every candidate computes each output element with the same operations
+// per site (k_dslash_split, 40), the sites per block (k_dslash_g2, 204 and
+// 203) and, with Ls a power of two <= 32, whether the fifth dimension comes
+// from warp shuffles or from memory (108, 106); every candidate computes each
+// output element with the same operations
 // and sums the partials over the same site groups in the same order, so the
 // results do not change.  THR_TUNE=0 in the environment keeps the defaults
 // (8, 4); THR_TUNE=<n> runs candidate n wherever it is one.  Launches made
@@ -1041,10 +1043,13 @@ constexpr int kSplitCode = 40;
 // (k_dslash_g2, up to 256 threads) at 4 or 3 resident blocks per SM: candidates
 // kG2Code + 4, kG2Code + 3
 constexpr int kG2Code = 200;
-constexpr int kTuneShamir64[6] = {8, 7, 6, kSplitCode, kG2Code + 4, kG2Code + 3};
+// and, where the fifth dimension comes from warp shuffles (Ls a power of two <= 32), the
+// same kernel reading the fifth-dimension neighbours from memory instead (the same
+// values, so the same bits): candidates kNoShflCode + 8, kNoShflCode + 6
+constexpr int kNoShflCode = 100;
 constexpr int kTuneWilson[3] = {4, 3, 2};
 constexpr int kTuneOverlap[3] = {4, 3, 1};  // k_odslash's 256-thread blocks
-constexpr int kMaxCand = 6;
+constexpr int kMaxCand = 8;
 struct TuneKey {
   int dev, sid, ker, dag, epi, lx, ly, lt, ls, layout;
   bool operator<(const TuneKey& o) const {
@@ -1244,6 +1249,9 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
       else THR_D(1, 256, false, 2);
     } else if (nt != 128) {
       THR_D(0, 1024, false, 1);
+    } else if (minb > kNoShflCode && minb < kG2Code) {
+      if (minb == kNoShflCode + 8) THR_D(0, 128, false, 8);
+      else THR_D(0, 128, false, 6);
     } else if (minb > kG2Code) {
       if constexpr (storage_id<S>() == 0) {
         const dim3 gblk(blk.x, 2 * blk.y, 1);
@@ -1313,8 +1321,20 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   // whole warps also the two-group blocks
   const bool split_ok = kernel == 0 && storage_id<S>() == 0;
   const bool g2_ok = split_ok && (blk.x * blk.y) % 32 == 0;
-  const int* cand = kernel == 0 ? (split_ok ? kTuneShamir64 : kTuneShamir) : kTuneWilson;
-  const int ncand = g2_ok ? 6 : split_ok ? 4 : 3;
+  int cand64[kMaxCand] = {8, 7, 6};
+  int ncand = 3;
+  if (split_ok) {
+    cand64[ncand++] = kSplitCode;
+    if (g2_ok) {
+      cand64[ncand++] = kG2Code + 4;
+      cand64[ncand++] = kG2Code + 3;
+    }
+    if (shfl) {
+      cand64[ncand++] = kNoShflCode + 8;
+      cand64[ncand++] = kNoShflCode + 6;
+    }
+  }
+  const int* cand = kernel == 0 ? (split_ok ? cand64 : kTuneShamir) : kTuneWilson;
   int minb = cand[0];
   if (tunable) {
     int dev = 0;
