@@ -58,16 +58,20 @@ def _epilogue_ref(L, u, R, aux, coef, am, imass, dag, mode):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("dims", [(8, 8, 8, 32), (16, 16, 16, 32), (8, 8, 4, 48)])
-@pytest.mark.parametrize("precision", [0, 2])
+@pytest.mark.parametrize("precision", [0, 2, 3])
 def test_fused_epilogues(dims, precision):
     """The epilogues the solvers run (congrad: |M p|^2 and r - alpha M^dagger x1;
     batched multishift: h = M r + gamma h and r + omega M^dagger h) at Ls = 32 and 48,
-    FP64 and FP32 storage, against the oracle's operator composed on the host."""
+    FP64, FP32 and BF16 storage, against the oracle's operator composed on the host.
+    BF16 keeps 8 significant bits: inputs and output each round by up to 2^-9
+    relative, FP32 arithmetic in between.  The same roundings emulated on the host
+    on these cases give at most 4.4e-3 (max-norm relative) and 5.8e-5 on |out|^2,
+    so the bounds are 1e-2 and 1e-3."""
     rng = np.random.default_rng(sum(dims) + precision)
     L = O.lat(*dims)
     u = rand_links(L, rng, beta=0.3)
     R, aux = rand_spinor(L, rng), rand_spinor(L, rng)
-    tol = TOL if precision == 0 else 2e-6
+    tol = {0: TOL, 2: 2e-6, 3: 1e-2}[precision]
     with thirring.Lattice(*dims) as G:
         G.set_links(u)
         for imass in (1, 3, 5):
@@ -77,7 +81,8 @@ def test_fused_epilogues(dims, precision):
                 got, n2 = G.dslash_fused(R, aux if mode else None, coef, 0.01, imass, dag, mode, precision)
                 e = rel_err(interior(got), ref)
                 assert e <= tol, (imass, mode, dag, e)
-                assert abs(n2 - n2_ref) <= (1e-12 if precision == 0 else 1e-5) * n2_ref, (imass, mode, dag)
+                n2_tol = {0: 1e-12, 2: 1e-5, 3: 1e-3}[precision]
+                assert abs(n2 - n2_ref) <= n2_tol * n2_ref, (imass, mode, dag)
 
 
 @pytest.mark.gpu
