@@ -194,14 +194,14 @@ __global__ void __launch_bounds__(NT, MINB)
   dslash_block<S, KER, DAG, EPI, NT, SHFL>(out, in, u, g, am, imass, am3, aux, om, bid, partials);
 }
 
-// Shamir kernel with two site groups per block (sites per CTA): blockDim = (Ls, 2 x the
+// Shamir kernel with K site groups per block (sites per CTA): blockDim = (Ls, K x the
 // sites of a k_dslash block), where a k_dslash block (Ls x sites threads) is whole warps
 // (128 threads for Ls 32, 16, 8; 96 for Ls 48).  Each group computes as one k_dslash
-// block and writes that block's partial (partials[2 bid + group], the same grouping,
+// block and writes that block's partial (partials[K bid + group], the same grouping,
 // order and index), so the results are the same bits; the autotuner times it as
-// candidates 200 + MINB (kG2Code).
-template <class S, bool DAG, int EPI, bool SHFL, int MINB>
-__global__ void __launch_bounds__(256, MINB)
+// candidates kG2Code + 10 K + MINB.
+template <class S, bool DAG, int EPI, bool SHFL, int K, int MINB>
+__global__ void __launch_bounds__(128 * K, MINB)
     k_dslash_g2(S* __restrict__ out, const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u, Geom g,
                 float am, int imass, float am3, const int* skip, const S* __restrict__ aux,
                 const double* __restrict__ coef, double* __restrict__ partials, int rev, int np) {
@@ -226,18 +226,18 @@ __global__ void __launch_bounds__(256, MINB)
     }
   }
   if (EPI != 0) {
-    __shared__ double red[256];
+    __shared__ double red[128 * K];
     const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-    const int gsz = (int)(blockDim.x * blockDim.y) >> 1;  // threads of one group (whole warps)
+    const int gsz = (int)(blockDim.x * blockDim.y) / K;  // threads of one group (whole warps)
     red[tid] = racc;
     __syncthreads();
-    const int grp = tid >= gsz ? 1 : 0, lt = tid - grp * gsz;
+    const int grp = tid / gsz, lt = tid - grp * gsz;
     if (lt < 32) {
       double v = 0.0;
       for (int i = lt; i < gsz; i += 32) v += red[grp * gsz + i];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-      if (lt == 0 && 2 * bid + grp < np) partials[2 * bid + grp] = v;
+      if (lt == 0 && K * bid + grp < np) partials[K * bid + grp] = v;
     }
   }
 }
@@ -1026,8 +1026,9 @@ unsigned stencil_grid(const Geom& g, int kernel) {
 // each candidate runs 1 + 3 times on the call's own fields (the launches are
 // idempotent: out and partials are overwritten), the fastest is kept for the
 // process.  For the FP64 Shamir stencil the candidates also vary the threads
-// per site (k_dslash_split, 40), the sites per block (k_dslash_g2, 204 and
-// 203) and, with Ls a power of two <= 32, whether the fifth dimension comes
+// per site (k_dslash_split, 40), the sites per block (k_dslash_g2: 2, 4 or 8
+// k_dslash blocks in one, 224, 223, 242, 281) and, with Ls a power of two <= 32,
+// whether the fifth dimension comes
 // from warp shuffles or from memory (108, 106); every candidate computes each
 // output element with the same operations
 // and sums the partials over the same site groups in the same order, so the
@@ -1039,9 +1040,9 @@ namespace {
 constexpr int kTuneShamir[3] = {8, 7, 6};
 // FP64 storage adds the four-threads-per-site kernel (k_dslash_split) as a candidate
 constexpr int kSplitCode = 40;
-// and, where a block's Ls x sites threads are whole warps, blocks of two site groups
-// (k_dslash_g2, up to 256 threads) at 4 or 3 resident blocks per SM: candidates
-// kG2Code + 4, kG2Code + 3
+// and, where a block's Ls x sites threads are whole warps, blocks of K site groups
+// (k_dslash_g2): K = 2 at 4 or 3 resident blocks per SM, K = 4 at 2, K = 8 at 1:
+// candidates kG2Code + 10 K + MINB
 constexpr int kG2Code = 200;
 // and, where the fifth dimension comes from warp shuffles (Ls a power of two <= 32), the
 // same kernel reading the fifth-dimension neighbours from memory instead (the same
@@ -1049,7 +1050,7 @@ constexpr int kG2Code = 200;
 constexpr int kNoShflCode = 100;
 constexpr int kTuneWilson[3] = {4, 3, 2};
 constexpr int kTuneOverlap[3] = {4, 3, 1};  // k_odslash's 256-thread blocks
-constexpr int kMaxCand = 8;
+constexpr int kMaxCand = 10;
 struct TuneKey {
   int dev, sid, ker, dag, epi, lx, ly, lt, ls, layout;
   bool operator<(const TuneKey& o) const {
@@ -1254,31 +1255,35 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
       else THR_D(0, 128, false, 6);
     } else if (minb > kG2Code) {
       if constexpr (storage_id<S>() == 0) {
-        const dim3 gblk(blk.x, 2 * blk.y, 1);
-        const dim3 ggrd((grd.x + 1) / 2);
+        const int K = (minb - kG2Code) / 10;
+        const dim3 gblk(blk.x, K * blk.y, 1);
+        const dim3 ggrd((grd.x + K - 1) / K);
         const int np = (int)grd.x;
-#define THR_G(D, E, SH, MB)                                                                                   \
-  launch_k(k_dslash_g2<S, D, E, SH, MB>, ggrd, gblk, 0, st, pdl, out, in, u, g, am, imass, am3, skip, aux, coef, \
-           partials, rev, np)
-#define THR_GE(D, SH, MB)                \
-  do {                                   \
-    if (e == 1) THR_G(D, 1, SH, MB);     \
-    else if (e == 2) THR_G(D, 2, SH, MB); \
-    else if (e == 3) THR_G(D, 3, SH, MB); \
-    else THR_G(D, 0, SH, MB);            \
+#define THR_G(D, E, SH, KK, MB)                                                                          \
+  launch_k(k_dslash_g2<S, D, E, SH, KK, MB>, ggrd, gblk, 0, st, pdl, out, in, u, g, am, imass, am3, skip, aux, \
+           coef, partials, rev, np)
+#define THR_GE(D, SH, KK, MB)                \
+  do {                                       \
+    if (e == 1) THR_G(D, 1, SH, KK, MB);     \
+    else if (e == 2) THR_G(D, 2, SH, KK, MB); \
+    else if (e == 3) THR_G(D, 3, SH, KK, MB); \
+    else THR_G(D, 0, SH, KK, MB);            \
   } while (0)
-#define THR_GM(SH, MB)                    \
-  do {                                    \
-    if (dag) THR_GE(true, SH, MB);        \
-    else THR_GE(false, SH, MB);           \
+#define THR_GM(SH, KK, MB)                  \
+  do {                                      \
+    if (dag) THR_GE(true, SH, KK, MB);      \
+    else THR_GE(false, SH, KK, MB);         \
   } while (0)
-        if (shfl) {
-          if (minb == kG2Code + 4) THR_GM(true, 4);
-          else THR_GM(true, 3);
-        } else {
-          if (minb == kG2Code + 4) THR_GM(false, 4);
-          else THR_GM(false, 3);
-        }
+#define THR_GK(SH)                                          \
+  do {                                                      \
+    if (minb == kG2Code + 24) THR_GM(SH, 2, 4);             \
+    else if (minb == kG2Code + 23) THR_GM(SH, 2, 3);        \
+    else if (minb == kG2Code + 42) THR_GM(SH, 4, 2);        \
+    else THR_GM(SH, 8, 1);                                  \
+  } while (0)
+        if (shfl) THR_GK(true);
+        else THR_GK(false);
+#undef THR_GK
 #undef THR_GM
 #undef THR_GE
 #undef THR_G
@@ -1326,8 +1331,10 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
   if (split_ok) {
     cand64[ncand++] = kSplitCode;
     if (g2_ok) {
-      cand64[ncand++] = kG2Code + 4;
-      cand64[ncand++] = kG2Code + 3;
+      cand64[ncand++] = kG2Code + 24;
+      cand64[ncand++] = kG2Code + 23;
+      cand64[ncand++] = kG2Code + 42;
+      cand64[ncand++] = kG2Code + 81;
     }
     if (shfl) {
       cand64[ncand++] = kNoShflCode + 8;
