@@ -850,7 +850,10 @@ def run_trajectory48(args):
     CUDA graph; Gaussian theta, site streams.  One trajectory, not the 20 of the config:
     a full one takes about a quarter of an hour on one GPU.  Its Delta H cannot be compared
     with the oracle here (the oracle would take days at this size); config 1 carries that
-    comparison."""
+    comparison.  --traj-mode plain runs the same trajectory on the plain FP64 GPU path (the
+    reference's multishift loop structure, FP64 guidance and action solves, host-driven
+    steps), for the speed-up over it (a short --traj-steps makes both comparable); ours64
+    is this build's path with FP64 guidance solves, the like-for-like comparison."""
     import thirring
     gold = os.path.join(REPO, "tests", "golden") + os.sep
     rat = thirring.remez_set(gold + "remez2", gold + "remez4", 25)
@@ -859,8 +862,13 @@ def run_trajectory48(args):
     nstep = args.traj_steps
     G = thirring.Lattice(lx, lx, lx, ls, beta=beta)
     G.set_remez(rat, ratg)
-    G.set_residuals(1e-9, 1e-6, 1)
-    G.set_action_precision(thirring.MIXED_FP32)
+    plain = args.traj_mode == "plain"
+    if plain:
+        G.set_solver(0)
+        G.set_residuals(1e-9, 1e-6, 0)
+    else:
+        G.set_residuals(1e-9, 1e-6, 0 if args.traj_mode == "ours64" else 1)
+        G.set_action_precision(thirring.MIXED_FP32)
     G.init_random(4139764973254.0)
     rng = np.random.default_rng(5)
     th = np.asfortranarray(rng.standard_normal((lx, lx, lx, 3)) / np.sqrt(beta), np.float32)
@@ -871,8 +879,11 @@ def run_trajectory48(args):
         t = time.perf_counter() - t0
     its = {k: v for k, v in G.md_counters().items() if v}
     G.close()
+    how = ("plain FP64 GPU path: per-iteration multishift, FP64 guidance and action solves, host-driven steps"
+           if plain else "%s guidance, mixed action solves, MD steps as CUDA graphs"
+           % ("FP64" if args.traj_mode == "ours64" else "spmd"))
     return {"workload": "config 5 sample: one RHMC trajectory, 48^2x48 Ls48, beta 0.28, am 0.005, imass 3, "
-                        "%d MD steps dt %g, spmd guidance, mixed action solves, MD steps as CUDA graphs" % (nstep, dt),
+                        "%d MD steps dt %g, %s" % (nstep, dt, how),
             "s_per_traj": round(t, 1), "traj_per_hr": round(3600 / t, 2), "dH": r.dh, "accepted": r.accepted,
             "steps": r.steps, "iterations": its, "clocks": clk.summary(), "sample": "1 trajectory"}
 
@@ -900,6 +911,9 @@ def main():
                     help="profiling case: stop every solve after this many iterations (not a full solve)")
     ap.add_argument("--no-dslash", action="store_true")
     ap.add_argument("--traj-steps", type=int, default=50, help="trajectory48: MD steps of the sample trajectory")
+    ap.add_argument("--traj-mode", default="ours", choices=["ours", "ours64", "plain"],
+                    help="trajectory48: this build's path (default; ours64: with FP64 guidance solves) or the "
+                         "plain FP64 GPU path")
     ap.add_argument("--sweep-l", default="", help="dslash_sweep: comma-separated lattice extents")
     ap.add_argument("--sweep-ls", default="", help="dslash_sweep: comma-separated fifth-dimension extents")
     ap.add_argument("--no-compare-plain", dest="compare_plain", action="store_false",
