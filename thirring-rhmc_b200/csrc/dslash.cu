@@ -1244,7 +1244,14 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
       return;
     }
     if (kernel == 1) {
+      // Ls a power of two <= 32: the fifth-dimension slices from warp shuffles
+      const bool wshfl = g.ls <= 32 && (g.ls & (g.ls - 1)) == 0;
       if (nt != 256) THR_D(1, 1024, false, 1);
+      else if (minb == kNoShflCode + 4) THR_D(1, 256, false, 4);  // the slices from memory
+      else if (minb == kNoShflCode + 2) THR_D(1, 256, false, 2);
+      else if (wshfl && minb == 4) THR_D(1, 256, true, 4);
+      else if (wshfl && minb == 3) THR_D(1, 256, true, 3);
+      else if (wshfl) THR_D(1, 256, true, 2);
       else if (minb == 4) THR_D(1, 256, false, 4);
       else if (minb == 3) THR_D(1, 256, false, 3);
       else THR_D(1, 256, false, 2);
@@ -1341,7 +1348,15 @@ int launch_dslash_mode(const Geom& g, int kernel, bool dag, S* out, const S* in,
       cand64[ncand++] = kNoShflCode + 6;
     }
   }
-  const int* cand = kernel == 0 ? (split_ok ? cand64 : kTuneShamir) : kTuneWilson;
+  // Wilson with Ls a power of two <= 32: the shuffle kernel's budgets, and the same kernel
+  // reading the fifth-dimension slices from memory (the same values and bits)
+  int candw[kMaxCand] = {kTuneWilson[0], kTuneWilson[1], kTuneWilson[2]};
+  if (kernel == 1 && g.ls <= 32 && (g.ls & (g.ls - 1)) == 0) {
+    candw[3] = kNoShflCode + 4;
+    candw[4] = kNoShflCode + 2;
+    ncand = 5;
+  }
+  const int* cand = kernel == 0 ? (split_ok ? cand64 : kTuneShamir) : candw;
   int minb = cand[0];
   if (tunable) {
     int dev = 0;

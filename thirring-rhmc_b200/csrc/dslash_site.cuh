@@ -176,8 +176,16 @@ __device__ __forceinline__ void shamir_site(const S* __restrict__ in, const type
 }
 
 // ---------------------------------------------------------------- Wilson
-// Q(s) components for the forward operator at (s, site)
-template <class S, bool COH>
+// a complex value from lane `src` of this lane's Ls-wide segment (every lane calls it)
+template <class C>
+__device__ __forceinline__ C seg_shfl(C v, int src, int Ls) {
+  return mk(__shfl_sync(0xffffffffu, v.x, src, Ls), __shfl_sync(0xffffffffu, v.y, src, Ls));
+}
+
+// Q(s) components for the forward operator at (s, site).  SHFL: the slices s-1, s+1 and
+// the walls' R(Ls), R(1) come from the lanes of the same site (blockDim.x = Ls a power of
+// two <= 32; every lane must call this): the same values, one load per spin instead of three.
+template <class S, bool COH, bool SHFL = false>
 __device__ __forceinline__ void wilson_q(const SpinorView<S, COH>& Rv, int s, int site, int Ls,
                                          typename Sto<S>::C c1, typename Sto<S>::C c2,
                                          typename Sto<S>::C* q) {
@@ -185,6 +193,19 @@ __device__ __forceinline__ void wilson_q(const SpinorView<S, COH>& Rv, int s, in
   C r[4];
 #pragma unroll
   for (int d = 0; d < 4; d++) r[d] = Rv(s, site, d);
+  if (SHFL) {
+#pragma unroll
+    for (int d = 0; d < 2; d++) {
+      const C prv = seg_shfl(r[d], s > 0 ? s - 1 : Ls - 1, Ls);
+      q[d] = (s > 0) ? r[d] + prv : r[d] + cmul(c1, prv);
+    }
+#pragma unroll
+    for (int d = 2; d < 4; d++) {
+      const C nxt = seg_shfl(r[d], s < Ls - 1 ? s + 1 : 0, Ls);
+      q[d] = (s < Ls - 1) ? r[d] + nxt : r[d] + cmul(c2, nxt);
+    }
+    return;
+  }
   // P+ (spins 0,1) from s-1, wall: c1 * R(Ls)
 #pragma unroll
   for (int d = 0; d < 2; d++) q[d] = (s > 0) ? r[d] + Rv(s - 1, site, d) : r[d] + cmul(c1, Rv(Ls - 1, site, d));
@@ -193,7 +214,7 @@ __device__ __forceinline__ void wilson_q(const SpinorView<S, COH>& Rv, int s, in
   for (int d = 2; d < 4; d++) q[d] = (s < Ls - 1) ? r[d] + Rv(s + 1, site, d) : r[d] + cmul(c2, Rv(0, site, d));
 }
 
-template <class S, bool DAG, bool COH = false>
+template <class S, bool DAG, bool COH = false, bool SHFL = false>
 __device__ __forceinline__ void wilson_site(const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u,
                                             const Geom& g, int s, int site, float am, int imass, float am3,
                                             typename Sto<S>::C* res) {
@@ -211,7 +232,7 @@ __device__ __forceinline__ void wilson_site(const S* __restrict__ in, const type
     const C c1 = imass == 1 ? mk(-a, R(0)) : mk(R(0), -a);
     const C c2 = imass == 1 ? mk(-a, R(0)) : mk(R(0), a);
     C q[4];
-    wilson_q<S, COH>(Rv, s, site, Ls, c1, c2, q);
+    wilson_q<S, COH, SHFL>(Rv, s, site, Ls, c1, c2, q);
 #pragma unroll
     for (int d = 0; d < 4; d++) res[d] = (dgw - R(1)) * q[d] + R(2) * Rv(s, site, d);
     // D_W hops of Q (dirac.F90:197-217), spin-projected as in the Shamir kernel
@@ -220,9 +241,9 @@ __device__ __forceinline__ void wilson_site(const S* __restrict__ in, const type
       const C U = __ldg(u + (size_t)mu * g.v3 + site);
       const C Ub = cconj(__ldg(u + (size_t)mu * g.v3 + nb.b[mu]));
       C q[4];
-      wilson_q<S, COH>(Rv, s, nb.f[mu], Ls, c1, c2, q);
+      wilson_q<S, COH, SHFL>(Rv, s, nb.f[mu], Ls, c1, c2, q);
       hop_projected<C, R>(mu, true, U, q, res);
-      wilson_q<S, COH>(Rv, s, nb.b[mu], Ls, c1, c2, q);
+      wilson_q<S, COH, SHFL>(Rv, s, nb.b[mu], Ls, c1, c2, q);
       hop_projected<C, R>(mu, false, Ub, q, res);
     }
   } else {
@@ -237,7 +258,9 @@ __device__ __forceinline__ void wilson_site(const S* __restrict__ in, const type
     auto qpair = [&](int st, C* q0, C* q1) {
 #pragma unroll
       for (int d = 0; d < 4; d++) {
-        const C r = Rv(s, st, d), a0 = Rv(sp0, st, d), a1 = Rv(sp1, st, d);
+        const C r = Rv(s, st, d);
+        const C a0 = SHFL ? seg_shfl(r, sp0, Ls) : Rv(sp0, st, d);
+        const C a1 = SHFL ? seg_shfl(r, sp1, Ls) : Rv(sp1, st, d);
         q0[d] = in0 ? r + a0 : r + cmul(zp, a0);
         q1[d] = in1 ? r + a1 : r + cmul(z, a1);
       }
@@ -278,7 +301,7 @@ template <class S, int KER, bool DAG, bool SHFL = false, bool COH = false>
 __device__ __forceinline__ void apply_site(const S* in, const typename Sto<S>::C* u, const Geom& g, int s, int site,
                                            float am, int imass, float am3, typename Sto<S>::C* acc) {
   if (KER == 0) shamir_site<S, DAG, SHFL, COH>(in, u, g, s, site, am, imass, am3, acc);
-  else wilson_site<S, DAG, COH>(in, u, g, s, site, am, imass, am3, acc);
+  else wilson_site<S, DAG, COH, SHFL>(in, u, g, s, site, am, imass, am3, acc);
 }
 
 // One block's sites of the stencil with its epilogue (blockDim = (Ls, sites per
