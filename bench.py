@@ -48,7 +48,7 @@ METRIC = "multishift solve throughput (qmrherm, 25 poles, FP64 residual 1e-9)"
 # kernel timing inside the timed region: every PROF_STRIDE-th launch of each kind
 PROF_STRIDE = 8
 PROF_KINDS = ((0, "k_dslash_M_hrec"), (2, "k_dslash_Mdag"), (1, "k_flush"), (3, "k_dslash_M_hrec_fp32"),
-              (4, "k_dslash_Mdag_fp32"))
+              (4, "k_dslash_Mdag_fp32"), (5, "k_alpha"), (6, "k_lambda"))
 UNIT = "solves/s"
 HBM_FALLBACK = 6650.0
 # arithmetic of each mode: the mixed modes run FP64 first and FP32 (BF16 storage,

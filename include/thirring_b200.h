@@ -441,7 +441,9 @@ int thr_get_stream(thr_ctx *ctx, void **stream);
  * batched multishift with its fused |M p|^2), kind 2 the stencil M^dagger
  * (kind 0 in the per-iteration multishift), kind 1 the shift-field update
  * (k_flush, or k_ms_pshift in the per-iteration solver), kinds 3 and 4 the
- * stencils M and M^dagger of the mixed multishift's low-precision phase.  thr_profile_read
+ * stencils M and M^dagger of the mixed multishift's low-precision phase, kinds 5
+ * and 6 the batched multishift's one-block scalar steps k_alpha and k_lambda (no
+ * algorithmic bytes).  thr_profile_read
  * returns, for one kind, the sampled launches that did work, their summed
  * device time in ms and their summed algorithmic bytes, and the number of
  * launches of that kind that did work (sampled or not). */

@@ -138,8 +138,12 @@ struct thr_ctx {
 
   // optional per-kernel timing: CUDA events around selected launches
   // kernel timing: every prof_stride-th launch of each kind is bracketed by events
-  // (P_DSLASH_LOW / P_DSLASH_DAG_LOW: the same stencils in the low-precision phase of the mixed multishift)
-  enum ProfKernel { P_DSLASH = 0, P_SHIFTUPD = 1, P_DSLASH_DAG = 2, P_DSLASH_LOW = 3, P_DSLASH_DAG_LOW = 4, P_COUNT = 6 };
+  // (P_DSLASH_LOW / P_DSLASH_DAG_LOW: the same stencils in the low-precision phase of the mixed multishift;
+  // P_ALPHA, P_LAMBDA: the batched multishift's one-block scalar steps k_alpha and k_lambda)
+  enum ProfKernel {
+    P_DSLASH = 0, P_SHIFTUPD = 1, P_DSLASH_DAG = 2, P_DSLASH_LOW = 3, P_DSLASH_DAG_LOW = 4, P_ALPHA = 5, P_LAMBDA = 6,
+    P_COUNT = 7
+  };
   bool prof_on = false;
   int prof_stride = 1;
   long long prof_seen[P_COUNT] = {};         // launches offered to prof_begin

@@ -64,13 +64,43 @@ __global__ void k_init(MsState* ms, MsHist* hist, const double* partials, int np
   }
 }
 
+// The two scalar steps of an iteration, one block each.  The solver state is copied into
+// shared memory at the start (one load per thread, issued with the partials' loads) and
+// the step runs on the copy, so that its chain of dependent scalar accesses costs
+// shared-memory latency instead of an L2 round trip each; the fields the step changes are
+// written back at the end (not batches or flush_fields: the side stream's flush of the
+// other ring half updates those meanwhile).  The arithmetic is ms_alpha_block's and
+// ms_lambda_block's.
+constexpr int kMsWords = (int)(sizeof(MsState) / sizeof(double));
+static_assert(sizeof(MsState) % sizeof(double) == 0, "MsState is copied as doubles");
+__device__ __forceinline__ void ms_stage(MsState* st, const MsState* ms) {
+  double* dst = reinterpret_cast<double*>(st);
+  const double* src = reinterpret_cast<const double*>(ms);
+  for (int i = threadIdx.x; i < kMsWords; i += blockDim.x) dst[i] = src[i];
+}
+
 // :104, :118-135, recording the step's omegas / zeta_iii / window
 __global__ void k_alpha(MsState* ms, MsHist* hist, const double* partials, int np) {
   pdl_wait();
   pdl_trigger();
-  if (ms->done) return;
-  const double alpha = block_sum_partials(partials, np);
-  ms_alpha_block(ms, hist, hist->nsteps, alpha, threadIdx.x);
+  __shared__ MsState st;
+  const int nsteps = hist->nsteps;
+  ms_stage(&st, ms);
+  const double alpha = block_sum_partials(partials, np);  // its barriers publish the copy
+  if (st.done) return;
+  ms_alpha_block(&st, hist, nsteps, alpha, threadIdx.x);
+  __syncthreads();
+  const int k = threadIdx.x;
+  if (k == 0) {
+    ms->it = st.it;
+    ms->alpha = st.alpha;
+    ms->omega_save = st.omega_save;
+    ms->omega = st.omega;
+  }
+  if (k < kMaxShift) {
+    ms->zeta_iii[k] = st.zeta_iii[k];
+    ms->omegas[k] = st.omegas[k];
+  }
 }
 
 // :143, :148-150, recording gammas; closes the step's record and ends the step
@@ -78,10 +108,32 @@ __global__ void k_alpha(MsState* ms, MsHist* hist, const double* partials, int n
 __global__ void k_lambda(MsState* ms, MsHist* hist, const double* partials, int np) {
   pdl_wait();
   pdl_trigger();
-  if (ms->done) return;
+  __shared__ MsState st;
   __shared__ int s_lo, s_hi;
+  const int nsteps = hist->nsteps;
+  ms_stage(&st, ms);
   const double lambda = block_sum_partials(partials, np);
-  ms_lambda_block(ms, hist, hist->nsteps, lambda, threadIdx.x, &s_lo, &s_hi);
+  if (st.done) return;
+  ms_lambda_block(&st, hist, nsteps, lambda, threadIdx.x, &s_lo, &s_hi);
+  __syncthreads();
+  const int k = threadIdx.x;
+  if (k == 0) {
+    ms->lambda = st.lambda;
+    ms->active_sum = st.active_sum;
+    ms->gammag = st.gammag;
+    ms->lo = st.lo;
+    ms->hi = st.hi;
+    ms->delta = st.delta;
+    ms->status = st.status;
+    ms->done = st.done;
+  }
+  if (k < kMaxShift) {
+    ms->gammas[k] = st.gammas[k];
+    ms->cg_returns[k] = st.cg_returns[k];
+    ms->flags[k] = st.flags[k];
+    ms->zeta_i[k] = st.zeta_i[k];
+    ms->zeta_ii[k] = st.zeta_ii[k];
+  }
 }
 
 // Fold each shift's recorded steps (:155-176 once per step) into one affine map
@@ -321,13 +373,17 @@ int enqueue_batch(thr_ctx* c, MsState* ms, MsHist* hist, MsCoef* cf, VO* out, VO
     THR_TRY(launch_dslash_accum<V>(c->g, c->p.kernel, false, hcur, rold, u, am, imass, c->p.am3, main, &ms->done,
                                    hprev, &ms->gammag, c->partials, 0, pdl && j > 0));
     c->prof_end(pe);
+    pe = prof ? c->prof_begin(thr_ctx::P_ALPHA, 0.0, k0 + j) : -1;
     launch_k(k_alpha, dim3(1), dim3(1024), 0, main, pdl, ms, rec, c->partials, (int)gs);
+    c->prof_end(pe);
     // s = M^dagger h is never stored: the epilogue forms r = r + omega*s (:137) and |r|^2 (:138)
     pe = prof ? c->prof_begin(fp64 ? thr_ctx::P_DSLASH_DAG : thr_ctx::P_DSLASH_DAG_LOW, b_md, k0 + j) : -1;
     THR_TRY(launch_dslash_axpy<V>(c->g, c->p.kernel, true, rnew, hcur, u, am, imass, c->p.am3, main, &ms->done,
                                   rold, &ms->omega, c->partials, rev_md, pdl));
     c->prof_end(pe);
+    pe = prof ? c->prof_begin(thr_ctx::P_LAMBDA, 0.0, k0 + j) : -1;
     launch_k(k_lambda, dim3(1), dim3(1024), 0, main, pdl, ms, rec, c->partials, (int)gs);
+    c->prof_end(pe);
   }
   (void)s;
   if (fork) THR_CUDA(cudaStreamWaitEvent(main, c->ev_join[half], 0));
@@ -569,6 +625,8 @@ int run_batches(thr_ctx* c, MsState* ms, MsState* h, MsHist* hist, MsCoef* cf, V
     c->prof_work[fp64 ? thr_ctx::P_DSLASH : thr_ctx::P_DSLASH_LOW] += h->it - it0;
     c->prof_work[fp64 ? thr_ctx::P_DSLASH_DAG : thr_ctx::P_DSLASH_DAG_LOW] += h->it - it0;
     c->prof_work[thr_ctx::P_SHIFTUPD] += flushes;
+    c->prof_work[thr_ctx::P_ALPHA] += h->it - it0;
+    c->prof_work[thr_ctx::P_LAMBDA] += h->it - it0;
   }
   return THR_OK;
 }
