@@ -42,5 +42,13 @@ template <class S>
 int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
                         float am, int imass, float am3, cudaStream_t st, const int* skip, const S* aux,
                         double* partials, int grid = 0);
+// the batch stencil with a CG epilogue: epi 2 out = M in with a partial of |out|^2 per work
+// block; epi 4 rv -= coef[e * coef_stride] (M in) in place (arithmetic type, out unused)
+// with a partial of |rv|^2 per work block
+template <class S>
+int launch_dslash_batch_fused(const BatchTable& b, int kernel, bool dag, int epi, S* out, const S* in,
+                              const typename Sto<S>::C* u, float am, int imass, float am3, cudaStream_t st,
+                              const int* skip, typename Sto<S>::C* rv, const double* coef, int coef_stride,
+                              double* partials, int grid = 0);
 
 }  // namespace thr

@@ -172,6 +172,7 @@ __global__ void k_inner_start(BcgState* stt, int* skip, const double* partials, 
   BcgState& s = stt[e];
   s.rr = rr;
   s.inner_it = 0;
+  s.done_at = -1;  // no step of this inner solve has run
   s.done_inner = s.done_outer || !(rr > s.target);
   skip[e] = s.done_inner;
 }
@@ -184,38 +185,13 @@ __global__ void k_alpha(const BatchEntry* tab, BcgState* stt, const double* part
   if (threadIdx.x == 0) stt[e].alpha = stt[e].rr / pq;
 }
 
-// e += alpha p ; r -= alpha q ; partials |r|^2
-template <class VS, class VA>
-__global__ void k_update(const BatchEntry* tab, const BcgState* stt, VA* ev, VA* r, const VS* p, const VS* q,
-                         double* partials) {
-  const int e = blockIdx.y;
-  double acc = 0.0;
-  if (!stt[e].done_inner) {
-    size_t off, n;
-    entry_range(tab, e, off, n);
-    using RA = typename Pr<VA>::R;
-    const RA a = (RA)stt[e].alpha;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-      const auto pv = Pr<VS>::ld(p, off + i);
-      const auto qv = Pr<VS>::ld(q, off + i);
-      VA x = ev[off + i];
-      x.x += a * (RA)pv.x;
-      x.y += a * (RA)pv.y;
-      ev[off + i] = x;
-      VA rv = r[off + i];
-      rv.x -= a * (RA)qv.x;
-      rv.y -= a * (RA)qv.y;
-      r[off + i] = rv;
-      acc += (double)rv.x * (double)rv.x + (double)rv.y * (double)rv.y;
-    }
-  }
-  block_write_partial(acc, partials + (size_t)e * gridDim.x);
-}
-
-__global__ void k_beta(BcgState* stt, int* skip, const double* partials, int gx, int inner_cap) {
+// measure_module.F90:102-110 with |r|^2 from the partials of the fused M^dagger stencil
+// (r -= alpha M^dagger M p in its epilogue, one partial per work block of the entry)
+__global__ void k_beta(const BatchEntry* tab, BcgState* stt, int* skip, const double* partials, int inner_cap,
+                       int step) {
   const int e = blockIdx.x;
   if (stt[e].done_inner) return;
-  const double rn = warp_entry_sum(partials, e * gx, gx);
+  const double rn = warp_entry_sum(partials, tab[e].blk0, tab[e].nblk);
   if (threadIdx.x != 0) return;
   BcgState& s = stt[e];
   s.beta = rn / s.rr;
@@ -226,26 +202,37 @@ __global__ void k_beta(BcgState* stt, int* skip, const double* partials, int gx,
     s.status = THR_ERR_NAN;
     s.done_outer = 1;
   }
-  if (!(rn > s.target) || s.inner_it >= inner_cap || s.iters >= s.cap || s.status) s.done_inner = 1;
+  if (!(rn > s.target) || s.inner_it >= inner_cap || s.iters >= s.cap || s.status) {
+    s.done_inner = 1;
+    s.done_at = step;
+  }
   skip[e] = s.done_inner;
 }
 
-// p = r + beta p
+// e += alpha p (:91); p = r + beta p (:110) -- one pass, the old p read once.  An entry
+// whose solve ended at this step (done_at) still takes its last e update, not the p update.
 template <class VS, class VA>
-__global__ void k_pupdate(const BatchEntry* tab, const BcgState* stt, VS* p, const VA* r) {
+__global__ void k_xp(const BatchEntry* tab, const BcgState* stt, VA* ev, VS* p, const VA* r, int step) {
   const int e = blockIdx.y;
-  if (stt[e].done_inner) return;
+  const bool last = stt[e].done_inner;
+  if (last && stt[e].done_at != step) return;
   size_t off, n;
   entry_range(tab, e, off, n);
   using RA = typename Pr<VA>::R;
-  const RA b = (RA)stt[e].beta;
+  const RA a = (RA)stt[e].alpha, b = (RA)stt[e].beta;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const auto pv = Pr<VS>::ld(p, off + i);
-    const VA rv = r[off + i];
-    VA v;
-    v.x = rv.x + b * (RA)pv.x;
-    v.y = rv.y + b * (RA)pv.y;
-    Pr<VS>::st(p, off + i, make_float2_or_double2<VS>(v));
+    VA x = ev[off + i];
+    x.x += a * (RA)pv.x;
+    x.y += a * (RA)pv.y;
+    ev[off + i] = x;
+    if (!last) {
+      const VA rv = r[off + i];
+      VA v;
+      v.x = rv.x + b * (RA)pv.x;
+      v.y = rv.y + b * (RA)pv.y;
+      Pr<VS>::st(p, off + i, make_float2_or_double2<VS>(v));
+    }
   }
 }
 
@@ -295,17 +282,26 @@ static int bcg_inner(BcgRun& br, VA* r, VS* p, VS* h, VS* q, VA* ev, float tol, 
   k_inner_start<<<tab.nent, 32, 0, br.st>>>(br.state, br.skip, br.partials, kGX);
   const int chunk = 16;
   std::vector<BcgState> h_state(tab.nent);
+  // per step: h = M p with |h|^2 = |M p|^2 (the reference's alphad, :70); alpha; r -= alpha
+  // M^dagger h with |r|^2 in the M^dagger epilogue (q = M^dagger M p never stored); beta;
+  // e += alpha p and p = r + beta p in one pass.  r is held in the stencil's arithmetic type.
+  static_assert(sizeof(BcgState) % sizeof(double) == 0, "BcgState scalars are addressed with a stride");
+  const int stride = (int)(sizeof(BcgState) / sizeof(double));
+  const double* alpha0 = &br.state[0].alpha;
+  using C = typename Sto<VS>::C;
+  static_assert(sizeof(C) == sizeof(VA), "r is held in the stencil's arithmetic type");
+  (void)q;
   for (int it = 0; it < inner_cap + chunk; it += chunk) {
     for (int k = 0; k < chunk; k++) {
-      THR_TRY(launch_dslash_batch<VS>(tab, br.kernel, false, h, p, u, br.am, br.imass, br.am3, br.st, br.skip, nullptr,
-                                      nullptr, br.grid));
-      THR_TRY(launch_dslash_batch<VS>(tab, br.kernel, true, q, h, u, br.am, br.imass, br.am3, br.st, br.skip, p,
-                                      br.partials, br.grid));
+      const int step = it + k;
+      THR_TRY(launch_dslash_batch_fused<VS>(tab, br.kernel, false, 2, h, p, u, br.am, br.imass, br.am3, br.st,
+                                            br.skip, nullptr, nullptr, 0, br.partials, br.grid));
       k_alpha<<<tab.nent, 32, 0, br.st>>>(tab.dev, br.state, br.partials);
-      k_update<VS, VA><<<vg, kT, 0, br.st>>>(tab.dev, br.state, ev, r, p, q, br.partials);
-      k_beta<<<tab.nent, 32, 0, br.st>>>(br.state, br.skip, br.partials, kGX, inner_cap);
-      k_pupdate<VS, VA><<<vg, kT, 0, br.st>>>(tab.dev, br.state, p, r);
-      br.launches += 6;
+      THR_TRY(launch_dslash_batch_fused<VS>(tab, br.kernel, true, 4, nullptr, h, u, br.am, br.imass, br.am3, br.st,
+                                            br.skip, reinterpret_cast<C*>(r), alpha0, stride, br.partials, br.grid));
+      k_beta<<<tab.nent, 32, 0, br.st>>>(tab.dev, br.state, br.skip, br.partials, inner_cap, step);
+      k_xp<VS, VA><<<vg, kT, 0, br.st>>>(tab.dev, br.state, ev, p, r, step);
+      br.launches += 5;
     }
     THR_CUDA(cudaMemcpyAsync(h_state.data(), br.state, sizeof(BcgState) * tab.nent, cudaMemcpyDeviceToHost, br.st));
     THR_CUDA(cudaStreamSynchronize(br.st));

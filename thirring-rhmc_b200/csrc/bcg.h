@@ -9,6 +9,7 @@ namespace thr {
 struct BcgState {
   double rr, pq, alpha, beta, target, resid, r2_true;
   int iters, inner_it, outer, done_outer, done_inner, cap, status, rounds;
+  int done_at;  // inner-loop step whose residual ended the entry's inner solve (-1: none)
 };
 
 struct BcgRun {

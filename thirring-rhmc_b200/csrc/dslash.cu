@@ -916,12 +916,18 @@ bool tile_maps(const Geom& g, const double2* in, const double2* u, tile::Maps* m
 // (right-hand sides or lattices).  Work block wb belongs to the entry e with
 // blk0[e] <= wb < blk0[e+1]; inside it, thread tid handles s = tid % Ls of
 // site (wb - blk0) * spb + tid / Ls.  Entries with skip[e] set are passed over.
+// EPI: 0 out = M in; 1 also a partial of Re<aux, M in> per work block; 2 also a partial
+// of |M in|^2; 4 the CG residual update fused in: rv -= coef_e (M in) in place, in the
+// arithmetic type, with a partial of |rv|^2 (coef_e = coef[e * coef_stride], the entry's
+// own CG scalar; out is not written)
 template <class S, int KER, bool DAG, int EPI>
 __global__ void __launch_bounds__(256, KER == 0 ? 4 : 1)
     k_dslash_batch(S* __restrict__ out, const S* __restrict__ in, const typename Sto<S>::C* __restrict__ u,
                    const BatchEntry* __restrict__ tab, int nent, int total_blocks, float am, int imass, float am3,
-                   const int* skip, const S* __restrict__ aux, double* __restrict__ partials) {
+                   const int* skip, const S* __restrict__ aux, double* __restrict__ partials,
+                   typename Sto<S>::C* rv, const double* coef, int coef_stride) {
   using C = typename Sto<S>::C;
+  using R = typename Sto<S>::R;
   for (int wb = blockIdx.x; wb < total_blocks; wb += gridDim.x) {
     int lo = 0, hi = nent - 1;  // last entry with blk0 <= wb
     while (lo < hi) {
@@ -939,13 +945,26 @@ __global__ void __launch_bounds__(256, KER == 0 ? 4 : 1)
     if (sub < E.spb && site < g.v3) {
       C acc[4];
       apply_site<S, KER, DAG>(in + E.off, u + E.uoff, g, s, site, am, imass, am3, acc);
+      if (EPI == 4) {
+        const R a = (R)coef[(size_t)lo * coef_stride];
+        C* r = rv + E.off;
 #pragma unroll
-      for (int d = 0; d < 4; d++) {
-        Sto<S>::st(out + E.off, sidx(g, s, site, d), acc[d]);
-        if (EPI == 1) racc += epi_redot<S>(aux + E.off, sidx(g, s, site, d), acc[d]);
+        for (int d = 0; d < 4; d++) {
+          const size_t i = sidx(g, s, site, d);
+          const C rn = r[i] - a * acc[d];  // r = r - alpha M^dagger M p (measure_module.F90:92)
+          r[i] = rn;
+          racc += epi_norm<S>(rn);
+        }
+      } else {
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+          Sto<S>::st(out + E.off, sidx(g, s, site, d), acc[d]);
+          if (EPI == 1) racc += epi_redot<S>(aux + E.off, sidx(g, s, site, d), acc[d]);
+          if (EPI == 2) racc += epi_norm<S>(acc[d]);
+        }
       }
     }
-    if (EPI == 1) block_partial(racc, partials + wb);
+    if (EPI != 0) block_partial(racc, partials + wb);
   }
 }
 
@@ -1452,7 +1471,7 @@ int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const
     const int g = grid > 0 ? grid : std::min(b.total_blocks, device_sms() * per_sm);
 #define THR_L(K, D, E)                                                                                          \
   k_dslash_batch<S, K, D, E><<<g, 256, 0, st>>>(out, in, u, b.dev, b.nent, b.total_blocks, am, imass, am3, skip, \
-                                                aux, partials)
+                                                aux, partials, nullptr, nullptr, 0)
     if (kernel == 1) {
       if (dag) { if (epi) THR_L(1, true, 1); else THR_L(1, true, 0); }
       else { if (epi) THR_L(1, false, 1); else THR_L(1, false, 0); }
@@ -1475,6 +1494,43 @@ int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
 
+template <class S>
+int launch_dslash_batch_fused(const BatchTable& b, int kernel, bool dag, int epi, S* out, const S* in,
+                              const typename Sto<S>::C* u, float am, int imass, float am3, cudaStream_t st,
+                              const int* skip, typename Sto<S>::C* rv, const double* coef, int coef_stride,
+                              double* partials, int grid) {
+  if (kernel == 1 && imass != 1 && imass != 3) return THR_ERR_UNSUPPORTED;
+  if (epi != 2 && epi != 4) return THR_ERR_BADARG;
+  auto launch = [&](int per_sm) {
+    const int g = grid > 0 ? grid : std::min(b.total_blocks, device_sms() * per_sm);
+#define THR_L(K, D, E)                                                                                          \
+  k_dslash_batch<S, K, D, E><<<g, 256, 0, st>>>(out, in, u, b.dev, b.nent, b.total_blocks, am, imass, am3, skip, \
+                                                nullptr, partials, rv, coef, coef_stride)
+    if (kernel == 1) {
+      if (dag) { if (epi == 4) THR_L(1, true, 4); else THR_L(1, true, 2); }
+      else { if (epi == 4) THR_L(1, false, 4); else THR_L(1, false, 2); }
+    } else {
+      if (dag) { if (epi == 4) THR_L(0, true, 4); else THR_L(0, true, 2); }
+      else { if (epi == 4) THR_L(0, false, 4); else THR_L(0, false, 2); }
+    }
+#undef THR_L
+  };
+  int per_sm = kTuneBatchGrid[0];
+  if (grid <= 0 && b.total_blocks > device_sms() * kTuneBatchGrid[1]) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    // epi 4 updates rv in place, so it is never launched for timing: it takes the grid
+    // tuned for the same batch's M with |M p|^2 (epi 2)
+    const TuneKey k2{dev, storage_id<S>(), 10 + kernel, 0, 2, b.total_blocks, b.nent, 0, 0, 0};
+    per_sm = epi == 4 ? tune_lookup(k2, kTuneBatchGrid)
+                      : tune_pick(TuneKey{dev, storage_id<S>(), 10 + kernel, dag ? 1 : 0, 2, b.total_blocks, b.nent,
+                                          0, 0, 0},
+                                  kTuneBatchGrid, 3, st, launch);
+  }
+  launch(per_sm);
+  return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
+}
+
 #define THR_INST(S, L)                                                                                            \
   template int launch_dslash<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float, cudaStream_t,   \
                                 const int*);                                                                      \
@@ -1487,7 +1543,9 @@ int launch_dslash_batch(const BatchTable& b, int kernel, bool dag, S* out, const
   template int launch_dslash_accum<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,          \
                                       cudaStream_t, const int*, const S*, const double*, double*, int, bool);     \
   template int launch_dslash_batch<S>(const BatchTable&, int, bool, S*, const S*, const L*, float, int, float,    \
-                                      cudaStream_t, const int*, const S*, double*, int);
+                                      cudaStream_t, const int*, const S*, double*, int);                          \
+  template int launch_dslash_batch_fused<S>(const BatchTable&, int, bool, int, S*, const S*, const L*, float, int, \
+                                            float, cudaStream_t, const int*, L*, const double*, int, double*, int);
 THR_INST(double2, double2)
 THR_INST(float2, float2)
 THR_INST(__nv_bfloat162, float2)
