@@ -46,6 +46,8 @@ __global__ void k_cg_norm2(const CgState* cs, const double2* a, size_t n, double
 
 // measure_module.F90:57, :66-75 (one block; fixed-order reduction of the partials)
 __global__ void k_cg_alpha(CgState* cs, const double* partials, int np) {
+  pdl_wait();
+  pdl_trigger();
   if (cs->done) return;
   const double alphad = block_sum_partials(partials, np);
   if (threadIdx.x != 0) return;
@@ -71,6 +73,8 @@ __global__ void k_cg_rupdate(CgState* cs, double2* r, const double2* x2, size_t 
 
 // :102-110, :120 (one block)
 __global__ void k_cg_beta(CgState* cs, const double* partials, int np) {
+  pdl_wait();
+  pdl_trigger();
   if (cs->done) return;
   const double betacgn = block_sum_partials(partials, np);
   if (threadIdx.x != 0) return;
@@ -89,6 +93,8 @@ __global__ void k_cg_beta(CgState* cs, const double* partials, int np) {
 // in site order: a thread takes the four spin planes of one (s, site) element of
 // the plane (np = n / 4 elements); rev: from the top site down
 __global__ void k_cg_xp(CgState* cs, double2* x, double2* p, const double2* r, size_t np, int rev) {
+  pdl_wait();
+  pdl_trigger();
   if (cs->done) return;
   const double alpha = cs->alpha, beta = cs->betacg;
   const bool upd = cs->nx != 1;
@@ -104,6 +110,8 @@ __global__ void k_cg_xp(CgState* cs, double2* x, double2* p, const double2* r, s
   }
 }
 __global__ void k_cg_latch(CgState* cs) {
+  pdl_wait();
+  pdl_trigger();
   if (cs->pending_done) cs->done = 1;
 }
 
@@ -134,6 +142,10 @@ int cg_enqueue_chunk(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r
   const size_t n = c->n4();
   const unsigned gb = vec_grid(n / 4);
   const unsigned gs = stencil_parts(c->g, c->p.kernel, true);
+  // every kernel of the chain is a programmatic dependent launch of the one before (the
+  // chunk's first, which follows the loop control, excepted; THR_PDL=0: none); each waits
+  // for its predecessor before it reads anything, so the results are the same
+  const bool pdl = c->use_pdl;
   for (int k = 0; k < kCgChunk; k++) {
     // sweep directions alternate with the iteration's parity (kCgChunk is even): each
     // kernel starts on the sites its predecessor wrote last (results do not depend on it)
@@ -141,15 +153,15 @@ int cg_enqueue_chunk(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r
     const int rev_m = odd, rev_md = c->rev_sweep ? 1 - odd : 0, rev_p = odd;
     // x1 = M p with alphad = |x1|^2 (:60, :70) from the stencil's epilogue
     THR_TRY(launch_dslash_norm<double2>(c->g, c->p.kernel, false, x1, p, c->u64, am, imass, c->p.am3, c->st,
-                                        &cs->done, c->partials, rev_m));
-    k_cg_alpha<<<1, 1024, 0, c->st>>>(cs, c->partials, gs);
+                                        &cs->done, c->partials, rev_m, pdl && k > 0));
+    launch_k(k_cg_alpha, dim3(1), dim3(1024), 0, c->st, pdl, cs, (const double*)c->partials, (int)gs);
     // x2 = M^dagger x1 is never stored: the epilogue forms r = r - alpha*x2 (:92) and
     // betacgn = |r|^2 (:102)
     THR_TRY(launch_dslash_axpy<double2>(c->g, c->p.kernel, true, r, x1, c->u64, am, imass, c->p.am3, c->st, &cs->done,
-                                        r, &cs->nalpha, c->partials, rev_md));
-    k_cg_beta<<<1, 1024, 0, c->st>>>(cs, c->partials, gs);
-    k_cg_xp<<<gb, kThreads, 0, c->st>>>(cs, X, p, r, n / 4, rev_p);
-    k_cg_latch<<<1, 1, 0, c->st>>>(cs);
+                                        r, &cs->nalpha, c->partials, rev_md, pdl));
+    launch_k(k_cg_beta, dim3(1), dim3(1024), 0, c->st, pdl, cs, (const double*)c->partials, (int)gs);
+    launch_k(k_cg_xp, dim3(gb), dim3(kThreads), 0, c->st, pdl, cs, X, p, (const double2*)r, n / 4, rev_p);
+    launch_k(k_cg_latch, dim3(1), dim3(1), 0, c->st, pdl, cs);
   }
   return cudaPeekAtLastError() == cudaSuccess ? THR_OK : THR_ERR_CUDA;
 }
@@ -171,8 +183,22 @@ struct CgGraph {
   }
 };
 
+int cg_graph_build(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r, double2* x1, double2* x2, float am,
+                   int imass, cudaGraphExec_t* exec_out);
+
+// a graph that cannot be built with dependent launches is built without them
 int cg_graph(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r, double2* x1, double2* x2, float am,
              int imass, cudaGraphExec_t* exec_out) {
+  int rc = cg_graph_build(c, cs, X, p, r, x1, x2, am, imass, exec_out);
+  if (rc != THR_OK && c->use_pdl) {
+    c->use_pdl = false;
+    rc = cg_graph_build(c, cs, X, p, r, x1, x2, am, imass, exec_out);
+  }
+  return rc;
+}
+
+int cg_graph_build(thr_ctx* c, CgState* cs, double2* X, double2* p, double2* r, double2* x1, double2* x2, float am,
+                   int imass, cudaGraphExec_t* exec_out) {
   if (!c->cg_graph) c->cg_graph = new CgGraph();
   CgGraph& G = *static_cast<CgGraph*>(c->cg_graph);
   if (G.exec && G.X == X && G.p == p && G.r == r && G.x1 == x1 && G.x2 == x2 && G.cs == cs && G.u == c->u64 &&

@@ -1408,9 +1408,10 @@ int launch_dslash_accum(const Geom& g, int kernel, bool dag, S* hnew, const S* i
 
 template <class S>
 int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
-                       float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials, int rev) {
+                       float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials, int rev,
+                       bool pdl) {
   return launch_dslash_mode<S>(g, kernel, dag, out, in, u, am, imass, am3, st, skip, nullptr, nullptr, partials, 2,
-                               rev);
+                               rev, true, pdl);
 }
 
 template <class S>
@@ -1539,7 +1540,7 @@ int launch_dslash_batch_fused(const BatchTable& b, int kernel, bool dag, int epi
   template int launch_dslash_axpy<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
                                      cudaStream_t, const int*, const S*, const double*, double*, int, bool);      \
   template int launch_dslash_norm<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,           \
-                                     cudaStream_t, const int*, double*, int);                                     \
+                                     cudaStream_t, const int*, double*, int, bool);                               \
   template int launch_dslash_accum<S>(const Geom&, int, bool, S*, const S*, const L*, float, int, float,          \
                                       cudaStream_t, const int*, const S*, const double*, double*, int, bool);     \
   template int launch_dslash_batch<S>(const BatchTable&, int, bool, S*, const S*, const L*, float, int, float,    \

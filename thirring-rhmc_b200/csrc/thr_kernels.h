@@ -63,7 +63,7 @@ int launch_dslash_axpy(const Geom& g, int kernel, bool dag, S* rnew, const S* in
 template <class S>
 int launch_dslash_norm(const Geom& g, int kernel, bool dag, S* out, const S* in, const typename Sto<S>::C* u,
                        float am, int imass, float am3, cudaStream_t st, const int* skip, double* partials,
-                       int rev = 0);
+                       int rev = 0, bool pdl = false);
 
 // odslash / odslashd (measure_OWilson.F90:14-167), FP64, with the slice coefficients zc[0..Ls-1] on the device
 int launch_odslash(const Geom& g, bool dag, double2* out, const double2* in, const double2* u, float am, int imass,
