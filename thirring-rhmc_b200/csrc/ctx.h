@@ -91,7 +91,7 @@ struct thr_ctx {
   int max_qmr_iters = 50000;
   int ms_algo = 1;          // multishift: 0 = per-iteration shift updates, 1 = batched
   bool use_graphs = true;   // batched solver loops as one CUDA graph (WHILE node) per solve
-  bool use_pdl = true;      // the batched multishift's kernel chain as dependent launches (THR_PDL=0: off)
+  bool use_pdl = true;      // the batched multishift's and congrad's kernel chains as dependent launches (THR_PDL=0: off)
   // a batch of the batched FP64 multishift as one persistent kernel (msp.cu): 0 (default)
   // never; 1 where every stencil site block gets its own resident block; 2 wherever the
   // block shape allows (THR_CHAIN=0|1|2).  Off by default: on B200 the kernel chain with
